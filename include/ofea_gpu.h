@@ -1,0 +1,148 @@
+/* ofea_gpu.h - C ABI of the B200 implicit-static hot path for OpenFEA models.
+ *
+ * One GPU, no CPU fallback: every compute entry point runs hand-written
+ * sm_100a kernels and fails with OFEA_ERR_NO_DEVICE when no CUDA device is
+ * present.  All functions return an int status (OFEA_OK = 0, negative codes
+ * below); none calls exit() or throws across the boundary.  ofea_last_error()
+ * gives a message for the calling thread's last failure.
+ *
+ * Threading: a context belongs to one host thread at a time; work on a context
+ * is ordered on its CUDA stream.  Host arrays passed in are borrowed for the
+ * duration of the call only.  The library owns all device memory it allocates.
+ *
+ * Conventions (those of the reference's data_management, so a host shim can
+ * pass its vectors straight through):
+ *   - node ids in `topo` are 1-based, 8 slots per element, C3D4 uses the first
+ *     4 (node_topos_, src/include/data_management.h:49);
+ *   - etype 0 = C3D4, 1 = C3D8 (ELE_TYPES, src/include/data_management.h:76);
+ *   - free_map[node] = free-node index or -1 (resort_free_nodes_,
+ *     src/set_bc.cpp:20-43); DOF d = 3*free_map[node] + component, n = 3*nfree;
+ *   - K is symmetric; exported in CSR, which equals the reference's CSC arrays
+ *     (col_idx_/row_idx_/nz_val_, src/include/assemble.h:41-43).
+ */
+#ifndef OFEA_GPU_H
+#define OFEA_GPU_H
+
+#if defined(__GNUC__)
+#define OFEA_API __attribute__((visibility("default")))
+#else
+#define OFEA_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OFEA_OK 0
+#define OFEA_ERR_INVALID_ARG (-1)   /* bad pointer, size, id or option */
+#define OFEA_ERR_CUDA (-2)          /* a CUDA runtime call failed */
+#define OFEA_ERR_OOM (-3)           /* device allocation failed */
+#define OFEA_ERR_NOT_CONVERGED (-4) /* max_iter reached above rtol */
+#define OFEA_ERR_TIMEOUT (-5)       /* time_budget_s exceeded */
+#define OFEA_ERR_STATE (-6)         /* call out of order (e.g. solve before assemble) */
+#define OFEA_ERR_CAPACITY (-7)      /* mesh exceeds a kernel limit (neighbour count) */
+#define OFEA_ERR_BREAKDOWN (-8)     /* p.Kp <= 0 or NaN: K not SPD (e.g. no BCs) */
+#define OFEA_ERR_NO_DEVICE (-9)     /* no CUDA device visible */
+#define OFEA_ERR_IO (-10)           /* file cannot be read / parsed / written */
+#define OFEA_ERR_UNKNOWN_SOLVER (-11)
+#define OFEA_ERR_REJECTED (-12)     /* learned stage rejected by the FP64 residual check */
+
+/* Solver methods (ofea_solve_opts.method). */
+#define OFEA_SOLVER_PCG64 0   /* FP64 PCG, 3x3 block-Jacobi */
+#define OFEA_SOLVER_MIXED 1   /* FP32 PCG with FP64 reliable-update refinement */
+#define OFEA_SOLVER_LEARNED 2 /* MIXED + graph-network coarse correction (flexible PCG) */
+
+typedef struct ofea_ctx ofea_ctx;
+
+typedef struct {
+    int method;           /* OFEA_SOLVER_* */
+    double rtol;          /* stop when ||f - K u||_2 <= rtol ||f||_2 (FP64 true residual) */
+    int max_iter;         /* inner iterations, summed over refinements */
+    double time_budget_s; /* <= 0: unlimited */
+    int check_every;      /* iterations between host convergence polls (0: default) */
+    double ru_delta;      /* MIXED: reliable-update trigger ||r32|| < ru_delta * max||r|| (0: default 0.1) */
+    int use_graph;        /* 1: replay iteration chunks as a captured CUDA graph; 0: plain launches */
+} ofea_solve_opts;
+
+typedef struct {
+    int status;            /* OFEA_OK or an error code */
+    int iterations;        /* inner iterations performed */
+    int refinements;       /* FP64 residual recomputations (MIXED/LEARNED) */
+    double rel_residual;   /* final ||f - K u|| / ||f|| in FP64 */
+    double seconds;        /* device time of the solve (CUDA events) */
+    int rejected_learned;  /* 1 when the learned stage was rejected and plain PCG finished */
+    long long kernel_launches;
+} ofea_solve_stats;
+
+/* ---- library ---------------------------------------------------------- */
+OFEA_API const char *ofea_version(void);
+OFEA_API const char *ofea_status_string(int status);
+OFEA_API const char *ofea_last_error(void);
+/* Fills opts with defaults: PCG64, rtol 1e-8, max_iter 100000, check_every 16,
+ * ru_delta 0.1, use_graph 1, no time budget. */
+OFEA_API void ofea_solve_opts_default(ofea_solve_opts *opts);
+
+/* ---- context ---------------------------------------------------------- */
+OFEA_API int ofea_ctx_create(ofea_ctx **out, int device);
+OFEA_API int ofea_ctx_destroy(ofea_ctx *ctx);
+/* Run this context's work on an existing cudaStream_t (NULL: library-owned stream). */
+OFEA_API int ofea_ctx_set_stream(ofea_ctx *ctx, void *cuda_stream);
+
+/* ---- mesh -------------------------------------------------------------- */
+/* Replaces the data the reference's assemblers read from data_management
+ * (src/include/data_management.h:48-62): coordinates nd x 3, topo ne x 8
+ * (1-based), etype, per-element Young's modulus E_elem (NULL: E0 everywhere;
+ * the reference has one material per element type, src/data_managrment.cpp:20-26),
+ * Poisson ratio nu, and the DOF numbering free_map (nd).  Copies to the device. */
+OFEA_API int ofea_mesh_upload(ofea_ctx *ctx, int nd, const double *xyz, int ne, const int *topo,
+                     const int *etype, const double *E_elem, double E0, double nu,
+                     const int *free_map);
+/* Replace the per-element Young's modulus (same mesh and pattern). */
+OFEA_API int ofea_mesh_set_modulus(ofea_ctx *ctx, const double *E_elem, double E0);
+
+/* ---- assembly ----------------------------------------------------------- */
+/* assamble_stiffness::build_CSR (src/assemble.cpp:19-77): the symmetric
+ * sparsity pattern, built on the device, plus the element-to-slot map used by
+ * the assembly kernels.  Returns n (free DOFs) and nnz (scalar non-zeros). */
+OFEA_API int ofea_assemble_pattern(ofea_ctx *ctx, int *n, long long *nnz);
+/* assamble_stiffness::fill_CSR_sparse_mat (src/assemble.cpp:95-151): FP64
+ * element integration (C3D8 2x2x2 Gauss, C3D4 one point) and atomic-free
+ * assembly into K on the device. */
+OFEA_API int ofea_assemble_linear(ofea_ctx *ctx);
+/* assamble_nl_stiffness::fill_CSR_sparse_mat (src/nl_assemble.cpp:94-166):
+ * tangent K_T(u) replaces K on the device; f_int (n, host) receives the
+ * internal force.  u: n free-DOF displacements (host). */
+OFEA_API int ofea_assemble_nl(ofea_ctx *ctx, const double *u, double *f_int);
+/* Copy K to the host as CSR: rowptr (n+1), col (nnz), val (nnz); any may be NULL. */
+OFEA_API int ofea_get_csr(ofea_ctx *ctx, int *rowptr, int *col, double *val);
+/* Element matrices of the last assembly, for checking: Ke of element e in the
+ * caller's element order, (3 npe)^2 row-major.  first..first+count-1. */
+OFEA_API int ofea_get_element_matrices(ofea_ctx *ctx, int first, int count, double *Ke);
+/* y = K x on the device (n values, host arrays). */
+OFEA_API int ofea_spmv(ofea_ctx *ctx, const double *x, double *y);
+
+/* ---- solve -------------------------------------------------------------- */
+/* solution_api (src/linear_solution.cpp:17-64) / solution_nl_api (:66-137):
+ * solve K u = f for nrhs right-hand sides (column-major n x nrhs, host).
+ * opts NULL: defaults.  stats may be NULL (one entry per rhs otherwise). */
+OFEA_API int ofea_solve(ofea_ctx *ctx, const double *f, double *u, int nrhs, const ofea_solve_opts *opts,
+               ofea_solve_stats *stats);
+/* Same with device pointers (f, u of n doubles each), stream-ordered. */
+OFEA_API int ofea_solve_device(ofea_ctx *ctx, const double *d_f, double *d_u, const ofea_solve_opts *opts,
+                      ofea_solve_stats *stats);
+
+/* ---- measurement ------------------------------------------------------- */
+/* No counterpart in the reference (it only prints clock() spans): times the
+ * solver's two per-iteration kernels (A: p update + SpMV + p.q, B: vector
+ * updates + block-Jacobi + dots) of `method` in isolation, `reps` launches
+ * each between CUDA events on the context's stream, on the current K and
+ * solver vectors (call after a solve).  ms[0], ms[1] = average milliseconds
+ * per launch of A and B; bytes[0], bytes[1] = algorithmic bytes per launch
+ * (every array the kernel must touch, counted once). */
+OFEA_API int ofea_profile_solver_kernels(ofea_ctx *ctx, int method, int reps, double *ms,
+                                         double *bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OFEA_GPU_H */

@@ -1,0 +1,346 @@
+"""openfea_b200: OpenFEA's implicit-static hot path on one B200 (sm_100a).
+
+The product is the C ABI in include/ofea_gpu.h / include/ofea_host.h,
+implemented by libofea_gpu.so (hand-written CUDA kernels + C++ host I/O).
+This module binds it with ctypes for Python callers and tests, and mirrors the
+reference's entry points (``AssambleStiffness.build_CSR`` /
+``fill_CSR_sparse_mat``, ``solution_api``) with GPU solver names.
+
+There is no CPU fallback: when the library or a GPU is missing, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libofea_gpu.so")
+
+OFEA_OK = 0
+STATUS = {
+    0: "OFEA_OK", -1: "OFEA_ERR_INVALID_ARG", -2: "OFEA_ERR_CUDA", -3: "OFEA_ERR_OOM",
+    -4: "OFEA_ERR_NOT_CONVERGED", -5: "OFEA_ERR_TIMEOUT", -6: "OFEA_ERR_STATE",
+    -7: "OFEA_ERR_CAPACITY", -8: "OFEA_ERR_BREAKDOWN", -9: "OFEA_ERR_NO_DEVICE",
+    -10: "OFEA_ERR_IO", -11: "OFEA_ERR_UNKNOWN_SOLVER", -12: "OFEA_ERR_REJECTED",
+}
+SOLVERS = {"GPU_PCG": 0, "GPU_MIXED": 1, "GPU_LEARNED": 2}
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+_LL = ctypes.c_longlong
+
+
+class OfeaError(RuntimeError):
+    def __init__(self, code, what, msg=""):
+        self.code = code
+        super().__init__(f"{what}: {STATUS.get(code, code)} {msg}".strip())
+
+
+class SolveOpts(ctypes.Structure):
+    _fields_ = [("method", _I), ("rtol", _D), ("max_iter", _I), ("time_budget_s", _D),
+                ("check_every", _I), ("ru_delta", _D), ("use_graph", _I)]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("status", _I), ("iterations", _I), ("refinements", _I), ("rel_residual", _D),
+                ("seconds", _D), ("rejected_learned", _I), ("kernel_launches", _LL)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib():
+    """Load libofea_gpu.so (built by ``python -m openfea_b200.build``)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} is not built: run python -m openfea_b200.build")
+    L = ctypes.CDLL(LIB_PATH)
+    sig = {
+        "ofea_version": (ctypes.c_char_p, []),
+        "ofea_status_string": (ctypes.c_char_p, [_I]),
+        "ofea_last_error": (ctypes.c_char_p, []),
+        "ofea_solve_opts_default": (None, [_P]),
+        "ofea_ctx_create": (_I, [ctypes.POINTER(_P), _I]),
+        "ofea_ctx_destroy": (_I, [_P]),
+        "ofea_ctx_set_stream": (_I, [_P, _P]),
+        "ofea_mesh_upload": (_I, [_P, _I, _P, _I, _P, _P, _P, _D, _D, _P]),
+        "ofea_mesh_set_modulus": (_I, [_P, _P, _D]),
+        "ofea_assemble_pattern": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_LL)]),
+        "ofea_assemble_linear": (_I, [_P]),
+        "ofea_assemble_nl": (_I, [_P, _P, _P]),
+        "ofea_get_csr": (_I, [_P, _P, _P, _P]),
+        "ofea_get_element_matrices": (_I, [_P, _I, _I, _P]),
+        "ofea_spmv": (_I, [_P, _P, _P]),
+        "ofea_solve": (_I, [_P, _P, _P, _I, _P, _P]),
+        "ofea_solve_device": (_I, [_P, _P, _P, _P, _P]),
+        "ofea_inp_read": (_I, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+        "ofea_model_free": (None, [_P]),
+        "ofea_model_sizes": (_I, [_P, _P, _P, _P, _P]),
+        "ofea_model_arrays": (_I, [_P, _P, _P, _P, _P, _P]),
+        "ofea_model_material": (_I, [_P, _P, _P, _P, _P]),
+        "ofea_model_cload": (_I, [_P, _P, _P]),
+        "ofea_build_free_index": (_I, [_I, _I, _P, _P, _P]),
+        "ofea_build_single_load": (_I, [_I, _P, _I, _P, _I, _D, _P]),
+        "ofea_full_displacement": (_I, [_I, _P, _P, _P]),
+        "ofea_write_vtk": (_I, [ctypes.c_char_p, _I, _P, _I, _P, _P, _P, _D]),
+        "ofea_profile_solver_kernels": (_I, [_P, _I, _I, _P, _P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _check(rc, what):
+    if rc != OFEA_OK:
+        raise OfeaError(rc, what, lib().ofea_last_error().decode(errors="replace"))
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def solve_opts(method="GPU_PCG", rtol=1e-8, max_iter=100000, time_budget_s=0.0, check_every=16,
+               ru_delta=0.1, use_graph=True) -> SolveOpts:
+    o = SolveOpts()
+    lib().ofea_solve_opts_default(ctypes.byref(o))
+    o.method = SOLVERS[method] if isinstance(method, str) else int(method)
+    o.rtol, o.max_iter, o.time_budget_s = rtol, max_iter, time_budget_s
+    o.check_every, o.ru_delta, o.use_graph = check_every, ru_delta, int(bool(use_graph))
+    return o
+
+
+class Context:
+    """One GPU context: mesh, pattern, K and solver state resident on the device."""
+
+    def __init__(self, device=0):
+        self.h = _P()
+        _check(lib().ofea_ctx_create(ctypes.byref(self.h), device), "ofea_ctx_create")
+        self.n = 0
+        self.nnz = 0
+
+    def close(self):
+        if self.h:
+            lib().ofea_ctx_destroy(self.h)
+            self.h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle):
+        _check(lib().ofea_ctx_set_stream(self.h, _P(stream_handle)), "ofea_ctx_set_stream")
+
+    def upload(self, xyz, topo, etype, free_map, E0, nu, E_elem=None):
+        xyz, topo, etype, fm = _f64(xyz), _i32(topo), _i32(etype), _i32(free_map)
+        E = _f64(E_elem) if E_elem is not None else None
+        self._keep = (xyz, topo, etype, fm, E)
+        _check(lib().ofea_mesh_upload(self.h, xyz.shape[0], _ptr(xyz), topo.shape[0], _ptr(topo),
+                                      _ptr(etype), _ptr(E), E0, nu, _ptr(fm)), "ofea_mesh_upload")
+
+    def upload_mesh(self, mesh, free_map=None):
+        fm = free_map if free_map is not None else build_free_index(mesh.nd, mesh.fix)
+        self.upload(mesh.xyz, mesh.topo, mesh.etype, fm, mesh.E0, mesh.nu, mesh.E)
+        return fm
+
+    def set_modulus(self, E_elem, E0):
+        E = _f64(E_elem) if E_elem is not None else None
+        _check(lib().ofea_mesh_set_modulus(self.h, _ptr(E), E0), "ofea_mesh_set_modulus")
+
+    def assemble_pattern(self):
+        n, nnz = _I(), _LL()
+        _check(lib().ofea_assemble_pattern(self.h, ctypes.byref(n), ctypes.byref(nnz)), "ofea_assemble_pattern")
+        self.n, self.nnz = n.value, nnz.value
+        return self.n, self.nnz
+
+    def assemble_linear(self):
+        _check(lib().ofea_assemble_linear(self.h), "ofea_assemble_linear")
+
+    def assemble_nl(self, u):
+        u = _f64(u)
+        fint = np.zeros(self.n)
+        _check(lib().ofea_assemble_nl(self.h, _ptr(u), _ptr(fint)), "ofea_assemble_nl")
+        return fint
+
+    def get_csr(self):
+        rp = np.zeros(self.n + 1, dtype=np.int32)
+        col = np.zeros(self.nnz, dtype=np.int32)
+        val = np.zeros(self.nnz)
+        _check(lib().ofea_get_csr(self.h, _ptr(rp), _ptr(col), _ptr(val)), "ofea_get_csr")
+        return rp, col, val
+
+    def element_matrices(self, first, count, npe):
+        m = 3 * npe
+        K = np.zeros((count, m, m))
+        _check(lib().ofea_get_element_matrices(self.h, first, count, _ptr(K)), "ofea_get_element_matrices")
+        return K
+
+    def spmv(self, x):
+        x = _f64(x)
+        y = np.zeros(self.n)
+        _check(lib().ofea_spmv(self.h, _ptr(x), _ptr(y)), "ofea_spmv")
+        return y
+
+    def solve(self, f, method="GPU_PCG", rtol=1e-8, raise_on_error=True, **kw):
+        F = _f64(f)
+        nrhs = 1 if F.ndim == 1 else F.shape[1]
+        Fc = np.asfortranarray(F.reshape(self.n, nrhs))
+        U = np.zeros((self.n, nrhs), order="F")
+        stats = (SolveStats * nrhs)()
+        o = solve_opts(method, rtol, **kw)
+        rc = lib().ofea_solve(self.h, Fc.ctypes.data_as(_P), U.ctypes.data_as(_P), nrhs,
+                              ctypes.byref(o), stats)
+        if rc != OFEA_OK and raise_on_error:
+            _check(rc, "ofea_solve")
+        st = [s.as_dict() for s in stats]
+        return (U[:, 0] if F.ndim == 1 else U), (st[0] if F.ndim == 1 else st)
+
+    def profile_kernels(self, method="GPU_MIXED", reps=20):
+        """Average ms and algorithmic bytes per launch of the solver's A and B
+        kernels (CUDA events on the context stream)."""
+        ms = np.zeros(2)
+        by = np.zeros(2)
+        m = SOLVERS[method] if isinstance(method, str) else int(method)
+        _check(lib().ofea_profile_solver_kernels(self.h, m, reps, _ptr(ms), _ptr(by)),
+               "ofea_profile_solver_kernels")
+        return ms, by
+
+    def solve_device(self, f_ptr, u_ptr, method="GPU_PCG", rtol=1e-8, **kw):
+        o = solve_opts(method, rtol, **kw)
+        st = SolveStats()
+        rc = lib().ofea_solve_device(self.h, _P(f_ptr), _P(u_ptr), ctypes.byref(o), ctypes.byref(st))
+        return rc, st.as_dict()
+
+
+# --------------------------------------------------------------- host I/O --
+
+def inp_read(path):
+    """ReadInfo (src/data2cae.cpp) through the C ABI; returns a dict of arrays."""
+    L = lib()
+    m = _P()
+    _check(L.ofea_inp_read(str(path).encode(), ctypes.byref(m)), "ofea_inp_read")
+    try:
+        nd, ne, nfix, nload = _I(), _I(), _I(), _I()
+        L.ofea_model_sizes(m, ctypes.byref(nd), ctypes.byref(ne), ctypes.byref(nfix), ctypes.byref(nload))
+        xyz = np.zeros((nd.value, 3))
+        topo = np.zeros((ne.value, 8), dtype=np.int32)
+        et = np.zeros(ne.value, dtype=np.int32)
+        fix = np.zeros(nfix.value, dtype=np.int32)
+        load = np.zeros(nload.value, dtype=np.int32)
+        L.ofea_model_arrays(m, _ptr(xyz), _ptr(topo), _ptr(et), _ptr(fix), _ptr(load))
+        E, nu, rho, has = _D(), _D(), _D(), _I()
+        L.ofea_model_material(m, ctypes.byref(E), ctypes.byref(nu), ctypes.byref(rho), ctypes.byref(has))
+        dof, val = _I(), _D()
+        L.ofea_model_cload(m, ctypes.byref(dof), ctypes.byref(val))
+        return dict(xyz=xyz, topo=topo, etype=et, fix=fix, load_set=load, E=E.value, nu=nu.value,
+                    density=rho.value, has_elastic=bool(has.value), load_dof=dof.value,
+                    load_value=val.value)
+    finally:
+        L.ofea_model_free(m)
+
+
+def build_free_index(nd, fix):
+    fix = _i32(fix)
+    fm = np.zeros(nd, dtype=np.int32)
+    nf = _I()
+    _check(lib().ofea_build_free_index(nd, fix.size, _ptr(fix), _ptr(fm), ctypes.byref(nf)),
+           "ofea_build_free_index")
+    return fm
+
+
+def build_single_load(nd, free_map, load_set, dof, value):
+    fm, ls = _i32(free_map), _i32(load_set)
+    f = np.zeros(3 * int((fm >= 0).sum()))
+    _check(lib().ofea_build_single_load(nd, _ptr(fm), ls.size, _ptr(ls), dof, value, _ptr(f)),
+           "ofea_build_single_load")
+    return f
+
+
+def full_displacement(nd, free_map, u):
+    out = np.zeros(3 * nd)
+    _check(lib().ofea_full_displacement(nd, _ptr(_i32(free_map)), _ptr(_f64(u)), _ptr(out)),
+           "ofea_full_displacement")
+    return out
+
+
+def write_vtk(path, xyz, topo, etype, u_full, scale=1.0):
+    xyz, topo, et, uf = _f64(xyz), _i32(topo), _i32(etype), _f64(u_full)
+    _check(lib().ofea_write_vtk(str(path).encode(), xyz.shape[0], _ptr(xyz), topo.shape[0], _ptr(topo),
+                                _ptr(et), _ptr(uf), scale), "ofea_write_vtk")
+
+
+# ------------------------------------------- reference-named entry points --
+
+@dataclass
+class DataManagement:
+    """The fields of data_management (src/include/data_management.h:48-62)
+    that the assembly and solve entry points read and write."""
+    nd_: int
+    ne_: int
+    coords_: np.ndarray          # nd x 3
+    node_topos_: np.ndarray      # ne x 8, 1-based
+    ele_list_idx_: np.ndarray    # 0 C3D4, 1 C3D8
+    dis_bc_set_: np.ndarray      # 1-based fixed nodes
+    young_modulus: float
+    poisson_ratio: float
+    E_elem: np.ndarray | None = None
+    resort_free_nodes_: np.ndarray | None = None
+    single_load_vec_: np.ndarray | None = None
+    single_dis_vec_: np.ndarray | None = None
+
+
+class AssambleStiffness:
+    """assamble_stiffness (src/include/assemble.h:35-72) with K on the GPU."""
+
+    def __init__(self, device=0):
+        self.ctx = Context(device)
+        self.num_nz_val_ = 0
+
+    def build_CSR(self, data: DataManagement):
+        if data.resort_free_nodes_ is None:
+            data.resort_free_nodes_ = build_free_index(data.nd_, data.dis_bc_set_)
+        self.ctx.upload(data.coords_, data.node_topos_, data.ele_list_idx_, data.resort_free_nodes_,
+                        data.young_modulus, data.poisson_ratio, data.E_elem)
+        n, nnz = self.ctx.assemble_pattern()
+        self.num_nz_val_ = nnz
+        return n, nnz
+
+    def fill_CSR_sparse_mat(self, data: DataManagement):
+        self.ctx.assemble_linear()
+
+    def csr(self):
+        return self.ctx.get_csr()
+
+
+def solution_api(item_ass: AssambleStiffness, data: DataManagement, solver_type: str, rtol=1e-8):
+    """solution_api (src/linear_solution.cpp:17-64) with the GPU solvers:
+    "GPU_PCG" (FP64) or "GPU_MIXED".  Returns False for an unknown solver
+    string, as the reference does; raises on solver failure (the reference
+    exits)."""
+    if solver_type not in ("GPU_PCG", "GPU_MIXED"):
+        return False
+    u, st = item_ass.ctx.solve(data.single_load_vec_, method=solver_type, rtol=rtol)
+    data.single_dis_vec_ = u
+    item_ass.last_stats = st
+    return True

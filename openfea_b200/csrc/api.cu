@@ -1,0 +1,437 @@
+// C ABI entry points (include/ofea_gpu.h).  Every function catches internal
+// failures and returns a status code; nothing throws or exits across the ABI.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "ofea_internal.cuh"
+
+namespace ofea {
+
+thread_local std::string g_last_error;
+
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+
+[[noreturn]] void fail(int code, const std::string &msg) { throw Failure{code, msg}; }
+
+[[noreturn]] void fail_cuda(cudaError_t e, const char *what, const char *file, int line) {
+    int code = (e == cudaErrorMemoryAllocation) ? OFEA_ERR_OOM
+               : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? OFEA_ERR_NO_DEVICE
+                                                                              : OFEA_ERR_CUDA;
+    cudaGetLastError();
+    throw Failure{code, std::string(what) + ": " + cudaGetErrorString(e) + " (" + file + ":" +
+                            std::to_string(line) + ")"};
+}
+
+template <class F>
+int guarded(F f) {
+    try {
+        f();
+        return OFEA_OK;
+    } catch (const Failure &e) {
+        set_last_error(e.msg);
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        set_last_error("host allocation failed");
+        return OFEA_ERR_OOM;
+    } catch (const std::exception &e) {
+        set_last_error(e.what());
+        return OFEA_ERR_INVALID_ARG;
+    }
+}
+
+static void use_device(ofea_ctx *c) { OFEA_CUDA(cudaSetDevice(c->device)); }
+
+static void need(bool cond, int code, const char *msg) {
+    if (!cond) fail(code, msg);
+}
+
+}  // namespace ofea
+
+using namespace ofea;
+
+extern "C" {
+
+const char *ofea_version(void) { return "ofea_gpu 0.1.0 (sm_100a)"; }
+
+const char *ofea_status_string(int s) {
+    switch (s) {
+        case OFEA_OK: return "ok";
+        case OFEA_ERR_INVALID_ARG: return "invalid argument";
+        case OFEA_ERR_CUDA: return "CUDA error";
+        case OFEA_ERR_OOM: return "out of device memory";
+        case OFEA_ERR_NOT_CONVERGED: return "not converged";
+        case OFEA_ERR_TIMEOUT: return "time budget exceeded";
+        case OFEA_ERR_STATE: return "call out of order";
+        case OFEA_ERR_CAPACITY: return "mesh exceeds a kernel limit";
+        case OFEA_ERR_BREAKDOWN: return "CG breakdown (K not positive definite)";
+        case OFEA_ERR_NO_DEVICE: return "no CUDA device";
+        case OFEA_ERR_IO: return "I/O error";
+        case OFEA_ERR_UNKNOWN_SOLVER: return "unknown solver";
+        case OFEA_ERR_REJECTED: return "learned stage rejected";
+        default: return "unknown status";
+    }
+}
+
+const char *ofea_last_error(void) { return g_last_error.c_str(); }
+
+void ofea_solve_opts_default(ofea_solve_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->method = OFEA_SOLVER_PCG64;
+    o->rtol = 1e-8;
+    o->max_iter = 100000;
+    o->time_budget_s = 0;
+    o->check_every = 16;
+    o->ru_delta = 0.1;
+    o->use_graph = 1;
+}
+
+int ofea_ctx_create(ofea_ctx **out, int device) {
+    return guarded([&] {
+        need(out != nullptr, OFEA_ERR_INVALID_ARG, "out is NULL");
+        *out = nullptr;
+        int count = 0;
+        cudaError_t e = cudaGetDeviceCount(&count);
+        if (e != cudaSuccess || count == 0) {
+            cudaGetLastError();
+            fail(OFEA_ERR_NO_DEVICE, "no CUDA device visible");
+        }
+        need(device >= 0 && device < count, OFEA_ERR_INVALID_ARG, "device out of range");
+        ofea_ctx *c = new ofea_ctx();
+        c->device = device;
+        try {
+            OFEA_CUDA(cudaSetDevice(device));
+            OFEA_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+            OFEA_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+            c->own_stream = true;
+            c->err_flag.ensure(4);
+            c->herr.ensure(4);
+        } catch (...) {
+            delete c;
+            throw;
+        }
+        *out = c;
+    });
+}
+
+int ofea_ctx_destroy(ofea_ctx *c) {
+    return guarded([&] {
+        if (!c) return;
+        cudaSetDevice(c->device);
+        if (c->stream) cudaStreamSynchronize(c->stream);
+        if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+        delete c;
+    });
+}
+
+int ofea_ctx_set_stream(ofea_ctx *c, void *stream) {
+    return guarded([&] {
+        need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
+        use_device(c);
+        OFEA_CUDA(cudaStreamSynchronize(c->stream));
+        if (c->own_stream) cudaStreamDestroy(c->stream);
+        if (stream) {
+            c->stream = (cudaStream_t)stream;
+            c->own_stream = false;
+        } else {
+            OFEA_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+            c->own_stream = true;
+        }
+    });
+}
+
+static void split_modulus(ofea_ctx *c, const double *E_elem, double E0, std::vector<double> &E8,
+                          std::vector<double> &E4) {
+    E8.assign(c->ne8, E0);
+    E4.assign(c->ne4, E0);
+    if (E_elem)
+        for (int e = 0; e < c->ne; ++e) {
+            double v = E_elem[e];
+            need(std::isfinite(v), OFEA_ERR_INVALID_ARG, "non-finite Young's modulus");
+            (c->elem_type[e] == 1 ? E8 : E4)[c->elem_local[e]] = v;
+        }
+}
+
+int ofea_mesh_upload(ofea_ctx *c, int nd, const double *xyz, int ne, const int *topo,
+                     const int *etype, const double *E_elem, double E0, double nu,
+                     const int *free_map) {
+    return guarded([&] {
+        need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
+        need(nd > 0 && ne > 0 && xyz && topo && etype && free_map, OFEA_ERR_INVALID_ARG,
+             "empty mesh or NULL array");
+        need(ne < (1 << 28), OFEA_ERR_CAPACITY, "more than 2^28 elements");
+        need(std::isfinite(E0) && std::isfinite(nu) && nu > -1.0 && nu < 0.5, OFEA_ERR_INVALID_ARG,
+             "invalid material (nu must be in (-1, 0.5))");
+        use_device(c);
+        c->mesh_ok = c->pattern_ok = c->K_ok = c->K32_ok = false;
+        c->nd = nd;
+        c->ne = ne;
+        c->E0 = E0;
+        c->nu = nu;
+        c->elem_type.assign(etype, etype + ne);
+        c->elem_local.resize(ne);
+        std::vector<int> t8, t4;
+        t8.reserve(8L * ne);
+        for (int e = 0; e < ne; ++e) {
+            int t = etype[e];
+            need(t == 0 || t == 1, OFEA_ERR_INVALID_ARG, "element type must be 0 (C3D4) or 1 (C3D8)");
+            int npe = t == 1 ? 8 : 4;
+            auto &dst = t == 1 ? t8 : t4;
+            c->elem_local[e] = (int)(dst.size() / npe);
+            for (int a = 0; a < npe; ++a) {
+                int v = topo[8L * e + a];
+                need(v >= 1 && v <= nd, OFEA_ERR_INVALID_ARG, "node id out of range 1..nd in topo");
+                for (int b = 0; b < a; ++b)
+                    need(topo[8L * e + b] != v, OFEA_ERR_INVALID_ARG, "element repeats a node");
+                dst.push_back(v - 1);  // device connectivity is 0-based
+            }
+        }
+        c->ne8 = (int)(t8.size() / 8);
+        c->ne4 = (int)(t4.size() / 4);
+        int nfree = 0;
+        std::vector<char> seen(nd, 0);
+        for (int i = 0; i < nd; ++i) {
+            int f = free_map[i];
+            need(f >= -1 && f < nd, OFEA_ERR_INVALID_ARG, "free_map entry out of range");
+            if (f >= 0) {
+                need(!seen[f], OFEA_ERR_INVALID_ARG, "free_map is not a numbering");
+                seen[f] = 1;
+                ++nfree;
+            }
+        }
+        for (int i = 0; i < nfree; ++i)
+            need(seen[i], OFEA_ERR_INVALID_ARG, "free_map must number free nodes 0..nfree-1");
+        for (long i = 0; i < 3L * nd; ++i)
+            need(std::isfinite(xyz[i]), OFEA_ERR_INVALID_ARG, "non-finite coordinate");
+        c->nfree = nfree;
+        c->n = 3 * nfree;
+        std::vector<double> E8, E4;
+        split_modulus(c, E_elem, E0, E8, E4);
+        cudaStream_t s = c->stream;
+        c->xyz.upload(xyz, 3L * nd, s);
+        c->topo8.upload(t8.data(), t8.size(), s);
+        c->topo4.upload(t4.data(), t4.size(), s);
+        c->E8.upload(E8.data(), E8.size(), s);
+        c->E4.upload(E4.data(), E4.size(), s);
+        c->free_map.upload(free_map, nd, s);
+        OFEA_CUDA(cudaStreamSynchronize(s));
+        c->mesh_ok = true;
+    });
+}
+
+int ofea_mesh_set_modulus(ofea_ctx *c, const double *E_elem, double E0) {
+    return guarded([&] {
+        need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
+        need(c->mesh_ok, OFEA_ERR_STATE, "no mesh uploaded");
+        use_device(c);
+        std::vector<double> E8, E4;
+        split_modulus(c, E_elem, E0, E8, E4);
+        c->E0 = E0;
+        c->E8.upload(E8.data(), E8.size(), c->stream);
+        c->E4.upload(E4.data(), E4.size(), c->stream);
+        OFEA_CUDA(cudaStreamSynchronize(c->stream));
+        c->K_ok = c->K32_ok = false;
+    });
+}
+
+int ofea_assemble_pattern(ofea_ctx *c, int *n, long long *nnz) {
+    return guarded([&] {
+        need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
+        need(c->mesh_ok, OFEA_ERR_STATE, "no mesh uploaded");
+        use_device(c);
+        build_pattern(c);
+        if (n) *n = c->n;
+        if (nnz) *nnz = 9 * c->nnzb;
+    });
+}
+
+static void after_assembly(ofea_ctx *c) {
+    build_block_jacobi(c);
+    OFEA_CUDA(cudaMemcpyAsync(c->herr.p, c->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    OFEA_CUDA(cudaStreamSynchronize(c->stream));
+    c->jacobi_ok = c->herr.p[0] == 0;
+}
+
+int ofea_assemble_linear(ofea_ctx *c) {
+    return guarded([&] {
+        need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
+        need(c->pattern_ok, OFEA_ERR_STATE, "ofea_assemble_pattern first");
+        use_device(c);
+        assemble_linear(c);
+        after_assembly(c);
+    });
+}
+
+int ofea_assemble_nl(ofea_ctx *c, const double *u, double *f_int) {
+    return guarded([&] {
+        need(c != nullptr && u != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
+        need(c->pattern_ok, OFEA_ERR_STATE, "ofea_assemble_pattern first");
+        use_device(c);
+        c->u_nl.upload(u, c->n, c->stream);
+        c->f_int.ensure(std::max(c->n, 1));
+        assemble_nl(c, c->u_nl.p, c->f_int.p);
+        if (f_int)
+            OFEA_CUDA(cudaMemcpyAsync(f_int, c->f_int.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost,
+                                      c->stream));
+        after_assembly(c);
+    });
+}
+
+int ofea_get_csr(ofea_ctx *c, int *rowptr, int *col, double *val) {
+    return guarded([&] {
+        need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
+        need(c->pattern_ok, OFEA_ERR_STATE, "no pattern");
+        need(val == nullptr || c->K_ok, OFEA_ERR_STATE, "K not assembled");
+        use_device(c);
+        const int nf = c->nfree;
+        std::vector<int> brp(nf + 1), bcol(c->nnzb);
+        std::vector<double> bval(val ? 9 * c->nnzb : 0);
+        OFEA_CUDA(cudaMemcpyAsync(brp.data(), c->rowptr.p, sizeof(int) * (nf + 1), cudaMemcpyDeviceToHost, c->stream));
+        OFEA_CUDA(cudaMemcpyAsync(bcol.data(), c->cols.p, sizeof(int) * c->nnzb, cudaMemcpyDeviceToHost, c->stream));
+        if (val)
+            OFEA_CUDA(cudaMemcpyAsync(bval.data(), c->Kb.p, sizeof(double) * 9 * c->nnzb,
+                                      cudaMemcpyDeviceToHost, c->stream));
+        OFEA_CUDA(cudaStreamSynchronize(c->stream));
+        // scalar row 3r+i: for each block (r, s): columns 3s+j, j = 0..2
+        long pos = 0;
+        if (rowptr) rowptr[0] = 0;
+        for (int r = 0; r < nf; ++r) {
+            int b0 = brp[r], b1 = brp[r + 1];
+            for (int i = 0; i < 3; ++i) {
+                for (int b = b0; b < b1; ++b)
+                    for (int j = 0; j < 3; ++j) {
+                        if (col) col[pos] = 3 * bcol[b] + j;
+                        if (val) val[pos] = bval[9L * b + 3 * i + j];
+                        ++pos;
+                    }
+                if (rowptr) rowptr[3 * r + i + 1] = (int)pos;
+            }
+        }
+    });
+}
+
+int ofea_get_element_matrices(ofea_ctx *c, int first, int count, double *Ke) {
+    return guarded([&] {
+        need(c != nullptr && Ke != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
+        need(c->K_ok && c->Ke.p, OFEA_ERR_STATE, "no assembly yet");
+        need(first >= 0 && count >= 0 && first + count <= c->ne, OFEA_ERR_INVALID_ARG, "range");
+        use_device(c);
+        std::vector<double> blk(576);
+        double *out = Ke;
+        for (int e = first; e < first + count; ++e) {
+            bool hex = c->elem_type[e] == 1;
+            int npe = hex ? 8 : 4, m = 3 * npe;
+            size_t off = hex ? 576L * c->elem_local[e] : 576L * c->ne8 + 144L * c->elem_local[e];
+            OFEA_CUDA(cudaMemcpyAsync(blk.data(), c->Ke.p + off, sizeof(double) * m * m,
+                                      cudaMemcpyDeviceToHost, c->stream));
+            OFEA_CUDA(cudaStreamSynchronize(c->stream));
+            // device layout [a][b][i][j] -> row-major (3a+i, 3b+j)
+            for (int a = 0; a < npe; ++a)
+                for (int b = 0; b < npe; ++b)
+                    for (int i = 0; i < 3; ++i)
+                        for (int j = 0; j < 3; ++j)
+                            out[(3 * a + i) * m + 3 * b + j] = blk[((a * npe + b) * 9) + 3 * i + j];
+            out += m * m;
+        }
+    });
+}
+
+int ofea_spmv(ofea_ctx *c, const double *x, double *y) {
+    return guarded([&] {
+        need(c != nullptr && x && y, OFEA_ERR_INVALID_ARG, "NULL argument");
+        need(c->K_ok, OFEA_ERR_STATE, "K not assembled");
+        use_device(c);
+        c->w.t.ensure(std::max(c->n, 1));
+        c->w.q.ensure(std::max(c->n, 1));
+        OFEA_CUDA(cudaMemcpyAsync(c->w.t.p, x, sizeof(double) * c->n, cudaMemcpyHostToDevice, c->stream));
+        spmv64(c, c->w.t.p, c->w.q.p);
+        OFEA_CUDA(cudaMemcpyAsync(y, c->w.q.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
+        OFEA_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+static void check_solve_ready(ofea_ctx *c, const ofea_solve_opts &o) {
+    need(c->K_ok, OFEA_ERR_STATE, "K not assembled");
+    need(o.rtol > 0 && o.max_iter > 0, OFEA_ERR_INVALID_ARG, "rtol and max_iter must be positive");
+    if (o.method != OFEA_SOLVER_PCG64 && o.method != OFEA_SOLVER_MIXED)
+        fail(OFEA_ERR_UNKNOWN_SOLVER, "unknown solver method");
+    if (!c->jacobi_ok) fail(OFEA_ERR_BREAKDOWN, "a diagonal block of K is not positive definite");
+}
+
+int ofea_solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_opts *opts,
+                      ofea_solve_stats *stats) {
+    ofea_solve_stats st{};
+    int rc = guarded([&] {
+        need(c != nullptr && d_f && d_u, OFEA_ERR_INVALID_ARG, "NULL argument");
+        ofea_solve_opts o;
+        if (opts)
+            o = *opts;
+        else
+            ofea_solve_opts_default(&o);
+        check_solve_ready(c, o);
+        use_device(c);
+        OFEA_CUDA(cudaMemsetAsync(d_u, 0, sizeof(double) * c->n, c->stream));
+        solve_device(c, d_f, d_u, o, st);
+        if (st.status != OFEA_OK)
+            set_last_error(std::string("solve: ") + ofea_status_string(st.status) +
+                           ", relative residual " + std::to_string(st.rel_residual));
+    });
+    if (rc != OFEA_OK) st.status = rc;
+    if (stats) *stats = st;
+    return st.status;
+}
+
+int ofea_solve(ofea_ctx *c, const double *f, double *u, int nrhs, const ofea_solve_opts *opts,
+               ofea_solve_stats *stats) {
+    int worst = OFEA_OK;
+    int rc = guarded([&] {
+        need(c != nullptr && f && u && nrhs > 0, OFEA_ERR_INVALID_ARG, "NULL argument or nrhs < 1");
+        ofea_solve_opts o;
+        if (opts)
+            o = *opts;
+        else
+            ofea_solve_opts_default(&o);
+        check_solve_ready(c, o);
+        use_device(c);
+        const int n = c->n;
+        c->w.f.ensure(std::max(n, 1));
+        c->w.u.ensure(std::max(n, 1));
+        for (int k = 0; k < nrhs; ++k) {
+            ofea_solve_stats st{};
+            OFEA_CUDA(cudaMemcpyAsync(c->w.f.p, f + (long)k * n, sizeof(double) * n,
+                                      cudaMemcpyHostToDevice, c->stream));
+            OFEA_CUDA(cudaMemsetAsync(c->w.u.p, 0, sizeof(double) * n, c->stream));
+            solve_device(c, c->w.f.p, c->w.u.p, o, st);
+            OFEA_CUDA(cudaMemcpyAsync(u + (long)k * n, c->w.u.p, sizeof(double) * n,
+                                      cudaMemcpyDeviceToHost, c->stream));
+            OFEA_CUDA(cudaStreamSynchronize(c->stream));
+            if (stats) stats[k] = st;
+            if (st.status != OFEA_OK && worst == OFEA_OK) {
+                worst = st.status;
+                set_last_error(std::string("solve: ") + ofea_status_string(st.status) +
+                               ", relative residual " + std::to_string(st.rel_residual));
+            }
+        }
+    });
+    if (rc != OFEA_OK) {
+        if (stats) stats[0].status = rc;
+        return rc;
+    }
+    return worst;
+}
+
+int ofea_profile_solver_kernels(ofea_ctx *c, int method, int reps, double *ms, double *bytes) {
+    return guarded([&] {
+        need(c != nullptr && ms && bytes && reps > 0, OFEA_ERR_INVALID_ARG, "bad argument");
+        need(c->K_ok, OFEA_ERR_STATE, "K not assembled");
+        need(method == OFEA_SOLVER_PCG64 || method == OFEA_SOLVER_MIXED, OFEA_ERR_UNKNOWN_SOLVER,
+             "method");
+        use_device(c);
+        c->w.t.ensure(std::max(c->n, 1));
+        profile_kernels(c, method, reps, ms, bytes);
+    });
+}
+
+}  // extern "C"

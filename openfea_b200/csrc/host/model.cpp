@@ -1,0 +1,355 @@
+// Host-side model I/O and DOF numbering (include/ofea_host.h): the .inp subset
+// OpenFEA reads, set_BCs numbering / load vector, legacy-VTK output.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../../include/ofea_gpu.h"
+#include "../../../include/ofea_host.h"
+
+struct ofea_model {
+    int nd = 0, ne = 0;
+    std::vector<double> xyz;
+    std::vector<int> topo, etype, fix, load_set;
+    int load_dof = 0;
+    double load_value = 0;
+    double E = 0, nu = 0, density = 0;
+    int has_elastic = 0;
+};
+
+namespace {
+
+struct IoError {
+    std::string msg;
+};
+
+// Lines with '\r' removed (the reference's safeGetline accepts \n, \r\n, \r).
+std::vector<std::string> read_lines(const char *path) {
+    std::ifstream in(path, std::ios::binary);
+    if (!in) throw IoError{std::string("cannot open ") + path};
+    std::stringstream ss;
+    ss << in.rdbuf();
+    std::string all = ss.str();
+    std::vector<std::string> lines;
+    std::string cur;
+    for (size_t i = 0; i < all.size(); ++i) {
+        char ch = all[i];
+        if (ch == '\n' || ch == '\r') {
+            lines.push_back(cur);
+            cur.clear();
+            if (ch == '\r' && i + 1 < all.size() && all[i + 1] == '\n') ++i;
+        } else {
+            cur.push_back(ch);
+        }
+    }
+    if (!cur.empty()) lines.push_back(cur);
+    return lines;
+}
+
+bool has(const std::string &s, const char *key) { return s.find(key) != std::string::npos; }
+
+std::string strip(const std::string &s) {
+    size_t b = s.find_first_not_of(" \t"), e = s.find_last_not_of(" \t");
+    return b == std::string::npos ? std::string() : s.substr(b, e - b + 1);
+}
+
+// Whitespace tokens with one trailing comma removed, as the reference's
+// "iss >> node_id; erase last ','" (src/data2cae.cpp:334-341).
+std::vector<int> id_list(const std::string &line) {
+    std::istringstream iss(line);
+    std::string tok;
+    std::vector<int> out;
+    while (iss >> tok) {
+        if (!tok.empty() && tok.back() == ',') tok.pop_back();
+        if (!tok.empty()) out.push_back(std::atoi(tok.c_str()));
+    }
+    return out;
+}
+
+// Value of the second token of a "a, b, c" generate line (read_ele_node_num).
+int generate_count(const std::string &line) {
+    std::istringstream iss(line);
+    std::string t1, t2;
+    iss >> t1 >> t2;
+    return std::atoi(t2.c_str());
+}
+
+void parse(const std::vector<std::string> &L, ofea_model &m) {
+    // counts from the first *Nset / *Elset generate lines (src/data2cae.cpp:28-47)
+    int nd_gen = -1, ne_gen = -1;
+    for (size_t i = 0; i + 1 < L.size(); ++i) {
+        if (has(L[i], "*Nset")) nd_gen = generate_count(L[i + 1]);
+        if (has(L[i], "*Elset")) {
+            ne_gen = generate_count(L[i + 1]);
+            break;
+        }
+    }
+    // nodes and elements (src/data2cae.cpp:89-163), up to *End Assembly
+    bool in_node = false, in_elem = false;
+    int etype = -1;
+    for (size_t i = 0; i < L.size(); ++i) {
+        const std::string &s = L[i];
+        if (has(s, "*End Assembly")) break;
+        if (has(s, "*")) {
+            in_node = has(s, "*Node") && !has(s, "*Nset") && !has(s, "*Node Output");
+            in_elem = false;
+            if (has(s, "*Element") && !has(s, "*Element Output")) {
+                size_t eq = s.find('=');
+                std::string t = eq == std::string::npos ? "" : strip(s.substr(eq + 1));
+                size_t comma = t.find(',');
+                if (comma != std::string::npos) t = strip(t.substr(0, comma));
+                if (t == "C3D4")
+                    etype = 0;
+                else if (t == "C3D8")
+                    etype = 1;
+                else
+                    throw IoError{"unsupported element type '" + t + "' (C3D4, C3D8 only)"};
+                in_elem = true;
+            }
+            continue;
+        }
+        if (in_node) {
+            std::string t = s;
+            std::replace(t.begin(), t.end(), ',', ' ');
+            std::istringstream iss(t);
+            double id, x, y, z;
+            if (!(iss >> id >> x >> y >> z)) throw IoError{"bad *Node line: " + s};
+            // stored in file order, ids not used (src/data2cae.cpp:103-115)
+            m.xyz.push_back(x);
+            m.xyz.push_back(y);
+            m.xyz.push_back(z);
+        } else if (in_elem) {
+            std::istringstream iss(s);
+            std::string tok;
+            std::vector<int> v;
+            while (std::getline(iss, tok, ',')) {
+                tok = strip(tok);
+                if (!tok.empty()) v.push_back(std::atoi(tok.c_str()));
+            }
+            int npe = etype == 1 ? 8 : 4;
+            if ((int)v.size() != npe + 1) throw IoError{"bad *Element line: " + s};
+            for (int a = 0; a < 8; ++a) m.topo.push_back(a < npe ? v[1 + a] : 0);
+            m.etype.push_back(etype);
+        }
+    }
+    m.nd = (int)(m.xyz.size() / 3);
+    m.ne = (int)m.etype.size();
+    if (m.nd == 0 || m.ne == 0) throw IoError{"no *Node or *Element data"};
+    if ((nd_gen >= 0 && nd_gen != m.nd) || (ne_gen >= 0 && ne_gen != m.ne))
+        throw IoError{"*Nset/*Elset generate counts disagree with the *Node/*Element data"};
+    for (int v : m.topo)
+        if (v < 0 || v > m.nd) throw IoError{"element references a node id outside 1..nd"};
+    // Set-load / Set-fix node lists before *End Assembly (src/data2cae.cpp:321-350, 382-411)
+    auto node_set = [&](const char *key, std::vector<int> &out) {
+        for (size_t i = 0; i < L.size(); ++i) {
+            if (has(L[i], "*End Assembly")) break;
+            if (has(L[i], key)) {
+                size_t j = i + 1;
+                for (; j < L.size() && !has(L[j], "*"); ++j) {
+                    auto ids = id_list(L[j]);
+                    out.insert(out.end(), ids.begin(), ids.end());
+                }
+                i = j - 1;
+            }
+        }
+    };
+    node_set("Set-load", m.load_set);
+    node_set("Set-fix", m.fix);
+    // Cload after *End Assembly: "set, dof, value" (src/data2cae.cpp:352-369)
+    bool after = false;
+    for (size_t i = 0; i < L.size(); ++i) {
+        if (has(L[i], "*End Assembly")) after = true;
+        if (after && has(L[i], "Cload") && i + 1 < L.size()) {
+            std::istringstream iss(L[i + 1]);
+            std::string name, dof, val;
+            iss >> name >> dof >> val;
+            if (!dof.empty() && dof.back() == ',') dof.pop_back();
+            m.load_dof = std::atoi(dof.c_str());
+            m.load_value = std::strtod(val.c_str(), nullptr);
+            break;
+        }
+    }
+    // *Density, *Elastic (last occurrence wins, src/data2cae.cpp:422-442)
+    for (size_t i = 0; i + 1 < L.size(); ++i) {
+        if (has(L[i], "*Density")) {
+            std::istringstream iss(L[i + 1]);
+            std::string d;
+            iss >> d;
+            if (!d.empty() && d.back() == ',') d.pop_back();
+            m.density = std::strtod(d.c_str(), nullptr);
+        }
+        if (has(L[i], "*Elastic")) {
+            std::istringstream iss(L[i + 1]);
+            std::string e, nu;
+            iss >> e >> nu;
+            if (!e.empty() && e.back() == ',') e.pop_back();
+            m.E = std::strtod(e.c_str(), nullptr);
+            m.nu = std::strtod(nu.c_str(), nullptr);
+            m.has_elastic = 1;
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int ofea_inp_read(const char *path, ofea_model **out) {
+    if (!path || !out) return OFEA_ERR_INVALID_ARG;
+    *out = nullptr;
+    try {
+        auto lines = read_lines(path);
+        auto *m = new ofea_model();
+        try {
+            parse(lines, *m);
+        } catch (...) {
+            delete m;
+            throw;
+        }
+        *out = m;
+        return OFEA_OK;
+    } catch (const IoError &) {
+        return OFEA_ERR_IO;
+    } catch (...) {
+        return OFEA_ERR_IO;
+    }
+}
+
+void ofea_model_free(ofea_model *m) { delete m; }
+
+int ofea_model_sizes(const ofea_model *m, int *nd, int *ne, int *nfix, int *nload) {
+    if (!m) return OFEA_ERR_INVALID_ARG;
+    if (nd) *nd = m->nd;
+    if (ne) *ne = m->ne;
+    if (nfix) *nfix = (int)m->fix.size();
+    if (nload) *nload = (int)m->load_set.size();
+    return OFEA_OK;
+}
+
+int ofea_model_arrays(const ofea_model *m, double *xyz, int *topo, int *etype, int *fix,
+                      int *load_set) {
+    if (!m) return OFEA_ERR_INVALID_ARG;
+    if (xyz) std::copy(m->xyz.begin(), m->xyz.end(), xyz);
+    if (topo) std::copy(m->topo.begin(), m->topo.end(), topo);
+    if (etype) std::copy(m->etype.begin(), m->etype.end(), etype);
+    if (fix) std::copy(m->fix.begin(), m->fix.end(), fix);
+    if (load_set) std::copy(m->load_set.begin(), m->load_set.end(), load_set);
+    return OFEA_OK;
+}
+
+int ofea_model_material(const ofea_model *m, double *E, double *nu, double *density,
+                        int *has_elastic) {
+    if (!m) return OFEA_ERR_INVALID_ARG;
+    if (E) *E = m->E;
+    if (nu) *nu = m->nu;
+    if (density) *density = m->density;
+    if (has_elastic) *has_elastic = m->has_elastic;
+    return OFEA_OK;
+}
+
+int ofea_model_cload(const ofea_model *m, int *dof, double *value) {
+    if (!m) return OFEA_ERR_INVALID_ARG;
+    if (dof) *dof = m->load_dof;
+    if (value) *value = m->load_value;
+    return OFEA_OK;
+}
+
+int ofea_build_free_index(int nd, int nfix, const int *fix_ids, int *free_map, int *nfree) {
+    if (nd <= 0 || nfix <= 0 || !fix_ids || !free_map) return OFEA_ERR_INVALID_ARG;
+    std::vector<int> s(fix_ids, fix_ids + nfix);
+    std::sort(s.begin(), s.end());
+    for (int k = 0; k < nfix; ++k)
+        if (s[k] < 1 || s[k] > nd || (k > 0 && s[k] == s[k - 1])) return OFEA_ERR_INVALID_ARG;
+    // walk the nodes against the sorted fixed ids (src/set_bc.cpp:25-42)
+    int next = 0, c = 0;
+    for (int i = 0; i < nd; ++i) {
+        if (c < nfix && i == s[c] - 1) {
+            free_map[i] = -1;
+            ++c;
+        } else {
+            free_map[i] = next++;
+        }
+    }
+    if (nfree) *nfree = next;
+    return OFEA_OK;
+}
+
+int ofea_build_single_load(int nd, const int *free_map, int nload, const int *load_set, int dof,
+                           double value, double *f) {
+    if (nd <= 0 || !free_map || (nload > 0 && !load_set) || !f) return OFEA_ERR_INVALID_ARG;
+    if (dof < 1 || dof > 3) return OFEA_ERR_INVALID_ARG;
+    int nfree = 0;
+    for (int i = 0; i < nd; ++i) nfree += free_map[i] >= 0;
+    std::fill(f, f + 3L * nfree, 0.0);
+    for (int k = 0; k < nload; ++k) {
+        int id = load_set[k];
+        if (id < 1 || id > nd) return OFEA_ERR_INVALID_ARG;
+        int r = free_map[id - 1];
+        if (r >= 0) f[3L * r + dof - 1] = value;
+    }
+    return OFEA_OK;
+}
+
+int ofea_full_displacement(int nd, const int *free_map, const double *u, double *u_full) {
+    if (nd <= 0 || !free_map || !u || !u_full) return OFEA_ERR_INVALID_ARG;
+    for (int i = 0; i < nd; ++i) {
+        int r = free_map[i];
+        for (int c = 0; c < 3; ++c) u_full[3L * i + c] = r >= 0 ? u[3L * r + c] : 0.0;
+    }
+    return OFEA_OK;
+}
+
+int ofea_write_vtk(const char *path, int nd, const double *xyz, int ne, const int *topo,
+                   const int *etype, const double *u_full, double scale) {
+    if (!path || nd <= 0 || ne < 0 || !xyz || !topo || !etype || !u_full) return OFEA_ERR_INVALID_ARG;
+    std::ofstream fout(path);
+    if (!fout) return OFEA_ERR_IO;
+    // same header, separators and default 6-significant-digit formatting as
+    // the reference writer (src/data2vtk.cpp:56-100, 143-196)
+    fout << "# vtk DataFile Version 3.0\n";
+    fout << "The density field of the optimized results\n";
+    fout << "ASCII\n";
+    fout << "DATASET UNSTRUCTURED_GRID\n\n";
+    fout << "POINTS\t" << nd << "\tdouble\n";
+    for (int i = 0; i < nd; ++i)
+        fout << xyz[3L * i] + scale * u_full[3L * i] << "\t\t" << xyz[3L * i + 1] + scale * u_full[3L * i + 1]
+             << "\t\t" << xyz[3L * i + 2] + scale * u_full[3L * i + 2] << "\n";
+    long n4 = 0, n8 = 0;
+    for (int e = 0; e < ne; ++e) (etype[e] == 1 ? n8 : n4)++;
+    fout << "CELLS\t" << ne << "\t" << n8 * 9 + n4 * 5 << "\n";
+    for (int e = 0; e < ne; ++e) {
+        const int *t = topo + 8L * e;
+        if (etype[e] == 1) {
+            static const int ord[8] = {0, 1, 3, 2, 4, 5, 7, 6};  // VTK_VOXEL order
+            fout << 8;
+            for (int a = 0; a < 8; ++a) fout << "\t" << t[ord[a]] - 1;
+            fout << "\n";
+        } else {
+            fout << 4 << "\t" << t[0] - 1 << "\t" << t[2] - 1 << "\t" << t[1] - 1 << "\t" << t[3] - 1 << "\n";
+        }
+    }
+    fout << "CELL_TYPES\t\t" << ne << "\n";
+    for (int e = 0; e < ne; ++e) fout << (etype[e] == 1 ? 11 : 10) << "\n";
+    const char *names[3] = {"u_x", "u_y", "u_z"};
+    fout << "\nPOINT_DATA\t" << nd;
+    for (int c = 0; c < 3; ++c) {
+        fout << "\nSCALARS " << names[c] << " double 1\n"
+             << "LOOKUP_TABLE  table" << c + 1 << "\n";
+        for (int i = 0; i < nd; ++i) fout << u_full[3L * i + c] << "\n";
+    }
+    fout << "\nSCALARS u_magnitude double 1\n"
+         << "LOOKUP_TABLE  table4\n";
+    for (int i = 0; i < nd; ++i) {
+        const double *u = u_full + 3L * i;
+        fout << std::sqrt(u[2] * u[2] + u[1] * u[1] + u[0] * u[0]) << "\n";
+    }
+    return fout.good() ? OFEA_OK : OFEA_ERR_IO;
+}
+
+}  // extern "C"

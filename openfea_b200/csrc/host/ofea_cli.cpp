@@ -1,0 +1,145 @@
+// ofea_cli: OpenFEA's implicit-static driver (CAE_process::Init / Solve /
+// implict_analysis, src/cae.cpp:18-301) with the assembly and the linear
+// solves running on the GPU through the C ABI.
+//
+//   ofea_cli -i model.inp [-o out.vtk] [-imp] [-nl] [-solver GPU_PCG|GPU_MIXED]
+//            [-rtol 1e-8] [-E <Young> -nu <Poisson>]
+//
+// -E/-nu override the file's material (the reference's code_test cases set it
+// in code for models without *Elastic, src/main.cpp:121-135).  The output VTK
+// name defaults to the input name with .vtk (src/cae.cpp:108-110).
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../../include/ofea_gpu.h"
+#include "../../../include/ofea_host.h"
+
+namespace {
+
+double now() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+int die(const char *what, int rc) {
+    std::fprintf(stderr, "ofea_cli: %s failed: %s (%s)\n", what, ofea_status_string(rc), ofea_last_error());
+    return 2;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    std::string in, out, solver = "GPU_PCG";
+    bool nl = false;
+    double rtol = 1e-8, E_over = -1, nu_over = -1;
+    for (int i = 1; i < argc; ++i) {
+        std::string a = argv[i];
+        if (a == "-i" && i + 1 < argc) in = argv[++i];
+        else if (a == "-o" && i + 1 < argc) out = argv[++i];
+        else if (a == "-nl") nl = true;
+        else if (a == "-imp") {}
+        else if (a == "-solver" && i + 1 < argc) solver = argv[++i];
+        else if (a == "-rtol" && i + 1 < argc) rtol = std::atof(argv[++i]);
+        else if (a == "-E" && i + 1 < argc) E_over = std::atof(argv[++i]);
+        else if (a == "-nu" && i + 1 < argc) nu_over = std::atof(argv[++i]);
+        else if (argc == 2) in = a;
+        else if (a == "-exp" || a == "-sfem" || a == "-re") {
+            std::fprintf(stderr, "ofea_cli: %s is not part of the GPU implicit-static path\n", a.c_str());
+            return 2;
+        }
+    }
+    if (in.size() < 5 || in.substr(in.size() - 4) != ".inp") {
+        std::fprintf(stderr, "Please enter the correct path to the input file ending in .inp\n");
+        return 2;
+    }
+    if (out.empty()) out = in.substr(0, in.size() - 4) + ".vtk";
+    ofea_solve_opts opts;
+    ofea_solve_opts_default(&opts);
+    opts.rtol = rtol;
+    if (solver == "GPU_PCG") opts.method = OFEA_SOLVER_PCG64;
+    else if (solver == "GPU_MIXED") opts.method = OFEA_SOLVER_MIXED;
+    else {
+        std::fprintf(stderr, "Please check your flag of solver !!!\n");
+        return 2;
+    }
+
+    ofea_model *m = nullptr;
+    int rc = ofea_inp_read(in.c_str(), &m);
+    if (rc) return die("reading the .inp file", rc);
+    int nd, ne, nfix, nload;
+    ofea_model_sizes(m, &nd, &ne, &nfix, &nload);
+    std::vector<double> xyz(3L * nd);
+    std::vector<int> topo(8L * ne), etype(ne), fix(nfix), load(nload);
+    ofea_model_arrays(m, xyz.data(), topo.data(), etype.data(), fix.data(), load.data());
+    double E, nu, rho;
+    int has_el, dof;
+    double val;
+    ofea_model_material(m, &E, &nu, &rho, &has_el);
+    ofea_model_cload(m, &dof, &val);
+    ofea_model_free(m);
+    if (E_over > 0) E = E_over;
+    if (nu_over >= 0) nu = nu_over;
+    if (!has_el && E_over <= 0) {
+        std::fprintf(stderr, "ofea_cli: the model has no *Elastic; pass -E and -nu\n");
+        return 2;
+    }
+    std::printf("the number of element is: %d\nthe number of node is: %d\n", ne, nd);
+
+    std::vector<int> fm(nd);
+    int nfree = 0;
+    if ((rc = ofea_build_free_index(nd, nfix, fix.data(), fm.data(), &nfree))) return die("build_free_index", rc);
+    const int n = 3 * nfree;
+    std::vector<double> f(n), u(n, 0.0);
+    if ((rc = ofea_build_single_load(nd, fm.data(), nload, load.data(), dof, val, f.data())))
+        return die("build_single_load", rc);
+
+    ofea_ctx *ctx = nullptr;
+    if ((rc = ofea_ctx_create(&ctx, 0))) return die("ofea_ctx_create", rc);
+    double t0 = now();
+    if ((rc = ofea_mesh_upload(ctx, nd, xyz.data(), ne, topo.data(), etype.data(), nullptr, E, nu, fm.data())))
+        return die("ofea_mesh_upload", rc);
+    int n_chk;
+    long long nnz;
+    if ((rc = ofea_assemble_pattern(ctx, &n_chk, &nnz))) return die("ofea_assemble_pattern", rc);
+    std::printf("The CSR index has been built (n = %d, nnz = %lld)\n", n_chk, nnz);
+    ofea_solve_stats st{};
+    if (!nl) {
+        if ((rc = ofea_assemble_linear(ctx))) return die("ofea_assemble_linear", rc);
+        rc = ofea_solve(ctx, f.data(), u.data(), 1, &opts, &st);
+        std::printf("solve: %s, %d iterations, relative residual %.3e, %.4f s on the GPU\n",
+                    ofea_status_string(st.status), st.iterations, st.rel_residual, st.seconds);
+        if (rc) return die("ofea_solve", rc);
+    } else {
+        // Newton loop of implict_analysis (src/cae.cpp:209-253), same stopping
+        // rule: ||f - f_int||_2 / (3 n_free_nodes) < 1e-6, at most 100 passes.
+        std::vector<double> fint(n), r(n), du(n);
+        double res = 1.0;
+        int loop = 0;
+        while (res > 1.0e-6 && loop < 100) {
+            if ((rc = ofea_assemble_nl(ctx, u.data(), fint.data()))) return die("ofea_assemble_nl", rc);
+            for (int i = 0; i < n; ++i) r[i] = f[i] - fint[i];
+            rc = ofea_solve(ctx, r.data(), du.data(), 1, &opts, &st);
+            if (rc) return die("ofea_solve", rc);
+            res = 0;
+            for (int i = 0; i < n; ++i) {
+                u[i] += du[i];
+                res += r[i] * r[i];
+            }
+            res = std::sqrt(res) / (3.0 * nfree);
+            ++loop;
+            std::printf("this is loop %d, and res is %g\n", loop, res);
+        }
+        std::printf("the loop is over\n");
+    }
+    std::printf("It took %g s to compute full analysis\n", now() - t0);
+    std::vector<double> uf(3L * nd);
+    ofea_full_displacement(nd, fm.data(), u.data(), uf.data());
+    if ((rc = ofea_write_vtk(out.c_str(), nd, xyz.data(), ne, topo.data(), etype.data(), uf.data(), 1.0)))
+        return die("writing the VTK file", rc);
+    ofea_ctx_destroy(ctx);
+    return 0;
+}

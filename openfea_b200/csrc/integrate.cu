@@ -1,0 +1,548 @@
+// Element integration and assembly on the device: the B200 replacement of
+// assamble_stiffness::fill_CSR_sparse_mat (src/assemble.cpp:95-151) and
+// assamble_nl_stiffness::fill_CSR_sparse_mat (src/nl_assemble.cpp:94-166).
+//
+// Stage 1 (integration, FP64): one warp-group (128 threads) integrates a batch
+// of elements: node coordinates are staged in shared memory, each thread
+// computes the Jacobian of one Gauss point redundantly and the physical shape
+// function gradients of one node, then one 3x3 nodal block of Ke per thread.
+// The nodal-block form of B^T D B used here (isotropic D, engineering shear,
+// strain order [xx, yy, zz, xy, yz, zx], src/Elements/C3D8.cpp:21-35) is
+//   K_ab[i][j] = sum_q w_q det_q (lam g_a[i] g_b[j] + mu g_a[j] g_b[i]
+//                                 + delta_ij mu g_a.g_b)
+// with g_a = J^-1 dN_a at Gauss point q; for C3D8 the 2x2x2 rule with weight
+// 1 (src/Elements/C3D8_Gauss.cpp:80-107), for C3D4 one point, weight 1/6 and
+// the signed determinant (src/Elements/C3D4_hammer.cpp:61-72).  Element
+// matrices go to a scratch buffer with coalesced stores.
+//
+// Stage 2 (assembly): one warp per free node owns its block row of K, walks
+// the node's incident elements in ascending order and adds their block rows
+// through the precomputed slot map in shared memory, then writes the row once:
+// no atomics, coalesced, bitwise reproducible.
+#include <algorithm>
+#include <cmath>
+
+#include "ofea_internal.cuh"
+
+namespace ofea {
+
+// dN/d(r,s,t) of the 8-node brick at the 8 Gauss points, [q][dim][node]
+// (node order src/Elements/C3D8_Gauss.cpp:27-52, points :84-92).
+__constant__ double c_hex_dN[8 * 3 * 8];
+
+// Per-device constant table; re-uploaded on every integration call (192
+// doubles), so contexts on several devices each see it.
+static void upload_hex_table() {
+    const int sr[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
+    const int ss[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
+    const int st[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+    double g = 1.0 / std::sqrt(3.0), t[192];
+    for (int q = 0; q < 8; ++q) {
+        double r = sr[q] * g, s = ss[q] * g, u = st[q] * g;
+        for (int a = 0; a < 8; ++a) {
+            t[(q * 3 + 0) * 8 + a] = 0.125 * sr[a] * (1.0 + ss[a] * s) * (1.0 + st[a] * u);
+            t[(q * 3 + 1) * 8 + a] = 0.125 * ss[a] * (1.0 + sr[a] * r) * (1.0 + st[a] * u);
+            t[(q * 3 + 2) * 8 + a] = 0.125 * st[a] * (1.0 + sr[a] * r) * (1.0 + ss[a] * s);
+        }
+    }
+    OFEA_CUDA(cudaMemcpyToSymbol(c_hex_dN, t, sizeof(t)));
+}
+
+struct Lame {
+    double lam, mu, fac;
+};
+// Same expressions as build_cons_mat (src/Elements/C3D8.cpp:23-27).
+__device__ __forceinline__ Lame lame(double E, double nu) {
+    double fac = (E * (1.0 - nu)) / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    return {fac * nu / (1.0 - nu), fac * (1.0 - 2.0 * nu) / (2.0 * (1.0 - nu)), fac};
+}
+
+// Determinant in the reference's expression (C3D8_Gauss.cpp:58-63) and the
+// cofactor inverse.
+__device__ __forceinline__ double det_sarrus(const double *J) {
+    return J[0] * J[4] * J[8] + J[1] * J[5] * J[6] + J[2] * J[3] * J[7] - J[2] * J[4] * J[6] -
+           J[5] * J[7] * J[0] - J[8] * J[1] * J[3];
+}
+__device__ __forceinline__ void inv3(const double *J, double *Ji) {
+    double c00 = J[4] * J[8] - J[5] * J[7];
+    double c01 = J[5] * J[6] - J[3] * J[8];
+    double c02 = J[3] * J[7] - J[4] * J[6];
+    double id = 1.0 / (J[0] * c00 + J[1] * c01 + J[2] * c02);
+    Ji[0] = c00 * id;
+    Ji[1] = (J[2] * J[7] - J[1] * J[8]) * id;
+    Ji[2] = (J[1] * J[5] - J[2] * J[4]) * id;
+    Ji[3] = c01 * id;
+    Ji[4] = (J[0] * J[8] - J[2] * J[6]) * id;
+    Ji[5] = (J[2] * J[3] - J[0] * J[5]) * id;
+    Ji[6] = c02 * id;
+    Ji[7] = (J[1] * J[6] - J[0] * J[7]) * id;
+    Ji[8] = (J[0] * J[4] - J[1] * J[3]) * id;
+}
+
+// Linear nodal block accumulation: k += w (lam ga gb^T + mu gb ga^T + mu (ga.gb) I).
+__device__ __forceinline__ void add_block_lin(double *k, const double *ga, const double *gb,
+                                              double wl, double wm) {
+    double d = ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double v = wl * ga[i] * gb[j] + wm * ga[j] * gb[i];
+            if (i == j) v += wm * d;
+            k[3 * i + j] += v;
+        }
+}
+
+// Total-Lagrangian quantities of one integration point from F:
+// S = D E_GL (Voigt [xx,yy,zz,xy,yz,zx], engineering shear as the reference's
+// Gl_vec, src/Elements/C3D8_Gauss.cpp:164-172) and C = F F^T.
+__device__ __forceinline__ void tl_point(const double *F, const Lame &L, double *S, double *C) {
+    double Eg[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double s = F[i] * F[j] + F[3 + i] * F[3 + j] + F[6 + i] * F[6 + j];  // (F^T F)_ij
+            Eg[3 * i + j] = 0.5 * (s - (i == j ? 1.0 : 0.0));
+        }
+    double e0 = Eg[0], e1 = Eg[4], e2 = Eg[8];
+    double fa = L.lam;
+    S[0] = L.fac * e0 + fa * e1 + fa * e2;
+    S[1] = fa * e0 + L.fac * e1 + fa * e2;
+    S[2] = fa * e0 + fa * e1 + L.fac * e2;
+    S[3] = L.mu * (2.0 * Eg[1]);
+    S[4] = L.mu * (2.0 * Eg[5]);
+    S[5] = L.mu * (2.0 * Eg[2]);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            C[3 * i + j] = F[3 * i] * F[3 * j] + F[3 * i + 1] * F[3 * j + 1] + F[3 * i + 2] * F[3 * j + 2];
+}
+
+// Smat g with Smat = [[S0,S3,S5],[S3,S1,S4],[S5,S4,S2]].
+__device__ __forceinline__ void smat_vec(const double *S, const double *g, double *o) {
+    o[0] = S[0] * g[0] + S[3] * g[1] + S[5] * g[2];
+    o[1] = S[3] * g[0] + S[1] * g[1] + S[4] * g[2];
+    o[2] = S[5] * g[0] + S[4] * g[1] + S[2] * g[2];
+}
+
+// Tangent nodal block: k += w (lam pa pb^T + mu pb pa^T + mu (ga.gb) C + (ga.S gb) I),
+// p = F g, which equals (B_L^T D B_L + B_NL^T SIG B_NL)_ab of the reference
+// (src/Elements/C3D8_Gauss.cpp:174-264).
+__device__ __forceinline__ void add_block_nl(double *k, const double *ga, const double *gb,
+                                             const double *pa, const double *pb, const double *C,
+                                             const double *S, double w, const Lame &L) {
+    double d = ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2];
+    double sg[3];
+    smat_vec(S, gb, sg);
+    double geo = ga[0] * sg[0] + ga[1] * sg[1] + ga[2] * sg[2];
+    double wl = w * L.lam, wm = w * L.mu, wc = w * L.mu * d;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            double v = wl * pa[i] * pb[j] + wm * pb[i] * pa[j] + wc * C[3 * i + j];
+            if (i == j) v += w * geo;
+            k[3 * i + j] += v;
+        }
+}
+
+// ------------------------------------------------------------------ C3D8 --
+
+constexpr int kHexPerCta = 2;  // 64 threads per element: (q,a) then (a,b)
+
+template <bool NL>
+__global__ void __launch_bounds__(128) k_hex_integrate(
+    int ne8, const int *__restrict__ topo8, const double *__restrict__ xyz,
+    const double *__restrict__ E8, double nu, const int *__restrict__ free_map,
+    const double *__restrict__ u, double *__restrict__ Ke, double *__restrict__ Fe) {
+    __shared__ double sX[kHexPerCta][24];
+    __shared__ double sU[kHexPerCta][24];       // [a][c]
+    __shared__ double sG[kHexPerCta][8 * 3 * 8];  // [q][d][a]
+    __shared__ double sP[kHexPerCta][NL ? 8 * 3 * 8 : 1];
+    __shared__ double sW[kHexPerCta][8];
+    __shared__ double sS[kHexPerCta][NL ? 8 * 6 : 1];
+    __shared__ double sC[kHexPerCta][NL ? 8 * 9 : 1];
+    __shared__ double sF[kHexPerCta][NL ? 8 * 9 : 1];
+    __shared__ double sK[kHexPerCta][576];
+    const int le = threadIdx.x >> 6, t = threadIdx.x & 63;
+    for (long base = (long)blockIdx.x * kHexPerCta; base < ne8; base += (long)gridDim.x * kHexPerCta) {
+        const long e = base + le;
+        const bool act = e < ne8;
+        if (act && t < 24) {
+            int a = t / 3, cc = t - 3 * a;
+            int node = topo8[8 * e + a];
+            sX[le][t] = xyz[3L * node + cc];
+            if (NL) {
+                int f = free_map[node];
+                sU[le][t] = f >= 0 ? u[3L * f + cc] : 0.0;
+            }
+        }
+        __syncthreads();
+        Lame L{0, 0, 0};
+        if (act) L = lame(E8[e], nu);
+        if (act) {
+            // thread (q, a): Jacobian at q (redundant over a), gradient of node a
+            const int q = t >> 3, a = t & 7;
+            const double *dN = c_hex_dN + q * 24;
+            double J[9];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    double s = 0;
+#pragma unroll
+                    for (int b = 0; b < 8; ++b) s += dN[i * 8 + b] * sX[le][3 * b + j];
+                    J[3 * i + j] = s;
+                }
+            double Ji[9];
+            inv3(J, Ji);
+            double g[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                g[d] = Ji[3 * d] * dN[a] + Ji[3 * d + 1] * dN[8 + a] + Ji[3 * d + 2] * dN[16 + a];
+                sG[le][(q * 3 + d) * 8 + a] = g[d];
+            }
+            if (a == 0) sW[le][q] = det_sarrus(J);  // Gauss weight 1
+            if (NL) {
+                // F = I + sum_b u_b (x) g_b needs every node's gradient: recompute
+                // them from Ji here (8 x 9 FMA) rather than wait for sG.
+                double F[9];
+#pragma unroll
+                for (int i = 0; i < 9; ++i) F[i] = (i % 4 == 0) ? 1.0 : 0.0;
+#pragma unroll
+                for (int b = 0; b < 8; ++b) {
+                    double gb[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+                        gb[d] = Ji[3 * d] * dN[b] + Ji[3 * d + 1] * dN[8 + b] + Ji[3 * d + 2] * dN[16 + b];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) F[3 * i + j] += sU[le][3 * b + i] * gb[j];
+                }
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    sP[le][(q * 3 + i) * 8 + a] = F[3 * i] * g[0] + F[3 * i + 1] * g[1] + F[3 * i + 2] * g[2];
+                if (a == 0) {
+                    double S[6], C[9];
+                    tl_point(F, L, S, C);
+#pragma unroll
+                    for (int i = 0; i < 6; ++i) sS[le][6 * q + i] = S[i];
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) {
+                        sC[le][9 * q + i] = C[i];
+                        sF[le][9 * q + i] = F[i];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (act) {
+            // thread (a, b): block K_ab summed over the Gauss points
+            const int a = t >> 3, b = t & 7;
+            double k[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            double fa[3] = {0, 0, 0};
+#pragma unroll 2
+            for (int q = 0; q < 8; ++q) {
+                double ga[3], gb[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    ga[d] = sG[le][(q * 3 + d) * 8 + a];
+                    gb[d] = sG[le][(q * 3 + d) * 8 + b];
+                }
+                double w = sW[le][q];
+                if (!NL) {
+                    add_block_lin(k, ga, gb, w * L.lam, w * L.mu);
+                } else {
+                    double pa[3], pb[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        pa[d] = sP[le][(q * 3 + d) * 8 + a];
+                        pb[d] = sP[le][(q * 3 + d) * 8 + b];
+                    }
+                    add_block_nl(k, ga, gb, pa, pb, &sC[le][9 * q], &sS[le][6 * q], w, L);
+                    if (b == 0) {
+                        // f_a += w F (Smat g_a)  (= B_L^T S, C3D8_Gauss.cpp:257)
+                        double sg[3];
+                        smat_vec(&sS[le][6 * q], ga, sg);
+                        const double *F = &sF[le][9 * q];
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+                            fa[i] += w * (F[3 * i] * sg[0] + F[3 * i + 1] * sg[1] + F[3 * i + 2] * sg[2]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 9; ++i) sK[le][(a * 8 + b) * 9 + i] = k[i];
+            if (NL && b == 0)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) Fe[24 * e + 3 * a + i] = fa[i];
+        }
+        __syncthreads();
+        // coalesced store of the batch's element matrices
+        for (int v = threadIdx.x; v < kHexPerCta * 576; v += blockDim.x) {
+            int l2 = v / 576;
+            long e2 = base + l2;
+            if (e2 < ne8) Ke[576 * e2 + (v - 576 * l2)] = sK[l2][v - 576 * l2];
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ C3D4 --
+
+constexpr int kTetPerCta = 8;  // 16 threads per element: (a,b)
+
+template <bool NL>
+__global__ void __launch_bounds__(128) k_tet_integrate(
+    int ne4, const int *__restrict__ topo4, const double *__restrict__ xyz,
+    const double *__restrict__ E4, double nu, const int *__restrict__ free_map,
+    const double *__restrict__ u, double *__restrict__ Ke, double *__restrict__ Fe) {
+    __shared__ double sX[kTetPerCta][12];
+    __shared__ double sU[kTetPerCta][12];
+    __shared__ double sK[kTetPerCta][144];
+    const int le = threadIdx.x >> 4, t = threadIdx.x & 15;
+    for (long base = (long)blockIdx.x * kTetPerCta; base < ne4; base += (long)gridDim.x * kTetPerCta) {
+        const long e = base + le;
+        const bool act = e < ne4;
+        if (act && t < 12) {
+            int a = t / 3, cc = t - 3 * a;
+            int node = topo4[4 * e + a];
+            sX[le][t] = xyz[3L * node + cc];
+            if (NL) {
+                int f = free_map[node];
+                sU[le][t] = f >= 0 ? u[3L * f + cc] : 0.0;
+            }
+        }
+        __syncthreads();
+        if (act) {
+            const int a = t >> 2, b = t & 3;
+            const double *X = sX[le];
+            // dN/d(rst) = [[-1,1,0,0],[-1,0,1,0],[-1,0,0,1]] (C3D4_hammer.cpp:26-28)
+            double J[9];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) J[3 * i + j] = X[3 * (i + 1) + j] - X[j];
+            double Ji[9];
+            inv3(J, Ji);
+            double G[4][3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                G[0][d] = -(Ji[3 * d] + Ji[3 * d + 1] + Ji[3 * d + 2]);
+                G[1][d] = Ji[3 * d];
+                G[2][d] = Ji[3 * d + 1];
+                G[3][d] = Ji[3 * d + 2];
+            }
+            const double w = (1.0 / 6.0) * det_sarrus(J);  // signed, no abs (C3D4_hammer.cpp:70)
+            const Lame L = lame(E4[e], nu);
+            double k[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            if (!NL) {
+                add_block_lin(k, G[a], G[b], w * L.lam, w * L.mu);
+            } else {
+                const double *U = sU[le];
+                double F[9];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        double s = (i == j) ? 1.0 : 0.0;
+#pragma unroll
+                        for (int c2 = 0; c2 < 4; ++c2) s += U[3 * c2 + i] * G[c2][j];
+                        F[3 * i + j] = s;
+                    }
+                double S[6], C[9], pa[3], pb[3];
+                tl_point(F, L, S, C);
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    pa[i] = F[3 * i] * G[a][0] + F[3 * i + 1] * G[a][1] + F[3 * i + 2] * G[a][2];
+                    pb[i] = F[3 * i] * G[b][0] + F[3 * i + 1] * G[b][1] + F[3 * i + 2] * G[b][2];
+                }
+                add_block_nl(k, G[a], G[b], pa, pb, C, S, w, L);
+                if (b == 0) {
+                    double sg[3];
+                    smat_vec(S, G[a], sg);
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+                        Fe[12 * e + 3 * a + i] = w * (F[3 * i] * sg[0] + F[3 * i + 1] * sg[1] + F[3 * i + 2] * sg[2]);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 9; ++i) sK[le][(a * 4 + b) * 9 + i] = k[i];
+        }
+        __syncthreads();
+        for (int v = threadIdx.x; v < kTetPerCta * 144; v += blockDim.x) {
+            int l2 = v / 144;
+            long e2 = base + l2;
+            if (e2 < ne4) Ke[144 * e2 + (v - 144 * l2)] = sK[l2][v - 144 * l2];
+        }
+        __syncthreads();
+    }
+}
+
+// -------------------------------------------------------------- assembly --
+
+constexpr int kRowCap = 64;  // blocks accumulated in shared memory per warp
+
+// One warp per free node (block row).  Rows wider than kRowCap accumulate in
+// global memory instead (still owned by the warp).
+template <bool WITH_F>
+__global__ void __launch_bounds__(kBlock) k_gather_assemble(
+    int nfree, int ne8, const int *__restrict__ node_of_free, const int *__restrict__ inc_ptr,
+    const int *__restrict__ inc, const uint16_t *__restrict__ slot, const int *__restrict__ rowptr,
+    const double *__restrict__ Ke, double *__restrict__ Kb, const double *__restrict__ Fe,
+    double *__restrict__ fint) {
+    __shared__ double s_acc[kWarpsPerBlock][kRowCap * 9];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long ke8 = 576L * ne8;
+    const int nwarps = gridDim.x * kWarpsPerBlock;
+    for (int r = blockIdx.x * kWarpsPerBlock + warp; r < nfree; r += nwarps) {
+        const int rb = rowptr[r], deg = rowptr[r + 1] - rb;
+        const bool in_smem = deg <= kRowCap;
+        double *acc = in_smem ? s_acc[warp] : Kb + 9L * rb;
+        for (int v = lane; v < 9 * deg; v += 32) acc[v] = 0.0;
+        __syncwarp();
+        const int node = node_of_free[r];
+        double fsum = 0.0;
+        for (int k = inc_ptr[node]; k < inc_ptr[node + 1]; ++k) {
+            const int ga = inc[k];
+            const int g = ga >> 3, a = ga & 7;
+            const bool hex = g < ne8;
+            const int npe = hex ? 8 : 4;
+            const double *row = hex ? Ke + 576L * g + 72 * a : Ke + ke8 + 144L * (g - ne8) + 36 * a;
+            const uint16_t *sl = slot + 8L * k;
+            for (int v = lane; v < 9 * npe; v += 32) {
+                int b = v / 9;
+                int s = sl[b];
+                if (s != kNoSlot) acc[9 * s + (v - 9 * b)] += row[v];
+            }
+            if (WITH_F && lane < 3)
+                fsum += hex ? Fe[24L * g + 3 * a + lane] : Fe[24L * ne8 + 12L * (g - ne8) + 3 * a + lane];
+            __syncwarp();
+        }
+        if (in_smem) {
+            double *out = Kb + 9L * rb;
+            for (int v = lane; v < 9 * deg; v += 32) out[v] = acc[v];
+        }
+        if (WITH_F && lane < 3) fint[3L * r + lane] = fsum;
+        __syncwarp();
+    }
+}
+
+// Block-Jacobi: invert each diagonal 3x3 block (FP64, and an FP32 copy).
+__global__ void k_block_jacobi(int nfree, const int *__restrict__ rowptr,
+                               const int *__restrict__ diag_pos, const double *__restrict__ Kb,
+                               double *__restrict__ Dinv, float *__restrict__ Dinv32,
+                               int *__restrict__ err) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nfree; r += gridDim.x * blockDim.x) {
+        const int dp = diag_pos[r];
+        double A[9], Ai[9];
+        if (dp >= 0) {
+            const double *D = Kb + 9L * (rowptr[r] + dp);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) A[i] = D[i];
+        } else {  // free node outside every element: K has an empty row
+#pragma unroll
+            for (int i = 0; i < 9; ++i) A[i] = 0.0;
+        }
+        double det = A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) +
+                     A[2] * (A[3] * A[7] - A[4] * A[6]);
+        if (!(det > 0.0) || !isfinite(det)) {
+            atomicExch(err, 1);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) Ai[i] = (i % 4 == 0) ? 1.0 : 0.0;
+        } else {
+            inv3(A, Ai);
+        }
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            Dinv[9L * r + i] = Ai[i];
+            Dinv32[9L * r + i] = (float)Ai[i];
+        }
+    }
+}
+
+__global__ void k_to_f32(long n, const double *__restrict__ a, float *__restrict__ b) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+static void integrate(ofea_ctx *c, bool nl, const double *d_u) {
+    upload_hex_table();
+    cudaStream_t s = c->stream;
+    size_t ke_len = 576L * c->ne8 + 144L * c->ne4;
+    c->Ke.ensure(ke_len);
+    if (nl) c->Fe.ensure(24L * c->ne8 + 12L * c->ne4 + 1);
+    double *Fe8 = nl ? c->Fe.p : nullptr;
+    double *Fe4 = nl ? c->Fe.p + 24L * c->ne8 : nullptr;
+    if (c->ne8 > 0) {
+        int g = grid_for(c, (c->ne8 + kHexPerCta - 1) / kHexPerCta, 1);
+        g = std::min(g, c->num_sms * 8);
+        if (nl)
+            k_hex_integrate<true><<<g, 128, 0, s>>>(c->ne8, c->topo8.p, c->xyz.p, c->E8.p, c->nu,
+                                                    c->free_map.p, d_u, c->Ke.p, Fe8);
+        else
+            k_hex_integrate<false><<<g, 128, 0, s>>>(c->ne8, c->topo8.p, c->xyz.p, c->E8.p, c->nu,
+                                                     nullptr, nullptr, c->Ke.p, nullptr);
+        OFEA_CHECK_LAUNCH();
+    }
+    if (c->ne4 > 0) {
+        int g = grid_for(c, (c->ne4 + kTetPerCta - 1) / kTetPerCta, 1);
+        g = std::min(g, c->num_sms * 12);
+        double *Ke4 = c->Ke.p + 576L * c->ne8;
+        if (nl)
+            k_tet_integrate<true><<<g, 128, 0, s>>>(c->ne4, c->topo4.p, c->xyz.p, c->E4.p, c->nu,
+                                                    c->free_map.p, d_u, Ke4, Fe4);
+        else
+            k_tet_integrate<false><<<g, 128, 0, s>>>(c->ne4, c->topo4.p, c->xyz.p, c->E4.p, c->nu,
+                                                     nullptr, nullptr, Ke4, nullptr);
+        OFEA_CHECK_LAUNCH();
+    }
+}
+
+static void gather(ofea_ctx *c, bool with_f, double *d_fint) {
+    c->Kb.ensure((size_t)std::max<long long>(9 * c->nnzb, 1));
+    int gw = grid_for(c, c->nfree, kWarpsPerBlock);
+    if (with_f)
+        k_gather_assemble<true><<<gw, kBlock, 0, c->stream>>>(
+            c->nfree, c->ne8, c->node_of_free.p, c->inc_ptr.p, c->inc.p, c->slot.p, c->rowptr.p,
+            c->Ke.p, c->Kb.p, c->Fe.p, d_fint);
+    else
+        k_gather_assemble<false><<<gw, kBlock, 0, c->stream>>>(
+            c->nfree, c->ne8, c->node_of_free.p, c->inc_ptr.p, c->inc.p, c->slot.p, c->rowptr.p,
+            c->Ke.p, c->Kb.p, nullptr, nullptr);
+    OFEA_CHECK_LAUNCH();
+    c->K_ok = true;
+    c->K32_ok = false;
+}
+
+void assemble_linear(ofea_ctx *c) {
+    integrate(c, false, nullptr);
+    gather(c, false, nullptr);
+}
+
+void assemble_nl(ofea_ctx *c, const double *d_u, double *d_fint) {
+    integrate(c, true, d_u);
+    gather(c, true, d_fint);
+}
+
+void build_block_jacobi(ofea_ctx *c) {
+    c->Dinv.ensure((size_t)9 * std::max(c->nfree, 1));
+    c->Dinv32.ensure((size_t)9 * std::max(c->nfree, 1));
+    OFEA_CUDA(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), c->stream));
+    k_block_jacobi<<<grid_for(c, c->nfree, kBlock), kBlock, 0, c->stream>>>(
+        c->nfree, c->rowptr.p, c->diag_pos.p, c->Kb.p, c->Dinv.p, c->Dinv32.p, c->err_flag.p);
+    OFEA_CHECK_LAUNCH();
+}
+
+void build_fp32_copy(ofea_ctx *c) {
+    long n = 9 * c->nnzb;
+    c->Kb32.ensure((size_t)std::max<long>(n, 1));
+    k_to_f32<<<grid_for(c, n, kBlock), kBlock, 0, c->stream>>>(n, c->Kb.p, c->Kb32.p);
+    OFEA_CHECK_LAUNCH();
+    c->K32_ok = true;
+}
+
+}  // namespace ofea

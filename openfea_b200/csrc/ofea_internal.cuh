@@ -1,0 +1,165 @@
+// Internal definitions shared by the CUDA translation units of libofea_gpu.
+//
+// Device data layout (all in HBM, resident for the life of the context):
+//   xyz        double[3*nd]            node coordinates
+//   topo8      int[8*ne8]              C3D8 connectivity (0-based), elements in caller order
+//   topo4      int[4*ne4]              C3D4 connectivity
+//   E8, E4     double[ne8], [ne4]      Young's modulus per element
+//   free_map   int[nd]                 node -> free index or -1
+//   node_of_free int[nfree]            free index -> node
+//   inc_ptr    int[nd+1], inc int[..]  node -> incident elements, packed g*8+local, sorted
+//              (g = unified element id: hexes 0..ne8-1, then tets ne8..ne8+ne4-1)
+//   rowptr     int[nfree+1], cols int[nnzb]   block (3x3) CSR pattern, columns sorted
+//   slot       uint16[8*len(inc)]      for incidence k and local node b: block
+//                                      position within the row, 0xFFFF if b is fixed
+//   Kb         double[9*nnzb]          K values, block-row-major, 3x3 blocks row-major
+//   Kb32       float[9*nnzb]           FP32 copy for the mixed-precision solver
+//   Ke         double[576*ne8 + 144*ne4]  element matrices (scratch of the assembly):
+//                                      element g, block (a,b), entries 3x3 row-major
+//   Dinv       double[9*nfree]         inverted diagonal blocks (block-Jacobi)
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/ofea_gpu.h"
+
+namespace ofea {
+
+struct Failure {
+    int code;
+    std::string msg;
+};
+
+[[noreturn]] void fail(int code, const std::string &msg);
+[[noreturn]] void fail_cuda(cudaError_t e, const char *what, const char *file, int line);
+void set_last_error(const std::string &msg);
+
+#define OFEA_CUDA(call)                                                   \
+    do {                                                                  \
+        cudaError_t e_ = (call);                                          \
+        if (e_ != cudaSuccess) ::ofea::fail_cuda(e_, #call, __FILE__, __LINE__); \
+    } while (0)
+
+#define OFEA_CHECK_LAUNCH() OFEA_CUDA(cudaGetLastError())
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    // Grow-only allocation; contents are not preserved on growth.
+    void ensure(size_t count) {
+        if (count <= n && p) return;
+        release();
+        size_t bytes = count * sizeof(T);
+        if (bytes == 0) bytes = sizeof(T);
+        cudaError_t e = cudaMalloc((void **)&p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            fail(OFEA_ERR_OOM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+        }
+        n = count;
+    }
+    void upload(const T *h, size_t count, cudaStream_t s) {
+        ensure(count);
+        if (count) OFEA_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+};
+
+// Pinned host scratch.
+template <class T>
+struct HostBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    ~HostBuf() {
+        if (p) cudaFreeHost(p);
+    }
+    void ensure(size_t count) {
+        if (count <= n && p) return;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        OFEA_CUDA(cudaMallocHost((void **)&p, count * sizeof(T)));
+        n = count;
+    }
+};
+
+constexpr int kBlock = 256;          // threads per CTA for streaming kernels
+constexpr int kWarpsPerBlock = kBlock / 32;
+constexpr uint16_t kNoSlot = 0xFFFF;
+
+// Solver workspace (vectors of n or nfree*9 entries).
+struct SolverWork {
+    DevBuf<double> r, z, q, p0, p1, u, f, t;  // FP64
+    DevBuf<float> r32, z32, q32, p32a, p32b, x32;
+    DevBuf<double> partials;   // reduction partials (several arrays of kMaxGrid)
+    DevBuf<int> flags;         // [0]=done [1]=iters [2]=status
+    HostBuf<int> hflags;
+    HostBuf<double> hscal;
+};
+
+constexpr int kMaxGrid = 4096;  // upper bound on CTAs of any reducing kernel
+
+}  // namespace ofea
+
+struct ofea_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    // mesh
+    int nd = 0, ne = 0, ne8 = 0, ne4 = 0, nfree = 0, n = 0;
+    double E0 = 0, nu = 0;
+    std::vector<int> elem_type;    // caller order
+    std::vector<int> elem_local;   // caller element -> index within its type
+    ofea::DevBuf<double> xyz, E8, E4;
+    ofea::DevBuf<int> topo8, topo4, free_map, node_of_free;
+    bool mesh_ok = false;
+    // pattern
+    ofea::DevBuf<int> inc_ptr, inc, rowptr, cols, diag_pos;
+    ofea::DevBuf<uint16_t> slot;
+    long long nnzb = 0;
+    int max_deg = 0;
+    bool pattern_ok = false;
+    // values
+    ofea::DevBuf<double> Kb, Ke, Fe, Dinv, u_nl, f_int;
+    ofea::DevBuf<float> Kb32, Dinv32;
+    bool K_ok = false, K32_ok = false, jacobi_ok = false;
+    ofea::SolverWork w;
+    ofea::DevBuf<int> scratch_i;
+    ofea::DevBuf<int> err_flag;
+    ofea::HostBuf<int> herr;
+};
+
+namespace ofea {
+// pattern.cu
+void build_pattern(ofea_ctx *c);
+// integrate.cu
+void assemble_linear(ofea_ctx *c);
+void assemble_nl(ofea_ctx *c, const double *d_u, double *d_fint);
+void build_block_jacobi(ofea_ctx *c);
+void build_fp32_copy(ofea_ctx *c);
+// solve.cu
+void spmv64(ofea_ctx *c, const double *d_x, double *d_y);
+void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_opts &o,
+                  ofea_solve_stats &st);
+void profile_kernels(ofea_ctx *c, int method, int reps, double *ms, double *bytes);
+// pattern.cu (scan)
+long long exclusive_scan(const int *d_in, int *d_out, int n, cudaStream_t s, int *d_tmp,
+                         int tmp_len);
+int grid_for(const ofea_ctx *c, long long work_items, int per_block);
+}  // namespace ofea
