@@ -6,8 +6,9 @@ free DOF, 122.7M non-zeros), E = 210 GPa, nu = 0.3, clamped at x = 0, 1 MPa end
 traction in -z (synthetic, seeded; the reference ships no benchmark input).
 
 One step = one solve K u = f to a true FP64 relative residual of 1e-8 with the
-mixed-precision solver (FP32 PCG + FP64 reliable updates), K assembled and f
-resident in HBM.  `value` = seconds per step (device time, CUDA events on the
+mixed-precision solver (FP64 flexible PCG, FP32 two-level V-cycle
+preconditioner, including its per-matrix setup), K assembled and f resident in
+HBM.  `value` = seconds per step (device time, CUDA events on the
 launching stream, max over ranks).  `e2e` = the reference-facing path through
 the C ABI with host buffers: mesh upload, pattern, FP64 assembly, solve, u
 back to the host - the span the reference times with clock()
@@ -129,7 +130,7 @@ class ClockSampler:
 
 # --------------------------------------------------------- reference (CPU) --
 
-def reference_sample(shape_full, sizes=((16, 4, 4), (32, 8, 8))):
+def reference_sample(shape_full, sizes=((24, 6, 6), (40, 10, 10))):
     """The reference's own path (set_BCs, build_CSR, fill_CSR_sparse_mat,
     solution_api("SuperLU_func")) from oracle/_ref on two geometrically similar
     blocks, extrapolated to the full workload: assembly linearly in n, the
@@ -287,17 +288,17 @@ def run_ours(args):
     # roofline of the dominant kernels (CUDA events on the launching stream)
     solve("GPU_MIXED")
     hbm, peak_kind = peaks()
-    msA32, byA32 = ctx.profile_kernels("GPU_MIXED", reps=30)
+    msM, byM = ctx.profile_kernels("GPU_MIXED", reps=30)
     solve("GPU_PCG")
-    msA64, byA64 = ctx.profile_kernels("GPU_PCG", reps=30)
-    gbs32 = byA32[0] / (msA32[0] * 1e-3) / 1e9
-    gbs64 = byA64[0] / (msA64[0] * 1e-3) / 1e9
+    msP, byP = ctx.profile_kernels("GPU_PCG", reps=30)
+    gbsA = byM[0] / (msM[0] * 1e-3) / 1e9
+    gbs32 = byM[1] / (msM[1] * 1e-3) / 1e9
+    gbs64 = byP[0] / (msP[0] * 1e-3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tpath):
         try:
-            tj = json.load(open(tpath))
-            traffic = tj.get(f"k_mx_A/{args.shape}")
+            traffic = json.load(open(tpath)).get(f"k_fcg_A/{args.shape}")
         except Exception:
             traffic = None
 
@@ -326,17 +327,20 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
         "config": {
             "workload": (f"C3D8 cantilever {args.shape} (h=5 mm), {n} DOF, nnz {nnz}, E=210 GPa, "
-                         f"nu=0.3, clamped x=0, 1 MPa end traction; mixed-precision PCG "
-                         f"(FP32 inner, FP64 reliable updates) to FP64 rel. residual {args.rtol:g}"),
+                         f"nu=0.3, clamped x=0, 1 MPa end traction; FP64 flexible PCG with the FP32 "
+                         f"two-level V-cycle preconditioner, to FP64 rel. residual {args.rtol:g}"),
             "n_dof": n, "nnz": nnz, "parallelism": f"replicas x{world}",
-            "l2": "inputs larger than L2 (FP32 K 0.49 GB, FP64 K 0.98 GB per SpMV)",
+            "l2": "inputs larger than L2 (FP64 K ~1 GB and FP32 K ~0.5 GB streamed per SpMV)",
         },
-        "roofline": {"bound": "hbm", "kernel": "k_mx_A (FP32 BSR3 SpMV + p update + p.q)",
-                     "achieved": gbs32, "peak": hbm, "unit": "GB/s", "frac": gbs32 / hbm,
+        "roofline": {"bound": "hbm", "kernel": "k_fcg_A (FP64 BSELL SpMV + p update + p.q)",
+                     "achieved": gbsA, "peak": hbm, "unit": "GB/s", "frac": gbsA / hbm,
                      "peak_kind": peak_kind, "traffic": traffic,
-                     "bytes_per_launch": byA32[0], "ms_per_launch": msA32[0]},
-        "spmv64": {"kernel": "k_pcg64_A (FP64 BSR3 SpMV + p update + p.q)", "achieved_gbs": gbs64,
-                   "frac": gbs64 / hbm, "bytes_per_launch": byA64[0], "ms_per_launch": msA64[0]},
+                     "bytes_per_launch": byM[0], "ms_per_launch": msM[0]},
+        "spmv32_smoother": {"kernel": "k_fcg_post (FP32 BSELL SpMV + block-Jacobi + dots)",
+                            "achieved_gbs": gbs32, "frac": gbs32 / hbm, "bytes_per_launch": byM[1],
+                            "ms_per_launch": msM[1]},
+        "spmv64_plain": {"kernel": "k_pcg64_A (FP64 BSELL SpMV, plain PCG)", "achieved_gbs": gbs64,
+                         "frac": gbs64 / hbm, "bytes_per_launch": byP[0], "ms_per_launch": msP[0]},
         "solver": {"iterations": stats[-1]["iterations"], "refinements": stats[-1]["refinements"],
                    "rel_residual": stats[-1]["rel_residual"], "plain_pcg64_s": plain_s,
                    "plain_pcg64_iterations": st64["iterations"],

@@ -48,8 +48,10 @@ extern "C" {
 #define OFEA_ERR_REJECTED (-12)     /* learned stage rejected by the FP64 residual check */
 
 /* Solver methods (ofea_solve_opts.method). */
-#define OFEA_SOLVER_PCG64 0   /* FP64 PCG, 3x3 block-Jacobi */
-#define OFEA_SOLVER_MIXED 1   /* FP32 PCG with FP64 reliable-update refinement */
+#define OFEA_SOLVER_PCG64 0   /* FP64 PCG, 3x3 block-Jacobi (the plain method) */
+#define OFEA_SOLVER_MIXED 1   /* FP64 flexible PCG, FP32 two-level V-cycle preconditioner:
+                                 block-Jacobi/Chebyshev smoothing with FP32 SpMV and a
+                                 rigid-body coarse correction */
 #define OFEA_SOLVER_LEARNED 2 /* MIXED + graph-network coarse correction (flexible PCG) */
 
 typedef struct ofea_ctx ofea_ctx;
@@ -60,14 +62,14 @@ typedef struct {
     int max_iter;         /* inner iterations, summed over refinements */
     double time_budget_s; /* <= 0: unlimited */
     int check_every;      /* iterations between host convergence polls (0: default) */
-    double ru_delta;      /* MIXED: reliable-update trigger ||r32|| < ru_delta * max||r|| (0: default 0.1) */
+    double ru_delta;      /* reserved (0) */
     int use_graph;        /* 1: replay iteration chunks as a captured CUDA graph; 0: plain launches */
 } ofea_solve_opts;
 
 typedef struct {
     int status;            /* OFEA_OK or an error code */
     int iterations;        /* inner iterations performed */
-    int refinements;       /* FP64 residual recomputations (MIXED/LEARNED) */
+    int refinements;       /* restarts from a recomputed FP64 residual */
     double rel_residual;   /* final ||f - K u|| / ||f|| in FP64 */
     double seconds;        /* device time of the solve (CUDA events) */
     int rejected_learned;  /* 1 when the learned stage was rejected and plain PCG finished */

@@ -20,7 +20,7 @@ OUT = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libofea_gpu.so")
 CLI = os.path.join(HERE, "ofea_cli")
 
-CU_SOURCES = ["api.cu", "pattern.cu", "integrate.cu", "solve.cu"]
+CU_SOURCES = ["api.cu", "pattern.cu", "integrate.cu", "sell.cu", "precond.cu", "solve.cu"]
 HOST_SOURCES = ["host/model.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -50,8 +50,8 @@ def _stale(target, deps):
 def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(OUT, exist_ok=True)
     inc = ["-I", os.path.join(ROOT, "include")]
-    headers = [os.path.join(CSRC, "ofea_internal.cuh"), os.path.join(ROOT, "include", "ofea_gpu.h"),
-               os.path.join(ROOT, "include", "ofea_host.h")]
+    headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(".cuh")]
+    headers += [os.path.join(ROOT, "include", "ofea_gpu.h"), os.path.join(ROOT, "include", "ofea_host.h")]
     objs = []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)

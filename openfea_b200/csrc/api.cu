@@ -165,7 +165,8 @@ int ofea_mesh_upload(ofea_ctx *c, int nd, const double *xyz, int ne, const int *
         need(std::isfinite(E0) && std::isfinite(nu) && nu > -1.0 && nu < 0.5, OFEA_ERR_INVALID_ARG,
              "invalid material (nu must be in (-1, 0.5))");
         use_device(c);
-        c->mesh_ok = c->pattern_ok = c->K_ok = c->K32_ok = false;
+        c->mesh_ok = c->pattern_ok = c->K_ok = c->sell_ok = false;
+        c->coarse.geom_ok = c->coarse.K_ok = false;
         c->nd = nd;
         c->ne = ne;
         c->E0 = E0;
@@ -207,6 +208,10 @@ int ofea_mesh_upload(ofea_ctx *c, int nd, const double *xyz, int ne, const int *
             need(std::isfinite(xyz[i]), OFEA_ERR_INVALID_ARG, "non-finite coordinate");
         c->nfree = nfree;
         c->n = 3 * nfree;
+        c->xyz_h.assign(xyz, xyz + 3L * nd);
+        c->fm_h.assign(free_map, free_map + nd);
+        c->topo_h.assign(8L * ne, 0);
+        for (long i = 0; i < 8L * ne; ++i) c->topo_h[i] = topo[i] > 0 ? topo[i] - 1 : 0;
         std::vector<double> E8, E4;
         split_modulus(c, E_elem, E0, E8, E4);
         cudaStream_t s = c->stream;
@@ -232,7 +237,8 @@ int ofea_mesh_set_modulus(ofea_ctx *c, const double *E_elem, double E0) {
         c->E8.upload(E8.data(), E8.size(), c->stream);
         c->E4.upload(E4.data(), E4.size(), c->stream);
         OFEA_CUDA(cudaStreamSynchronize(c->stream));
-        c->K_ok = c->K32_ok = false;
+        c->K_ok = c->sell_ok = false;
+        c->coarse.K_ok = false;
     });
 }
 
@@ -249,6 +255,7 @@ int ofea_assemble_pattern(ofea_ctx *c, int *n, long long *nnz) {
 
 static void after_assembly(ofea_ctx *c) {
     build_block_jacobi(c);
+    build_sell(c);
     OFEA_CUDA(cudaMemcpyAsync(c->herr.p, c->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     OFEA_CUDA(cudaStreamSynchronize(c->stream));
     c->jacobi_ok = c->herr.p[0] == 0;
@@ -352,6 +359,12 @@ int ofea_spmv(ofea_ctx *c, const double *x, double *y) {
     });
 }
 
+static std::string fmt_e(double v) {
+    char b[32];
+    std::snprintf(b, sizeof(b), "%.3e", v);
+    return b;
+}
+
 static void check_solve_ready(ofea_ctx *c, const ofea_solve_opts &o) {
     need(c->K_ok, OFEA_ERR_STATE, "K not assembled");
     need(o.rtol > 0 && o.max_iter > 0, OFEA_ERR_INVALID_ARG, "rtol and max_iter must be positive");
@@ -376,7 +389,7 @@ int ofea_solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_so
         solve_device(c, d_f, d_u, o, st);
         if (st.status != OFEA_OK)
             set_last_error(std::string("solve: ") + ofea_status_string(st.status) +
-                           ", relative residual " + std::to_string(st.rel_residual));
+                           ", relative residual " + fmt_e(st.rel_residual));
     });
     if (rc != OFEA_OK) st.status = rc;
     if (stats) *stats = st;
@@ -411,7 +424,7 @@ int ofea_solve(ofea_ctx *c, const double *f, double *u, int nrhs, const ofea_sol
             if (st.status != OFEA_OK && worst == OFEA_OK) {
                 worst = st.status;
                 set_last_error(std::string("solve: ") + ofea_status_string(st.status) +
-                               ", relative residual " + std::to_string(st.rel_residual));
+                               ", relative residual " + fmt_e(st.rel_residual));
             }
         }
     });

@@ -464,11 +464,6 @@ __global__ void k_block_jacobi(int nfree, const int *__restrict__ rowptr,
     }
 }
 
-__global__ void k_to_f32(long n, const double *__restrict__ a, float *__restrict__ b) {
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-        b[i] = (float)a[i];
-}
-
 static void integrate(ofea_ctx *c, bool nl, const double *d_u) {
     upload_hex_table();
     cudaStream_t s = c->stream;
@@ -515,7 +510,8 @@ static void gather(ofea_ctx *c, bool with_f, double *d_fint) {
             c->Ke.p, c->Kb.p, nullptr, nullptr);
     OFEA_CHECK_LAUNCH();
     c->K_ok = true;
-    c->K32_ok = false;
+    c->sell_ok = false;
+    c->coarse.K_ok = false;
 }
 
 void assemble_linear(ofea_ctx *c) {
@@ -537,12 +533,5 @@ void build_block_jacobi(ofea_ctx *c) {
     OFEA_CHECK_LAUNCH();
 }
 
-void build_fp32_copy(ofea_ctx *c) {
-    long n = 9 * c->nnzb;
-    c->Kb32.ensure((size_t)std::max<long>(n, 1));
-    k_to_f32<<<grid_for(c, n, kBlock), kBlock, 0, c->stream>>>(n, c->Kb.p, c->Kb32.p);
-    OFEA_CHECK_LAUNCH();
-    c->K32_ok = true;
-}
 
 }  // namespace ofea

@@ -13,10 +13,12 @@
 //   slot       uint16[8*len(inc)]      for incidence k and local node b: block
 //                                      position within the row, 0xFFFF if b is fixed
 //   Kb         double[9*nnzb]          K values, block-row-major, 3x3 blocks row-major
-//   Kb32       float[9*nnzb]           FP32 copy for the mixed-precision solver
+//   sl_ptr, scols, sv64, sv32          the solver's copy of K in BSELL-32 (sell.cuh),
+//                                      FP64 values and an FP32 rounding
 //   Ke         double[576*ne8 + 144*ne4]  element matrices (scratch of the assembly):
 //                                      element g, block (a,b), entries 3x3 row-major
-//   Dinv       double[9*nfree]         inverted diagonal blocks (block-Jacobi)
+//   Dinv       double[9*nfree]         inverted diagonal blocks (block-Jacobi), + FP32 copy
+//   coarse                             aggregates, E = Z^T K Z and its FP32 inverse (precond.cu)
 #pragma once
 #include <cuda_runtime.h>
 
@@ -105,7 +107,7 @@ constexpr uint16_t kNoSlot = 0xFFFF;
 // Solver workspace (vectors of n or nfree*9 entries).
 struct SolverWork {
     DevBuf<double> r, z, q, p0, p1, u, f, t;  // FP64
-    DevBuf<float> r32, z32, q32, p32a, p32b, x32;
+    DevBuf<float> b32, x32, t32, z32a, z32b;    // FP32 preconditioner vectors
     DevBuf<double> partials;   // reduction partials (several arrays of kMaxGrid)
     DevBuf<int> flags;         // [0]=done [1]=iters [2]=status
     HostBuf<int> hflags;
@@ -113,6 +115,17 @@ struct SolverWork {
 };
 
 constexpr int kMaxGrid = 4096;  // upper bound on CTAs of any reducing kernel
+
+// Coarse space of the two-level preconditioner (precond.cu).
+struct Coarse {
+    bool geom_ok = false, K_ok = false;
+    int target = 0, na = 0, m = 0, max_agg = 0;
+    int nc[3] = {1, 1, 1};
+    double inv_scale = 1.0, lmax = 0.0;
+    DevBuf<int> agg_of, agg_ptr, agg_nodes, agg_cell, cell_agg;
+    DevBuf<double> centroid, E, S, P, diag0, pp;
+    DevBuf<float> Einv32, cvec, evec, pw;
+};
 
 }  // namespace ofea
 
@@ -126,6 +139,8 @@ struct ofea_ctx {
     double E0 = 0, nu = 0;
     std::vector<int> elem_type;    // caller order
     std::vector<int> elem_local;   // caller element -> index within its type
+    std::vector<double> xyz_h;     // host copies for the coarse-space setup
+    std::vector<int> fm_h, topo_h; // topo_h: ne x 8, 0-based
     ofea::DevBuf<double> xyz, E8, E4;
     ofea::DevBuf<int> topo8, topo4, free_map, node_of_free;
     bool mesh_ok = false;
@@ -137,8 +152,16 @@ struct ofea_ctx {
     bool pattern_ok = false;
     // values
     ofea::DevBuf<double> Kb, Ke, Fe, Dinv, u_nl, f_int;
-    ofea::DevBuf<float> Kb32, Dinv32;
-    bool K_ok = false, K32_ok = false, jacobi_ok = false;
+    ofea::DevBuf<float> Dinv32;
+    bool K_ok = false, jacobi_ok = false;
+    // solver layout of K (sell.cuh): BSELL-32, FP64 and FP32 values
+    ofea::DevBuf<int> sl_ptr, scols;
+    ofea::DevBuf<double> sv64;
+    ofea::DevBuf<float> sv32;
+    long long sell_len = 0;
+    bool sell_ok = false;
+    ofea::Coarse coarse;
+    int coarse_nodes = 1000;  // target free nodes per aggregate
     ofea::SolverWork w;
     ofea::DevBuf<int> scratch_i;
     ofea::DevBuf<int> err_flag;
@@ -152,7 +175,8 @@ void build_pattern(ofea_ctx *c);
 void assemble_linear(ofea_ctx *c);
 void assemble_nl(ofea_ctx *c, const double *d_u, double *d_fint);
 void build_block_jacobi(ofea_ctx *c);
-void build_fp32_copy(ofea_ctx *c);
+// sell.cu
+void build_sell(ofea_ctx *c);
 // solve.cu
 void spmv64(ofea_ctx *c, const double *d_x, double *d_y);
 void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_opts &o,

@@ -331,7 +331,9 @@ void build_pattern(ofea_ctx *c) {
     OFEA_CUDA(cudaStreamSynchronize(s));
     c->pattern_ok = true;
     c->K_ok = false;
-    c->K32_ok = false;
+    c->sell_ok = false;
+    c->coarse.geom_ok = false;
+    c->coarse.K_ok = false;
 }
 
 }  // namespace ofea

@@ -1,0 +1,601 @@
+// Two-level preconditioner of the mixed-precision solver.
+//
+//   M(r) = V(1,1) cycle in FP32:  x0 = w D^-1 b            (pre-smoothing, Chebyshev degree 1)
+//                                 t  = b - K32 x0
+//                                 x1 = x0 + Z E^-1 Z^T t   (coarse correction)
+//                                 z  = x1 + w D^-1 (b - K32 x1)   (post-smoothing)
+// with b = float(r), D the 3x3 diagonal blocks, w = 1/theta of the Chebyshev
+// interval [lmax/30, 1.1 lmax] of D^-1 K, and Z the rigid-body modes of node
+// aggregates: the free nodes are binned into a grid of cells of about
+// `coarse_nodes` nodes; each non-empty cell I is an aggregate with six modes
+// (three translations, three rotations about its centroid, scaled by the
+// cell size).  E = Z^T K Z (FP64, 6 x 6 blocks between neighbouring cells) is
+// inverted on the device by blocked Gauss-Jordan and applied as an FP32 GEMV.
+//
+// The FP32 SpMV is accurate for the high-frequency error the smoother damps;
+// the smooth modes that FP32 rounding of K would corrupt are carried by the
+// exact FP64 coarse operator, so the FP64 outer iteration keeps the iteration
+// count of an all-FP64 preconditioner.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "precond.cuh"
+#include "sell.cuh"
+#include "solver_common.cuh"
+
+namespace ofea {
+
+// ---------------------------------------------------------- aggregation --
+
+void build_aggregation(ofea_ctx *c, int target_nodes) {
+    Coarse &C = c->coarse;
+    const int nd = c->nd, nf = c->nfree;
+    const std::vector<double> &X = c->xyz_h;
+    const std::vector<int> &fm = c->fm_h;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    std::vector<int> nof(nf);
+    for (int i = 0; i < nd; ++i)
+        if (fm[i] >= 0) {
+            nof[fm[i]] = i;
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = std::min(lo[d], X[3L * i + d]);
+                hi[d] = std::max(hi[d], X[3L * i + d]);
+            }
+        }
+    // largest element extent per direction: cells must be at least 2.5x wider
+    // so that every K coupling stays between neighbouring cells
+    double emax[3] = {0, 0, 0};
+    for (int e = 0; e < c->ne; ++e) {
+        const int *t = &c->topo_h[8L * e];
+        int npe = c->elem_type[e] == 1 ? 8 : 4;
+        for (int d = 0; d < 3; ++d) {
+            double a = 1e300, b = -1e300;
+            for (int k = 0; k < npe; ++k) {
+                a = std::min(a, X[3L * t[k] + d]);
+                b = std::max(b, X[3L * t[k] + d]);
+            }
+            emax[d] = std::max(emax[d], b - a);
+        }
+    }
+    double ext[3], vol = 1.0;
+    int flat = 0;
+    for (int d = 0; d < 3; ++d) {
+        ext[d] = hi[d] - lo[d];
+        if (ext[d] > 0) vol *= ext[d];
+        else ++flat;
+    }
+    const double target = std::max(8, target_nodes);
+    double s = std::pow(vol * target / std::max(nf, 1), 1.0 / std::max(1, 3 - flat));
+    int nc[3];
+    for (int d = 0; d < 3; ++d) {
+        if (!(ext[d] > 0)) {
+            nc[d] = 1;
+            continue;
+        }
+        double cell = std::max(s, 2.5 * emax[d]);
+        nc[d] = std::max(1, (int)std::lround(ext[d] / cell));
+    }
+    C.nc[0] = nc[0];
+    C.nc[1] = nc[1];
+    C.nc[2] = nc[2];
+    const long ncell = (long)nc[0] * nc[1] * nc[2];
+    std::vector<int> cell_of(nf), cnt(ncell, 0);
+    for (int r = 0; r < nf; ++r) {
+        int node = nof[r], ci[3];
+        for (int d = 0; d < 3; ++d) {
+            ci[d] = ext[d] > 0 ? (int)std::floor((X[3L * node + d] - lo[d]) / ext[d] * nc[d]) : 0;
+            ci[d] = std::min(std::max(ci[d], 0), nc[d] - 1);
+        }
+        cell_of[r] = (ci[0] * nc[1] + ci[1]) * nc[2] + ci[2];
+        cnt[cell_of[r]]++;
+    }
+    std::vector<int> cell_agg(ncell, -1), agg_cell3;
+    int na = 0;
+    for (long k = 0; k < ncell; ++k)
+        if (cnt[k] > 0) {
+            cell_agg[k] = na++;
+            agg_cell3.push_back((int)(k / ((long)nc[1] * nc[2])));
+            agg_cell3.push_back((int)((k / nc[2]) % nc[1]));
+            agg_cell3.push_back((int)(k % nc[2]));
+        }
+    std::vector<int> agg_of(nf), ptr(na + 1, 0), nodes(nf);
+    for (int r = 0; r < nf; ++r) {
+        agg_of[r] = cell_agg[cell_of[r]];
+        ptr[agg_of[r] + 1]++;
+    }
+    for (int a = 0; a < na; ++a) ptr[a + 1] += ptr[a];
+    std::vector<int> cur(ptr.begin(), ptr.end() - 1);
+    for (int r = 0; r < nf; ++r) nodes[cur[agg_of[r]]++] = r;  // ascending within each aggregate
+    std::vector<double> cen(3L * na, 0.0);
+    for (int r = 0; r < nf; ++r)
+        for (int d = 0; d < 3; ++d) cen[3L * agg_of[r] + d] += X[3L * nof[r] + d];
+    for (int a = 0; a < na; ++a)
+        for (int d = 0; d < 3; ++d) cen[3L * a + d] /= (ptr[a + 1] - ptr[a]);
+    double scale = 0;
+    for (int d = 0; d < 3; ++d) scale = std::max(scale, ext[d] > 0 ? ext[d] / nc[d] : 0.0);
+    C.inv_scale = scale > 0 ? 1.0 / scale : 1.0;
+    C.na = na;
+    C.m = 6 * na;
+    C.max_agg = 0;
+    for (int a = 0; a < na; ++a) C.max_agg = std::max(C.max_agg, ptr[a + 1] - ptr[a]);
+    cudaStream_t st = c->stream;
+    C.agg_of.upload(agg_of.data(), nf, st);
+    C.agg_ptr.upload(ptr.data(), na + 1, st);
+    C.agg_nodes.upload(nodes.data(), nf, st);
+    C.agg_cell.upload(agg_cell3.data(), agg_cell3.size(), st);
+    C.cell_agg.upload(cell_agg.data(), ncell, st);
+    C.centroid.upload(cen.data(), cen.size(), st);
+    OFEA_CUDA(cudaStreamSynchronize(st));
+    C.geom_ok = true;
+    C.K_ok = false;
+}
+
+// ------------------------------------------------------- coarse matrix --
+
+constexpr int kEGroups = 4;             // node groups per CTA
+constexpr int kEThreads = 36 * kEGroups;  // one thread per (k,l) entry of a 6x6 block
+
+__device__ __forceinline__ void rigid_col(int k, const double *d, double *z) {
+    // column k of Z_a: translations e_k, rotations e_(k-3) x d
+    z[0] = z[1] = z[2] = 0.0;
+    if (k < 3) {
+        z[k] = 1.0;
+    } else if (k == 3) {
+        z[1] = -d[2];
+        z[2] = d[1];
+    } else if (k == 4) {
+        z[0] = d[2];
+        z[2] = -d[0];
+    } else {
+        z[0] = -d[1];
+        z[1] = d[0];
+    }
+}
+
+// One CTA per aggregate I: E[6I+k][6J+l] = sum_{a in I} sum_b Z_a^T K_ab Z_b.
+// Each group of 36 threads walks its share of I's nodes in ascending order,
+// stages a block row (kStage blocks at a time) in shared memory, and every
+// thread accumulates its (k,l) entry per neighbour cell;
+// the groups are summed in a fixed order: deterministic.
+constexpr int kStage = 32;
+__global__ void __launch_bounds__(kEThreads) k_coarse_E(
+    int na, const int *__restrict__ agg_ptr, const int *__restrict__ agg_nodes,
+    const int *__restrict__ agg_of, const int *__restrict__ agg_cell, const int *__restrict__ cell_agg,
+    const int *__restrict__ node_of_free, const double *__restrict__ xyz,
+    const double *__restrict__ centroid, double inv_scale, const int *__restrict__ rowptr,
+    const int *__restrict__ cols, const double *__restrict__ Kb, int ncx, int ncy, int ncz, int m,
+    double *__restrict__ E, int *__restrict__ err) {
+    __shared__ double acc[kEGroups][27][36];
+    __shared__ double sK[kEGroups][kStage][9];
+    __shared__ double sD[kEGroups][kStage][3];
+    __shared__ int sSlot[kEGroups][kStage];
+    __shared__ int s_chunks[kEGroups];
+    const int g = threadIdx.x / 36, kl = threadIdx.x % 36, k = kl / 6, l = kl % 6;
+    for (int I = blockIdx.x; I < na; I += gridDim.x) {
+        for (int v = threadIdx.x; v < kEGroups * 27 * 36; v += blockDim.x) (&acc[0][0][0])[v] = 0.0;
+        __syncthreads();
+        const int cx = agg_cell[3 * I], cy = agg_cell[3 * I + 1], cz = agg_cell[3 * I + 2];
+        const double ci[3] = {centroid[3L * I], centroid[3L * I + 1], centroid[3L * I + 2]};
+        const int b0 = agg_ptr[I], b1 = agg_ptr[I + 1];
+        // groups take nodes round-robin; iterate a uniform trip count so all
+        // threads of the CTA reach the barriers together
+        const int per = (b1 - b0 + kEGroups - 1) / kEGroups;
+        for (int it = 0; it < per; ++it) {
+            const int idx = b0 + it * kEGroups + g;
+            const bool live = idx < b1;
+            int r = 0, rb = 0, deg = 0;
+            double da[3] = {0, 0, 0};
+            if (live) {
+                r = agg_nodes[idx];
+                rb = rowptr[r];
+                deg = rowptr[r + 1] - rb;
+                const int node = node_of_free[r];
+                for (int d = 0; d < 3; ++d) da[d] = (xyz[3L * node + d] - ci[d]) * inv_scale;
+            }
+            double za[3];
+            rigid_col(k, da, za);
+            // rows of the groups differ in length: agree on the chunk count
+            const int nchunks = (deg + kStage - 1) / kStage;
+            __syncthreads();
+            if (kl == 0) s_chunks[g] = nchunks;
+            __syncthreads();
+            int maxchunks = 0;
+            for (int q = 0; q < kEGroups; ++q) maxchunks = max(maxchunks, s_chunks[q]);
+            for (int ch = 0; ch < maxchunks; ++ch) {
+                const int p0 = ch * kStage;
+                const int cnt = live ? min(kStage, deg - p0) : 0;
+                // stage: thread kl < cnt loads block p0+kl of this group's row
+                if (kl < cnt) {
+                    const int p = rb + p0 + kl;
+                    const int s = cols[p];
+                    const int J = agg_of[s];
+                    const int dx = agg_cell[3 * J] - cx, dy = agg_cell[3 * J + 1] - cy,
+                              dz = agg_cell[3 * J + 2] - cz;
+                    int slot = -1;
+                    if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1)
+                        slot = (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
+                    else
+                        atomicExch(err, 1);
+                    sSlot[g][kl] = slot;
+                    const int nb = node_of_free[s];
+                    for (int d = 0; d < 3; ++d)
+                        sD[g][kl][d] = (xyz[3L * nb + d] - centroid[3L * J + d]) * inv_scale;
+                    for (int e = 0; e < 9; ++e) sK[g][kl][e] = Kb[9L * p + e];
+                }
+                __syncthreads();
+                for (int q = 0; q < cnt; ++q) {
+                    const int slot = sSlot[g][q];
+                    if (slot < 0) continue;
+                    double zb[3];
+                    rigid_col(l, sD[g][q], zb);
+                    const double *K = sK[g][q];
+                    double v = 0.0;
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+                        v += za[i] * (K[3 * i] * zb[0] + K[3 * i + 1] * zb[1] + K[3 * i + 2] * zb[2]);
+                    acc[g][slot][kl] += v;
+                }
+                __syncthreads();
+            }
+        }
+        __syncthreads();
+        // fixed-order sum of the groups, written into the dense E
+        for (int v = threadIdx.x; v < 27 * 36; v += blockDim.x) {
+            const int slot = v / 36, e = v % 36, kk = e / 6, ll = e % 6;
+            const int x = cx + slot / 9 - 1, y = cy + (slot / 3) % 3 - 1, z = cz + slot % 3 - 1;
+            if (x < 0 || y < 0 || z < 0 || x >= ncx || y >= ncy || z >= ncz) continue;
+            const int J = cell_agg[((long)x * ncy + y) * ncz + z];
+            if (J < 0) continue;
+            double s = 0.0;
+            for (int q = 0; q < kEGroups; ++q) s += acc[q][slot][e];
+            E[(6L * I + kk) * m + 6L * J + ll] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// --------------------------------------------- blocked Gauss-Jordan inverse --
+//
+// In-place inverse of the SPD matrix A (m x m, row-major) without pivoting,
+// panel width kGJ.  For the diagonal block J (indices j0 .. j0+bb-1):
+//   S = A_JJ^-1; P = A_{:,J} (saved);
+//   A_{J,k} <- S A_{J,k}            for k outside J     (row panel)
+//   A_{i,k} <- A_{i,k} - P_i A_{J,k} for i, k outside J (rank-bb update)
+//   A_{i,J} <- -P_i S               for i outside J;  A_JJ <- S.
+// A pivot that vanishes (a degenerate aggregate) drops its direction: its
+// row and column of the result are zero.
+
+constexpr int kGJ = 32;
+
+__global__ void __launch_bounds__(1024) k_gj_diag(int m, int j0, int bb, double *__restrict__ A,
+                                                  double *__restrict__ S, double *__restrict__ P,
+                                                  const double *__restrict__ diag0) {
+    __shared__ double a[kGJ][kGJ + 1];
+    const int tx = threadIdx.x % kGJ, ty = threadIdx.x / kGJ;
+    if (ty < bb && tx < bb) a[ty][tx] = A[(long)(j0 + ty) * m + j0 + tx];
+    __syncthreads();
+    for (int p = 0; p < bb; ++p) {
+        double piv = a[p][p];
+        const bool drop = !(piv > 1e-12 * diag0[j0 + p]);
+        __syncthreads();
+        if (drop) {
+            if (ty == p && tx < bb) a[p][tx] = 0.0;
+            if (tx == p && ty < bb) a[ty][p] = 0.0;
+            __syncthreads();
+            continue;
+        }
+        const double inv = 1.0 / piv;
+        double rowp = (tx < bb) ? a[p][tx] : 0.0, colp = (ty < bb) ? a[ty][p] : 0.0;
+        __syncthreads();
+        if (ty < bb && tx < bb) {
+            if (ty == p && tx == p) a[ty][tx] = inv;
+            else if (ty == p) a[ty][tx] = rowp * inv;
+            else if (tx == p) a[ty][tx] = -colp * inv;
+            else a[ty][tx] -= colp * rowp * inv;
+        }
+        __syncthreads();
+    }
+    if (ty < bb && tx < bb) S[ty * kGJ + tx] = a[ty][tx];
+    // save the column panel P = A[:, J] (all rows)
+    for (long i = threadIdx.x; i < (long)m * bb; i += blockDim.x) {
+        long row = i / bb;
+        int j = (int)(i % bb);
+        P[row * kGJ + j] = A[row * m + j0 + j];
+    }
+}
+
+// Row panel: A_{J,k} <- S A_{J,k}, one thread per column k outside J.
+__global__ void k_gj_rows(int m, int j0, int bb, double *__restrict__ A, const double *__restrict__ S) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+        if (k >= j0 && k < j0 + bb) continue;
+        double v[kGJ], o[kGJ];
+        for (int j = 0; j < bb; ++j) v[j] = A[(long)(j0 + j) * m + k];
+        for (int i = 0; i < bb; ++i) {
+            double s = 0.0;
+            for (int j = 0; j < bb; ++j) s += S[i * kGJ + j] * v[j];
+            o[i] = s;
+        }
+        for (int i = 0; i < bb; ++i) A[(long)(j0 + i) * m + k] = o[i];
+    }
+}
+
+// Rank-bb update of the outside block, 64 x 64 tiles, 256 threads (4 x 4 each).
+__global__ void __launch_bounds__(256) k_gj_update(int m, int j0, int bb, double *__restrict__ A,
+                                                   const double *__restrict__ P) {
+    __shared__ double sP[64][kGJ + 1];
+    __shared__ double sR[kGJ][64 + 1];
+    const int i0 = blockIdx.y * 64, k0 = blockIdx.x * 64;
+    const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
+    for (int v = threadIdx.x; v < 64 * kGJ; v += 256) {
+        int ii = v / kGJ, jj = v % kGJ;
+        sP[ii][jj] = (i0 + ii < m && jj < bb) ? P[(long)(i0 + ii) * kGJ + jj] : 0.0;
+        int jr = v / 64, kk = v % 64;
+        sR[jr][kk] = (jr < bb && k0 + kk < m) ? A[(long)(j0 + jr) * m + k0 + kk] : 0.0;
+    }
+    __syncthreads();
+    double acc[4][4] = {};
+    for (int j = 0; j < bb; ++j) {
+        double pv[4], rv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) pv[a] = sP[tr * 4 + a][j];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) rv[b] = sR[j][tc * 4 + b];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] = fma(pv[a], rv[b], acc[a][b]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int i = i0 + tr * 4 + a;
+        if (i >= m || (i >= j0 && i < j0 + bb)) continue;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int k = k0 + tc * 4 + b;
+            if (k >= m || (k >= j0 && k < j0 + bb)) continue;
+            A[(long)i * m + k] -= acc[a][b];
+        }
+    }
+}
+
+// Column panel: A_{i,J} <- -P_i S (i outside J), A_JJ <- S.
+__global__ void k_gj_cols(int m, int j0, int bb, double *__restrict__ A, const double *__restrict__ S,
+                          const double *__restrict__ P) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const bool in = i >= j0 && i < j0 + bb;
+        for (int j = 0; j < bb; ++j) {
+            double s = 0.0;
+            if (in) {
+                s = S[(i - j0) * kGJ + j];
+            } else {
+                for (int q = 0; q < bb; ++q) s -= P[(long)i * kGJ + q] * S[q * kGJ + j];
+            }
+            A[(long)i * m + j0 + j] = s;
+        }
+    }
+}
+
+__global__ void k_diag_of(int m, const double *__restrict__ A, double *__restrict__ d) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+        d[i] = fabs(A[(long)i * m + i]);
+}
+
+__global__ void k_round_f32(long n, const double *__restrict__ a, float *__restrict__ b) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+static void invert_spd(ofea_ctx *c, double *A, int m) {
+    Coarse &C = c->coarse;
+    cudaStream_t s = c->stream;
+    C.S.ensure(kGJ * kGJ);
+    C.P.ensure((size_t)m * kGJ);
+    C.diag0.ensure(m);
+    k_diag_of<<<grid_for(c, m, kBlock), kBlock, 0, s>>>(m, A, C.diag0.p);
+    OFEA_CHECK_LAUNCH();
+    dim3 tiles((m + 63) / 64, (m + 63) / 64);
+    for (int j0 = 0; j0 < m; j0 += kGJ) {
+        const int bb = std::min(kGJ, m - j0);
+        k_gj_diag<<<1, 1024, 0, s>>>(m, j0, bb, A, C.S.p, C.P.p, C.diag0.p);
+        k_gj_rows<<<grid_for(c, m, 128), 128, 0, s>>>(m, j0, bb, A, C.S.p);
+        k_gj_update<<<tiles, 256, 0, s>>>(m, j0, bb, A, C.P.p);
+        k_gj_cols<<<grid_for(c, m, 128), 128, 0, s>>>(m, j0, bb, A, C.S.p, C.P.p);
+    }
+    OFEA_CHECK_LAUNCH();
+}
+
+// ----------------------------------------------------- lambda_max(D^-1 K) --
+
+// w = Dinv32 K32 (v * sc), sc = 1/||v|| from the previous partials.
+__global__ void __launch_bounds__(kBlock) k_power(int nfree, const int *__restrict__ sl_ptr,
+                                                  const int *__restrict__ scols,
+                                                  const float *__restrict__ sv32,
+                                                  const float *__restrict__ Dinv32,
+                                                  const float *__restrict__ v, float *__restrict__ w,
+                                                  const double *__restrict__ Pin, int Gin,
+                                                  double *__restrict__ Pout, int first) {
+    __shared__ double sh[kWarpsPerBlock];
+    double nrm2 = first ? 1.0 : sum_partials(Pin, Gin, sh);
+    const float sc = (float)(1.0 / sqrt(nrm2));
+    double acc = 0.0;
+    for_each_sell_row(nfree, sl_ptr, [&](int r, long S, int t, int W) {
+        float y[3];
+        sell_row<float, 4>(S, t, W, scols, sv32, [&](int k) { return v[k] * sc; }, y[0], y[1], y[2]);
+        float o[3];
+        block3_apply(Dinv32 + 9L * r, y, o);
+        for (int i = 0; i < 3; ++i) {
+            w[3L * r + i] = o[i];
+            acc += (double)o[i] * o[i];
+        }
+    });
+    double s = block_sum(acc, sh);
+    if (threadIdx.x == 0) Pout[blockIdx.x] = s;
+}
+
+__global__ void k_hash_vec(long n, float *v) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        unsigned h = (unsigned)(i * 2654435761u) ^ 0x9e3779b9u;
+        h ^= h >> 15;
+        h *= 2246822519u;
+        h ^= h >> 13;
+        v[i] = 0.5f + (float)(h & 0xffff) / 65536.0f;
+    }
+}
+
+static double estimate_lambda_max(ofea_ctx *c, int steps) {
+    cudaStream_t s = c->stream;
+    const int n = c->n;
+    const int G = std::min(kMaxGrid, c->num_sms * (2048 / kBlock));
+    Coarse &C = c->coarse;
+    C.pw.ensure(2L * std::max(n, 1));
+    C.pp.ensure(2L * kMaxGrid);
+    float *v = C.pw.p, *w = C.pw.p + n;
+    k_hash_vec<<<grid_for(c, n, kBlock), kBlock, 0, s>>>(n, v);
+    for (int k = 0; k < steps; ++k) {
+        double *Pin = C.pp.p + (k & 1) * kMaxGrid, *Pout = C.pp.p + ((k + 1) & 1) * kMaxGrid;
+        k_power<<<G, kBlock, 0, s>>>(c->nfree, c->sl_ptr.p, c->scols.p, c->sv32.p, c->Dinv32.p, v, w,
+                                     Pin, G, Pout, k == 0);
+        std::swap(v, w);
+    }
+    OFEA_CHECK_LAUNCH();
+    std::vector<double> h(G);
+    OFEA_CUDA(cudaMemcpyAsync(h.data(), C.pp.p + (steps & 1) * kMaxGrid, sizeof(double) * G,
+                              cudaMemcpyDeviceToHost, s));
+    OFEA_CUDA(cudaStreamSynchronize(s));
+    double nrm2 = 0;
+    for (double x : h) nrm2 += x;
+    return std::sqrt(nrm2);
+}
+
+// ------------------------------------------------------------ setup entry --
+
+void setup_coarse(ofea_ctx *c, int target_nodes) {
+    Coarse &C = c->coarse;
+    if (!C.geom_ok || C.target != target_nodes) {
+        C.target = target_nodes;
+        build_aggregation(c, target_nodes);
+    }
+    if (C.K_ok) return;
+    cudaStream_t s = c->stream;
+    const int m = C.m;
+    C.E.ensure((size_t)m * m);
+    C.Einv32.ensure((size_t)m * m);
+    C.cvec.ensure(std::max(m, 1));
+    C.evec.ensure(std::max(m, 1));
+    OFEA_CUDA(cudaMemsetAsync(C.E.p, 0, sizeof(double) * m * m, s));
+    OFEA_CUDA(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), s));
+    k_coarse_E<<<std::min(C.na, c->num_sms * 8), kEThreads, 0, s>>>(
+        C.na, C.agg_ptr.p, C.agg_nodes.p, C.agg_of.p, C.agg_cell.p, C.cell_agg.p, c->node_of_free.p,
+        c->xyz.p, C.centroid.p, C.inv_scale, c->rowptr.p, c->cols.p, c->Kb.p, C.nc[0], C.nc[1],
+        C.nc[2], m, C.E.p, c->err_flag.p);
+    OFEA_CHECK_LAUNCH();
+    OFEA_CUDA(cudaMemcpyAsync(c->herr.p, c->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    OFEA_CUDA(cudaStreamSynchronize(s));
+    if (c->herr.p[0]) fail(OFEA_ERR_CAPACITY, "coarse cells smaller than the element couplings");
+    invert_spd(c, C.E.p, m);
+    k_round_f32<<<grid_for(c, (long)m * m, kBlock), kBlock, 0, s>>>((long)m * m, C.E.p, C.Einv32.p);
+    OFEA_CHECK_LAUNCH();
+    C.lmax = estimate_lambda_max(c, 12);
+    C.K_ok = true;
+}
+
+// ---------------------------------------------------------- V-cycle kernels --
+
+// t = b - K32 x (x complete), per row.
+__global__ void __launch_bounds__(kBlock) k_vc_resid(int nfree, const int *__restrict__ sl_ptr,
+                                                     const int *__restrict__ scols,
+                                                     const float *__restrict__ sv32,
+                                                     const float *__restrict__ b,
+                                                     const float *__restrict__ x, float *__restrict__ t) {
+    for_each_sell_row(nfree, sl_ptr, [&](int r, long S, int tt, int W) {
+        float y[3];
+        sell_row<float, 4>(S, tt, W, scols, sv32, [&](int k) { return x[k]; }, y[0], y[1], y[2]);
+        for (int i = 0; i < 3; ++i) t[3L * r + i] = b[3L * r + i] - y[i];
+    });
+}
+
+// c_I = Z_I^T t: one CTA per aggregate, fixed-order reduction.
+__global__ void __launch_bounds__(kBlock) k_restrict(int na, const int *__restrict__ agg_ptr,
+                                                     const int *__restrict__ agg_nodes,
+                                                     const int *__restrict__ node_of_free,
+                                                     const double *__restrict__ xyz,
+                                                     const double *__restrict__ centroid,
+                                                     double inv_scale, const float *__restrict__ t,
+                                                     float *__restrict__ cvec) {
+    __shared__ float sh[kWarpsPerBlock];
+    for (int I = blockIdx.x; I < na; I += gridDim.x) {
+        float a[6] = {0, 0, 0, 0, 0, 0};
+        const float cx = (float)centroid[3L * I], cy = (float)centroid[3L * I + 1],
+                    cz = (float)centroid[3L * I + 2];
+        for (int idx = agg_ptr[I] + threadIdx.x; idx < agg_ptr[I + 1]; idx += blockDim.x) {
+            const int r = agg_nodes[idx], node = node_of_free[r];
+            const float dx = ((float)xyz[3L * node] - cx) * (float)inv_scale;
+            const float dy = ((float)xyz[3L * node + 1] - cy) * (float)inv_scale;
+            const float dz = ((float)xyz[3L * node + 2] - cz) * (float)inv_scale;
+            const float tx = t[3L * r], ty = t[3L * r + 1], tz = t[3L * r + 2];
+            a[0] += tx;
+            a[1] += ty;
+            a[2] += tz;
+            a[3] += -dz * ty + dy * tz;  // (e_x x d) . t
+            a[4] += dz * tx - dx * tz;   // (e_y x d) . t
+            a[5] += -dy * tx + dx * ty;  // (e_z x d) . t
+        }
+        for (int k = 0; k < 6; ++k) {
+            float s = block_sum(a[k], sh);
+            if (threadIdx.x == 0) cvec[6 * I + k] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// e = Einv32 c: one warp per row.
+__global__ void __launch_bounds__(kBlock) k_coarse_gemv(int m, const float *__restrict__ Ainv,
+                                                        const float *__restrict__ cvec,
+                                                        float *__restrict__ evec) {
+    const int lane = threadIdx.x & 31;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32; i < m; i += gridDim.x * blockDim.x / 32) {
+        const float *row = Ainv + (long)i * m;
+        float s = 0.0f;
+        for (int j = lane; j < m; j += 32) s = fmaf(row[j], cvec[j], s);
+        s = warp_sum(s);
+        if (lane == 0) evec[i] = s;
+    }
+}
+
+// x_a += Z_a e_I(a), per free node.
+__global__ void k_prolong(int nfree, const int *__restrict__ agg_of, const int *__restrict__ node_of_free,
+                          const double *__restrict__ xyz, const double *__restrict__ centroid,
+                          double inv_scale, const float *__restrict__ evec, float *__restrict__ x) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nfree; r += gridDim.x * blockDim.x) {
+        const int I = agg_of[r], node = node_of_free[r];
+        const float dx = (float)((xyz[3L * node] - centroid[3L * I]) * inv_scale);
+        const float dy = (float)((xyz[3L * node + 1] - centroid[3L * I + 1]) * inv_scale);
+        const float dz = (float)((xyz[3L * node + 2] - centroid[3L * I + 2]) * inv_scale);
+        const float *e = evec + 6L * I;
+        x[3L * r] += e[0] + dz * e[4] - dy * e[5];
+        x[3L * r + 1] += e[1] - dz * e[3] + dx * e[5];
+        x[3L * r + 2] += e[2] + dy * e[3] - dx * e[4];
+    }
+}
+
+void coarse_correct(ofea_ctx *c, const float *t, float *x) {
+    Coarse &C = c->coarse;
+    cudaStream_t s = c->stream;
+    k_restrict<<<std::min(C.na, c->num_sms * 8), kBlock, 0, s>>>(C.na, C.agg_ptr.p, C.agg_nodes.p,
+                                                                 c->node_of_free.p, c->xyz.p,
+                                                                 C.centroid.p, C.inv_scale, t, C.cvec.p);
+    k_coarse_gemv<<<grid_for(c, (long)C.m * 32, kBlock), kBlock, 0, s>>>(C.m, C.Einv32.p, C.cvec.p, C.evec.p);
+    k_prolong<<<grid_for(c, c->nfree, kBlock), kBlock, 0, s>>>(c->nfree, C.agg_of.p, c->node_of_free.p,
+                                                               c->xyz.p, C.centroid.p, C.inv_scale,
+                                                               C.evec.p, x);
+    OFEA_CHECK_LAUNCH();
+}
+
+void vc_resid(ofea_ctx *c, const float *b, const float *x, float *t) {
+    k_vc_resid<<<grid_for(c, (c->nfree + 31) / 32, kWarpsPerBlock), kBlock, 0, c->stream>>>(
+        c->nfree, c->sl_ptr.p, c->scols.p, c->sv32.p, b, x, t);
+    OFEA_CHECK_LAUNCH();
+}
+
+}  // namespace ofea

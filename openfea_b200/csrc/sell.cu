@@ -1,0 +1,69 @@
+// Conversion of the assembled block-CSR K into the solver's BSELL-32 layout
+// (sell.cuh), FP64 values and an FP32 copy.  Runs once per assembly.
+#include <algorithm>
+
+#include "sell.cuh"
+
+namespace ofea {
+
+__global__ void k_slice_width(int nfree, const int *__restrict__ rowptr, int *__restrict__ width) {
+    const int nslice = (nfree + kSlice - 1) / kSlice;
+    const int lane = threadIdx.x & 31;
+    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) / 32; s < nslice;
+         s += gridDim.x * blockDim.x / 32) {
+        int r = s * kSlice + lane;
+        int d = r < nfree ? rowptr[r + 1] - rowptr[r] : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) d = max(d, __shfl_xor_sync(0xffffffffu, d, o));
+        if (lane == 0) width[s] = d;
+    }
+}
+
+__global__ void k_fill_sell(int nfree, const int *__restrict__ rowptr, const int *__restrict__ cols,
+                            const double *__restrict__ Kb, const int *__restrict__ sl_ptr,
+                            int *__restrict__ scols, double *__restrict__ sv64,
+                            float *__restrict__ sv32) {
+    const int nslice = (nfree + kSlice - 1) / kSlice;
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < (long)nslice * kSlice;
+         g += (long)gridDim.x * blockDim.x) {
+        const int s = (int)(g / kSlice), t = (int)(g % kSlice);
+        const int r = s * kSlice + t;
+        const long S = sl_ptr[s];
+        const int W = sl_ptr[s + 1] - (int)S;
+        const int rb = r < nfree ? rowptr[r] : 0;
+        const int deg = r < nfree ? rowptr[r + 1] - rb : 0;
+        for (int k = 0; k < W; ++k) {
+            const bool real = k < deg;
+            scols[(S + k) * kSlice + t] = real ? cols[rb + k] : (r < nfree ? r : 0);
+#pragma unroll
+            for (int e = 0; e < 9; ++e) {
+                double v = real ? Kb[9L * (rb + k) + e] : 0.0;
+                sv64[((S + k) * 9 + e) * kSlice + t] = v;
+                sv32[((S + k) * 9 + e) * kSlice + t] = (float)v;
+            }
+        }
+    }
+}
+
+void build_sell(ofea_ctx *c) {
+    cudaStream_t s = c->stream;
+    const int nslice = (c->nfree + kSlice - 1) / kSlice;
+    c->sl_ptr.ensure((size_t)nslice + 1);
+    int tmp_len = nslice / 1024 + 4;
+    c->scratch_i.ensure((size_t)nslice + 1 + tmp_len);
+    int *width = c->scratch_i.p;
+    k_slice_width<<<grid_for(c, (long)nslice * 32, kBlock), kBlock, 0, s>>>(c->nfree, c->rowptr.p, width);
+    OFEA_CHECK_LAUNCH();
+    long long tot = exclusive_scan(width, c->sl_ptr.p, nslice, s, width + nslice + 1, tmp_len);
+    c->sell_len = tot;
+    size_t slots = (size_t)std::max<long long>(tot, 1) * kSlice;
+    c->scols.ensure(slots);
+    c->sv64.ensure(9 * slots);
+    c->sv32.ensure(9 * slots);
+    k_fill_sell<<<grid_for(c, (long)nslice * kSlice, kBlock), kBlock, 0, s>>>(
+        c->nfree, c->rowptr.p, c->cols.p, c->Kb.p, c->sl_ptr.p, c->scols.p, c->sv64.p, c->sv32.p);
+    OFEA_CHECK_LAUNCH();
+    c->sell_ok = true;
+}
+
+}  // namespace ofea

@@ -1,0 +1,76 @@
+// Sliced-ELL storage of the 3x3-block matrix (BSELL-32) and its SpMV row.
+//
+// Slice s holds block rows 32s .. 32s+31; its width W_s is the largest block
+// count of those rows.  For slot k < W_s and lane t (row 32s+t):
+//   column  scols[(S_s + k) * 32 + t]
+//   entry e svals[((S_s + k) * 9 + e) * 32 + t]      e = 3 i + j of the 3x3 block
+// with S_s = sl_ptr[s].  Rows shorter than W_s are padded with their own
+// column and zero values.  One thread owns one block row (3 DOF rows): every
+// value load of a warp is one coalesced 256 B (FP64) / 128 B (FP32) line, the
+// 9 planes of a slot and several slots are in flight at once, and for
+// structured node orderings neighbouring threads gather neighbouring x.
+#pragma once
+#include "ofea_internal.cuh"
+
+namespace ofea {
+
+constexpr int kSlice = 32;
+
+// y_i (i = 0..2) of block row (slice base S, lane t, width W); x(k) returns
+// entry k of the operand vector.
+template <class V, int UNROLL, class XF>
+__device__ __forceinline__ void sell_row(long S, int t, int W, const int *__restrict__ scols,
+                                         const V *__restrict__ svals, XF x, V &y0, V &y1, V &y2) {
+    y0 = 0;
+    y1 = 0;
+    y2 = 0;
+    const int *cp = scols + S * kSlice + t;
+    const V *vp = svals + S * 9 * kSlice + t;
+    int k = 0;
+    for (; k + UNROLL <= W; k += UNROLL) {
+        int c[UNROLL];
+        V v[UNROLL][9];
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+            c[u] = __ldg(cp + (long)(k + u) * kSlice);
+#pragma unroll
+            for (int e = 0; e < 9; ++e) v[u][e] = __ldg(vp + ((long)(k + u) * 9 + e) * kSlice);
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+            V x0 = x(3 * c[u]), x1 = x(3 * c[u] + 1), x2 = x(3 * c[u] + 2);
+            y0 = fma(v[u][0], x0, fma(v[u][1], x1, fma(v[u][2], x2, y0)));
+            y1 = fma(v[u][3], x0, fma(v[u][4], x1, fma(v[u][5], x2, y1)));
+            y2 = fma(v[u][6], x0, fma(v[u][7], x1, fma(v[u][8], x2, y2)));
+        }
+    }
+    for (; k < W; ++k) {
+        int c = __ldg(cp + (long)k * kSlice);
+        V v[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) v[e] = __ldg(vp + ((long)k * 9 + e) * kSlice);
+        V x0 = x(3 * c), x1 = x(3 * c + 1), x2 = x(3 * c + 2);
+        y0 = fma(v[0], x0, fma(v[1], x1, fma(v[2], x2, y0)));
+        y1 = fma(v[3], x0, fma(v[4], x1, fma(v[5], x2, y1)));
+        y2 = fma(v[6], x0, fma(v[7], x1, fma(v[8], x2, y2)));
+    }
+}
+
+// Iterate over this thread's block rows: f(r, S, t, W) for each row r < nfree.
+template <class F>
+__device__ __forceinline__ void for_each_sell_row(int nfree, const int *__restrict__ sl_ptr, F f) {
+    const int nslice = (nfree + kSlice - 1) / kSlice;
+    const int t = threadIdx.x & (kSlice - 1);
+    const int slices_per_cta = blockDim.x / kSlice;
+    for (int s = blockIdx.x * slices_per_cta + (threadIdx.x / kSlice); s < nslice;
+         s += gridDim.x * slices_per_cta) {
+        const int r = s * kSlice + t;
+        if (r >= nfree) continue;
+        const int S = sl_ptr[s], W = sl_ptr[s + 1] - S;
+        f(r, (long)S, t, W);
+    }
+}
+
+void build_sell(ofea_ctx *c);
+
+}  // namespace ofea
