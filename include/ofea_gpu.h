@@ -71,7 +71,8 @@ typedef struct {
     int iterations;        /* inner iterations performed */
     int refinements;       /* restarts from a recomputed FP64 residual */
     double rel_residual;   /* final ||f - K u|| / ||f|| in FP64 */
-    double seconds;        /* device time of the solve (CUDA events) */
+    double seconds;        /* device time of the solve (CUDA events), setup included */
+    double setup_seconds;  /* part of `seconds` spent building the preconditioner */
     int rejected_learned;  /* 1 when the learned stage was rejected and plain PCG finished */
     long long kernel_launches;
 } ofea_solve_stats;
@@ -129,6 +130,9 @@ OFEA_API int ofea_spmv(ofea_ctx *ctx, const double *x, double *y);
  * opts NULL: defaults.  stats may be NULL (one entry per rhs otherwise). */
 OFEA_API int ofea_solve(ofea_ctx *ctx, const double *f, double *u, int nrhs, const ofea_solve_opts *opts,
                ofea_solve_stats *stats);
+/* Drop the preconditioner built for the current K (coarse operator, smoother
+ * bounds), so the next solve rebuilds it; a new assembly does this too. */
+OFEA_API int ofea_precond_reset(ofea_ctx *ctx);
 /* Same with device pointers (f, u of n doubles each), stream-ordered. */
 OFEA_API int ofea_solve_device(ofea_ctx *ctx, const double *d_f, double *d_u, const ofea_solve_opts *opts,
                       ofea_solve_stats *stats);

@@ -47,7 +47,8 @@ class SolveOpts(ctypes.Structure):
 
 class SolveStats(ctypes.Structure):
     _fields_ = [("status", _I), ("iterations", _I), ("refinements", _I), ("rel_residual", _D),
-                ("seconds", _D), ("rejected_learned", _I), ("kernel_launches", _LL)]
+                ("seconds", _D), ("setup_seconds", _D), ("rejected_learned", _I),
+                ("kernel_launches", _LL)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -93,6 +94,7 @@ def lib():
         "ofea_full_displacement": (_I, [_I, _P, _P, _P]),
         "ofea_write_vtk": (_I, [ctypes.c_char_p, _I, _P, _I, _P, _P, _P, _D]),
         "ofea_profile_solver_kernels": (_I, [_P, _I, _I, _P, _P]),
+        "ofea_precond_reset": (_I, [_P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -215,6 +217,10 @@ class Context:
             _check(rc, "ofea_solve")
         st = [s.as_dict() for s in stats]
         return (U[:, 0] if F.ndim == 1 else U), (st[0] if F.ndim == 1 else st)
+
+    def precond_reset(self):
+        """Rebuild the preconditioner at the next solve (as after a new assembly)."""
+        _check(lib().ofea_precond_reset(self.h), "ofea_precond_reset")
 
     def profile_kernels(self, method="GPU_MIXED", reps=20):
         """Average ms and algorithmic bytes per launch of the solver's A and B

@@ -373,6 +373,13 @@ static void check_solve_ready(ofea_ctx *c, const ofea_solve_opts &o) {
     if (!c->jacobi_ok) fail(OFEA_ERR_BREAKDOWN, "a diagonal block of K is not positive definite");
 }
 
+int ofea_precond_reset(ofea_ctx *c) {
+    return guarded([&] {
+        need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
+        c->coarse.K_ok = false;
+    });
+}
+
 int ofea_solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_opts *opts,
                       ofea_solve_stats *stats) {
     ofea_solve_stats st{};

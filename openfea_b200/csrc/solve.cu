@@ -486,9 +486,16 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
     w.p0.ensure(n);
     w.p1.ensure(n);
     const bool mixed = o.method == OFEA_SOLVER_MIXED;
+    float setup_ms = 0.f;
     if (mixed) {
         const bool had = c->coarse.K_ok;
+        cudaEvent_t es;
+        OFEA_CUDA(cudaEventCreate(&es));
         setup_coarse(c, c->coarse_nodes);
+        OFEA_CUDA(cudaEventRecord(es, s));
+        OFEA_CUDA(cudaEventSynchronize(es));
+        OFEA_CUDA(cudaEventElapsedTime(&setup_ms, e0, es));
+        cudaEventDestroy(es);
         if (!had) launches += 4 + 4 * ((c->coarse.m + 31) / 32) + 14;
         w.b32.ensure(n);
         w.x32.ensure(n);
@@ -582,6 +589,7 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
     st.refinements = restarts;
     st.rel_residual = rel;
     st.seconds = ms * 1e-3;
+    st.setup_seconds = setup_ms * 1e-3;
     st.kernel_launches = launches;
     if (hf.status == OFEA_ERR_BREAKDOWN)
         st.status = OFEA_ERR_BREAKDOWN;
