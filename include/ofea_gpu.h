@@ -137,6 +137,22 @@ OFEA_API int ofea_precond_reset(ofea_ctx *ctx);
 OFEA_API int ofea_solve_device(ofea_ctx *ctx, const double *d_f, double *d_u, const ofea_solve_opts *opts,
                       ofea_solve_stats *stats);
 
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory (an application whose own pool allocator reserves the GPU up front, a
+ * latency-critical loop that must not call cudaMalloc/cudaFree because they
+ * can synchronize the device): norms[2k] = ||f_k - K u_k||_2 and
+ * norms[2k+1] = ||f_k||_2 for load cases k < nrhs, with f, u device arrays of
+ * n x nrhs (column-major) and norms a device array of 2 nrhs doubles.  K is
+ * the context's assembled matrix.  Allocates nothing: its partial sums live
+ * in a 512 KB static device array that every GPU loading this library holds
+ * until the process exits.  At most 16 load cases per call; more returns
+ * OFEA_ERR_CAPACITY.  The first call on each device looks up that array's
+ * device address; make that first call before any stream capture.  Calls
+ * share the array: calls that overlap on one GPU race and must be ordered by
+ * the caller.  Enqueued on the context's stream; returns without waiting. */
+OFEA_API int ofea_residual_norms_noalloc(ofea_ctx *ctx, int nrhs, const double *d_f,
+                                         const double *d_u, double *d_norms);
+
 /* ---- measurement ------------------------------------------------------- */
 /* No counterpart in the reference (it only prints clock() spans): times the
  * solver's two per-iteration kernels (A: p update + SpMV + p.q, B: vector

@@ -442,6 +442,16 @@ int ofea_solve(ofea_ctx *c, const double *f, double *u, int nrhs, const ofea_sol
     return worst;
 }
 
+int ofea_residual_norms_noalloc(ofea_ctx *c, int nrhs, const double *d_f, const double *d_u,
+                                double *d_norms) {
+    return guarded([&] {
+        need(c != nullptr && d_f && d_u && d_norms, OFEA_ERR_INVALID_ARG, "NULL argument");
+        need(c->K_ok && c->sell_ok, OFEA_ERR_STATE, "K not assembled");
+        OFEA_CUDA(cudaSetDevice(c->device));
+        residual_norms_noalloc(c, nrhs, d_f, d_u, d_norms);
+    });
+}
+
 int ofea_profile_solver_kernels(ofea_ctx *c, int method, int reps, double *ms, double *bytes) {
     return guarded([&] {
         need(c != nullptr && ms && bytes && reps > 0, OFEA_ERR_INVALID_ARG, "bad argument");

@@ -182,6 +182,9 @@ void spmv64(ofea_ctx *c, const double *d_x, double *d_y);
 void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_opts &o,
                   ofea_solve_stats &st);
 void profile_kernels(ofea_ctx *c, int method, int reps, double *ms, double *bytes);
+// noalloc.cu
+void residual_norms_noalloc(ofea_ctx *c, int nrhs, const double *d_f, const double *d_u,
+                            double *d_norms);
 // pattern.cu (scan)
 long long exclusive_scan(const int *d_in, int *d_out, int n, cudaStream_t s, int *d_tmp,
                          int tmp_len);
