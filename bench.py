@@ -50,6 +50,9 @@ def parse():
     p.add_argument("--rtol", type=float, default=1e-8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--mode", default="full", choices=["full", "solve-only"],
+                   help="solve-only: assemble, one MIXED and one plain solve, nothing else "
+                        "(a short launch list for profilers)")
     return p.parse_args()
 
 
@@ -252,6 +255,18 @@ def run_ours(args):
         if rc != 0:
             raise RuntimeError(f"{method} solve failed: {st}")
         return st
+
+    if args.mode == "solve-only":
+        st_m = solve("GPU_MIXED")
+        st_p = solve("GPU_PCG")
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"mode": "solve-only", "shape": args.shape, "n": n, "nnz": nnz,
+                              "mixed": st_m, "plain": st_p}), flush=True)
+        ctx.close()
+        if dist:
+            dist.destroy_process_group()
+        return 0
 
     for _ in range(args.warmup):
         solve("GPU_MIXED")
