@@ -123,7 +123,7 @@ struct Coarse {
     int nc[3] = {1, 1, 1};
     double inv_scale = 1.0, lmax = 0.0;
     DevBuf<int> agg_of, agg_ptr, agg_nodes, agg_cell, cell_agg;
-    DevBuf<double> centroid, E, S, P, diag0, pp;
+    DevBuf<double> centroid, E, S, P, diag0, pp, part;
     DevBuf<float> Einv32, cvec, evec, pw;
 };
 

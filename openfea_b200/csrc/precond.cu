@@ -153,41 +153,47 @@ __device__ __forceinline__ void rigid_col(int k, const double *d, double *z) {
     }
 }
 
-// One CTA per aggregate I: E[6I+k][6J+l] = sum_{a in I} sum_b Z_a^T K_ab Z_b.
-// Each group of 36 threads walks its share of I's nodes in ascending order,
-// stages a block row (kStage blocks at a time) in shared memory, and every
-// thread accumulates its (k,l) entry per neighbour cell;
-// the groups are summed in a fixed order: deterministic.
+// E[6I+k][6J+l] = sum_{a in I} sum_b Z_a^T K_ab Z_b, in two deterministic
+// stages.  Stage 1: one CTA per (aggregate I, chunk of kChunkNodes of I's
+// nodes); each group of 36 threads walks its share of the chunk's nodes in
+// ascending order, stages a block row (kStage blocks at a time) in shared
+// memory, and every thread accumulates its (k,l) entry per neighbour cell
+// slot; the groups are summed in a fixed order into the chunk's partial.
+// Stage 2: per (I, slot, k, l), the chunks are summed in order into E.
 constexpr int kStage = 32;
-__global__ void __launch_bounds__(kEThreads) k_coarse_E(
-    int na, const int *__restrict__ agg_ptr, const int *__restrict__ agg_nodes,
-    const int *__restrict__ agg_of, const int *__restrict__ agg_cell, const int *__restrict__ cell_agg,
+constexpr int kChunkNodes = 64;
+__global__ void __launch_bounds__(kEThreads) k_coarse_E_chunks(
+    int na, int nchunk_max, const int *__restrict__ agg_ptr, const int *__restrict__ agg_nodes,
+    const int *__restrict__ agg_of, const int *__restrict__ agg_cell,
     const int *__restrict__ node_of_free, const double *__restrict__ xyz,
     const double *__restrict__ centroid, double inv_scale, const int *__restrict__ rowptr,
-    const int *__restrict__ cols, const double *__restrict__ Kb, int ncx, int ncy, int ncz, int m,
-    double *__restrict__ E, int *__restrict__ err) {
+    const int *__restrict__ cols, const double *__restrict__ Kb, double *__restrict__ part,
+    int *__restrict__ err) {
     __shared__ double acc[kEGroups][27][36];
     __shared__ double sK[kEGroups][kStage][9];
     __shared__ double sD[kEGroups][kStage][3];
     __shared__ int sSlot[kEGroups][kStage];
     __shared__ int s_chunks[kEGroups];
     const int g = threadIdx.x / 36, kl = threadIdx.x % 36, k = kl / 6, l = kl % 6;
-    for (int I = blockIdx.x; I < na; I += gridDim.x) {
+    const long nwork = (long)na * nchunk_max;
+    for (long wi = blockIdx.x; wi < nwork; wi += gridDim.x) {
+        const int I = (int)(wi / nchunk_max), ch = (int)(wi % nchunk_max);
         for (int v = threadIdx.x; v < kEGroups * 27 * 36; v += blockDim.x) (&acc[0][0][0])[v] = 0.0;
         __syncthreads();
         const int cx = agg_cell[3 * I], cy = agg_cell[3 * I + 1], cz = agg_cell[3 * I + 2];
         const double ci[3] = {centroid[3L * I], centroid[3L * I + 1], centroid[3L * I + 2]};
-        const int b0 = agg_ptr[I], b1 = agg_ptr[I + 1];
-        // groups take nodes round-robin; iterate a uniform trip count so all
-        // threads of the CTA reach the barriers together
-        const int per = (b1 - b0 + kEGroups - 1) / kEGroups;
+        const int b0 = agg_ptr[I] + ch * kChunkNodes;
+        const int b1 = min(agg_ptr[I + 1], b0 + kChunkNodes);
+        // groups take nodes round-robin; a uniform trip count keeps every
+        // thread of the CTA at the same barriers
+        const int per = b1 > b0 ? (b1 - b0 + kEGroups - 1) / kEGroups : 0;
         for (int it = 0; it < per; ++it) {
             const int idx = b0 + it * kEGroups + g;
             const bool live = idx < b1;
-            int r = 0, rb = 0, deg = 0;
+            int rb = 0, deg = 0;
             double da[3] = {0, 0, 0};
             if (live) {
-                r = agg_nodes[idx];
+                const int r = agg_nodes[idx];
                 rb = rowptr[r];
                 deg = rowptr[r + 1] - rb;
                 const int node = node_of_free[r];
@@ -195,17 +201,15 @@ __global__ void __launch_bounds__(kEThreads) k_coarse_E(
             }
             double za[3];
             rigid_col(k, da, za);
-            // rows of the groups differ in length: agree on the chunk count
             const int nchunks = (deg + kStage - 1) / kStage;
             __syncthreads();
             if (kl == 0) s_chunks[g] = nchunks;
             __syncthreads();
             int maxchunks = 0;
             for (int q = 0; q < kEGroups; ++q) maxchunks = max(maxchunks, s_chunks[q]);
-            for (int ch = 0; ch < maxchunks; ++ch) {
-                const int p0 = ch * kStage;
+            for (int cc = 0; cc < maxchunks; ++cc) {
+                const int p0 = cc * kStage;
                 const int cnt = live ? min(kStage, deg - p0) : 0;
-                // stage: thread kl < cnt loads block p0+kl of this group's row
                 if (kl < cnt) {
                     const int p = rb + p0 + kl;
                     const int s = cols[p];
@@ -240,18 +244,33 @@ __global__ void __launch_bounds__(kEThreads) k_coarse_E(
             }
         }
         __syncthreads();
-        // fixed-order sum of the groups, written into the dense E
+        double *out = part + wi * (27L * 36);
         for (int v = threadIdx.x; v < 27 * 36; v += blockDim.x) {
-            const int slot = v / 36, e = v % 36, kk = e / 6, ll = e % 6;
-            const int x = cx + slot / 9 - 1, y = cy + (slot / 3) % 3 - 1, z = cz + slot % 3 - 1;
-            if (x < 0 || y < 0 || z < 0 || x >= ncx || y >= ncy || z >= ncz) continue;
-            const int J = cell_agg[((long)x * ncy + y) * ncz + z];
-            if (J < 0) continue;
             double s = 0.0;
-            for (int q = 0; q < kEGroups; ++q) s += acc[q][slot][e];
-            E[(6L * I + kk) * m + 6L * J + ll] = s;
+            for (int q = 0; q < kEGroups; ++q) s += (&acc[q][0][0])[v];
+            out[v] = s;
         }
         __syncthreads();
+    }
+}
+
+// Stage 2: E entries from the chunk partials, fixed chunk order.
+__global__ void k_coarse_E_sum(int na, int nchunk_max, const int *__restrict__ agg_cell,
+                               const int *__restrict__ cell_agg, int ncx, int ncy, int ncz, int m,
+                               const double *__restrict__ part, double *__restrict__ E) {
+    const long total = (long)na * 27 * 36;
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < total; g += (long)gridDim.x * blockDim.x) {
+        const int I = (int)(g / (27 * 36));
+        const int v = (int)(g % (27 * 36));
+        const int slot = v / 36, e = v % 36, kk = e / 6, ll = e % 6;
+        const int x = agg_cell[3 * I] + slot / 9 - 1, y = agg_cell[3 * I + 1] + (slot / 3) % 3 - 1,
+                  z = agg_cell[3 * I + 2] + slot % 3 - 1;
+        if (x < 0 || y < 0 || z < 0 || x >= ncx || y >= ncy || z >= ncz) continue;
+        const int J = cell_agg[((long)x * ncy + y) * ncz + z];
+        if (J < 0) continue;
+        double s = 0.0;
+        for (int ch = 0; ch < nchunk_max; ++ch) s += part[((long)I * nchunk_max + ch) * (27 * 36) + v];
+        E[(6L * I + kk) * m + 6L * J + ll] = s;
     }
 }
 
@@ -266,71 +285,123 @@ __global__ void __launch_bounds__(kEThreads) k_coarse_E(
 // A pivot that vanishes (a degenerate aggregate) drops its direction: its
 // row and column of the result are zero.
 
-constexpr int kGJ = 32;
+constexpr int kGJ = 64;
 
-__global__ void __launch_bounds__(1024) k_gj_diag(int m, int j0, int bb, double *__restrict__ A,
-                                                  double *__restrict__ S, double *__restrict__ P,
-                                                  const double *__restrict__ diag0) {
+// Inverse of the diagonal block A_JJ -> S (kGJ x kGJ), one CTA of 1024
+// threads, thread (ty, tx) owning rows ty, ty+16, ty+32, ty+48 of column tx.
+__global__ void __launch_bounds__(1024) k_gj_diag(int m, int j0, int bb, const double *__restrict__ A,
+                                                  double *__restrict__ S, const double *__restrict__ diag0) {
     __shared__ double a[kGJ][kGJ + 1];
-    const int tx = threadIdx.x % kGJ, ty = threadIdx.x / kGJ;
-    if (ty < bb && tx < bb) a[ty][tx] = A[(long)(j0 + ty) * m + j0 + tx];
+    const int tx = threadIdx.x % kGJ, ty = threadIdx.x / kGJ;  // ty in 0..15
+    for (int rr = ty; rr < kGJ; rr += 16) a[rr][tx] = (rr < bb && tx < bb) ? A[(long)(j0 + rr) * m + j0 + tx] : 0.0;
     __syncthreads();
     for (int p = 0; p < bb; ++p) {
-        double piv = a[p][p];
+        const double piv = a[p][p];
         const bool drop = !(piv > 1e-12 * diag0[j0 + p]);
+        double rowp = a[p][tx];
+        double colp[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) colp[q] = a[ty + 16 * q][p];
         __syncthreads();
         if (drop) {
-            if (ty == p && tx < bb) a[p][tx] = 0.0;
-            if (tx == p && ty < bb) a[ty][p] = 0.0;
-            __syncthreads();
-            continue;
-        }
-        const double inv = 1.0 / piv;
-        double rowp = (tx < bb) ? a[p][tx] : 0.0, colp = (ty < bb) ? a[ty][p] : 0.0;
-        __syncthreads();
-        if (ty < bb && tx < bb) {
-            if (ty == p && tx == p) a[ty][tx] = inv;
-            else if (ty == p) a[ty][tx] = rowp * inv;
-            else if (tx == p) a[ty][tx] = -colp * inv;
-            else a[ty][tx] -= colp * rowp * inv;
+            // a vanishing pivot (degenerate aggregate) drops its direction
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int rr = ty + 16 * q;
+                if (rr == p || tx == p) a[rr][tx] = 0.0;
+            }
+        } else {
+            const double inv = 1.0 / piv;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int rr = ty + 16 * q;
+                if (rr >= bb || tx >= bb) continue;
+                if (rr == p && tx == p) a[rr][tx] = inv;
+                else if (rr == p) a[rr][tx] = rowp * inv;
+                else if (tx == p) a[rr][tx] = -colp[q] * inv;
+                else a[rr][tx] -= colp[q] * rowp * inv;
+            }
         }
         __syncthreads();
     }
-    if (ty < bb && tx < bb) S[ty * kGJ + tx] = a[ty][tx];
-    // save the column panel P = A[:, J] (all rows)
-    for (long i = threadIdx.x; i < (long)m * bb; i += blockDim.x) {
-        long row = i / bb;
-        int j = (int)(i % bb);
-        P[row * kGJ + j] = A[row * m + j0 + j];
+    for (int rr = ty; rr < kGJ; rr += 16) S[rr * kGJ + tx] = a[rr][tx];
+}
+
+// Column panel, one warp per row i: P_i = A_{i,J} (saved for the update),
+// A_{i,J} <- -P_i S (i outside J) or S (i inside J).
+__global__ void __launch_bounds__(256) k_gj_panel(int m, int j0, int bb, double *__restrict__ A,
+                                                  const double *__restrict__ S, double *__restrict__ P) {
+    __shared__ double sS[kGJ][kGJ];
+    for (int v = threadIdx.x; v < kGJ * kGJ; v += blockDim.x) sS[v / kGJ][v % kGJ] = S[v];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32; i < m; i += gridDim.x * blockDim.x / 32) {
+        const bool in = i >= j0 && i < j0 + bb;
+        double p0 = lane < bb ? A[(long)i * m + j0 + lane] : 0.0;
+        double p1 = lane + 32 < bb ? A[(long)i * m + j0 + lane + 32] : 0.0;
+        P[(long)i * kGJ + lane] = p0;
+        P[(long)i * kGJ + lane + 32] = p1;
+        double o0 = 0.0, o1 = 0.0;
+        if (in) {
+            o0 = sS[i - j0][lane];
+            o1 = sS[i - j0][lane + 32];
+        } else {
+            for (int q = 0; q < 32; ++q) {
+                const double pq = __shfl_sync(0xffffffffu, p0, q);
+                o0 -= pq * sS[q][lane];
+                o1 -= pq * sS[q][lane + 32];
+            }
+            for (int q = 0; q < 32; ++q) {
+                const double pq = __shfl_sync(0xffffffffu, p1, q);
+                o0 -= pq * sS[q + 32][lane];
+                o1 -= pq * sS[q + 32][lane + 32];
+            }
+        }
+        if (lane < bb) A[(long)i * m + j0 + lane] = o0;
+        if (lane + 32 < bb) A[(long)i * m + j0 + lane + 32] = o1;
     }
 }
 
-// Row panel: A_{J,k} <- S A_{J,k}, one thread per column k outside J.
-__global__ void k_gj_rows(int m, int j0, int bb, double *__restrict__ A, const double *__restrict__ S) {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
-        if (k >= j0 && k < j0 + bb) continue;
-        double v[kGJ], o[kGJ];
-        for (int j = 0; j < bb; ++j) v[j] = A[(long)(j0 + j) * m + k];
-        for (int i = 0; i < bb; ++i) {
+// Row panel: A_{J,k} <- S A_{J,k} for k outside J; one CTA per 32 columns.
+__global__ void __launch_bounds__(256) k_gj_rows(int m, int j0, int bb, double *__restrict__ A,
+                                                 const double *__restrict__ S) {
+    __shared__ double sS[kGJ][kGJ];  // read as broadcasts: no padding needed
+    __shared__ double sR[kGJ][32];
+    for (int v = threadIdx.x; v < kGJ * kGJ; v += blockDim.x) sS[v / kGJ][v % kGJ] = S[v];
+    for (int k0 = blockIdx.x * 32; k0 < m; k0 += gridDim.x * 32) {
+        __syncthreads();
+        for (int v = threadIdx.x; v < kGJ * 32; v += blockDim.x) {
+            const int j = v / 32, kk = v % 32, k = k0 + kk;
+            sR[j][kk] = (j < bb && k < m) ? A[(long)(j0 + j) * m + k] : 0.0;
+        }
+        __syncthreads();
+        // thread: column kk = tid % 32, rows i = tid / 32 + 8 q
+        const int kk = threadIdx.x % 32, k = k0 + kk;
+        const bool skip = k >= m || (k >= j0 && k < j0 + bb);
+        for (int q = 0; q < kGJ / 8; ++q) {
+            const int i = threadIdx.x / 32 + 8 * q;
+            if (i >= bb || skip) continue;
             double s = 0.0;
-            for (int j = 0; j < bb; ++j) s += S[i * kGJ + j] * v[j];
-            o[i] = s;
+            for (int j = 0; j < bb; ++j) s = fma(sS[i][j], sR[j][kk], s);
+            A[(long)(j0 + i) * m + k] = s;
         }
-        for (int i = 0; i < bb; ++i) A[(long)(j0 + i) * m + k] = o[i];
     }
 }
 
-// Rank-bb update of the outside block, 64 x 64 tiles, 256 threads (4 x 4 each).
+// Rank-bb update of the outside block: A_ik -= P_i . A_{J,k}, 64 x 64 tiles,
+// 256 threads with 4 x 4 outputs each; dynamic shared memory (66 KB).
 __global__ void __launch_bounds__(256) k_gj_update(int m, int j0, int bb, double *__restrict__ A,
                                                    const double *__restrict__ P) {
-    __shared__ double sP[64][kGJ + 1];
-    __shared__ double sR[kGJ][64 + 1];
+    extern __shared__ double smem[];
+    double (*sP)[kGJ + 1] = reinterpret_cast<double (*)[kGJ + 1]>(smem);             // [64][65]
+    double (*sR)[64 + 1] = reinterpret_cast<double (*)[64 + 1]>(smem + 64 * (kGJ + 1));  // [64][65]
     const int i0 = blockIdx.y * 64, k0 = blockIdx.x * 64;
+    if (i0 >= j0 && i0 + 64 <= j0 + bb) return;  // every row of the tile is in J: nothing to update
     const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
     for (int v = threadIdx.x; v < 64 * kGJ; v += 256) {
-        int ii = v / kGJ, jj = v % kGJ;
+        const int ii = v / kGJ, jj = v % kGJ;
         sP[ii][jj] = (i0 + ii < m && jj < bb) ? P[(long)(i0 + ii) * kGJ + jj] : 0.0;
-        int jr = v / 64, kk = v % 64;
+        const int jr = v / 64, kk = v % 64;
         sR[jr][kk] = (jr < bb && k0 + kk < m) ? A[(long)(j0 + jr) * m + k0 + kk] : 0.0;
     }
     __syncthreads();
@@ -359,23 +430,6 @@ __global__ void __launch_bounds__(256) k_gj_update(int m, int j0, int bb, double
     }
 }
 
-// Column panel: A_{i,J} <- -P_i S (i outside J), A_JJ <- S.
-__global__ void k_gj_cols(int m, int j0, int bb, double *__restrict__ A, const double *__restrict__ S,
-                          const double *__restrict__ P) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        const bool in = i >= j0 && i < j0 + bb;
-        for (int j = 0; j < bb; ++j) {
-            double s = 0.0;
-            if (in) {
-                s = S[(i - j0) * kGJ + j];
-            } else {
-                for (int q = 0; q < bb; ++q) s -= P[(long)i * kGJ + q] * S[q * kGJ + j];
-            }
-            A[(long)i * m + j0 + j] = s;
-        }
-    }
-}
-
 __global__ void k_diag_of(int m, const double *__restrict__ A, double *__restrict__ d) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
         d[i] = fabs(A[(long)i * m + i]);
@@ -394,13 +448,15 @@ static void invert_spd(ofea_ctx *c, double *A, int m) {
     C.diag0.ensure(m);
     k_diag_of<<<grid_for(c, m, kBlock), kBlock, 0, s>>>(m, A, C.diag0.p);
     OFEA_CHECK_LAUNCH();
+    const size_t upd_smem = sizeof(double) * (64 * (kGJ + 1) + kGJ * 65);
+    OFEA_CUDA(cudaFuncSetAttribute(k_gj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem));
     dim3 tiles((m + 63) / 64, (m + 63) / 64);
     for (int j0 = 0; j0 < m; j0 += kGJ) {
         const int bb = std::min(kGJ, m - j0);
-        k_gj_diag<<<1, 1024, 0, s>>>(m, j0, bb, A, C.S.p, C.P.p, C.diag0.p);
-        k_gj_rows<<<grid_for(c, m, 128), 128, 0, s>>>(m, j0, bb, A, C.S.p);
-        k_gj_update<<<tiles, 256, 0, s>>>(m, j0, bb, A, C.P.p);
-        k_gj_cols<<<grid_for(c, m, 128), 128, 0, s>>>(m, j0, bb, A, C.S.p, C.P.p);
+        k_gj_diag<<<1, 1024, 0, s>>>(m, j0, bb, A, C.S.p, C.diag0.p);
+        k_gj_panel<<<grid_for(c, (long)m * 32, 256), 256, 0, s>>>(m, j0, bb, A, C.S.p, C.P.p);
+        k_gj_rows<<<std::max(1, std::min((m + 31) / 32, c->num_sms * 4)), 256, 0, s>>>(m, j0, bb, A, C.S.p);
+        k_gj_update<<<tiles, 256, upd_smem, s>>>(m, j0, bb, A, C.P.p);
     }
     OFEA_CHECK_LAUNCH();
 }
@@ -485,10 +541,13 @@ void setup_coarse(ofea_ctx *c, int target_nodes) {
     C.evec.ensure(std::max(m, 1));
     OFEA_CUDA(cudaMemsetAsync(C.E.p, 0, sizeof(double) * m * m, s));
     OFEA_CUDA(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), s));
-    k_coarse_E<<<std::min(C.na, c->num_sms * 8), kEThreads, 0, s>>>(
-        C.na, C.agg_ptr.p, C.agg_nodes.p, C.agg_of.p, C.agg_cell.p, C.cell_agg.p, c->node_of_free.p,
-        c->xyz.p, C.centroid.p, C.inv_scale, c->rowptr.p, c->cols.p, c->Kb.p, C.nc[0], C.nc[1],
-        C.nc[2], m, C.E.p, c->err_flag.p);
+    const int nchunk = (C.max_agg + kChunkNodes - 1) / kChunkNodes;
+    C.part.ensure((size_t)C.na * nchunk * 27 * 36);
+    k_coarse_E_chunks<<<(int)std::min<long>((long)C.na * nchunk, (long)c->num_sms * 32), kEThreads, 0, s>>>(
+        C.na, nchunk, C.agg_ptr.p, C.agg_nodes.p, C.agg_of.p, C.agg_cell.p, c->node_of_free.p, c->xyz.p,
+        C.centroid.p, C.inv_scale, c->rowptr.p, c->cols.p, c->Kb.p, C.part.p, c->err_flag.p);
+    k_coarse_E_sum<<<grid_for(c, (long)C.na * 27 * 36, kBlock), kBlock, 0, s>>>(
+        C.na, nchunk, C.agg_cell.p, C.cell_agg.p, C.nc[0], C.nc[1], C.nc[2], m, C.part.p, C.E.p);
     OFEA_CHECK_LAUNCH();
     OFEA_CUDA(cudaMemcpyAsync(c->herr.p, c->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     OFEA_CUDA(cudaStreamSynchronize(s));
@@ -496,7 +555,7 @@ void setup_coarse(ofea_ctx *c, int target_nodes) {
     invert_spd(c, C.E.p, m);
     k_round_f32<<<grid_for(c, (long)m * m, kBlock), kBlock, 0, s>>>((long)m * m, C.E.p, C.Einv32.p);
     OFEA_CHECK_LAUNCH();
-    C.lmax = estimate_lambda_max(c, 12);
+    C.lmax = estimate_lambda_max(c, 10);
     C.K_ok = true;
 }
 
