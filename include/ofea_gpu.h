@@ -153,6 +153,53 @@ OFEA_API int ofea_solve_device(ofea_ctx *ctx, const double *d_f, double *d_u, co
 OFEA_API int ofea_residual_norms_noalloc(ofea_ctx *ctx, int nrhs, const double *d_f,
                                          const double *d_u, double *d_norms);
 
+/* ---- learned coarse-correction stage -------------------------------------- */
+/* No counterpart in the reference.  A 4-layer message-passing network (hidden
+ * width 64, FP32 weights and accumulation) on the graph of nested aggregates
+ * (cells half as wide as the exact coarse level's) maps the restricted
+ * residual to a rigid-body-mode correction; OFEA_SOLVER_LEARNED adds it to the
+ * mixed V-cycle.  Trained on the GPU by this library's forward/backward/Adam
+ * kernels from the residuals of plain-PCG iterates on the current K, with the
+ * energy loss whose minimiser is the level's exact Galerkin correction.  A
+ * LEARNED solve whose FP64 true residual misses rtol is redone by plain
+ * PCG64 (stats.rejected_learned = 1). */
+typedef struct {
+    int sample_iters;  /* plain-PCG iterations whose residuals are sampled (600) */
+    int sample_every;  /* one sample every this many iterations (4) */
+    int steps;         /* Adam steps (400) */
+    int batch;         /* samples per step (16) */
+    float lr;          /* learning rate (1e-3) */
+    unsigned seed;     /* weight initialisation and batch order (1234) */
+    int reset;         /* 1: re-initialise the weights before training (0) */
+} ofea_learn_opts;
+
+typedef struct {
+    int samples;
+    int steps;
+    double loss_first; /* energy loss of the first and the last batch */
+    double loss_last;
+    double seconds;    /* wall time of sampling + training */
+} ofea_learn_stats;
+
+OFEA_API void ofea_learn_opts_default(ofea_learn_opts *opts);
+/* f: load of the sampling solves (n host values); NULL: a seeded random load. */
+OFEA_API int ofea_learned_train(ofea_ctx *ctx, const double *f, const ofea_learn_opts *opts,
+                                ofea_learn_stats *stats);
+/* Flat FP32 weight vector: count in *count; w may be NULL to query the size. */
+OFEA_API int ofea_learned_get_weights(ofea_ctx *ctx, float *w, long long *count);
+OFEA_API int ofea_learned_set_weights(ofea_ctx *ctx, const float *w, long long count);
+OFEA_API int ofea_learned_save(ofea_ctx *ctx, const char *path);
+OFEA_API int ofea_learned_load(ofea_ctx *ctx, const char *path);
+/* The nested level of the current K, for checking: na aggregates, the
+ * 27-slot neighbour table (na x 27, -1 = none, slot (dx+1)*9+(dy+1)*3+(dz+1)),
+ * the Jacobi-scaled coarse blocks Ehat (na x 27 x 6 x 6) and the stiffness
+ * feature (na).  Arrays may be NULL to query na. */
+OFEA_API int ofea_learned_level(ofea_ctx *ctx, int *na, int *nbr, float *Ehat, float *feat);
+/* Energy loss (sum over the batch) and its gradient w.r.t. every weight for
+ * given network inputs x (batch x na x 6, scaled residuals). */
+OFEA_API int ofea_learned_gradient(ofea_ctx *ctx, const float *x, int batch, double *loss,
+                                   float *grad);
+
 /* ---- measurement ------------------------------------------------------- */
 /* No counterpart in the reference (it only prints clock() spans): times the
  * solver's two per-iteration kernels (A: p update + SpMV + p.q, B: vector

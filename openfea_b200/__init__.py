@@ -54,6 +54,18 @@ class SolveStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class LearnOpts(ctypes.Structure):
+    _fields_ = [("sample_iters", _I), ("sample_every", _I), ("steps", _I), ("batch", _I),
+                ("lr", ctypes.c_float), ("seed", ctypes.c_uint), ("reset", _I)]
+
+
+class LearnStats(ctypes.Structure):
+    _fields_ = [("samples", _I), ("steps", _I), ("loss_first", _D), ("loss_last", _D), ("seconds", _D)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -95,6 +107,14 @@ def lib():
         "ofea_write_vtk": (_I, [ctypes.c_char_p, _I, _P, _I, _P, _P, _P, _D]),
         "ofea_profile_solver_kernels": (_I, [_P, _I, _I, _P, _P]),
         "ofea_precond_reset": (_I, [_P]),
+        "ofea_learn_opts_default": (None, [_P]),
+        "ofea_learned_train": (_I, [_P, _P, _P, _P]),
+        "ofea_learned_get_weights": (_I, [_P, _P, ctypes.POINTER(_LL)]),
+        "ofea_learned_set_weights": (_I, [_P, _P, _LL]),
+        "ofea_learned_save": (_I, [_P, ctypes.c_char_p]),
+        "ofea_learned_load": (_I, [_P, ctypes.c_char_p]),
+        "ofea_learned_level": (_I, [_P, ctypes.POINTER(_I), _P, _P, _P]),
+        "ofea_learned_gradient": (_I, [_P, _P, _I, ctypes.POINTER(_D), _P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -232,6 +252,56 @@ class Context:
                "ofea_profile_solver_kernels")
         return ms, by
 
+    # ---- learned coarse-correction stage
+    def learned_train(self, f=None, sample_iters=600, sample_every=4, steps=400, batch=16, lr=1e-3,
+                      seed=1234, reset=False):
+        o = LearnOpts()
+        lib().ofea_learn_opts_default(ctypes.byref(o))
+        o.sample_iters, o.sample_every, o.steps, o.batch = sample_iters, sample_every, steps, batch
+        o.lr, o.seed, o.reset = lr, seed, int(bool(reset))
+        st = LearnStats()
+        fa = _f64(f) if f is not None else None
+        _check(lib().ofea_learned_train(self.h, _ptr(fa), ctypes.byref(o), ctypes.byref(st)),
+               "ofea_learned_train")
+        return st.as_dict()
+
+    def learned_weights(self):
+        n = _LL()
+        _check(lib().ofea_learned_get_weights(self.h, None, ctypes.byref(n)), "ofea_learned_get_weights")
+        w = np.zeros(n.value, dtype=np.float32)
+        _check(lib().ofea_learned_get_weights(self.h, _ptr(w), ctypes.byref(n)), "ofea_learned_get_weights")
+        return w
+
+    def set_learned_weights(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(lib().ofea_learned_set_weights(self.h, _ptr(w), w.size), "ofea_learned_set_weights")
+
+    def learned_save(self, path):
+        _check(lib().ofea_learned_save(self.h, str(path).encode()), "ofea_learned_save")
+
+    def learned_load(self, path):
+        _check(lib().ofea_learned_load(self.h, str(path).encode()), "ofea_learned_load")
+
+    def learned_level(self):
+        na = _I()
+        _check(lib().ofea_learned_level(self.h, ctypes.byref(na), None, None, None), "ofea_learned_level")
+        nbr = np.zeros((na.value, 27), dtype=np.int32)
+        E = np.zeros((na.value, 27, 6, 6), dtype=np.float32)
+        feat = np.zeros(na.value, dtype=np.float32)
+        _check(lib().ofea_learned_level(self.h, ctypes.byref(na), _ptr(nbr), _ptr(E), _ptr(feat)),
+               "ofea_learned_level")
+        return nbr, E, feat
+
+    def learned_gradient(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        n = _LL()
+        _check(lib().ofea_learned_get_weights(self.h, None, ctypes.byref(n)), "ofea_learned_get_weights")
+        g = np.zeros(n.value, dtype=np.float32)
+        loss = _D()
+        _check(lib().ofea_learned_gradient(self.h, _ptr(x), x.shape[0], ctypes.byref(loss), _ptr(g)),
+               "ofea_learned_gradient")
+        return loss.value, g
+
     def solve_device(self, f_ptr, u_ptr, method="GPU_PCG", rtol=1e-8, **kw):
         o = solve_opts(method, rtol, **kw)
         st = SolveStats()
@@ -341,10 +411,10 @@ class AssambleStiffness:
 
 def solution_api(item_ass: AssambleStiffness, data: DataManagement, solver_type: str, rtol=1e-8):
     """solution_api (src/linear_solution.cpp:17-64) with the GPU solvers:
-    "GPU_PCG" (FP64) or "GPU_MIXED".  Returns False for an unknown solver
+    "GPU_PCG" (FP64), "GPU_MIXED" or "GPU_LEARNED" (after learned_train).  Returns False for an unknown solver
     string, as the reference does; raises on solver failure (the reference
     exits)."""
-    if solver_type not in ("GPU_PCG", "GPU_MIXED"):
+    if solver_type not in ("GPU_PCG", "GPU_MIXED", "GPU_LEARNED"):
         return False
     u, st = item_ass.ctx.solve(data.single_load_vec_, method=solver_type, rtol=rtol)
     data.single_dis_vec_ = u

@@ -1,11 +1,15 @@
 // C ABI entry points (include/ofea_gpu.h).  Every function catches internal
 // failures and returns a status code; nothing throws or exits across the ABI.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
+#include <fstream>
 #include <mutex>
+#include <random>
 
 #include "ofea_internal.cuh"
+#include "precond.cuh"
 
 namespace ofea {
 
@@ -167,6 +171,7 @@ int ofea_mesh_upload(ofea_ctx *c, int nd, const double *xyz, int ne, const int *
         use_device(c);
         c->mesh_ok = c->pattern_ok = c->K_ok = c->sell_ok = false;
         c->coarse.geom_ok = c->coarse.K_ok = false;
+        c->coarse2.geom_ok = c->coarse2.K_ok = false;
         c->nd = nd;
         c->ne = ne;
         c->E0 = E0;
@@ -239,6 +244,7 @@ int ofea_mesh_set_modulus(ofea_ctx *c, const double *E_elem, double E0) {
         OFEA_CUDA(cudaStreamSynchronize(c->stream));
         c->K_ok = c->sell_ok = false;
         c->coarse.K_ok = false;
+        c->coarse2.K_ok = false;
     });
 }
 
@@ -368,7 +374,7 @@ static std::string fmt_e(double v) {
 static void check_solve_ready(ofea_ctx *c, const ofea_solve_opts &o) {
     need(c->K_ok, OFEA_ERR_STATE, "K not assembled");
     need(o.rtol > 0 && o.max_iter > 0, OFEA_ERR_INVALID_ARG, "rtol and max_iter must be positive");
-    if (o.method != OFEA_SOLVER_PCG64 && o.method != OFEA_SOLVER_MIXED)
+    if (o.method != OFEA_SOLVER_PCG64 && o.method != OFEA_SOLVER_MIXED && o.method != OFEA_SOLVER_LEARNED)
         fail(OFEA_ERR_UNKNOWN_SOLVER, "unknown solver method");
     if (!c->jacobi_ok) fail(OFEA_ERR_BREAKDOWN, "a diagonal block of K is not positive definite");
 }
@@ -377,6 +383,7 @@ int ofea_precond_reset(ofea_ctx *c) {
     return guarded([&] {
         need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
         c->coarse.K_ok = false;
+        c->coarse2.K_ok = false;
     });
 }
 
@@ -440,6 +447,151 @@ int ofea_solve(ofea_ctx *c, const double *f, double *u, int nrhs, const ofea_sol
         return rc;
     }
     return worst;
+}
+
+void ofea_learn_opts_default(ofea_learn_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->sample_iters = 600;
+    o->sample_every = 4;
+    o->steps = 400;
+    o->batch = 16;
+    o->lr = 1e-3f;
+    o->seed = 1234u;
+}
+
+static void prepare_learned_level(ofea_ctx *c) {
+    need(c->K_ok, OFEA_ERR_STATE, "K not assembled");
+    use_device(c);
+    setup_coarse(c, c->coarse_nodes);
+    setup_learned_level(c);
+}
+
+int ofea_learned_train(ofea_ctx *c, const double *f, const ofea_learn_opts *opts, ofea_learn_stats *stats) {
+    return guarded([&] {
+        need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
+        ofea_learn_opts o;
+        if (opts) o = *opts;
+        else ofea_learn_opts_default(&o);
+        need(o.sample_iters > 0 && o.sample_every > 0 && o.steps >= 0 && o.batch > 0 && o.lr > 0,
+             OFEA_ERR_INVALID_ARG, "bad training options");
+        const auto t0 = std::chrono::steady_clock::now();
+        prepare_learned_level(c);
+        Learned &N = c->learned;
+        if (o.reset || !N.have_weights) N.init_weights(o.seed);
+        const int n = c->n;
+        c->w.f.ensure(std::max(n, 1));
+        c->w.u.ensure(std::max(n, 1));
+        std::vector<double> hf(n);
+        if (f) {
+            std::copy(f, f + n, hf.begin());
+        } else {
+            std::mt19937 rng(o.seed);
+            std::normal_distribution<double> nd(0.0, 1.0);
+            for (double &v : hf) v = nd(rng);
+        }
+        OFEA_CUDA(cudaMemcpyAsync(c->w.f.p, hf.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+        OFEA_CUDA(cudaMemsetAsync(c->w.u.p, 0, sizeof(double) * n, c->stream));
+        learned_begin_dataset(c, o.sample_iters / o.sample_every + 2);
+        ofea_solve_opts so;
+        ofea_solve_opts_default(&so);
+        so.method = OFEA_SOLVER_PCG64;
+        so.rtol = 1e-14;  // run the full sampling budget
+        so.max_iter = o.sample_iters;
+        so.check_every = o.sample_every;
+        ofea_solve_stats st{};
+        solve_device(c, c->w.f.p, c->w.u.p, so, st, [&](const double *r) { learned_add_sample(c, r); });
+        double l0 = 0, l1 = 0;
+        if (o.steps > 0) learned_train(c, o.steps, o.batch, o.lr, o.seed, &l0, &l1);
+        if (stats) {
+            stats->samples = N.nsamples;
+            stats->steps = o.steps;
+            stats->loss_first = l0;
+            stats->loss_last = l1;
+            stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        }
+    });
+}
+
+int ofea_learned_get_weights(ofea_ctx *c, float *w, long long *count) {
+    return guarded([&] {
+        need(c != nullptr && count != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
+        const size_t n = Learned::layout().total;
+        *count = (long long)n;
+        if (!w) return;
+        Learned &N = c->learned;
+        if (!N.have_weights) N.init_weights(1234u);
+        std::copy(N.host_w.begin(), N.host_w.end(), w);
+    });
+}
+
+int ofea_learned_set_weights(ofea_ctx *c, const float *w, long long count) {
+    return guarded([&] {
+        need(c != nullptr && w != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
+        need(count == (long long)Learned::layout().total, OFEA_ERR_INVALID_ARG, "weight count mismatch");
+        Learned &N = c->learned;
+        N.host_w.assign(w, w + count);
+        N.have_weights = true;
+        N.uploaded = false;
+    });
+}
+
+int ofea_learned_save(ofea_ctx *c, const char *path) {
+    return guarded([&] {
+        need(c != nullptr && path != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
+        need(c->learned.have_weights, OFEA_ERR_STATE, "no weights");
+        std::ofstream o(path, std::ios::binary);
+        if (!o) fail(OFEA_ERR_IO, std::string("cannot write ") + path);
+        const long long n = (long long)c->learned.host_w.size();
+        o.write("OFEAGNN1", 8);
+        o.write(reinterpret_cast<const char *>(&n), sizeof(n));
+        o.write(reinterpret_cast<const char *>(c->learned.host_w.data()), sizeof(float) * n);
+        if (!o) fail(OFEA_ERR_IO, std::string("cannot write ") + path);
+    });
+}
+
+int ofea_learned_load(ofea_ctx *c, const char *path) {
+    return guarded([&] {
+        need(c != nullptr && path != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
+        std::ifstream in(path, std::ios::binary);
+        if (!in) fail(OFEA_ERR_IO, std::string("cannot read ") + path);
+        char magic[8];
+        long long n = 0;
+        in.read(magic, 8);
+        in.read(reinterpret_cast<char *>(&n), sizeof(n));
+        if (!in || std::memcmp(magic, "OFEAGNN1", 8) != 0 || n != (long long)Learned::layout().total)
+            fail(OFEA_ERR_IO, std::string("not a weight file of this network: ") + path);
+        std::vector<float> w(n);
+        in.read(reinterpret_cast<char *>(w.data()), sizeof(float) * n);
+        if (!in) fail(OFEA_ERR_IO, std::string("truncated weight file: ") + path);
+        c->learned.host_w = std::move(w);
+        c->learned.have_weights = true;
+        c->learned.uploaded = false;
+    });
+}
+
+int ofea_learned_level(ofea_ctx *c, int *na, int *nbr, float *Ehat, float *feat) {
+    return guarded([&] {
+        need(c != nullptr && na != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
+        prepare_learned_level(c);
+        const Coarse &C2 = c->coarse2;
+        *na = C2.na;
+        cudaStream_t s = c->stream;
+        if (nbr) OFEA_CUDA(cudaMemcpyAsync(nbr, C2.nbr.p, sizeof(int) * 27 * C2.na, cudaMemcpyDeviceToHost, s));
+        if (Ehat)
+            OFEA_CUDA(cudaMemcpyAsync(Ehat, c->learned.Ehat.p, sizeof(float) * 27 * 36 * C2.na,
+                                      cudaMemcpyDeviceToHost, s));
+        if (feat) OFEA_CUDA(cudaMemcpyAsync(feat, c->learned.feat.p, sizeof(float) * C2.na, cudaMemcpyDeviceToHost, s));
+        OFEA_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int ofea_learned_gradient(ofea_ctx *c, const float *x, int batch, double *loss, float *grad) {
+    return guarded([&] {
+        need(c != nullptr && x && loss && grad && batch > 0, OFEA_ERR_INVALID_ARG, "bad argument");
+        prepare_learned_level(c);
+        learned_gradient(c, x, batch, loss, grad);
+    });
 }
 
 int ofea_residual_norms_noalloc(ofea_ctx *c, int nrhs, const double *d_f, const double *d_u,

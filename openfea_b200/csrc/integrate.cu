@@ -512,6 +512,7 @@ static void gather(ofea_ctx *c, bool with_f, double *d_fint) {
     c->K_ok = true;
     c->sell_ok = false;
     c->coarse.K_ok = false;
+    c->coarse2.K_ok = false;
 }
 
 void assemble_linear(ofea_ctx *c) {

@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -121,10 +122,30 @@ struct Coarse {
     bool geom_ok = false, K_ok = false;
     int target = 0, na = 0, m = 0, max_agg = 0;
     int nc[3] = {1, 1, 1};
+    double lo[3] = {0, 0, 0}, ext[3] = {0, 0, 0};
     double inv_scale = 1.0, lmax = 0.0;
-    DevBuf<int> agg_of, agg_ptr, agg_nodes, agg_cell, cell_agg;
+    DevBuf<int> agg_of, agg_ptr, agg_nodes, agg_cell, cell_agg, nbr;
     DevBuf<double> centroid, E, S, P, diag0, pp, part;
     DevBuf<float> Einv32, cvec, evec, pw;
+};
+
+// Learned coarse-correction stage (learned.cu): network weights, Adam state,
+// per-K data of the nested level and activation buffers.
+struct Learned {
+    struct Layout {
+        size_t W0, b0, W[4], b[4], Wd, bd, total;
+    };
+    static Layout layout();
+    void init_weights(unsigned seed);
+    std::vector<float> host_w;
+    bool have_weights = false, uploaded = false;
+    int trained_steps = 0;
+    DevBuf<float> w, g, m, v, part;
+    DevBuf<double> Eb, sigma, lossp;
+    DevBuf<float> Ehat, dsq, feat;
+    DevBuf<float> X, Z0, H[5], A[4], Zl[4], Y, Yz, dY, dH, dZ, dA, batch_src, r32, data;
+    long cap_rows = 0;
+    int nlossp = 0, nsamples = 0, max_samples = 0;
 };
 
 }  // namespace ofea
@@ -160,7 +181,9 @@ struct ofea_ctx {
     ofea::DevBuf<float> sv32;
     long long sell_len = 0;
     bool sell_ok = false;
-    ofea::Coarse coarse;
+    ofea::Coarse coarse;      // exact coarse level
+    ofea::Coarse coarse2;     // nested finer level of the learned stage
+    ofea::Learned learned;
     int coarse_nodes = 1000;  // target free nodes per aggregate
     ofea::SolverWork w;
     ofea::DevBuf<int> scratch_i;
@@ -180,8 +203,16 @@ void build_sell(ofea_ctx *c);
 // solve.cu
 void spmv64(ofea_ctx *c, const double *d_x, double *d_y);
 void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_opts &o,
-                  ofea_solve_stats &st);
+                  ofea_solve_stats &st, const std::function<void(const double *)> &on_chunk = {});
 void profile_kernels(ofea_ctx *c, int method, int reps, double *ms, double *bytes);
+// learned.cu
+void setup_learned_level(ofea_ctx *c);
+void learned_prepare_inference(ofea_ctx *c);
+void learned_apply(ofea_ctx *c, const float *t, float *x);
+void learned_begin_dataset(ofea_ctx *c, int max_samples);
+void learned_add_sample(ofea_ctx *c, const double *d_r);
+void learned_train(ofea_ctx *c, int steps, int batch, float lr, unsigned seed, double *loss0, double *loss1);
+void learned_gradient(ofea_ctx *c, const float *h_x, int B, double *loss, float *h_grad);
 // noalloc.cu
 void residual_norms_noalloc(ofea_ctx *c, int nrhs, const double *d_f, const double *d_u,
                             double *d_norms);

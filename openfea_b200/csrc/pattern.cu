@@ -334,6 +334,8 @@ void build_pattern(ofea_ctx *c) {
     c->sell_ok = false;
     c->coarse.geom_ok = false;
     c->coarse.K_ok = false;
+    c->coarse2.geom_ok = false;
+    c->coarse2.K_ok = false;
 }
 
 }  // namespace ofea

@@ -28,57 +28,18 @@ namespace ofea {
 
 // ---------------------------------------------------------- aggregation --
 
-void build_aggregation(ofea_ctx *c, int target_nodes) {
-    Coarse &C = c->coarse;
+// Bins the free nodes into the nc[0] x nc[1] x nc[2] cell grid over [lo, lo+ext]
+// and fills C's aggregate arrays (non-empty cells in cell order, nodes in
+// ascending free index, centroids, the cell -> aggregate table and, for the
+// learned level, the 27-slot neighbour table).
+static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3], const double ext[3]) {
     const int nd = c->nd, nf = c->nfree;
     const std::vector<double> &X = c->xyz_h;
     const std::vector<int> &fm = c->fm_h;
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     std::vector<int> nof(nf);
     for (int i = 0; i < nd; ++i)
-        if (fm[i] >= 0) {
-            nof[fm[i]] = i;
-            for (int d = 0; d < 3; ++d) {
-                lo[d] = std::min(lo[d], X[3L * i + d]);
-                hi[d] = std::max(hi[d], X[3L * i + d]);
-            }
-        }
-    // largest element extent per direction: cells must be at least 2.5x wider
-    // so that every K coupling stays between neighbouring cells
-    double emax[3] = {0, 0, 0};
-    for (int e = 0; e < c->ne; ++e) {
-        const int *t = &c->topo_h[8L * e];
-        int npe = c->elem_type[e] == 1 ? 8 : 4;
-        for (int d = 0; d < 3; ++d) {
-            double a = 1e300, b = -1e300;
-            for (int k = 0; k < npe; ++k) {
-                a = std::min(a, X[3L * t[k] + d]);
-                b = std::max(b, X[3L * t[k] + d]);
-            }
-            emax[d] = std::max(emax[d], b - a);
-        }
-    }
-    double ext[3], vol = 1.0;
-    int flat = 0;
-    for (int d = 0; d < 3; ++d) {
-        ext[d] = hi[d] - lo[d];
-        if (ext[d] > 0) vol *= ext[d];
-        else ++flat;
-    }
-    const double target = std::max(8, target_nodes);
-    double s = std::pow(vol * target / std::max(nf, 1), 1.0 / std::max(1, 3 - flat));
-    int nc[3];
-    for (int d = 0; d < 3; ++d) {
-        if (!(ext[d] > 0)) {
-            nc[d] = 1;
-            continue;
-        }
-        double cell = std::max(s, 2.5 * emax[d]);
-        nc[d] = std::max(1, (int)std::lround(ext[d] / cell));
-    }
-    C.nc[0] = nc[0];
-    C.nc[1] = nc[1];
-    C.nc[2] = nc[2];
+        if (fm[i] >= 0) nof[fm[i]] = i;
+    for (int d = 0; d < 3; ++d) C.nc[d] = nc[d];
     const long ncell = (long)nc[0] * nc[1] * nc[2];
     std::vector<int> cell_of(nf), cnt(ncell, 0);
     for (int r = 0; r < nf; ++r) {
@@ -119,6 +80,15 @@ void build_aggregation(ofea_ctx *c, int target_nodes) {
     C.m = 6 * na;
     C.max_agg = 0;
     for (int a = 0; a < na; ++a) C.max_agg = std::max(C.max_agg, ptr[a + 1] - ptr[a]);
+    // neighbour table: slot (dx+1)*9 + (dy+1)*3 + (dz+1), -1 where the cell is empty/outside
+    std::vector<int> nbr(27L * na, -1);
+    for (int a = 0; a < na; ++a)
+        for (int sl = 0; sl < 27; ++sl) {
+            const int x = agg_cell3[3 * a] + sl / 9 - 1, y = agg_cell3[3 * a + 1] + (sl / 3) % 3 - 1,
+                      z = agg_cell3[3 * a + 2] + sl % 3 - 1;
+            if (x < 0 || y < 0 || z < 0 || x >= nc[0] || y >= nc[1] || z >= nc[2]) continue;
+            nbr[27L * a + sl] = cell_agg[((long)x * nc[1] + y) * nc[2] + z];
+        }
     cudaStream_t st = c->stream;
     C.agg_of.upload(agg_of.data(), nf, st);
     C.agg_ptr.upload(ptr.data(), na + 1, st);
@@ -126,9 +96,72 @@ void build_aggregation(ofea_ctx *c, int target_nodes) {
     C.agg_cell.upload(agg_cell3.data(), agg_cell3.size(), st);
     C.cell_agg.upload(cell_agg.data(), ncell, st);
     C.centroid.upload(cen.data(), cen.size(), st);
+    C.nbr.upload(nbr.data(), nbr.size(), st);
     OFEA_CUDA(cudaStreamSynchronize(st));
     C.geom_ok = true;
     C.K_ok = false;
+}
+
+void build_aggregation(ofea_ctx *c, int target_nodes) {
+    Coarse &C = c->coarse;
+    const int nd = c->nd, nf = c->nfree;
+    const std::vector<double> &X = c->xyz_h;
+    const std::vector<int> &fm = c->fm_h;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int i = 0; i < nd; ++i)
+        if (fm[i] >= 0)
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = std::min(lo[d], X[3L * i + d]);
+                hi[d] = std::max(hi[d], X[3L * i + d]);
+            }
+    // largest element extent per direction: cells must be at least 2.5x wider
+    // so that every K coupling stays between neighbouring cells (the nested
+    // level, half as wide, then still spans an element)
+    double emax[3] = {0, 0, 0};
+    for (int e = 0; e < c->ne; ++e) {
+        const int *t = &c->topo_h[8L * e];
+        int npe = c->elem_type[e] == 1 ? 8 : 4;
+        for (int d = 0; d < 3; ++d) {
+            double a = 1e300, b = -1e300;
+            for (int k = 0; k < npe; ++k) {
+                a = std::min(a, X[3L * t[k] + d]);
+                b = std::max(b, X[3L * t[k] + d]);
+            }
+            emax[d] = std::max(emax[d], b - a);
+        }
+    }
+    double ext[3], vol = 1.0;
+    int flat = 0;
+    for (int d = 0; d < 3; ++d) {
+        ext[d] = hi[d] - lo[d];
+        if (ext[d] > 0) vol *= ext[d];
+        else ++flat;
+    }
+    const double target = std::max(8, target_nodes);
+    double s = std::pow(vol * target / std::max(nf, 1), 1.0 / std::max(1, 3 - flat));
+    int nc[3];
+    for (int d = 0; d < 3; ++d) {
+        if (!(ext[d] > 0)) {
+            nc[d] = 1;
+            continue;
+        }
+        double cell = std::max(s, 2.5 * emax[d]);
+        nc[d] = std::max(1, (int)std::lround(ext[d] / cell));
+    }
+    for (int d = 0; d < 3; ++d) {
+        C.lo[d] = lo[d];
+        C.ext[d] = ext[d];
+    }
+    bin_nodes(c, C, nc, lo, ext);
+}
+
+// The learned level: the same box, twice as many cells per direction, so each
+// coarse cell is the union of 2 x 2 x 2 of these.
+void build_aggregation_fine(ofea_ctx *c) {
+    const Coarse &C = c->coarse;
+    int nc[3];
+    for (int d = 0; d < 3; ++d) nc[d] = C.ext[d] > 0 ? 2 * C.nc[d] : 1;
+    bin_nodes(c, c->coarse2, nc, C.lo, C.ext);
 }
 
 // ------------------------------------------------------- coarse matrix --
@@ -526,6 +559,14 @@ static double estimate_lambda_max(ofea_ctx *c, int steps) {
 
 // ------------------------------------------------------------ setup entry --
 
+void coarse_E_partials(ofea_ctx *c, Coarse &C, int nchunk) {
+    k_coarse_E_chunks<<<(int)std::min<long>((long)C.na * nchunk, (long)c->num_sms * 32), kEThreads, 0,
+                        c->stream>>>(C.na, nchunk, C.agg_ptr.p, C.agg_nodes.p, C.agg_of.p, C.agg_cell.p,
+                                     c->node_of_free.p, c->xyz.p, C.centroid.p, C.inv_scale, c->rowptr.p,
+                                     c->cols.p, c->Kb.p, C.part.p, c->err_flag.p);
+    OFEA_CHECK_LAUNCH();
+}
+
 void setup_coarse(ofea_ctx *c, int target_nodes) {
     Coarse &C = c->coarse;
     if (!C.geom_ok || C.target != target_nodes) {
@@ -543,9 +584,7 @@ void setup_coarse(ofea_ctx *c, int target_nodes) {
     OFEA_CUDA(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), s));
     const int nchunk = (C.max_agg + kChunkNodes - 1) / kChunkNodes;
     C.part.ensure((size_t)C.na * nchunk * 27 * 36);
-    k_coarse_E_chunks<<<(int)std::min<long>((long)C.na * nchunk, (long)c->num_sms * 32), kEThreads, 0, s>>>(
-        C.na, nchunk, C.agg_ptr.p, C.agg_nodes.p, C.agg_of.p, C.agg_cell.p, c->node_of_free.p, c->xyz.p,
-        C.centroid.p, C.inv_scale, c->rowptr.p, c->cols.p, c->Kb.p, C.part.p, c->err_flag.p);
+    coarse_E_partials(c, C, nchunk);
     k_coarse_E_sum<<<grid_for(c, (long)C.na * 27 * 36, kBlock), kBlock, 0, s>>>(
         C.na, nchunk, C.agg_cell.p, C.cell_agg.p, C.nc[0], C.nc[1], C.nc[2], m, C.part.p, C.E.p);
     OFEA_CHECK_LAUNCH();
@@ -638,17 +677,25 @@ __global__ void k_prolong(int nfree, const int *__restrict__ agg_of, const int *
     }
 }
 
+void restrict_level(ofea_ctx *c, const Coarse &C, const float *t, float *cvec) {
+    k_restrict<<<std::min(C.na, c->num_sms * 8), kBlock, 0, c->stream>>>(
+        C.na, C.agg_ptr.p, C.agg_nodes.p, c->node_of_free.p, c->xyz.p, C.centroid.p, C.inv_scale, t, cvec);
+    OFEA_CHECK_LAUNCH();
+}
+
+void prolong_level(ofea_ctx *c, const Coarse &C, const float *g, float *x) {
+    k_prolong<<<grid_for(c, c->nfree, kBlock), kBlock, 0, c->stream>>>(
+        c->nfree, C.agg_of.p, c->node_of_free.p, c->xyz.p, C.centroid.p, C.inv_scale, g, x);
+    OFEA_CHECK_LAUNCH();
+}
+
 void coarse_correct(ofea_ctx *c, const float *t, float *x) {
     Coarse &C = c->coarse;
-    cudaStream_t s = c->stream;
-    k_restrict<<<std::min(C.na, c->num_sms * 8), kBlock, 0, s>>>(C.na, C.agg_ptr.p, C.agg_nodes.p,
-                                                                 c->node_of_free.p, c->xyz.p,
-                                                                 C.centroid.p, C.inv_scale, t, C.cvec.p);
-    k_coarse_gemv<<<grid_for(c, (long)C.m * 32, kBlock), kBlock, 0, s>>>(C.m, C.Einv32.p, C.cvec.p, C.evec.p);
-    k_prolong<<<grid_for(c, c->nfree, kBlock), kBlock, 0, s>>>(c->nfree, C.agg_of.p, c->node_of_free.p,
-                                                               c->xyz.p, C.centroid.p, C.inv_scale,
-                                                               C.evec.p, x);
+    restrict_level(c, C, t, C.cvec.p);
+    k_coarse_gemv<<<grid_for(c, (long)C.m * 32, kBlock), kBlock, 0, c->stream>>>(C.m, C.Einv32.p, C.cvec.p,
+                                                                                 C.evec.p);
     OFEA_CHECK_LAUNCH();
+    prolong_level(c, C, C.evec.p, x);
 }
 
 void vc_resid(ofea_ctx *c, const float *b, const float *x, float *t) {

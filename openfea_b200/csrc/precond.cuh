@@ -5,6 +5,7 @@
 namespace ofea {
 
 void build_aggregation(ofea_ctx *c, int target_nodes);
+void build_aggregation_fine(ofea_ctx *c);
 // Aggregation (once per mesh), E = Z^T K Z, its inverse and lambda_max(D^-1 K)
 // (once per K).
 void setup_coarse(ofea_ctx *c, int target_nodes);
@@ -12,5 +13,10 @@ void setup_coarse(ofea_ctx *c, int target_nodes);
 void coarse_correct(ofea_ctx *c, const float *t, float *x);
 // t = b - K32 x
 void vc_resid(ofea_ctx *c, const float *b, const float *x, float *t);
+// Level-generic pieces (also used by the learned level):
+// cvec = Z^T t, x += Z g, and the chunk partials of Z^T K Z into C.part.
+void restrict_level(ofea_ctx *c, const Coarse &C, const float *t, float *cvec);
+void prolong_level(ofea_ctx *c, const Coarse &C, const float *g, float *x);
+void coarse_E_partials(ofea_ctx *c, Coarse &C, int nchunk);
 
 }  // namespace ofea

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <functional>
 
 #include "precond.cuh"
 #include "sell.cuh"
@@ -404,7 +405,8 @@ double now_s() {
 // device flags say done, max_iter is reached or the time budget runs out.
 template <class ChunkFn>
 void drive(ofea_ctx *c, const ofea_solve_opts &o, Workspace &ws, int per_chunk, ChunkFn chunk,
-           Flags &hf, long long &launches, int kernels_per_iter, bool &timed_out, double t_start) {
+           Flags &hf, long long &launches, int kernels_per_iter, bool &timed_out, double t_start,
+           const std::function<void()> &after_chunk) {
     cudaStream_t s = c->stream;
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
@@ -432,6 +434,7 @@ void drive(ofea_ctx *c, const ofea_solve_opts &o, Workspace &ws, int per_chunk, 
             OFEA_CUDA(cudaMemcpyAsync(h, ws.fl, sizeof(Flags), cudaMemcpyDeviceToHost, s));
             OFEA_CUDA(cudaStreamSynchronize(s));
             if (h->done || launched >= o.max_iter) break;
+            if (after_chunk) after_chunk();
             if (o.time_budget_s > 0 && now_s() - t_start > o.time_budget_s) {
                 timed_out = true;
                 break;
@@ -459,7 +462,7 @@ float smoother_weight(const ofea_ctx *c) {
 }  // namespace
 
 void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_opts &o,
-                  ofea_solve_stats &st) {
+                  ofea_solve_stats &st, const std::function<void(const double *)> &on_chunk) {
     cudaStream_t s = c->stream;
     const int n = c->n, nf = c->nfree;
     if (n == 0) {
@@ -485,13 +488,19 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
     w.q.ensure(n);
     w.p0.ensure(n);
     w.p1.ensure(n);
-    const bool mixed = o.method == OFEA_SOLVER_MIXED;
+    const bool learned = o.method == OFEA_SOLVER_LEARNED;
+    const bool mixed = o.method == OFEA_SOLVER_MIXED || learned;
     float setup_ms = 0.f;
     if (mixed) {
         const bool had = c->coarse.K_ok;
         cudaEvent_t es;
         OFEA_CUDA(cudaEventCreate(&es));
         setup_coarse(c, c->coarse_nodes);
+        if (learned) {
+            if (!c->learned.have_weights) fail(OFEA_ERR_STATE, "train or load the learned stage first");
+            setup_learned_level(c);
+            learned_prepare_inference(c);
+        }
         OFEA_CUDA(cudaEventRecord(es, s));
         OFEA_CUDA(cudaEventSynchronize(es));
         OFEA_CUDA(cudaEventElapsedTime(&setup_ms, e0, es));
@@ -546,6 +555,7 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
             k_set_itB<<<1, 1, 0, s>>>(ws.fl, -1);
             vc_resid(c, w.b32.p, w.x32.p, w.t32.p);
             coarse_correct(c, w.t32.p, w.x32.p);
+            if (learned) learned_apply(c, w.t32.p, w.x32.p);
             k_fcg_post<<<G, kBlock, 0, s>>>(nf, c->sl_ptr.p, c->scols.p, c->sv32.p, c->Dinv32.p, wsm, w.b32.p,
                                             w.x32.p, w.r.p, w.z32a.p, w.z32b.p, ws.P, ws.fl);
             OFEA_CHECK_LAUNCH();
@@ -558,12 +568,13 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
                                                  w.b32.p, w.x32.p, ws.P, ws.fl);
                     vc_resid(c, w.b32.p, w.x32.p, w.t32.p);
                     coarse_correct(c, w.t32.p, w.x32.p);
+                    if (learned) learned_apply(c, w.t32.p, w.x32.p);
                     k_fcg_post<<<G, kBlock, 0, s>>>(nf, c->sl_ptr.p, c->scols.p, c->sv32.p, c->Dinv32.p, wsm,
                                                     w.b32.p, w.x32.p, w.r.p, w.z32a.p, w.z32b.p, ws.P, ws.fl);
                 }
                 OFEA_CHECK_LAUNCH();
             };
-            drive(c, oo, ws, per_chunk, chunk, hf, launches, 7, timed_out, t_start);
+            drive(c, oo, ws, per_chunk, chunk, hf, launches, learned ? 7 + 15 : 7, timed_out, t_start, {});
         } else {
             auto chunk = [&](int iters) {
                 for (int it = 0; it < iters; ++it) {
@@ -574,7 +585,9 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
                 }
                 OFEA_CHECK_LAUNCH();
             };
-            drive(c, oo, ws, per_chunk, chunk, hf, launches, 2, timed_out, t_start);
+            std::function<void()> after;
+            if (on_chunk) after = [&] { on_chunk(w.r.p); };
+            drive(c, oo, ws, per_chunk, chunk, hf, launches, 2, timed_out, t_start, after);
         }
         total_iters += hf.iters;
         if (hf.status == OFEA_ERR_BREAKDOWN) break;
@@ -597,6 +610,21 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
         st.status = timed_out ? OFEA_ERR_TIMEOUT : OFEA_ERR_NOT_CONVERGED;
     else
         st.status = OFEA_OK;
+    if (learned && st.status != OFEA_OK) {
+        // The learned stage is judged by the FP64 true residual: it missed the
+        // target, so plain FP64 PCG restarts from zero and finishes the solve.
+        ofea_solve_opts plain = o;
+        plain.method = OFEA_SOLVER_PCG64;
+        ofea_solve_stats st2{};
+        OFEA_CUDA(cudaMemsetAsync(d_u, 0, sizeof(double) * n, s));
+        solve_device(c, d_f, d_u, plain, st2, {});
+        st2.iterations += st.iterations;
+        st2.seconds += st.seconds;
+        st2.setup_seconds += st.setup_seconds;
+        st2.kernel_launches += st.kernel_launches;
+        st2.rejected_learned = 1;
+        st = st2;
+    }
 }
 
 // Times the per-iteration kernels in isolation on the current state (after a

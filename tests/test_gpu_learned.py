@@ -1,0 +1,71 @@
+"""The learned coarse-correction stage on the GPU: gradients of the
+library's backward kernels against the CPU oracle (oracle/gnn_oracle.py),
+training, the gain over the same solver without the stage, and the FP64
+judge that rejects it in favour of plain PCG."""
+import numpy as np
+import pytest
+
+import openfea_b200 as ob
+from openfea_b200 import meshgen as mg
+from oracle.gnn_oracle import TOTAL, GNNOracle, he_weights
+
+pytestmark = pytest.mark.gpu
+
+
+def cantilever_ctx(factory, nx, ny, nz):
+    m, ffull = mg.cantilever_large(nx, ny, nz)
+    ctx = factory()
+    fm = ctx.upload_mesh(m)
+    ctx.assemble_pattern()
+    ctx.assemble_linear()
+    return ctx, mg.to_free(ffull, fm)
+
+
+def test_gradient_matches_cpu_oracle(gpu_ctx_factory):
+    ctx, f = cantilever_ctx(gpu_ctx_factory, 40, 10, 10)
+    nbr, E, feat = ctx.learned_level()
+    assert nbr.shape[0] >= 8
+    w = he_weights(5, out_gain=1.0).astype(np.float32)
+    ctx.set_learned_weights(w)
+    x = np.random.default_rng(6).normal(0, 1, (2, nbr.shape[0], 6)).astype(np.float32)
+    loss_g, g_gpu = ctx.learned_gradient(x)
+    net = GNNOracle(nbr, E.astype(np.float64), feat.astype(np.float64))
+    loss_c, g_cpu = net.grad(w.astype(np.float64), x.astype(np.float64))
+    assert g_gpu.size == TOTAL
+    # FP32 kernels against the FP64 oracle
+    assert abs(loss_g - loss_c) <= 1e-4 * abs(loss_c)
+    assert np.abs(g_gpu - g_cpu).max() <= 1e-4 * np.abs(g_cpu).max()
+
+
+def test_training_reduces_loss_and_stage_gains_iterations(gpu_ctx_factory):
+    ctx, f = cantilever_ctx(gpu_ctx_factory, 80, 20, 20)
+    u64, s64 = ctx.solve(f, method="GPU_PCG", rtol=1e-10)
+    um, sm = ctx.solve(f, method="GPU_MIXED", rtol=1e-8)
+    st = ctx.learned_train(sample_iters=400, sample_every=4, steps=300, batch=16, lr=1e-3)
+    assert st["samples"] >= 50
+    assert st["loss_last"] < st["loss_first"]
+    ul, sl = ctx.solve(f, method="GPU_LEARNED", rtol=1e-8)
+    assert sl["status"] == 0 and sl["rejected_learned"] == 0 and sl["rel_residual"] <= 1e-8
+    assert np.linalg.norm(ul - u64) / np.linalg.norm(u64) < 1e-6
+    # what the trained stage gains over the same solver without it
+    assert sl["iterations"] < sm["iterations"], (sl["iterations"], sm["iterations"])
+
+
+def test_rejected_stage_falls_back_to_plain_pcg(gpu_ctx_factory, tmp_path):
+    ctx, f = cantilever_ctx(gpu_ctx_factory, 40, 10, 10)
+    ctx.learned_train(sample_iters=64, sample_every=4, steps=5, batch=4)
+    w = ctx.learned_weights()
+    ctx.learned_save(tmp_path / "w.bin")
+    bad = np.full_like(w, np.nan)
+    ctx.set_learned_weights(bad)
+    u, st = ctx.solve(f, method="GPU_LEARNED", rtol=1e-8, max_iter=4000)
+    assert st["rejected_learned"] == 1 and st["status"] == 0 and st["rel_residual"] <= 1e-8
+    ctx.learned_load(tmp_path / "w.bin")
+    assert np.array_equal(ctx.learned_weights(), w)
+
+
+def test_learned_solve_needs_weights(gpu_ctx_factory):
+    ctx, f = cantilever_ctx(gpu_ctx_factory, 20, 4, 4)
+    with pytest.raises(ob.OfeaError) as e:
+        ctx.solve(f, method="GPU_LEARNED")
+    assert e.value.code == -6
