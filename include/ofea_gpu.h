@@ -154,15 +154,20 @@ OFEA_API int ofea_residual_norms_noalloc(ofea_ctx *ctx, int nrhs, const double *
                                          const double *d_u, double *d_norms);
 
 /* ---- learned coarse-correction stage -------------------------------------- */
-/* No counterpart in the reference.  A 4-layer message-passing network (hidden
- * width 64, FP32 weights and accumulation) on the graph of nested aggregates
- * (cells half as wide as the exact coarse level's) maps the restricted
- * residual to a rigid-body-mode correction; OFEA_SOLVER_LEARNED adds it to the
- * mixed V-cycle.  Trained on the GPU by this library's forward/backward/Adam
+/* No counterpart in the reference.  OFEA_SOLVER_LEARNED adds a second coarse
+ * stage to the mixed V-cycle, on nested aggregates (cells half as wide as the
+ * exact coarse level's): the level's residual, with the exact coarse
+ * correction taken out, is mapped to rigid-body-mode corrections by
+ * y = s * M(s * x), M a degree-2 polynomial in the block-Jacobi-preconditioned
+ * level operator with trainable coefficients, s per-aggregate scalings set by
+ * a 4-layer message-passing network (hidden width 64, FP32 weights and
+ * accumulation) from the aggregates' features.  The stage is linear and
+ * symmetric.  Trained on the GPU by this library's forward/backward/Adam
  * kernels from the residuals of plain-PCG iterates on the current K, with the
  * energy loss whose minimiser is the level's exact Galerkin correction.  A
  * LEARNED solve whose FP64 true residual misses rtol is redone by plain
  * PCG64 (stats.rejected_learned = 1). */
+#define OFEA_LEARN_NFEAT 8 /* features per aggregate */
 typedef struct {
     int sample_iters;  /* plain-PCG iterations whose residuals are sampled (600) */
     int sample_every;  /* one sample every this many iterations (4) */
@@ -176,8 +181,8 @@ typedef struct {
 typedef struct {
     int samples;
     int steps;
-    double loss_first; /* energy loss of the first and the last batch */
-    double loss_last;
+    double loss_first; /* energy loss of the first batch before the first step */
+    double loss_last;  /* ... and of the same batch after the last step */
     double seconds;    /* wall time of sampling + training */
 } ofea_learn_stats;
 
@@ -192,11 +197,13 @@ OFEA_API int ofea_learned_save(ofea_ctx *ctx, const char *path);
 OFEA_API int ofea_learned_load(ofea_ctx *ctx, const char *path);
 /* The nested level of the current K, for checking: na aggregates, the
  * 27-slot neighbour table (na x 27, -1 = none, slot (dx+1)*9+(dy+1)*3+(dz+1)),
- * the Jacobi-scaled coarse blocks Ehat (na x 27 x 6 x 6) and the stiffness
- * feature (na).  Arrays may be NULL to query na. */
+ * the Jacobi-scaled coarse blocks Ehat (na x 27 x 6 x 6) and the network's
+ * input features (na x OFEA_LEARN_NFEAT: centred log stiffness, neighbour
+ * count / 26, log of the diagonal of the inverse diagonal blocks of Ehat).
+ * Arrays may be NULL to query na. */
 OFEA_API int ofea_learned_level(ofea_ctx *ctx, int *na, int *nbr, float *Ehat, float *feat);
 /* Energy loss (sum over the batch) and its gradient w.r.t. every weight for
- * given network inputs x (batch x na x 6, scaled residuals). */
+ * given stage inputs x (batch x na x 6, scaled level residuals). */
 OFEA_API int ofea_learned_gradient(ofea_ctx *ctx, const float *x, int batch, double *loss,
                                    float *grad);
 

@@ -287,7 +287,7 @@ class Context:
         _check(lib().ofea_learned_level(self.h, ctypes.byref(na), None, None, None), "ofea_learned_level")
         nbr = np.zeros((na.value, 27), dtype=np.int32)
         E = np.zeros((na.value, 27, 6, 6), dtype=np.float32)
-        feat = np.zeros(na.value, dtype=np.float32)
+        feat = np.zeros((na.value, 8), dtype=np.float32)
         _check(lib().ofea_learned_level(self.h, ctypes.byref(na), _ptr(nbr), _ptr(E), _ptr(feat)),
                "ofea_learned_level")
         return nbr, E, feat

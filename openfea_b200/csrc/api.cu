@@ -532,6 +532,7 @@ int ofea_learned_set_weights(ofea_ctx *c, const float *w, long long count) {
         Learned &N = c->learned;
         N.host_w.assign(w, w + count);
         N.have_weights = true;
+        N.fitted = true;  // the caller's coefficients are kept by later training
         N.uploaded = false;
     });
 }
@@ -566,6 +567,7 @@ int ofea_learned_load(ofea_ctx *c, const char *path) {
         if (!in) fail(OFEA_ERR_IO, std::string("truncated weight file: ") + path);
         c->learned.host_w = std::move(w);
         c->learned.have_weights = true;
+        c->learned.fitted = true;
         c->learned.uploaded = false;
     });
 }
@@ -581,7 +583,9 @@ int ofea_learned_level(ofea_ctx *c, int *na, int *nbr, float *Ehat, float *feat)
         if (Ehat)
             OFEA_CUDA(cudaMemcpyAsync(Ehat, c->learned.Ehat.p, sizeof(float) * 27 * 36 * C2.na,
                                       cudaMemcpyDeviceToHost, s));
-        if (feat) OFEA_CUDA(cudaMemcpyAsync(feat, c->learned.feat.p, sizeof(float) * C2.na, cudaMemcpyDeviceToHost, s));
+        if (feat)
+            OFEA_CUDA(cudaMemcpyAsync(feat, c->learned.X0.p, sizeof(float) * OFEA_LEARN_NFEAT * C2.na,
+                                      cudaMemcpyDeviceToHost, s));
         OFEA_CUDA(cudaStreamSynchronize(s));
     });
 }

@@ -127,23 +127,28 @@ struct Coarse {
     DevBuf<int> agg_of, agg_ptr, agg_nodes, agg_cell, cell_agg, nbr;
     DevBuf<double> centroid, E, S, P, diag0, pp, part;
     DevBuf<float> Einv32, cvec, evec, pw;
+    std::vector<int> agg_cell_h, cell_agg_h;  // host copies (nesting of the learned level)
+    std::vector<double> centroid_h;
 };
 
 // Learned coarse-correction stage (learned.cu): network weights, Adam state,
 // per-K data of the nested level and activation buffers.
 struct Learned {
     struct Layout {
-        size_t W0, b0, W[4], b[4], Wd, bd, total;
+        size_t W0, b0, W[4], b[4], Wd, bd, c0, total;
     };
     static Layout layout();
     void init_weights(unsigned seed);
     std::vector<float> host_w;
-    bool have_weights = false, uploaded = false;
+    bool have_weights = false, uploaded = false, fitted = false, inference_ready = false;
     int trained_steps = 0;
-    DevBuf<float> w, g, m, v, part;
-    DevBuf<double> Eb, sigma, lossp;
-    DevBuf<float> Ehat, dsq, feat;
-    DevBuf<float> X, Z0, H[5], A[4], Zl[4], Y, Yz, dY, dH, dZ, dA, batch_src, r32, data;
+    DevBuf<float> w, g, m, v, part;              // weights, gradient, Adam moments, wgrad partials
+    DevBuf<double> Eb, sigma, lossp, cpart;      // E2 blocks, sample RMS, loss / coefficient partials
+    DevBuf<float> Ehat, dsq, feat, pdel, shifted, invdeg, Binv, X0, scale;
+    DevBuf<int> parent;
+    DevBuf<float> Z0, H[5], A[4], Zl[4], Y, dY, dH, dZ, dA;  // network activations (one row per aggregate)
+    DevBuf<float> pv[9];                                      // stage vectors (rows of a batch)
+    DevBuf<float> batch_src, r32, data;
     long cap_rows = 0;
     int nlossp = 0, nsamples = 0, max_samples = 0;
 };

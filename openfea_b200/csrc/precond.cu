@@ -98,6 +98,9 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
     C.centroid.upload(cen.data(), cen.size(), st);
     C.nbr.upload(nbr.data(), nbr.size(), st);
     OFEA_CUDA(cudaStreamSynchronize(st));
+    C.agg_cell_h = std::move(agg_cell3);
+    C.cell_agg_h = std::move(cell_agg);
+    C.centroid_h = std::move(cen);
     C.geom_ok = true;
     C.K_ok = false;
 }
@@ -689,12 +692,16 @@ void prolong_level(ofea_ctx *c, const Coarse &C, const float *g, float *x) {
     OFEA_CHECK_LAUNCH();
 }
 
+void coarse_gemv(ofea_ctx *c, const float *cvec, float *evec) {
+    Coarse &C = c->coarse;
+    k_coarse_gemv<<<grid_for(c, (long)C.m * 32, kBlock), kBlock, 0, c->stream>>>(C.m, C.Einv32.p, cvec, evec);
+    OFEA_CHECK_LAUNCH();
+}
+
 void coarse_correct(ofea_ctx *c, const float *t, float *x) {
     Coarse &C = c->coarse;
     restrict_level(c, C, t, C.cvec.p);
-    k_coarse_gemv<<<grid_for(c, (long)C.m * 32, kBlock), kBlock, 0, c->stream>>>(C.m, C.Einv32.p, C.cvec.p,
-                                                                                 C.evec.p);
-    OFEA_CHECK_LAUNCH();
+    coarse_gemv(c, C.cvec.p, C.evec.p);
     prolong_level(c, C, C.evec.p, x);
 }
 

@@ -10,6 +10,8 @@ void build_aggregation_fine(ofea_ctx *c);
 // (once per K).
 void setup_coarse(ofea_ctx *c, int target_nodes);
 // x += Z E^-1 Z^T t  (FP32 vectors of n entries)
+// evec = E^-1 cvec (FP32 GEMV with the coarse level's inverse)
+void coarse_gemv(ofea_ctx *c, const float *cvec, float *evec);
 void coarse_correct(ofea_ctx *c, const float *t, float *x);
 // t = b - K32 x
 void vc_resid(ofea_ctx *c, const float *b, const float *x, float *t);

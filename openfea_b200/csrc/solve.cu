@@ -574,7 +574,7 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
                 }
                 OFEA_CHECK_LAUNCH();
             };
-            drive(c, oo, ws, per_chunk, chunk, hf, launches, learned ? 7 + 15 : 7, timed_out, t_start, {});
+            drive(c, oo, ws, per_chunk, chunk, hf, launches, learned ? 7 + 7 : 7, timed_out, t_start, {});
         } else {
             auto chunk = [&](int iters) {
                 for (int it = 0; it < iters; ++it) {

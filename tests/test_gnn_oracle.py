@@ -1,5 +1,5 @@
-"""The CPU restatement of the learned stage's network (oracle/gnn_oracle.py):
-its backward pass against central finite differences.  It is then the
+"""The CPU restatement of the learned stage (oracle/gnn_oracle.py): its
+backward pass against central finite differences, and the stage's algebra.  It is then the
 reference the GPU gradients are checked against (tests/test_gpu_learned.py)."""
 import numpy as np
 
@@ -10,7 +10,7 @@ def test_gnn_oracle_gradient_matches_finite_differences():
     nbr, E, feat = random_level((3, 2, 2), seed=1)
     net = GNNOracle(nbr, E, feat)
     rng = np.random.default_rng(2)
-    w = he_weights(2, out_gain=1.0)
+    w = he_weights(2, out_gain=1.0, c0=(0.8, -0.3, 0.1))
     x = rng.normal(0, 1, (2, net.na, 6))
     loss, g = net.grad(w, x)
     assert np.isfinite(loss)
@@ -40,3 +40,16 @@ def test_gnn_oracle_energy_minimum_is_galerkin_solution():
     y = np.linalg.solve(M, x.reshape(-1)).reshape(1, na, 6)
     grad_y = (net.apply_E(y) - x) / (6 * na)
     assert np.abs(grad_y).max() < 1e-12
+
+
+def test_gnn_oracle_stage_is_linear_and_symmetric():
+    """y = s * M(s * x) with M a polynomial in B Ehat times B: symmetric for any
+    scalings s the network sets."""
+    nbr, E, feat = random_level((2, 2, 2), seed=5)
+    net = GNNOracle(nbr, E, feat)
+    w = he_weights(6, out_gain=1.0, c0=(1.5, -0.4, 0.05))
+    na = net.na
+    basis = np.eye(6 * na).reshape(6 * na, na, 6)
+    S = net.stage(w, basis).reshape(6 * na, 6 * na)
+    assert np.abs(S - S.T).max() < 1e-10 * np.abs(S).max()
+    assert np.abs(net.scales(w) - 1.0).max() > 1e-2  # the scalings are not trivial here

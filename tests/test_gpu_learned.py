@@ -1,7 +1,7 @@
 """The learned coarse-correction stage on the GPU: gradients of the
 library's backward kernels against the CPU oracle (oracle/gnn_oracle.py),
-training, the gain over the same solver without the stage, and the FP64
-judge that rejects it in favour of plain PCG."""
+training, what the trained stage gains over the same solver without it, and
+the FP64 judge that rejects it in favour of plain PCG."""
 import numpy as np
 import pytest
 
@@ -25,7 +25,7 @@ def test_gradient_matches_cpu_oracle(gpu_ctx_factory):
     ctx, f = cantilever_ctx(gpu_ctx_factory, 40, 10, 10)
     nbr, E, feat = ctx.learned_level()
     assert nbr.shape[0] >= 8
-    w = he_weights(5, out_gain=1.0).astype(np.float32)
+    w = he_weights(5, out_gain=0.3, c0=(1.2, -0.5, 0.1)).astype(np.float32)
     ctx.set_learned_weights(w)
     x = np.random.default_rng(6).normal(0, 1, (2, nbr.shape[0], 6)).astype(np.float32)
     loss_g, g_gpu = ctx.learned_gradient(x)
