@@ -6,13 +6,18 @@ free DOF, 122.7M non-zeros), E = 210 GPa, nu = 0.3, clamped at x = 0, 1 MPa end
 traction in -z (synthetic, seeded; the reference ships no benchmark input).
 
 One step = one solve K u = f to a true FP64 relative residual of 1e-8 with the
-mixed-precision solver (FP64 flexible PCG, FP32 two-level V-cycle
-preconditioner, including its per-matrix setup), K assembled and f resident in
-HBM.  `value` = seconds per step (device time, CUDA events on the
-launching stream, max over ranks).  `e2e` = the reference-facing path through
-the C ABI with host buffers: mesh upload, pattern, FP64 assembly, solve, u
-back to the host - the span the reference times with clock()
-(src/cae.cpp:257-281).
+learned + mixed-precision solver (FP64 flexible PCG, FP32 two-level V-cycle
+preconditioner plus the learned coarse stage, including the per-matrix setup
+of both levels and the network's evaluation), K assembled and f resident in
+HBM.  The learned stage is trained once, before the warm-up, on residuals of
+plain-PCG solves of a seeded random load (not the benchmark's load); its
+training time is reported beside the number.  `value` = seconds per step
+(device time, CUDA events on the launching stream, max over ranks).  The
+mixed solver without the learned stage and the plain FP64 PCG are timed on
+the same K and f for comparison.  `e2e` = the reference-facing path through
+the C ABI with host buffers: mesh upload, pattern, FP64 assembly, solve
+(trained weights handed to the new context), u back to the host - the span
+the reference times with clock() (src/cae.cpp:257-281).
 
     python bench.py [--gpus N --steps K --warmup W]      # this library
     python bench.py --impl reference                    # the reference's CPU path
@@ -268,8 +273,14 @@ def run_ours(args):
             dist.destroy_process_group()
         return 0
 
+    # the learned stage: trained once on plain-PCG residuals of a seeded random load
+    t_tr = time.perf_counter()
+    train = ctx.learned_train(None, sample_iters=600, sample_every=4, steps=400, batch=16, lr=1e-3, seed=1234)
+    train["wall_s"] = time.perf_counter() - t_tr
+    weights = ctx.learned_weights()
+
     for _ in range(args.warmup):
-        solve("GPU_MIXED")
+        solve("GPU_LEARNED")
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -286,7 +297,7 @@ def run_ours(args):
         with torch.cuda.stream(stream):
             ev0.record(stream)
         for _ in range(args.steps):
-            stats.append(solve("GPU_MIXED"))
+            stats.append(solve("GPU_LEARNED"))
         with torch.cuda.stream(stream):
             ev1.record(stream)
         torch.cuda.synchronize()
@@ -296,13 +307,17 @@ def run_ours(args):
     sec = total_ms / 1e3 / args.steps
     for st in stats:
         assert st["status"] == 0 and st["rel_residual"] <= args.rtol, st
-    u_mixed = u_dev.clone()
+    u_learned = u_dev.clone()
+
+    # the same solver without the learned stage (same K, f, set-up included)
+    stm = [solve("GPU_MIXED") for _ in range(2)]
+    mixed_s = max_over_ranks(min(s_["seconds"] for s_ in stm))
 
     # the plain FP64 PCG the metric compares against (same workload, outside the timed steps)
     st64 = solve("GPU_PCG")
     st64b = solve("GPU_PCG")
     plain_s = max_over_ranks(min(st64["seconds"], st64b["seconds"]))
-    err_vs_plain = float(torch.linalg.norm(u_mixed - u_dev) / torch.linalg.norm(u_dev))
+    err_vs_plain = float(torch.linalg.norm(u_learned - u_dev) / torch.linalg.norm(u_dev))
 
     # roofline of the dominant kernels (CUDA events on the launching stream)
     solve("GPU_MIXED")
@@ -334,8 +349,9 @@ def run_ours(args):
         c2.assemble_pattern()
         t2 = time.perf_counter()
         c2.assemble_linear()
+        c2.set_learned_weights(weights)
         t3 = time.perf_counter()
-        u_host, st = c2.solve(f, method="GPU_MIXED", rtol=args.rtol)
+        u_host, st = c2.solve(f, method="GPU_LEARNED", rtol=args.rtol)
         t4 = time.perf_counter()
         c2.close()
         if i > 0:
@@ -353,7 +369,8 @@ def run_ours(args):
         "config": {
             "workload": (f"C3D8 cantilever {args.shape} (h=5 mm), {n} DOF, nnz {nnz}, E=210 GPa, "
                          f"nu=0.3, clamped x=0, 1 MPa end traction; FP64 flexible PCG with the FP32 "
-                         f"two-level V-cycle preconditioner, to FP64 rel. residual {args.rtol:g}"),
+                         f"two-level V-cycle preconditioner and the learned coarse stage, to FP64 rel. "
+                         f"residual {args.rtol:g}"),
             "n_dof": n, "nnz": nnz, "parallelism": f"replicas x{world}",
             "l2": "inputs larger than L2 (FP64 K ~1 GB and FP32 K ~0.5 GB streamed per SpMV)",
         },
@@ -366,10 +383,14 @@ def run_ours(args):
                             "ms_per_launch": msM[1]},
         "spmv64_plain": {"kernel": "k_pcg64_A (FP64 BSELL SpMV, plain PCG)", "achieved_gbs": gbs64,
                          "frac": gbs64 / hbm, "bytes_per_launch": byP[0], "ms_per_launch": msP[0]},
-        "solver": {"iterations": stats[-1]["iterations"], "refinements": stats[-1]["refinements"],
+        "solver": {"method": "GPU_LEARNED", "iterations": stats[-1]["iterations"],
+                   "refinements": stats[-1]["refinements"], "rejected_learned": stats[-1]["rejected_learned"],
                    "rel_residual": stats[-1]["rel_residual"], "plain_pcg64_s": plain_s,
                    "plain_pcg64_iterations": st64["iterations"],
                    "speedup_vs_plain": plain_s / sec, "rel_diff_vs_plain": err_vs_plain,
+                   "mixed_without_learned_s": mixed_s, "mixed_without_learned_iterations": stm[-1]["iterations"],
+                   "learned_gain_vs_mixed": mixed_s / sec,
+                   "learned_training": train,
                    "precond_setup_s": stats[-1]["setup_seconds"],
                    "mesh_pattern_assembly_s": setup_s},
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
