@@ -207,6 +207,46 @@ OFEA_API int ofea_learned_level(ofea_ctx *ctx, int *na, int *nbr, float *Ehat, f
 OFEA_API int ofea_learned_gradient(ofea_ctx *ctx, const float *x, int batch, double *loss,
                                    float *grad);
 
+/* ---- batched reanalysis ---------------------------------------------------- */
+/* Replaces the per-variant factor + per-load-case dgstrs loop of the
+ * reference's reanalysis (src/solver/solver_superlu.cpp:31-94 SuperLU_class /
+ * superlu_solution_next, driven by src/ca_analysis.cpp:148-248): many
+ * assembled variants (one context each, all on one GPU) times up to 32 load
+ * cases each, solved together by one persistent cooperative kernel launched
+ * from a CUDA graph.  Methods OFEA_SOLVER_MIXED (FP64 flexible CG + FP32
+ * two-level V-cycle per variant) and OFEA_SOLVER_PCG64.  Its tile sizes (load
+ * cases per thread, CTA size, CTAs per SM) are chosen by timing candidates on
+ * the first solve of a problem class and kept in a JSON file (OFEA_TUNE_FILE,
+ * default ~/.cache/openfea_b200_tune.json).  The batch borrows the contexts:
+ * keep them alive and unchanged until ofea_batch_destroy. */
+typedef struct ofea_batch ofea_batch;
+#define OFEA_BATCH_MAX_RHS 32
+OFEA_API int ofea_batch_create(ofea_batch **out, ofea_ctx *const *ctxs, int n_variants, int nrhs);
+OFEA_API int ofea_batch_destroy(ofea_batch *batch);
+/* f[v]: the nrhs load cases of variant v, case j at f[v] + j * n_v (host). */
+OFEA_API int ofea_batch_set_rhs(ofea_batch *batch, const double *const *f);
+/* Solves on the load cases last set; the solution stays on the device.
+ * stats: n_variants entries (worst load case of each variant). */
+OFEA_API int ofea_batch_solve_resident(ofea_batch *batch, const ofea_solve_opts *opts,
+                                       ofea_solve_stats *stats);
+/* u[v]: nrhs * n_v host values, laid out like f. */
+OFEA_API int ofea_batch_get_solution(ofea_batch *batch, double *const *u);
+/* set_rhs + solve_resident + get_solution. */
+OFEA_API int ofea_batch_solve(ofea_batch *batch, const double *const *f, double *const *u,
+                              const ofea_solve_opts *opts, ofea_solve_stats *stats);
+/* The tile configuration used for `method` (tuning it now if needed). */
+OFEA_API int ofea_batch_tuning(ofea_batch *batch, int method, int *rhs_per_thread, int *threads,
+                               int *ctas_per_sm, double *ms_per_iteration);
+/* One-call form: create, solve, destroy. */
+OFEA_API int ofea_solve_batched(ofea_ctx *const *ctxs, int n_variants, const double *const *f,
+                                double *const *u, int nrhs, const ofea_solve_opts *opts,
+                                ofea_solve_stats *stats);
+/* Checks the failure path of the batched solver's grid barrier: launches a
+ * cooperative kernel whose barrier waits for one CTA more than exists; every
+ * wait gives up after limit_ms and *released is set to 0 (1 would mean the
+ * barrier opened).  The context stays usable. */
+OFEA_API int ofea_check_barrier_timeout(ofea_ctx *ctx, int limit_ms, int *released);
+
 /* ---- measurement ------------------------------------------------------- */
 /* No counterpart in the reference (it only prints clock() spans): times the
  * solver's two per-iteration kernels (A: p update + SpMV + p.q, B: vector

@@ -108,6 +108,16 @@ def lib():
         "ofea_profile_solver_kernels": (_I, [_P, _I, _I, _P, _P]),
         "ofea_precond_reset": (_I, [_P]),
         "ofea_learn_opts_default": (None, [_P]),
+        "ofea_batch_create": (_I, [ctypes.POINTER(_P), _P, _I, _I]),
+        "ofea_batch_destroy": (_I, [_P]),
+        "ofea_batch_set_rhs": (_I, [_P, _P]),
+        "ofea_batch_solve_resident": (_I, [_P, _P, _P]),
+        "ofea_batch_get_solution": (_I, [_P, _P]),
+        "ofea_batch_solve": (_I, [_P, _P, _P, _P, _P]),
+        "ofea_batch_tuning": (_I, [_P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I),
+                                   ctypes.POINTER(_D)]),
+        "ofea_solve_batched": (_I, [_P, _I, _P, _P, _I, _P, _P]),
+        "ofea_check_barrier_timeout": (_I, [_P, _I, ctypes.POINTER(_I)]),
         "ofea_learned_train": (_I, [_P, _P, _P, _P]),
         "ofea_learned_get_weights": (_I, [_P, _P, ctypes.POINTER(_LL)]),
         "ofea_learned_set_weights": (_I, [_P, _P, _LL]),
@@ -139,6 +149,86 @@ def _f64(a):
 
 def _i32(a):
     return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class Batch:
+    """Many assembled variants (Contexts on one GPU) x up to 32 load cases each,
+    solved together by the persistent batched solver (ofea_batch_* in
+    include/ofea_gpu.h).  Load cases are given per variant as an array of
+    shape (nrhs, n_v)."""
+
+    def __init__(self, contexts, nrhs):
+        self.contexts = list(contexts)
+        self.nrhs = int(nrhs)
+        self.h = _P()
+        arr = (_P * len(self.contexts))(*[c.h for c in self.contexts])
+        _check(lib().ofea_batch_create(ctypes.byref(self.h), arr, len(self.contexts), self.nrhs),
+               "ofea_batch_create")
+
+    def close(self):
+        if self.h:
+            lib().ofea_batch_destroy(self.h)
+            self.h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_rhs(self, loads):
+        self._f = [np.ascontiguousarray(np.asarray(F, dtype=np.float64).reshape(self.nrhs, c.n))
+                   for F, c in zip(loads, self.contexts)]
+        ptrs = (_P * len(self._f))(*[F.ctypes.data for F in self._f])
+        _check(lib().ofea_batch_set_rhs(self.h, ptrs), "ofea_batch_set_rhs")
+
+    def solve_resident(self, method="GPU_MIXED", rtol=1e-8, raise_on_error=True, **kw):
+        o = solve_opts(method, rtol, **kw)
+        stats = (SolveStats * len(self.contexts))()
+        rc = lib().ofea_batch_solve_resident(self.h, ctypes.byref(o), stats)
+        if rc != OFEA_OK and raise_on_error:
+            _check(rc, "ofea_batch_solve_resident")
+        return [s_.as_dict() for s_ in stats]
+
+    def solution(self):
+        U = [np.zeros((self.nrhs, c.n)) for c in self.contexts]
+        ptrs = (_P * len(U))(*[u.ctypes.data for u in U])
+        _check(lib().ofea_batch_get_solution(self.h, ptrs), "ofea_batch_get_solution")
+        return U
+
+    def solve(self, loads, method="GPU_MIXED", rtol=1e-8, **kw):
+        self.set_rhs(loads)
+        st = self.solve_resident(method, rtol, **kw)
+        return self.solution(), st
+
+    def tuning(self, method="GPU_MIXED"):
+        r, t, c, ms = _I(), _I(), _I(), _D()
+        _check(lib().ofea_batch_tuning(self.h, SOLVERS[method], ctypes.byref(r), ctypes.byref(t), ctypes.byref(c),
+                                       ctypes.byref(ms)), "ofea_batch_tuning")
+        return {"rhs_per_thread": r.value, "threads": t.value, "ctas_per_sm": c.value, "ms_per_iteration": ms.value}
+
+
+def solve_batched(contexts, loads, method="GPU_MIXED", rtol=1e-8, **kw):
+    """One-call batched solve through ofea_solve_batched: loads[v] has shape
+    (nrhs, n_v); returns the solutions in the same shapes and per-variant stats."""
+    nrhs = int(np.asarray(loads[0]).shape[0])
+    F = [np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(nrhs, c.n)) for x, c in zip(loads, contexts)]
+    U = [np.zeros_like(x) for x in F]
+    ctx = (_P * len(contexts))(*[c.h for c in contexts])
+    fp = (_P * len(F))(*[x.ctypes.data for x in F])
+    up = (_P * len(U))(*[x.ctypes.data for x in U])
+    o = solve_opts(method, rtol, **kw)
+    stats = (SolveStats * len(contexts))()
+    _check(lib().ofea_solve_batched(ctx, len(contexts), fp, up, nrhs, ctypes.byref(o), stats), "ofea_solve_batched")
+    return U, [s_.as_dict() for s_ in stats]
+
+
+def check_barrier_timeout(ctx, limit_ms=20):
+    """The batched solver's grid barrier given a CTA that never arrives: returns
+    1 if it opened (it must not), 0 when every wait ran out as designed."""
+    r = _I(-1)
+    _check(lib().ofea_check_barrier_timeout(ctx.h, int(limit_ms), ctypes.byref(r)), "ofea_check_barrier_timeout")
+    return r.value
 
 
 def solve_opts(method="GPU_PCG", rtol=1e-8, max_iter=100000, time_budget_s=0.0, check_every=16,

@@ -608,6 +608,78 @@ int ofea_residual_norms_noalloc(ofea_ctx *c, int nrhs, const double *d_f, const 
     });
 }
 
+int ofea_batch_create(ofea_batch **out, ofea_ctx *const *ctxs, int n_variants, int nrhs) {
+    return guarded([&] {
+        need(out != nullptr && ctxs != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
+        *out = nullptr;
+        *out = batch_create(ctxs, n_variants, nrhs);
+    });
+}
+
+int ofea_batch_destroy(ofea_batch *b) {
+    return guarded([&] { batch_destroy(b); });
+}
+
+int ofea_batch_set_rhs(ofea_batch *b, const double *const *f) {
+    return guarded([&] {
+        need(b != nullptr && f != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
+        batch_set_rhs(b, f);
+    });
+}
+
+int ofea_batch_solve_resident(ofea_batch *b, const ofea_solve_opts *opts, ofea_solve_stats *stats) {
+    return guarded([&] {
+        need(b != nullptr, OFEA_ERR_INVALID_ARG, "NULL batch");
+        ofea_solve_opts o;
+        if (opts) o = *opts;
+        else ofea_solve_opts_default(&o);
+        batch_solve(b, o, stats);
+    });
+}
+
+int ofea_batch_get_solution(ofea_batch *b, double *const *u) {
+    return guarded([&] {
+        need(b != nullptr && u != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
+        batch_get_solution(b, u);
+    });
+}
+
+int ofea_batch_solve(ofea_batch *b, const double *const *f, double *const *u, const ofea_solve_opts *opts,
+                     ofea_solve_stats *stats) {
+    int rc = ofea_batch_set_rhs(b, f);
+    if (rc != OFEA_OK) return rc;
+    rc = ofea_batch_solve_resident(b, opts, stats);
+    if (rc != OFEA_OK) return rc;
+    return ofea_batch_get_solution(b, u);
+}
+
+int ofea_batch_tuning(ofea_batch *b, int method, int *rpt, int *threads, int *ctas_per_sm, double *ms) {
+    return guarded([&] {
+        need(b != nullptr, OFEA_ERR_INVALID_ARG, "NULL batch");
+        need(method == OFEA_SOLVER_PCG64 || method == OFEA_SOLVER_MIXED, OFEA_ERR_UNKNOWN_SOLVER, "method");
+        batch_tuning(b, method, rpt, threads, ctas_per_sm, ms);
+    });
+}
+
+int ofea_solve_batched(ofea_ctx *const *ctxs, int n_variants, const double *const *f, double *const *u, int nrhs,
+                       const ofea_solve_opts *opts, ofea_solve_stats *stats) {
+    ofea_batch *b = nullptr;
+    int rc = ofea_batch_create(&b, ctxs, n_variants, nrhs);
+    if (rc != OFEA_OK) return rc;
+    rc = ofea_batch_solve(b, f, u, opts, stats);
+    ofea_batch_destroy(b);
+    return rc;
+}
+
+int ofea_check_barrier_timeout(ofea_ctx *c, int limit_ms, int *released) {
+    return guarded([&] {
+        need(c != nullptr && released != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
+        need(limit_ms >= 1 && limit_ms <= 10000, OFEA_ERR_INVALID_ARG, "limit_ms must be 1..10000");
+        use_device(c);
+        barrier_probe(c, limit_ms, released);
+    });
+}
+
 int ofea_profile_solver_kernels(ofea_ctx *c, int method, int reps, double *ms, double *bytes) {
     return guarded([&] {
         need(c != nullptr && ms && bytes && reps > 0, OFEA_ERR_INVALID_ARG, "bad argument");

@@ -1,0 +1,1261 @@
+// Batched reanalysis: many design variants (each an assembled context on one
+// GPU) times up to kMaxBatchRhs load cases each, solved by ONE persistent
+// cooperative kernel launched from a CUDA graph.  The reference solves such
+// batches variant by variant with a kept SuperLU factor and dgstrs per load
+// case (src/solver/solver_superlu.cpp:31-94, the CA reanalysis of
+// src/ca_analysis.cpp:148-248).
+//
+// Layout in HBM: the variants' DOF are concatenated (variant v starts at dof0[v])
+// and every vector is load-case interleaved, x[(dof0 + i) * NR + j], so that a
+// gather of one DOF fetches the values of all load cases in one contiguous
+// run.  Matrices stay where their contexts keep them (BSELL-32, FP64 and FP32
+// copies); a table of per-variant descriptors points at them.
+//
+// Algorithm per (variant, load case): the MIXED method of solve.cu, FP64
+// flexible CG with the FP32 two-level V(1,1) preconditioner of precond.cu, or
+// PCG64 (FP64 CG, block Jacobi).  The kernel runs every variant in lock step
+// through phases separated by grid barriers; a phase's work items are the
+// (slice of 32 block rows, group of RPT load cases) pairs of all variants, or
+// (aggregate, group), (coarse row, group), (variant, load case).  A warp
+// takes one item: lane t owns block row t of the slice, so the matrix loads
+// are coalesced BSELL lines shared by the RPT load cases the lane carries.
+// Per-(variant, load case) scalars come from per-slice partial sums reduced
+// in a fixed order: results are bitwise reproducible.  Converged load cases
+// stop updating; the kernel ends when none is left or at max_iter.
+//
+// Every wait at a grid barrier is bounded (time limit on %globaltimer): on
+// expiry the kernel records an error and every CTA returns.
+#include <cuda/atomic>
+#include <sys/stat.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "precond.cuh"
+#include "sell.cuh"
+#include "solver_common.cuh"
+
+namespace ofea {
+
+constexpr int kMaxBatchRhs = 32;
+
+// Per-variant descriptor (device copy).
+struct BVar {
+    int nfree, nslice, slice0, na, m, agg0, crow0, pad;
+    long dof0;  // first DOF of the variant in the batch vectors (times NR)
+    long c0;    // first coarse entry of the variant (times NR)
+    const int *sl_ptr, *scols;
+    const double *sv64, *Dinv;
+    const float *sv32, *Dinv32;
+    const int *agg_of, *agg_ptr, *agg_nodes, *node_of_free;
+    const double *xyz, *centroid;
+    const float *Einv32;
+    double inv_scale;
+    float wsm, pad2;
+};
+
+struct GridSync {
+    unsigned count, gen;
+    int err, pad;
+};
+
+struct BArgs {
+    int V, NR, NG, nslices, naggs, ncrows, max_iter, extra_arrivals;
+    unsigned long long limit_ns;
+    double rtol;
+    const BVar *var;
+    const int *slice_var, *agg_var, *crow_var;
+    const double *f;
+    double *u, *r, *p0, *p1, *q, *z64;
+    float *b32, *x32, *t32, *zA, *zB, *cvec, *evec;
+    double *pa, *pb;                                    // partials [slice][NR]
+    double *ff, *tol2, *rz, *alpha, *beta;              // [V * NR]
+    int *live, *iters, *status, *live_cnt;              // [V * NR], live_cnt[3]
+    GridSync *gs;
+};
+
+namespace {
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid barrier for a cooperative launch.  Returns false when the batch has
+// failed (a wait ran out here or elsewhere): the caller returns.
+__device__ bool grid_barrier(GridSync *gs, unsigned nblocks, unsigned long long limit_ns) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(gs->gen), cnt(gs->count);
+        cuda::atomic_ref<int, cuda::thread_scope_device> err(gs->err);
+        const unsigned g = gen.load(cuda::memory_order_acquire);
+        __threadfence();
+        const unsigned arrived = cnt.fetch_add(1u, cuda::memory_order_acq_rel) + 1u;
+        if (arrived == nblocks) {
+            cnt.store(0u, cuda::memory_order_relaxed);
+            gen.fetch_add(1u, cuda::memory_order_release);
+        } else {
+            const unsigned long long t0 = global_ns();
+            while (gen.load(cuda::memory_order_acquire) == g) {
+                if (err.load(cuda::memory_order_relaxed) != 0) break;
+                if (global_ns() - t0 > limit_ns) {
+                    err.store(1, cuda::memory_order_relaxed);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = err.load(cuda::memory_order_relaxed) == 0;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// y[c][jj] = sum over the block row's slots of K_blk x(col, jj).
+template <class V, int RPT, class XF>
+__device__ __forceinline__ void sell_row_multi(long S, int t, int W, const int *__restrict__ scols,
+                                               const V *__restrict__ svals, XF xf, V (&y)[3][RPT]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int jj = 0; jj < RPT; ++jj) y[c][jj] = 0;
+    const int *cp = scols + S * kSlice + t;
+    const V *vp = svals + S * 9 * kSlice + t;
+    for (int k = 0; k < W; ++k) {
+        const int col = __ldg(cp + (long)k * kSlice);
+        V v[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) v[e] = __ldg(vp + ((long)k * 9 + e) * kSlice);
+#pragma unroll
+        for (int jj = 0; jj < RPT; ++jj) {
+            const V x0 = xf(3 * col, jj), x1 = xf(3 * col + 1, jj), x2 = xf(3 * col + 2, jj);
+            y[0][jj] = fma(v[0], x0, fma(v[1], x1, fma(v[2], x2, y[0][jj])));
+            y[1][jj] = fma(v[3], x0, fma(v[4], x1, fma(v[5], x2, y[1][jj])));
+            y[2][jj] = fma(v[6], x0, fma(v[7], x1, fma(v[8], x2, y[2][jj])));
+        }
+    }
+}
+
+// ------------------------------------------------------------ phases --
+
+// Work loop over (slice, group) items, one warp per item.  f(BVar, v, gs, row, j0)
+// is called by every lane (row may be >= nfree: the lane then skips the row
+// but takes part in the warp's reductions).
+template <class F>
+__device__ __forceinline__ void for_slices(const BArgs &a, F f) {
+    const int warps = blockDim.x / 32, w = threadIdx.x / 32, lane = threadIdx.x & 31;
+    const long items = (long)a.nslices * a.NG;
+    for (long it = (long)blockIdx.x * warps + w; it < items; it += (long)gridDim.x * warps) {
+        const int gsl = (int)(it / a.NG), g = (int)(it % a.NG);
+        const int v = a.slice_var[gsl];
+        const BVar &B = a.var[v];
+        const int row = (gsl - B.slice0) * kSlice + lane;
+        f(B, v, gsl, row, g);
+    }
+}
+
+// Reduce phase: one warp per (variant, load case); s(v, j, sum_pa, sum_pb).
+template <class F>
+__device__ __forceinline__ void for_pairs(const BArgs &a, bool two, F f) {
+    const int warps = blockDim.x / 32, w = threadIdx.x / 32, lane = threadIdx.x & 31;
+    for (int it = blockIdx.x * warps + w; it < a.V * a.NR; it += gridDim.x * warps) {
+        const int v = it / a.NR, j = it % a.NR;
+        const BVar &B = a.var[v];
+        double sa = 0, sb = 0;
+        for (int s = lane; s < B.nslice; s += 32) {
+            sa += a.pa[(long)(B.slice0 + s) * a.NR + j];
+            if (two) sb += a.pb[(long)(B.slice0 + s) * a.NR + j];
+        }
+        sa = warp_sum(sa);
+        sb = warp_sum(sb);
+        if (lane == 0) f(v, j, sa, sb);
+    }
+}
+
+template <int RPT>
+__device__ __forceinline__ void live_mask(const BArgs &a, int v, int j0, bool (&lv)[RPT], bool &any) {
+    any = false;
+#pragma unroll
+    for (int jj = 0; jj < RPT; ++jj) {
+        const int j = j0 + jj;
+        lv[jj] = j < a.NR && a.live[v * a.NR + j] != 0;
+        any |= lv[jj];
+    }
+}
+
+// Warp-reduce RPT partials and store them for the slice (lane 0).
+template <int RPT>
+__device__ __forceinline__ void store_partials(const BArgs &a, double *P, int gsl, int j0, double (&p)[RPT]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int jj = 0; jj < RPT; ++jj) {
+        const double s = warp_sum(p[jj]);
+        if (lane == 0 && j0 + jj < a.NR) P[(long)gsl * a.NR + j0 + jj] = s;
+    }
+}
+
+}  // namespace
+
+// The persistent batched solver.  MIXED: FP64 FCG + FP32 V-cycle; else PCG64.
+template <int RPT, bool MIXED>
+__global__ void __launch_bounds__(256) k_batch_solve(BArgs a) {
+    const unsigned nb = gridDim.x + a.extra_arrivals;
+    const int NR = a.NR;
+    auto sync = [&]() { return grid_barrier(a.gs, nb, a.limit_ns); };
+    auto X = [&](const BVar &B, int row, int c) { return (B.dof0 + 3L * row + c) * NR; };
+
+    // ---- init: r = f - K u, partials ||r||^2 (pa), ||f||^2 (pb); start of M(r)
+    for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
+        const int j0 = g * RPT;
+        double prr[RPT], pff[RPT];
+#pragma unroll
+        for (int jj = 0; jj < RPT; ++jj) prr[jj] = pff[jj] = 0;
+        if (row < B.nfree) {
+            const int ls = gsl - B.slice0, S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
+            double y[3][RPT];
+            sell_row_multi<double, RPT>(S, row & 31, W, B.scols, B.sv64,
+                                        [&](int k, int jj) {
+                                            return j0 + jj < NR ? a.u[(B.dof0 + k) * NR + j0 + jj] : 0.0;
+                                        },
+                                        y);
+#pragma unroll
+            for (int jj = 0; jj < RPT; ++jj) {
+                const int j = j0 + jj;
+                if (j >= NR) continue;
+                double rv[3];
+                for (int c = 0; c < 3; ++c) {
+                    const long d = X(B, row, c) + j;
+                    const double fv = a.f[d];
+                    rv[c] = fv - y[c][jj];
+                    a.r[d] = rv[c];
+                    prr[jj] += rv[c] * rv[c];
+                    pff[jj] += fv * fv;
+                }
+                if (MIXED) {
+                    float b[3], x[3];
+                    for (int c = 0; c < 3; ++c) b[c] = (float)rv[c];
+                    block3_apply(B.Dinv32 + 9L * row, b, x);
+                    for (int c = 0; c < 3; ++c) {
+                        a.b32[X(B, row, c) + j] = b[c];
+                        a.x32[X(B, row, c) + j] = B.wsm * x[c];
+                    }
+                } else {
+                    double z[3];
+                    block3_apply(B.Dinv + 9L * row, rv, z);
+                    for (int c = 0; c < 3; ++c) a.z64[X(B, row, c) + j] = z[c];
+                }
+            }
+        }
+        store_partials<RPT>(a, a.pa, gsl, j0, prr);
+        store_partials<RPT>(a, a.pb, gsl, j0, pff);
+    });
+    if (!sync()) return;
+    for_pairs(a, true, [&](int v, int j, double rr, double ff) {
+        const int vj = v * NR + j;
+        a.ff[vj] = ff;
+        const double t = 0.5 * a.rtol;
+        a.tol2[vj] = t * t * ff;
+        a.live[vj] = (ff > 0.0 && rr > a.tol2[vj] && isfinite(rr)) ? 1 : 0;
+        a.iters[vj] = 0;
+        a.status[vj] = isfinite(rr) ? OFEA_OK : OFEA_ERR_BREAKDOWN;
+        a.beta[vj] = 0.0;
+    });
+    if (!sync()) return;
+
+    // Preconditioner application z_new = M(r) (MIXED: V-cycle from b32/x32;
+    // PCG64: z64 already written with r).  Partials r.z_new (pa), r.z_old (pb).
+    auto precondition = [&](float *znew, const float *zold) -> bool {
+        if (!MIXED) return true;
+        // t = b - K32 x
+        for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
+            const int j0 = g * RPT;
+            bool lv[RPT], any;
+            live_mask<RPT>(a, v, j0, lv, any);
+            if (!any || row >= B.nfree) return;
+            const int ls = gsl - B.slice0, S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
+            float y[3][RPT];
+            sell_row_multi<float, RPT>(S, row & 31, W, B.scols, B.sv32,
+                                       [&](int k, int jj) {
+                                           return j0 + jj < NR ? a.x32[(B.dof0 + k) * NR + j0 + jj] : 0.f;
+                                       },
+                                       y);
+#pragma unroll
+            for (int jj = 0; jj < RPT; ++jj) {
+                if (!lv[jj]) continue;
+                for (int c = 0; c < 3; ++c) {
+                    const long d = X(B, row, c) + j0 + jj;
+                    a.t32[d] = a.b32[d] - y[c][jj];
+                }
+            }
+        });
+        if (!sync()) return false;
+        // c = Z^T t per aggregate (warp per (aggregate, group))
+        {
+            const int warps = blockDim.x / 32, w = threadIdx.x / 32, lane = threadIdx.x & 31;
+            const long items = (long)a.naggs * a.NG;
+            for (long it = (long)blockIdx.x * warps + w; it < items; it += (long)gridDim.x * warps) {
+                const int ga = (int)(it / a.NG), g = (int)(it % a.NG), j0 = g * RPT;
+                const int v = a.agg_var[ga];
+                const BVar &B = a.var[v];
+                bool lv[RPT], any;
+                live_mask<RPT>(a, v, j0, lv, any);
+                if (!any) continue;
+                const int I = ga - B.agg0;
+                float acc[6][RPT];
+#pragma unroll
+                for (int k = 0; k < 6; ++k)
+#pragma unroll
+                    for (int jj = 0; jj < RPT; ++jj) acc[k][jj] = 0.f;
+                const float cx = (float)B.centroid[3L * I], cy = (float)B.centroid[3L * I + 1],
+                            cz = (float)B.centroid[3L * I + 2];
+                const float sc = (float)B.inv_scale;
+                for (int idx = B.agg_ptr[I] + lane; idx < B.agg_ptr[I + 1]; idx += 32) {
+                    const int r = B.agg_nodes[idx], node = B.node_of_free[r];
+                    const float dx = ((float)B.xyz[3L * node] - cx) * sc;
+                    const float dy = ((float)B.xyz[3L * node + 1] - cy) * sc;
+                    const float dz = ((float)B.xyz[3L * node + 2] - cz) * sc;
+#pragma unroll
+                    for (int jj = 0; jj < RPT; ++jj) {
+                        if (j0 + jj >= NR) continue;
+                        const float tx = a.t32[X(B, r, 0) + j0 + jj], ty = a.t32[X(B, r, 1) + j0 + jj],
+                                    tz = a.t32[X(B, r, 2) + j0 + jj];
+                        acc[0][jj] += tx;
+                        acc[1][jj] += ty;
+                        acc[2][jj] += tz;
+                        acc[3][jj] += -dz * ty + dy * tz;
+                        acc[4][jj] += dz * tx - dx * tz;
+                        acc[5][jj] += -dy * tx + dx * ty;
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < 6; ++k)
+#pragma unroll
+                    for (int jj = 0; jj < RPT; ++jj) {
+                        const float s = warp_sum(acc[k][jj]);
+                        if (lane == 0 && j0 + jj < NR) a.cvec[(B.c0 + 6L * I + k) * NR + j0 + jj] = s;
+                    }
+            }
+        }
+        if (!sync()) return false;
+        // e = E^-1 c (warp per (coarse row, group))
+        {
+            const int warps = blockDim.x / 32, w = threadIdx.x / 32, lane = threadIdx.x & 31;
+            const long items = (long)a.ncrows * a.NG;
+            for (long it = (long)blockIdx.x * warps + w; it < items; it += (long)gridDim.x * warps) {
+                const int gr = (int)(it / a.NG), g = (int)(it % a.NG), j0 = g * RPT;
+                const int v = a.crow_var[gr];
+                const BVar &B = a.var[v];
+                bool lv[RPT], any;
+                live_mask<RPT>(a, v, j0, lv, any);
+                if (!any) continue;
+                const int i = gr - B.crow0, m = B.m;
+                float acc[RPT];
+#pragma unroll
+                for (int jj = 0; jj < RPT; ++jj) acc[jj] = 0.f;
+                const float *row = B.Einv32 + (long)i * m;
+                for (int k = lane; k < m; k += 32) {
+                    const float e = __ldg(row + k);
+#pragma unroll
+                    for (int jj = 0; jj < RPT; ++jj)
+                        if (j0 + jj < NR) acc[jj] = fmaf(e, a.cvec[(B.c0 + k) * NR + j0 + jj], acc[jj]);
+                }
+#pragma unroll
+                for (int jj = 0; jj < RPT; ++jj) {
+                    const float s = warp_sum(acc[jj]);
+                    if (lane == 0 && j0 + jj < NR) a.evec[(B.c0 + i) * NR + j0 + jj] = s;
+                }
+            }
+        }
+        if (!sync()) return false;
+        // x += Z e
+        for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
+            const int j0 = g * RPT;
+            bool lv[RPT], any;
+            live_mask<RPT>(a, v, j0, lv, any);
+            if (!any || row >= B.nfree) return;
+            const int I = B.agg_of[row], node = B.node_of_free[row];
+            const float dx = (float)((B.xyz[3L * node] - B.centroid[3L * I]) * B.inv_scale);
+            const float dy = (float)((B.xyz[3L * node + 1] - B.centroid[3L * I + 1]) * B.inv_scale);
+            const float dz = (float)((B.xyz[3L * node + 2] - B.centroid[3L * I + 2]) * B.inv_scale);
+#pragma unroll
+            for (int jj = 0; jj < RPT; ++jj) {
+                if (!lv[jj]) continue;
+                const int j = j0 + jj;
+                float e[6];
+                for (int k = 0; k < 6; ++k) e[k] = a.evec[(B.c0 + 6L * I + k) * NR + j];
+                a.x32[X(B, row, 0) + j] += e[0] + dz * e[4] - dy * e[5];
+                a.x32[X(B, row, 1) + j] += e[1] - dz * e[3] + dx * e[5];
+                a.x32[X(B, row, 2) + j] += e[2] + dy * e[3] - dx * e[4];
+            }
+        });
+        if (!sync()) return false;
+        // post-smoothing: z_new = x + w Dinv32 (b - K32 x); partials r.z_new, r.z_old
+        for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
+            const int j0 = g * RPT;
+            bool lv[RPT], any;
+            live_mask<RPT>(a, v, j0, lv, any);
+            double pn[RPT], po[RPT];
+#pragma unroll
+            for (int jj = 0; jj < RPT; ++jj) pn[jj] = po[jj] = 0;
+            if (any && row < B.nfree) {
+                const int ls = gsl - B.slice0, S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
+                float y[3][RPT];
+                sell_row_multi<float, RPT>(S, row & 31, W, B.scols, B.sv32,
+                                           [&](int k, int jj) {
+                                               return j0 + jj < NR ? a.x32[(B.dof0 + k) * NR + j0 + jj] : 0.f;
+                                           },
+                                           y);
+#pragma unroll
+                for (int jj = 0; jj < RPT; ++jj) {
+                    if (!lv[jj]) continue;
+                    const int j = j0 + jj;
+                    float res[3], cor[3];
+                    for (int c = 0; c < 3; ++c) res[c] = a.b32[X(B, row, c) + j] - y[c][jj];
+                    block3_apply(B.Dinv32 + 9L * row, res, cor);
+                    for (int c = 0; c < 3; ++c) {
+                        const long d = X(B, row, c) + j;
+                        const float z = a.x32[d] + B.wsm * cor[c];
+                        const double rv = a.r[d];
+                        pn[jj] += rv * (double)z;
+                        if (zold) po[jj] += rv * (double)zold[d];
+                        znew[d] = z;
+                    }
+                }
+            }
+            store_partials<RPT>(a, a.pa, gsl, j0, pn);
+            store_partials<RPT>(a, a.pb, gsl, j0, po);
+        });
+        return sync();
+    };
+
+    float *zcur = a.zA, *znext = a.zB;
+    if (MIXED) {
+        if (!precondition(zcur, nullptr)) return;
+        for_pairs(a, false, [&](int v, int j, double rz, double) { a.rz[v * NR + j] = rz; });
+    } else {
+        // PCG64: r.z from z64 = Dinv r
+        for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
+            const int j0 = g * RPT;
+            double p[RPT];
+#pragma unroll
+            for (int jj = 0; jj < RPT; ++jj) {
+                p[jj] = 0;
+                if (row < B.nfree && j0 + jj < NR)
+                    for (int c = 0; c < 3; ++c) p[jj] += a.r[X(B, row, c) + j0 + jj] * a.z64[X(B, row, c) + j0 + jj];
+            }
+            store_partials<RPT>(a, a.pa, gsl, j0, p);
+        });
+        if (!sync()) return;
+        for_pairs(a, false, [&](int v, int j, double rz, double) { a.rz[v * NR + j] = rz; });
+    }
+    if (!sync()) return;
+
+    for (int k = 0; k < a.max_iter; ++k) {
+        double *pnew = (k & 1) ? a.p1 : a.p0;
+        const double *pold = (k & 1) ? a.p0 : a.p1;
+        // live_cnt[k % 3] counts the load cases still running after iteration k;
+        // slot (k + 1) % 3 was last read two barriers ago at least
+        if (blockIdx.x == 0 && threadIdx.x == 0) a.live_cnt[(k + 1) % 3] = 0;
+        // A: p = z + beta p_old, q = K64 p, partial p.q
+        for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
+            const int j0 = g * RPT;
+            bool lv[RPT], any;
+            live_mask<RPT>(a, v, j0, lv, any);
+            double ppq[RPT], bt[RPT];
+#pragma unroll
+            for (int jj = 0; jj < RPT; ++jj) {
+                ppq[jj] = 0;
+                bt[jj] = lv[jj] ? a.beta[v * NR + j0 + jj] : 0.0;
+            }
+            if (any && row < B.nfree) {
+                const int ls = gsl - B.slice0, S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
+                double y[3][RPT];
+                auto zval = [&](long d) -> double { return MIXED ? (double)zcur[d] : a.z64[d]; };
+                sell_row_multi<double, RPT>(S, row & 31, W, B.scols, B.sv64,
+                                            [&](int kk, int jj) {
+                                                if (!lv[jj]) return 0.0;
+                                                const long d = (B.dof0 + kk) * NR + j0 + jj;
+                                                return fma(bt[jj], pold[d], zval(d));
+                                            },
+                                            y);
+#pragma unroll
+                for (int jj = 0; jj < RPT; ++jj) {
+                    if (!lv[jj]) continue;
+                    for (int c = 0; c < 3; ++c) {
+                        const long d = X(B, row, c) + j0 + jj;
+                        const double pn = fma(bt[jj], pold[d], zval(d));
+                        pnew[d] = pn;
+                        a.q[d] = y[c][jj];
+                        ppq[jj] += pn * y[c][jj];
+                    }
+                }
+            }
+            store_partials<RPT>(a, a.pa, gsl, j0, ppq);
+        });
+        if (!sync()) return;
+        for_pairs(a, false, [&](int v, int j, double pq, double) {
+            const int vj = v * NR + j;
+            if (!a.live[vj]) return;
+            if (!(pq > 0.0) || !isfinite(pq)) {
+                a.live[vj] = 0;
+                a.status[vj] = OFEA_ERR_BREAKDOWN;
+                a.iters[vj] = k;
+                return;
+            }
+            a.alpha[vj] = a.rz[vj] / pq;
+        });
+        if (!sync()) return;
+        // B: u += alpha p, r -= alpha q, partial ||r||^2; start of M(r)
+        for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
+            const int j0 = g * RPT;
+            bool lv[RPT], any;
+            live_mask<RPT>(a, v, j0, lv, any);
+            double prr[RPT], prz[RPT];
+#pragma unroll
+            for (int jj = 0; jj < RPT; ++jj) prr[jj] = prz[jj] = 0;
+            if (any && row < B.nfree) {
+#pragma unroll
+                for (int jj = 0; jj < RPT; ++jj) {
+                    if (!lv[jj]) continue;
+                    const int j = j0 + jj;
+                    const double al = a.alpha[v * NR + j];
+                    double rv[3];
+                    for (int c = 0; c < 3; ++c) {
+                        const long d = X(B, row, c) + j;
+                        a.u[d] = fma(al, pnew[d], a.u[d]);
+                        rv[c] = fma(-al, a.q[d], a.r[d]);
+                        a.r[d] = rv[c];
+                        prr[jj] += rv[c] * rv[c];
+                    }
+                    if (MIXED) {
+                        float b[3], x[3];
+                        for (int c = 0; c < 3; ++c) b[c] = (float)rv[c];
+                        block3_apply(B.Dinv32 + 9L * row, b, x);
+                        for (int c = 0; c < 3; ++c) {
+                            a.b32[X(B, row, c) + j] = b[c];
+                            a.x32[X(B, row, c) + j] = B.wsm * x[c];
+                        }
+                    } else {
+                        double z[3];
+                        block3_apply(B.Dinv + 9L * row, rv, z);
+                        for (int c = 0; c < 3; ++c) {
+                            a.z64[X(B, row, c) + j] = z[c];
+                            prz[jj] += rv[c] * z[c];
+                        }
+                    }
+                }
+            }
+            store_partials<RPT>(a, a.pa, gsl, j0, prr);
+            if (!MIXED) store_partials<RPT>(a, a.pb, gsl, j0, prz);
+        });
+        if (!sync()) return;
+        for_pairs(a, !MIXED, [&](int v, int j, double rr, double rz) {
+            const int vj = v * NR + j;
+            if (!a.live[vj]) return;
+            a.iters[vj] = k + 1;
+            if (!isfinite(rr)) {
+                a.live[vj] = 0;
+                a.status[vj] = OFEA_ERR_BREAKDOWN;
+                return;
+            }
+            if (rr <= a.tol2[vj]) {
+                a.live[vj] = 0;
+                return;
+            }
+            if (k + 1 >= a.max_iter) {
+                a.live[vj] = 0;
+                a.status[vj] = OFEA_ERR_NOT_CONVERGED;
+                return;
+            }
+            if (!MIXED) {
+                a.beta[vj] = rz / a.rz[vj];
+                a.rz[vj] = rz;
+            }
+            atomicAdd(&a.live_cnt[k % 3], 1);
+        });
+        if (!sync()) return;
+        if (*(volatile int *)&a.live_cnt[k % 3] == 0) break;
+        if (MIXED) {
+            if (!precondition(znext, zcur)) return;
+            for_pairs(a, true, [&](int v, int j, double rzn, double rzo) {
+                const int vj = v * NR + j;
+                if (!a.live[vj]) return;
+                a.beta[vj] = (rzn - rzo) / a.rz[vj];
+                a.rz[vj] = rzn;
+            });
+            if (!sync()) return;
+            float *tz = zcur;
+            zcur = znext;
+            znext = tz;
+        }
+    }
+}
+
+// Load-case interleaving of the host-ordered right-hand sides / solutions:
+// dst[(dof0 + i) * NR + j] = src[j * n + i] (and back).
+__global__ void k_interleave(long n, int nrhs, int NR, long dof0, const double *__restrict__ src,
+                             double *__restrict__ dst) {
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < n * nrhs; g += (long)gridDim.x * blockDim.x) {
+        const long j = g / n, i = g % n;
+        dst[(dof0 + i) * NR + j] = src[g];
+    }
+}
+__global__ void k_deinterleave(long n, int nrhs, int NR, long dof0, const double *__restrict__ src,
+                               double *__restrict__ dst) {
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < n * nrhs; g += (long)gridDim.x * blockDim.x) {
+        const long j = g / n, i = g % n;
+        dst[g] = src[(dof0 + i) * NR + j];
+    }
+}
+
+// True FP64 residual partials per (slice, load case): ||f - K u||^2 (pa), ||f||^2 (pb).
+template <int RPT>
+__global__ void __launch_bounds__(256) k_batch_residual(BArgs a) {
+    const int NR = a.NR;
+    for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
+        const int j0 = g * RPT;
+        double prr[RPT], pff[RPT];
+#pragma unroll
+        for (int jj = 0; jj < RPT; ++jj) prr[jj] = pff[jj] = 0;
+        if (row < B.nfree) {
+            const int ls = gsl - B.slice0, S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
+            double y[3][RPT];
+            sell_row_multi<double, RPT>(S, row & 31, W, B.scols, B.sv64,
+                                        [&](int k, int jj) {
+                                            return j0 + jj < NR ? a.u[(B.dof0 + k) * NR + j0 + jj] : 0.0;
+                                        },
+                                        y);
+#pragma unroll
+            for (int jj = 0; jj < RPT; ++jj) {
+                if (j0 + jj >= NR) continue;
+                for (int c = 0; c < 3; ++c) {
+                    const double fv = a.f[(B.dof0 + 3L * row + c) * NR + j0 + jj];
+                    const double rv = fv - y[c][jj];
+                    prr[jj] += rv * rv;
+                    pff[jj] += fv * fv;
+                }
+            }
+        }
+        store_partials<RPT>(a, a.pa, gsl, j0, prr);
+        store_partials<RPT>(a, a.pb, gsl, j0, pff);
+    });
+}
+
+// Per (variant, load case): rel = sqrt(rr / ff) into alpha (reused as output).
+__global__ void k_batch_rel(BArgs a, double *rel) {
+    for_pairs(a, true, [&](int v, int j, double rr, double ff) {
+        rel[v * a.NR + j] = ff > 0.0 ? sqrt(rr / ff) : 0.0;
+    });
+}
+
+// A bounded wait that nothing releases: one extra arrival is expected at
+// the first barrier, so every CTA's wait runs out after limit_ns and the
+// kernel reports the failure (used to test the failure path).
+__global__ void k_barrier_probe(GridSync *gs, unsigned extra, unsigned long long limit_ns, int *out) {
+    const bool ok = grid_barrier(gs, gridDim.x + extra, limit_ns);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *out = ok ? 1 : 0;
+}
+
+
+// ------------------------------------------------------------------ host --
+
+namespace {
+
+struct TuneCfg {
+    int rpt = 4, threads = 256, ctas_per_sm = 1;
+    double ms_per_iter = 0.0;
+};
+
+// Kernel instance for (rpt, mixed).
+const void *solve_kernel(int rpt, bool mixed) {
+    switch (rpt) {
+        case 1: return mixed ? (const void *)k_batch_solve<1, true> : (const void *)k_batch_solve<1, false>;
+        case 2: return mixed ? (const void *)k_batch_solve<2, true> : (const void *)k_batch_solve<2, false>;
+        case 4: return mixed ? (const void *)k_batch_solve<4, true> : (const void *)k_batch_solve<4, false>;
+        case 8: return mixed ? (const void *)k_batch_solve<8, true> : (const void *)k_batch_solve<8, false>;
+    }
+    fail(OFEA_ERR_INVALID_ARG, "unsupported load cases per thread");
+}
+const void *residual_kernel(int rpt) {
+    switch (rpt) {
+        case 1: return (const void *)k_batch_residual<1>;
+        case 2: return (const void *)k_batch_residual<2>;
+        case 4: return (const void *)k_batch_residual<4>;
+        case 8: return (const void *)k_batch_residual<8>;
+    }
+    fail(OFEA_ERR_INVALID_ARG, "unsupported load cases per thread");
+}
+
+// ---- the on-disk tuning cache: one JSON object per line inside "entries"
+std::mutex g_tune_mu;
+
+std::string tune_path() {
+    if (const char *p = std::getenv("OFEA_TUNE_FILE")) return p;
+    const char *home = std::getenv("HOME");
+    return std::string(home ? home : ".") + "/.cache/openfea_b200_tune.json";
+}
+
+std::map<std::string, TuneCfg> tune_load(const std::string &path) {
+    std::map<std::string, TuneCfg> out;
+    std::ifstream in(path);
+    std::string line;
+    auto num = [](const std::string &l, const char *k, double dflt) {
+        const std::string key = std::string("\"") + k + "\": ";
+        const size_t p = l.find(key);
+        return p == std::string::npos ? dflt : std::strtod(l.c_str() + p + key.size(), nullptr);
+    };
+    while (std::getline(in, line)) {
+        const size_t p = line.find("\"key\": \"");
+        if (p == std::string::npos) continue;
+        const size_t b = p + 8, e = line.find('"', b);
+        if (e == std::string::npos) continue;
+        TuneCfg t;
+        t.rpt = (int)num(line, "rpt", 4);
+        t.threads = (int)num(line, "threads", 256);
+        t.ctas_per_sm = (int)num(line, "ctas_per_sm", 1);
+        t.ms_per_iter = num(line, "ms_per_iter", 0);
+        out[line.substr(b, e - b)] = t;
+    }
+    return out;
+}
+
+void tune_store(const std::string &path, const std::string &key, const TuneCfg &t) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto all = tune_load(path);
+    all[key] = t;
+    const size_t slash = path.rfind('/');
+    if (slash != std::string::npos && slash > 0) mkdir(path.substr(0, slash).c_str(), 0755);  // one level (~/.cache)
+    std::ofstream o(path);
+    if (!o) return;  // the cache is an optimisation: an unwritable path is not an error
+    o << "{\n  \"entries\": [\n";
+    size_t i = 0;
+    for (const auto &kv : all) {
+        char buf[512];
+        std::snprintf(buf, sizeof(buf),
+                      "    {\"key\": \"%s\", \"rpt\": %d, \"threads\": %d, \"ctas_per_sm\": %d, \"ms_per_iter\": %.6f}%s\n",
+                      kv.first.c_str(), kv.second.rpt, kv.second.threads, kv.second.ctas_per_sm,
+                      kv.second.ms_per_iter, ++i < all.size() ? "," : "");
+        o << buf;
+    }
+    o << "  ]\n}\n";
+}
+
+}  // namespace
+
+// ---- the batch plan
+
+}  // namespace ofea
+
+struct ofea_batch {
+    int device = 0, V = 0, NR = 0, num_sms = 148;
+    cudaStream_t stream = nullptr;
+    std::vector<ofea_ctx *> ctx;
+    std::vector<long> dof0, c0;
+    long ndof = 0, ncoarse = 0;
+    int nslices = 0, naggs = 0, ncrows = 0;
+    bool mixed_ready = false, have_rhs = false;
+    ofea::DevBuf<ofea::BVar> var;
+    ofea::DevBuf<int> slice_var, agg_var, crow_var;
+    ofea::DevBuf<double> f, u, r, p0, p1, q, z64, pa, pb, ff, tol2, rz, alpha, beta, rel, stage;
+    ofea::DevBuf<float> b32, x32, t32, zA, zB, cvec, evec;
+    ofea::DevBuf<int> live, iters, status, live_cnt;
+    ofea::DevBuf<ofea::GridSync> gs;
+    std::map<int, ofea::TuneCfg> tuned;  // by method
+    // the captured graph of one launch and what it was captured for
+    cudaGraphExec_t exec = nullptr;
+    std::string exec_key;
+    ~ofea_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+    }
+};
+
+namespace ofea {
+
+namespace {
+
+std::string device_name(int dev) {
+    cudaDeviceProp p{};
+    if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) return "gpu";
+    return p.name;
+}
+
+// Descriptor table; with `mixed` also the coarse levels' pointers and offsets.
+void build_desc(ofea_batch *b, bool mixed) {
+    std::vector<BVar> d(b->V);
+    std::vector<int> sv, av, cv;
+    long c0 = 0;
+    int slice0 = 0, agg0 = 0, crow0 = 0;
+    b->c0.assign(b->V, 0);
+    for (int v = 0; v < b->V; ++v) {
+        ofea_ctx *c = b->ctx[v];
+        BVar &B = d[v];
+        std::memset(&B, 0, sizeof(B));
+        B.nfree = c->nfree;
+        B.nslice = (c->nfree + kSlice - 1) / kSlice;
+        B.slice0 = slice0;
+        B.dof0 = b->dof0[v];
+        B.sl_ptr = c->sl_ptr.p;
+        B.scols = c->scols.p;
+        B.sv64 = c->sv64.p;
+        B.Dinv = c->Dinv.p;
+        B.sv32 = c->sv32.p;
+        B.Dinv32 = c->Dinv32.p;
+        for (int s = 0; s < B.nslice; ++s) sv.push_back(v);
+        slice0 += B.nslice;
+        if (mixed) {
+            const Coarse &C = c->coarse;
+            B.na = C.na;
+            B.m = C.m;
+            B.agg0 = agg0;
+            B.crow0 = crow0;
+            B.c0 = c0;
+            b->c0[v] = c0;
+            B.agg_of = C.agg_of.p;
+            B.agg_ptr = C.agg_ptr.p;
+            B.agg_nodes = C.agg_nodes.p;
+            B.node_of_free = c->node_of_free.p;
+            B.xyz = c->xyz.p;
+            B.centroid = C.centroid.p;
+            B.Einv32 = C.Einv32.p;
+            B.inv_scale = C.inv_scale;
+            B.wsm = smoother_weight(c);
+            for (int a = 0; a < C.na; ++a) av.push_back(v);
+            for (int i = 0; i < C.m; ++i) cv.push_back(v);
+            agg0 += C.na;
+            crow0 += C.m;
+            c0 += C.m;
+        }
+    }
+    b->nslices = slice0;
+    b->naggs = agg0;
+    b->ncrows = crow0;
+    b->ncoarse = c0;
+    cudaStream_t s = b->stream;
+    b->var.upload(d.data(), d.size(), s);
+    b->slice_var.upload(sv.data(), sv.size(), s);
+    if (mixed) {
+        b->agg_var.upload(av.data(), av.size(), s);
+        b->crow_var.upload(cv.data(), cv.size(), s);
+    }
+    const size_t NR = b->NR;
+    b->pa.ensure(std::max<size_t>(1, (size_t)b->nslices * NR));
+    b->pb.ensure(std::max<size_t>(1, (size_t)b->nslices * NR));
+    OFEA_CUDA(cudaStreamSynchronize(s));
+}
+
+void prepare(ofea_batch *b, bool mixed) {
+    if (mixed && !b->mixed_ready) {
+        for (ofea_ctx *c : b->ctx) {
+            setup_coarse(c, c->coarse_nodes);
+            OFEA_CUDA(cudaStreamSynchronize(c->stream));
+        }
+        build_desc(b, true);
+        const size_t n = (size_t)b->ndof * b->NR, nc = std::max<size_t>(1, (size_t)b->ncoarse * b->NR);
+        b->b32.ensure(n);
+        b->x32.ensure(n);
+        b->t32.ensure(n);
+        b->zA.ensure(n);
+        b->zB.ensure(n);
+        b->cvec.ensure(nc);
+        b->evec.ensure(nc);
+        b->mixed_ready = true;
+    }
+    if (!mixed) b->z64.ensure((size_t)b->ndof * b->NR);
+}
+
+BArgs make_args(ofea_batch *b, bool mixed, const TuneCfg &t, int max_iter, double rtol) {
+    BArgs a{};
+    a.V = b->V;
+    a.NR = b->NR;
+    a.NG = (b->NR + t.rpt - 1) / t.rpt;
+    a.nslices = b->nslices;
+    a.naggs = mixed ? b->naggs : 0;
+    a.ncrows = mixed ? b->ncrows : 0;
+    a.max_iter = max_iter;
+    a.extra_arrivals = 0;
+    a.limit_ns = 5000000000ull;  // 5 s: far above any phase
+    a.rtol = rtol;
+    a.var = b->var.p;
+    a.slice_var = b->slice_var.p;
+    a.agg_var = b->agg_var.p;
+    a.crow_var = b->crow_var.p;
+    a.f = b->f.p;
+    a.u = b->u.p;
+    a.r = b->r.p;
+    a.p0 = b->p0.p;
+    a.p1 = b->p1.p;
+    a.q = b->q.p;
+    a.z64 = b->z64.p;
+    a.b32 = b->b32.p;
+    a.x32 = b->x32.p;
+    a.t32 = b->t32.p;
+    a.zA = b->zA.p;
+    a.zB = b->zB.p;
+    a.cvec = b->cvec.p;
+    a.evec = b->evec.p;
+    a.pa = b->pa.p;
+    a.pb = b->pb.p;
+    a.ff = b->ff.p;
+    a.tol2 = b->tol2.p;
+    a.rz = b->rz.p;
+    a.alpha = b->alpha.p;
+    a.beta = b->beta.p;
+    a.live = b->live.p;
+    a.iters = b->iters.p;
+    a.status = b->status.p;
+    a.live_cnt = b->live_cnt.p;
+    a.gs = b->gs.p;
+    return a;
+}
+
+int grid_of(ofea_batch *b, const void *fn, const TuneCfg &t) {
+    int occ = 0;
+    OFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, t.threads, 0));
+    if (occ < 1) fail(OFEA_ERR_CAPACITY, "batched solver kernel does not fit on an SM");
+    return b->num_sms * std::min(occ, t.ctas_per_sm);
+}
+
+// Enqueue one launch: reset of the per-launch state + the cooperative kernel.
+void enqueue(ofea_batch *b, const BArgs &a, const TuneCfg &t, bool mixed) {
+    cudaStream_t s = b->stream;
+    const size_t n = (size_t)b->ndof * b->NR;
+    OFEA_CUDA(cudaMemsetAsync(b->p0.p, 0, sizeof(double) * n, s));
+    OFEA_CUDA(cudaMemsetAsync(b->p1.p, 0, sizeof(double) * n, s));
+    OFEA_CUDA(cudaMemsetAsync(b->gs.p, 0, sizeof(GridSync), s));
+    OFEA_CUDA(cudaMemsetAsync(b->live_cnt.p, 0, sizeof(int) * 3, s));
+    const void *fn = solve_kernel(t.rpt, mixed);
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid_of(b, fn, t));
+    cfg.blockDim = dim3(t.threads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void *args[] = {(void *)&a};
+    OFEA_CUDA(cudaLaunchKernelExC(&cfg, fn, args));
+}
+
+// True FP64 residuals per (variant, load case) into b->rel.
+void residuals(ofea_batch *b, const TuneCfg &t) {
+    BArgs a = make_args(b, false, t, 0, 0.0);
+    cudaStream_t s = b->stream;
+    const void *fn = residual_kernel(t.rpt);
+    const int G = std::min(kMaxGrid, b->num_sms * 8);
+    void *args[] = {(void *)&a};
+    OFEA_CUDA(cudaLaunchKernel(fn, dim3(G), dim3(256), args, 0, s));
+    k_batch_rel<<<std::max(1, std::min(kMaxGrid, (b->V * b->NR + 7) / 8)), 256, 0, s>>>(a, b->rel.p);
+    OFEA_CHECK_LAUNCH();
+}
+
+std::string tune_key(ofea_batch *b, bool mixed) {
+    // problem class: device, method, load cases, rows rounded to 2 significant digits
+    long rows = (long)b->nslices * kSlice;
+    long scale = 1;
+    while (rows / scale >= 100) scale *= 10;
+    std::ostringstream k;
+    k << device_name(b->device) << "|" << (mixed ? "mixed" : "pcg64") << "|nrhs=" << b->NR
+      << "|rows~" << (rows / scale) * scale << "|variants=" << b->V;
+    return k.str();
+}
+
+// Times a few iterations of every candidate and keeps the fastest; the
+// result is cached in the batch and on disk (OFEA_TUNE_FILE or
+// ~/.cache/openfea_b200_tune.json), keyed by device and problem class.
+TuneCfg autotune(ofea_batch *b, bool mixed, double rtol) {
+    const std::string key = tune_key(b, mixed);
+    const std::string path = tune_path();
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto all = tune_load(path);
+        auto it = all.find(key);
+        if (it != all.end()) {
+            TuneCfg t = it->second;
+            if ((t.rpt == 1 || t.rpt == 2 || t.rpt == 4 || t.rpt == 8) && (t.threads == 128 || t.threads == 256) &&
+                t.ctas_per_sm >= 1 && t.ctas_per_sm <= 16)
+                return t;
+        }
+    }
+    std::vector<TuneCfg> cand;
+    for (int rpt : {1, 2, 4, 8}) {
+        if (rpt > 1 && rpt / 2 >= b->NR) continue;  // groups wider than the load cases
+        for (int th : {128, 256}) {
+            int occ = 0;
+            OFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_kernel(rpt, mixed), th, 0));
+            std::vector<int> cps{1, 2, occ};
+            std::sort(cps.begin(), cps.end());
+            cps.erase(std::unique(cps.begin(), cps.end()), cps.end());
+            for (int c : cps)
+                if (c >= 1 && c <= occ) cand.push_back(TuneCfg{rpt, th, c, 0.0});
+        }
+    }
+    const int iters = 6;
+    cudaEvent_t e0, e1;
+    OFEA_CUDA(cudaEventCreate(&e0));
+    OFEA_CUDA(cudaEventCreate(&e1));
+    TuneCfg best;
+    double best_ms = 1e300;
+    cudaStream_t s = b->stream;
+    for (TuneCfg &t : cand) {
+        double ms_min = 1e300;
+        for (int rep = 0; rep < 2; ++rep) {
+            OFEA_CUDA(cudaMemsetAsync(b->u.p, 0, sizeof(double) * b->ndof * b->NR, s));
+            BArgs a = make_args(b, mixed, t, iters, rtol);
+            OFEA_CUDA(cudaEventRecord(e0, s));
+            enqueue(b, a, t, mixed);
+            OFEA_CUDA(cudaEventRecord(e1, s));
+            OFEA_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            OFEA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            GridSync g{};
+            OFEA_CUDA(cudaMemcpy(&g, b->gs.p, sizeof(g), cudaMemcpyDeviceToHost));
+            if (g.err) fail(OFEA_ERR_TIMEOUT, "batched solver: a grid-barrier wait ran out while tuning");
+            ms_min = std::min(ms_min, (double)ms);
+        }
+        t.ms_per_iter = ms_min / iters;
+        if (ms_min < best_ms) {
+            best_ms = ms_min;
+            best = t;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    tune_store(path, key, best);
+    return best;
+}
+
+}  // namespace
+
+ofea_batch *batch_create(ofea_ctx *const *ctxs, int nv, int nrhs) {
+    if (!ctxs || nv < 1) fail(OFEA_ERR_INVALID_ARG, "batch: no variants");
+    if (nrhs < 1 || nrhs > kMaxBatchRhs)
+        fail(OFEA_ERR_CAPACITY, "batch: 1 to " + std::to_string(kMaxBatchRhs) + " load cases per variant");
+    auto b = std::make_unique<ofea_batch>();
+    b->V = nv;
+    b->NR = nrhs;
+    for (int v = 0; v < nv; ++v) {
+        ofea_ctx *c = ctxs[v];
+        if (!c) fail(OFEA_ERR_INVALID_ARG, "batch: NULL context");
+        if (!c->K_ok || !c->sell_ok) fail(OFEA_ERR_STATE, "batch: variant " + std::to_string(v) + " not assembled");
+        if (c->device != ctxs[0]->device) fail(OFEA_ERR_INVALID_ARG, "batch: variants on different GPUs");
+        b->ctx.push_back(c);
+    }
+    b->device = ctxs[0]->device;
+    b->num_sms = ctxs[0]->num_sms;
+    b->stream = ctxs[0]->stream;
+    OFEA_CUDA(cudaSetDevice(b->device));
+    int coop = 0;
+    OFEA_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, b->device));
+    if (!coop) fail(OFEA_ERR_NO_DEVICE, "batch: the GPU does not support cooperative launches");
+    long d0 = 0;
+    for (ofea_ctx *c : b->ctx) {
+        b->dof0.push_back(d0);
+        d0 += c->n;
+    }
+    b->ndof = d0;
+    const size_t n = std::max<size_t>(1, (size_t)b->ndof * nrhs), vj = (size_t)nv * nrhs;
+    for (auto *buf : {&b->f, &b->u, &b->r, &b->p0, &b->p1, &b->q}) buf->ensure(n);
+    for (auto *buf : {&b->ff, &b->tol2, &b->rz, &b->alpha, &b->beta, &b->rel}) buf->ensure(vj);
+    for (auto *buf : {&b->live, &b->iters, &b->status}) buf->ensure(vj);
+    b->live_cnt.ensure(3);
+    b->gs.ensure(1);
+    OFEA_CUDA(cudaMemsetAsync(b->f.p, 0, sizeof(double) * n, b->stream));
+    OFEA_CUDA(cudaMemsetAsync(b->u.p, 0, sizeof(double) * n, b->stream));
+    build_desc(b.get(), false);
+    return b.release();
+}
+
+void batch_destroy(ofea_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    delete b;
+}
+
+void batch_set_rhs(ofea_batch *b, const double *const *f) {
+    OFEA_CUDA(cudaSetDevice(b->device));
+    cudaStream_t s = b->stream;
+    for (int v = 0; v < b->V; ++v) {
+        const long n = b->ctx[v]->n;
+        if (!f[v]) fail(OFEA_ERR_INVALID_ARG, "batch: NULL load array");
+        b->stage.ensure((size_t)n * b->NR);
+        OFEA_CUDA(cudaMemcpyAsync(b->stage.p, f[v], sizeof(double) * n * b->NR, cudaMemcpyHostToDevice, s));
+        k_interleave<<<std::max(1, std::min(kMaxGrid, (int)((n * b->NR + 255) / 256))), 256, 0, s>>>(
+            n, b->NR, b->NR, b->dof0[v], b->stage.p, b->f.p);
+        OFEA_CHECK_LAUNCH();
+    }
+    OFEA_CUDA(cudaStreamSynchronize(s));
+    b->have_rhs = true;
+}
+
+void batch_get_solution(ofea_batch *b, double *const *u) {
+    OFEA_CUDA(cudaSetDevice(b->device));
+    cudaStream_t s = b->stream;
+    for (int v = 0; v < b->V; ++v) {
+        const long n = b->ctx[v]->n;
+        if (!u[v]) fail(OFEA_ERR_INVALID_ARG, "batch: NULL solution array");
+        b->stage.ensure((size_t)n * b->NR);
+        k_deinterleave<<<std::max(1, std::min(kMaxGrid, (int)((n * b->NR + 255) / 256))), 256, 0, s>>>(
+            n, b->NR, b->NR, b->dof0[v], b->u.p, b->stage.p);
+        OFEA_CHECK_LAUNCH();
+        OFEA_CUDA(cudaMemcpyAsync(u[v], b->stage.p, sizeof(double) * n * b->NR, cudaMemcpyDeviceToHost, s));
+        OFEA_CUDA(cudaStreamSynchronize(s));
+    }
+}
+
+void batch_tuning(ofea_batch *b, int method, int *rpt, int *threads, int *ctas_per_sm, double *ms_per_iter) {
+    const bool mixed = method == OFEA_SOLVER_MIXED;
+    OFEA_CUDA(cudaSetDevice(b->device));
+    prepare(b, mixed);
+    auto it = b->tuned.find(method);
+    if (it == b->tuned.end()) it = b->tuned.emplace(method, autotune(b, mixed, 1e-8)).first;
+    const TuneCfg &t = it->second;
+    if (rpt) *rpt = t.rpt;
+    if (threads) *threads = t.threads;
+    if (ctas_per_sm) *ctas_per_sm = t.ctas_per_sm;
+    if (ms_per_iter) *ms_per_iter = t.ms_per_iter;
+}
+
+// Solves all (variant, load case) pairs on the resident right-hand sides.
+// One graph launch per attempt; a pair whose true FP64 residual misses rtol
+// after the kernel (recurrence drift) is resumed from its u by the next
+// attempt.  stats: one per variant (worst load case).
+void batch_solve(ofea_batch *b, const ofea_solve_opts &o, ofea_solve_stats *stats) {
+    if (o.method != OFEA_SOLVER_MIXED && o.method != OFEA_SOLVER_PCG64)
+        fail(OFEA_ERR_UNKNOWN_SOLVER, "batch: method must be OFEA_SOLVER_PCG64 or OFEA_SOLVER_MIXED");
+    if (!b->have_rhs) fail(OFEA_ERR_STATE, "batch: no load cases set");
+    if (!(o.rtol > 0) || o.max_iter < 1) fail(OFEA_ERR_INVALID_ARG, "batch: bad rtol / max_iter");
+    const bool mixed = o.method == OFEA_SOLVER_MIXED;
+    OFEA_CUDA(cudaSetDevice(b->device));
+    prepare(b, mixed);
+    int rpt = 0;
+    batch_tuning(b, o.method, &rpt, nullptr, nullptr, nullptr);
+    const TuneCfg t = b->tuned[o.method];
+    cudaStream_t s = b->stream;
+    const int VJ = b->V * b->NR;
+    std::vector<int> iters_tot(VJ, 0), hit(VJ), hst(VJ);
+    std::vector<double> hrel(VJ);
+    cudaEvent_t e0, e1;
+    OFEA_CUDA(cudaEventCreate(&e0));
+    OFEA_CUDA(cudaEventCreate(&e1));
+    OFEA_CUDA(cudaMemsetAsync(b->u.p, 0, sizeof(double) * b->ndof * b->NR, s));
+    OFEA_CUDA(cudaEventRecord(e0, s));
+    int attempts = 0, launches = 0, remaining = o.max_iter;
+    bool failed_barrier = false;
+    for (; attempts < 4 && remaining > 0; ++attempts) {
+        BArgs a = make_args(b, mixed, t, remaining, o.rtol);
+        std::ostringstream k;
+        k << o.method << "/" << t.rpt << "/" << t.threads << "/" << t.ctas_per_sm << "/" << remaining << "/"
+          << o.rtol;
+        if (o.use_graph) {
+            if (!b->exec || b->exec_key != k.str()) {
+                if (b->exec) {
+                    cudaGraphExecDestroy(b->exec);
+                    b->exec = nullptr;
+                }
+                cudaGraph_t g = nullptr;
+                OFEA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                try {
+                    enqueue(b, a, t, mixed);
+                } catch (...) {
+                    cudaStreamEndCapture(s, &g);
+                    if (g) cudaGraphDestroy(g);
+                    throw;
+                }
+                OFEA_CUDA(cudaStreamEndCapture(s, &g));
+                cudaError_t e = cudaGraphInstantiate(&b->exec, g, 0);
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess) fail_cuda(e, "cudaGraphInstantiate(batched solve)", __FILE__, __LINE__);
+                b->exec_key = k.str();
+            }
+            OFEA_CUDA(cudaGraphLaunch(b->exec, s));
+        } else {
+            enqueue(b, a, t, mixed);
+        }
+        ++launches;
+        residuals(b, t);
+        launches += 2;
+        GridSync g{};
+        OFEA_CUDA(cudaMemcpyAsync(&g, b->gs.p, sizeof(g), cudaMemcpyDeviceToHost, s));
+        OFEA_CUDA(cudaMemcpyAsync(hit.data(), b->iters.p, sizeof(int) * VJ, cudaMemcpyDeviceToHost, s));
+        OFEA_CUDA(cudaMemcpyAsync(hst.data(), b->status.p, sizeof(int) * VJ, cudaMemcpyDeviceToHost, s));
+        OFEA_CUDA(cudaMemcpyAsync(hrel.data(), b->rel.p, sizeof(double) * VJ, cudaMemcpyDeviceToHost, s));
+        OFEA_CUDA(cudaStreamSynchronize(s));
+        if (g.err) {
+            failed_barrier = true;
+            break;
+        }
+        int most = 0;
+        bool again = false;
+        for (int i = 0; i < VJ; ++i) {
+            iters_tot[i] += hit[i];
+            most = std::max(most, hit[i]);
+            if (hst[i] == OFEA_OK && !(hrel[i] <= o.rtol)) again = true;
+        }
+        remaining -= std::max(most, 1);
+        if (!again) break;
+    }
+    OFEA_CUDA(cudaEventRecord(e1, s));
+    OFEA_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    OFEA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (failed_barrier) fail(OFEA_ERR_TIMEOUT, "batched solver: a grid-barrier wait ran out");
+    if (stats) {
+        for (int v = 0; v < b->V; ++v) {
+            ofea_solve_stats &st = stats[v];
+            st = ofea_solve_stats{};
+            int worst = OFEA_OK;
+            for (int j = 0; j < b->NR; ++j) {
+                const int i = v * b->NR + j;
+                st.iterations = std::max(st.iterations, iters_tot[i]);
+                st.rel_residual = std::max(st.rel_residual, hrel[i]);
+                int sj = hst[i];
+                if (sj == OFEA_OK && !(hrel[i] <= o.rtol)) sj = OFEA_ERR_NOT_CONVERGED;
+                if (sj != OFEA_OK) worst = sj;
+            }
+            st.status = worst;
+            st.refinements = attempts;
+            st.seconds = ms * 1e-3;
+            st.kernel_launches = launches;
+        }
+    }
+}
+
+// A cooperative launch whose barrier expects one CTA more than it has: every
+// wait runs out after limit_ms and the kernel reports it (*released = 0).
+void barrier_probe(ofea_ctx *c, int limit_ms, int *released) {
+    DevBuf<GridSync> gs;
+    DevBuf<int> out;
+    gs.ensure(1);
+    out.ensure(1);
+    cudaStream_t s = c->stream;
+    OFEA_CUDA(cudaMemsetAsync(gs.p, 0, sizeof(GridSync), s));
+    OFEA_CUDA(cudaMemsetAsync(out.p, 0xff, sizeof(int), s));
+    unsigned extra = 1;
+    unsigned long long lim = (unsigned long long)limit_ms * 1000000ull;
+    void *args[] = {(void *)&gs.p, (void *)&extra, (void *)&lim, (void *)&out.p};
+    OFEA_CUDA(cudaLaunchCooperativeKernel((const void *)k_barrier_probe, dim3(c->num_sms), dim3(64), args, 0, s));
+    int h = -1;
+    OFEA_CUDA(cudaMemcpyAsync(&h, out.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    OFEA_CUDA(cudaStreamSynchronize(s));
+    *released = h;
+}
+
+}  // namespace ofea

@@ -9,6 +9,8 @@ void build_aggregation_fine(ofea_ctx *c);
 // Aggregation (once per mesh), E = Z^T K Z, its inverse and lambda_max(D^-1 K)
 // (once per K).
 void setup_coarse(ofea_ctx *c, int target_nodes);
+// Damping weight of the block-Jacobi smoother (needs setup_coarse's lmax).
+float smoother_weight(const ofea_ctx *c);
 // x += Z E^-1 Z^T t  (FP32 vectors of n entries)
 // evec = E^-1 cvec (FP32 GEMV with the coarse level's inverse)
 void coarse_gemv(ofea_ctx *c, const float *cvec, float *evec);

@@ -452,14 +452,14 @@ void drive(ofea_ctx *c, const ofea_solve_opts &o, Workspace &ws, int per_chunk, 
 
 int solver_grid(const ofea_ctx *c) { return std::min(kMaxGrid, c->num_sms * (2048 / kBlock)); }
 
+}  // namespace
+
 // Chebyshev degree-1 damping of the smoother: 1/theta, theta the midpoint of
 // [lmax/30, 1.1 lmax].
 float smoother_weight(const ofea_ctx *c) {
     const double hi = 1.1 * c->coarse.lmax, lo = hi / 30.0;
     return (float)(2.0 / (hi + lo));
 }
-
-}  // namespace
 
 void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_opts &o,
                   ofea_solve_stats &st, const std::function<void(const double *)> &on_chunk) {

@@ -1,0 +1,90 @@
+"""The persistent batched solver (ofea_batch_*): several SIMP design variants
+of uneven length x several load cases, solved by one cooperative kernel,
+against the per-variant solver, the oracle's assembly + a direct solve, its
+own determinism, and the failure path of its grid barrier."""
+import json
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+import openfea_b200 as ob
+from openfea_b200 import meshgen as mg
+
+pytestmark = pytest.mark.gpu
+
+
+def variants(factory, count=4, nrhs=5, nmin=4, nmax=9):
+    out = []
+    for m, F in mg.design_variants(count=count, nrhs=nrhs, ny=4, nz=4, nmin=nmin, nmax=nmax):
+        ctx = factory()
+        fm = ctx.upload_mesh(m)
+        ctx.assemble_pattern()
+        ctx.assemble_linear()
+        loads = np.stack([mg.to_free(F[j], fm) for j in range(nrhs)])
+        out.append((ctx, m, fm, loads))
+    return out
+
+
+def true_rel_residual(ctx, U, F):
+    rp, ci, val = ctx.get_csr()
+    K = sp.csr_matrix((val, ci, rp), shape=(ctx.n, ctx.n))
+    return max(np.linalg.norm(F[j] - K @ U[j]) / np.linalg.norm(F[j]) for j in range(F.shape[0]))
+
+
+@pytest.mark.parametrize("method", ["GPU_MIXED", "GPU_PCG"])
+def test_batched_matches_per_variant_solves(gpu_ctx_factory, tmp_path, monkeypatch, method):
+    monkeypatch.setenv("OFEA_TUNE_FILE", str(tmp_path / "tune.json"))
+    vs = variants(gpu_ctx_factory)
+    b = ob.Batch([v[0] for v in vs], 5)
+    U, st = b.solve([v[3] for v in vs], method=method, rtol=1e-10)
+    for (ctx, m, fm, F), u, s in zip(vs, U, st):
+        assert s["status"] == 0 and s["rel_residual"] <= 1e-10, s
+        assert true_rel_residual(ctx, u, F) <= 1e-10
+        ref, _ = ctx.solve(F.T, method="GPU_PCG", rtol=1e-12)
+        assert np.linalg.norm(u - ref.T) / np.linalg.norm(ref) < 1e-6
+    # the autotuner chose a configuration and kept it on disk
+    t = b.tuning(method)
+    assert t["rhs_per_thread"] in (1, 2, 4, 8) and t["threads"] in (128, 256) and t["ms_per_iteration"] > 0
+    data = json.load(open(tmp_path / "tune.json"))
+    assert any("nrhs=5" in e["key"] for e in data["entries"])
+    b.close()
+
+
+def test_batched_against_oracle_direct_solve(gpu_ctx_factory, oracle):
+    vs = variants(gpu_ctx_factory, count=2, nrhs=3)
+    U, st = ob.solve_batched([v[0] for v in vs], [v[3] for v in vs], method="GPU_MIXED", rtol=1e-10)
+    for (ctx, m, fm, F), u in zip(vs, U):
+        cp, ri, val = oracle.assemble(m, fm)
+        K = sp.csc_matrix((val, ri, cp), shape=(ctx.n, ctx.n))
+        ref = spla.spsolve(K, F.T)
+        assert np.linalg.norm(u - ref.T) / np.linalg.norm(ref) < 1e-6
+
+
+def test_batched_is_deterministic_and_handles_one_load_case(gpu_ctx_factory):
+    vs = variants(gpu_ctx_factory, count=3, nrhs=1)
+    b = ob.Batch([v[0] for v in vs], 1)
+    U1, _ = b.solve([v[3] for v in vs], method="GPU_MIXED", rtol=1e-9)
+    U2, _ = b.solve([v[3] for v in vs], method="GPU_MIXED", rtol=1e-9)
+    for a, c in zip(U1, U2):
+        assert np.array_equal(a, c)
+    b.close()
+
+
+def test_batched_rejects_too_many_load_cases(gpu_ctx_factory):
+    vs = variants(gpu_ctx_factory, count=1, nrhs=1)
+    with pytest.raises(ob.OfeaError) as e:
+        ob.Batch([vs[0][0]], 33)
+    assert e.value.code == -7
+
+
+def test_grid_barrier_wait_runs_out_and_context_stays_usable(gpu_ctx_factory):
+    vs = variants(gpu_ctx_factory, count=1, nrhs=2)
+    ctx = vs[0][0]
+    assert ob.check_barrier_timeout(ctx, limit_ms=20) == 0
+    b = ob.Batch([ctx], 2)
+    U, st = b.solve([vs[0][3]], method="GPU_MIXED", rtol=1e-9)
+    assert st[0]["status"] == 0
+    b.close()
