@@ -5,20 +5,22 @@
 // case (src/solver/solver_superlu.cpp:31-94, the CA reanalysis of
 // src/ca_analysis.cpp:148-248).
 //
-// Layout in HBM: the variants' DOF are concatenated (variant v starts at dof0[v])
-// and every vector is load-case interleaved, x[(dof0 + i) * NR + j], so that a
-// gather of one DOF fetches the values of all load cases in one contiguous
-// run.  Matrices stay where their contexts keep them (BSELL-32, FP64 and FP32
-// copies); a table of per-variant descriptors points at them.
+// Layout in HBM: the variants' DOF are concatenated (variant v starts at
+// dof0[v]) and every vector is load-case interleaved, x[(dof0 + d) * NR + j]:
+// the NR load cases of one DOF are one contiguous run.  Matrices stay where their contexts
+// keep them (BSELL-32, FP64 and FP32 copies); a table of per-variant
+// descriptors points at them.
 //
 // Algorithm per (variant, load case): the MIXED method of solve.cu, FP64
 // flexible CG with the FP32 two-level V(1,1) preconditioner of precond.cu, or
 // PCG64 (FP64 CG, block Jacobi).  The kernel runs every variant in lock step
-// through phases separated by grid barriers; a phase's work items are the
-// (slice of 32 block rows, group of RPT load cases) pairs of all variants, or
-// (aggregate, group), (coarse row, group), (variant, load case).  A warp
-// takes one item: lane t owns block row t of the slice, so the matrix loads
-// are coalesced BSELL lines shared by the RPT load cases the lane carries.
+// through phases separated by grid barriers.  In the matrix phases a CTA owns
+// one slice (32 block rows) of some variant at a time: it stages the slice's
+// BSELL slots in shared memory (cp.async, double-buffered), and its
+// threads take (block row, load case) pairs, JW lanes per row, so each matrix
+// value is read from HBM once for all load cases and every gather of x is one
+// contiguous run of load cases.  Other phases take (aggregate), (coarse row)
+// or (variant, load case) items per warp.
 // Per-(variant, load case) scalars come from per-slice partial sums reduced
 // in a fixed order: results are bitwise reproducible.  Converged load cases
 // stop updating; the kernel ends when none is left or at max_iter.
@@ -52,8 +54,8 @@ constexpr int kMaxBatchRhs = 32;
 
 // Per-variant descriptor (device copy).
 struct BVar {
-    int nfree, nslice, slice0, na, m, agg0, crow0, pad;
-    long dof0;  // first DOF of the variant in the batch vectors (times NR)
+    int nfree, nslice, slice0, na, m, agg0, crow0, n;
+    long dof0;  // first DOF of the variant in the batch (its vectors start at dof0 * NR)
     long c0;    // first coarse entry of the variant (times NR)
     const int *sl_ptr, *scols;
     const double *sv64, *Dinv;
@@ -71,7 +73,7 @@ struct GridSync {
 };
 
 struct BArgs {
-    int V, NR, NG, nslices, naggs, ncrows, max_iter, extra_arrivals;
+    int V, NR, kc, nslices, naggs, ncrows, max_iter, extra_arrivals;
     unsigned long long limit_ns;
     double rtol;
     const BVar *var;
@@ -125,56 +127,122 @@ __device__ bool grid_barrier(GridSync *gs, unsigned nblocks, unsigned long long 
     return s_ok != 0;
 }
 
-// y[c][jj] = sum over the block row's slots of K_blk x(col, jj).
-template <class V, int RPT, class XF>
-__device__ __forceinline__ void sell_row_multi(long S, int t, int W, const int *__restrict__ scols,
-                                               const V *__restrict__ svals, XF xf, V (&y)[3][RPT]) {
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int jj = 0; jj < RPT; ++jj) y[c][jj] = 0;
-    const int *cp = scols + S * kSlice + t;
-    const V *vp = svals + S * 9 * kSlice + t;
-    for (int k = 0; k < W; ++k) {
-        const int col = __ldg(cp + (long)k * kSlice);
-        V v[9];
-#pragma unroll
-        for (int e = 0; e < 9; ++e) v[e] = __ldg(vp + ((long)k * 9 + e) * kSlice);
-#pragma unroll
-        for (int jj = 0; jj < RPT; ++jj) {
-            const V x0 = xf(3 * col, jj), x1 = xf(3 * col + 1, jj), x2 = xf(3 * col + 2, jj);
-            y[0][jj] = fma(v[0], x0, fma(v[1], x1, fma(v[2], x2, y[0][jj])));
-            y[1][jj] = fma(v[3], x0, fma(v[4], x1, fma(v[5], x2, y[1][jj])));
-            y[2][jj] = fma(v[6], x0, fma(v[7], x1, fma(v[8], x2, y[2][jj])));
+// Entry (node i, component c, load case j) of a variant in a batch vector.
+__device__ __forceinline__ long vidx(const BVar &B, int NR, long i, int c, int j) {
+    return (B.dof0 + 3 * i + c) * NR + j;
+}
+
+// Thread roles inside the CTA that owns one slice: JW lanes per block row
+// (one load case each), 32 / JW rows per warp, 32 rows per CTA.
+template <int JW>
+struct Lanes {
+    static constexpr int kRowsPerWarp = 32 / JW;
+    static constexpr int kWarps = 32 / kRowsPerWarp;  // = JW
+    __device__ static int row() { return (threadIdx.x >> 5) * kRowsPerWarp + (threadIdx.x & 31) / JW; }
+    __device__ static int rhs() { return threadIdx.x & (JW - 1); }
+};
+
+// Shared-memory stage of a slice's BSELL slots: two buffers of kKC slots
+// (values in FP64 or FP32, then columns), filled with cp.async while the
+// other buffer is consumed.
+constexpr int kKC = 4;
+struct __align__(128) Stage {
+    double v[2][kKC * 9 * kSlice];  // FP32 values use the first half of each buffer
+    int col[2][kKC * kSlice];
+    double red[32][32];             // [warp][lane] partial sums
+};
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Start copying slots [k0, k0 + kc) of the slice at S into buffer b (16-byte
+// pieces: every chunk is a multiple of 16 bytes at a 16-byte-aligned offset).
+template <class V>
+__device__ __forceinline__ void stage_chunk(Stage &st, int b, long S, int k0, int kc, const int *__restrict__ scols,
+                                            const V *__restrict__ svals) {
+    const char *gv = reinterpret_cast<const char *>(svals + (S + k0) * 9L * kSlice);
+    char *sv = reinterpret_cast<char *>(st.v[b]);
+    const int nv = kc * 9 * kSlice * (int)sizeof(V) / 16;
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) cp_async16(sv + 16 * i, gv + 16 * i);
+    const char *gc = reinterpret_cast<const char *>(scols + (S + k0) * (long)kSlice);
+    char *sc = reinterpret_cast<char *>(st.col[b]);
+    const int nc = kc * kSlice * 4 / 16;
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) cp_async16(sc + 16 * i, gc + 16 * i);
+    cp_async_commit();
+}
+
+// y[c] = (K x)_row for this thread's load case.  The slice's slots stream
+// through shared memory kKC at a time, double-buffered, shared by every load
+// case; a chunk's gathers are all issued before its FMAs.  Called by all
+// threads of the CTA (rows beyond nfree read padding: column 0, value 0).
+template <class V, int JW, class XF>
+__device__ __forceinline__ void spmm_slice(Stage &st, long S, int W, const int *__restrict__ scols,
+                                           const V *__restrict__ svals, XF xf, V (&y)[3]) {
+    const int r = Lanes<JW>::row();
+    y[0] = y[1] = y[2] = 0;
+    const int nch = (W + kKC - 1) / kKC;
+    __syncthreads();  // both buffers are free
+    if (nch > 0) stage_chunk<V>(st, 0, S, 0, min(kKC, W), scols, svals);
+    for (int ch = 0; ch < nch; ++ch) {
+        const int b = ch & 1, k0 = ch * kKC, kc = min(kKC, W - k0);
+        if (ch + 1 < nch) {
+            stage_chunk<V>(st, b ^ 1, S, k0 + kKC, min(kKC, W - k0 - kKC), scols, svals);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
         }
+        __syncthreads();
+        const V *sv = reinterpret_cast<const V *>(st.v[b]);
+        V x[kKC][3];
+#pragma unroll
+        for (int kk = 0; kk < kKC; ++kk)
+            if (kk < kc) {
+                const int col = st.col[b][kk * kSlice + r];
+                x[kk][0] = xf(col, 0);
+                x[kk][1] = xf(col, 1);
+                x[kk][2] = xf(col, 2);
+            }
+#pragma unroll
+        for (int kk = 0; kk < kKC; ++kk)
+            if (kk < kc) {
+                const V *v = sv + kk * 9 * kSlice + r;
+                y[0] = fma(v[0 * kSlice], x[kk][0], fma(v[1 * kSlice], x[kk][1], fma(v[2 * kSlice], x[kk][2], y[0])));
+                y[1] = fma(v[3 * kSlice], x[kk][0], fma(v[4 * kSlice], x[kk][1], fma(v[5 * kSlice], x[kk][2], y[1])));
+                y[2] = fma(v[6 * kSlice], x[kk][0], fma(v[7 * kSlice], x[kk][1], fma(v[8 * kSlice], x[kk][2], y[2])));
+            }
+        __syncthreads();  // buffer b is consumed before it is refilled
     }
 }
 
-// ------------------------------------------------------------ phases --
-
-// Work loop over (slice, group) items, one warp per item.  f(BVar, v, gs, row, j0)
-// is called by every lane (row may be >= nfree: the lane then skips the row
-// but takes part in the warp's reductions).
-template <class F>
-__device__ __forceinline__ void for_slices(const BArgs &a, F f) {
-    const int warps = blockDim.x / 32, w = threadIdx.x / 32, lane = threadIdx.x & 31;
-    const long items = (long)a.nslices * a.NG;
-    for (long it = (long)blockIdx.x * warps + w; it < items; it += (long)gridDim.x * warps) {
-        const int gsl = (int)(it / a.NG), g = (int)(it % a.NG);
-        const int v = a.slice_var[gsl];
-        const BVar &B = a.var[v];
-        const int row = (gsl - B.slice0) * kSlice + lane;
-        f(B, v, gsl, row, g);
+// Sum of p over the CTA's 32 rows for this thread's load case, stored as
+// P[gsl * NR + j] (fixed order: lanes, then warps).
+template <int JW>
+__device__ __forceinline__ void slice_partial(Stage &st, double p, double *P, int gsl, int NR) {
+#pragma unroll
+    for (int off = JW; off < 32; off <<= 1) p += __shfl_xor_sync(0xffffffffu, p, off);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane < JW) st.red[w][lane] = p;
+    __syncthreads();
+    if (threadIdx.x < JW && (int)threadIdx.x < NR) {
+        double s = 0;
+        for (int q = 0; q < Lanes<JW>::kWarps; ++q) s += st.red[q][threadIdx.x];
+        P[(long)gsl * NR + threadIdx.x] = s;
     }
 }
 
-// Reduce phase: one warp per (variant, load case); s(v, j, sum_pa, sum_pb).
+// Reduce phase: one warp per (variant, load case); f(v, j, sum_pa, sum_pb).
 template <class F>
 __device__ __forceinline__ void for_pairs(const BArgs &a, bool two, F f) {
     const int warps = blockDim.x / 32, w = threadIdx.x / 32, lane = threadIdx.x & 31;
     for (int it = blockIdx.x * warps + w; it < a.V * a.NR; it += gridDim.x * warps) {
         const int v = it / a.NR, j = it % a.NR;
-        const BVar &B = a.var[v];
+        const BVar B = a.var[v];
         double sa = 0, sb = 0;
         for (int s = lane; s < B.nslice; s += 32) {
             sa += a.pa[(long)(B.slice0 + s) * a.NR + j];
@@ -186,86 +254,68 @@ __device__ __forceinline__ void for_pairs(const BArgs &a, bool two, F f) {
     }
 }
 
-template <int RPT>
-__device__ __forceinline__ void live_mask(const BArgs &a, int v, int j0, bool (&lv)[RPT], bool &any) {
-    any = false;
-#pragma unroll
-    for (int jj = 0; jj < RPT; ++jj) {
-        const int j = j0 + jj;
-        lv[jj] = j < a.NR && a.live[v * a.NR + j] != 0;
-        any |= lv[jj];
-    }
-}
-
-// Warp-reduce RPT partials and store them for the slice (lane 0).
-template <int RPT>
-__device__ __forceinline__ void store_partials(const BArgs &a, double *P, int gsl, int j0, double (&p)[RPT]) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int jj = 0; jj < RPT; ++jj) {
-        const double s = warp_sum(p[jj]);
-        if (lane == 0 && j0 + jj < a.NR) P[(long)gsl * a.NR + j0 + jj] = s;
-    }
-}
-
 }  // namespace
 
 // The persistent batched solver.  MIXED: FP64 FCG + FP32 V-cycle; else PCG64.
-template <int RPT, bool MIXED>
-__global__ void __launch_bounds__(256) k_batch_solve(BArgs a) {
+// One CTA per slice item (grid-stride), JW lanes per block row.
+template <int JW, bool MIXED>
+__global__ void __launch_bounds__(32 * JW) k_batch_solve(BArgs a) {
+    __shared__ Stage st;
     const unsigned nb = gridDim.x + a.extra_arrivals;
     const int NR = a.NR;
+    const int r = Lanes<JW>::row(), j = Lanes<JW>::rhs();
+    const bool jok = j < NR;
     auto sync = [&]() { return grid_barrier(a.gs, nb, a.limit_ns); };
-    auto X = [&](const BVar &B, int row, int c) { return (B.dof0 + 3L * row + c) * NR; };
+    auto X = [&](const BVar &B, int row, int c) { return vidx(B, NR, row, c, j); };
+    // CTA-level loop over slices: f(B, v, gsl, ls, row, live)
+    auto for_slices = [&](auto f) {
+        for (int gsl = blockIdx.x; gsl < a.nslices; gsl += gridDim.x) {
+            const int v = a.slice_var[gsl];
+            const BVar B = a.var[v];
+            const int ls = gsl - B.slice0;
+            const int row = ls * kSlice + r;
+            const bool live = jok && a.live[v * NR + j] != 0;
+            f(B, v, gsl, ls, row, live);
+        }
+    };
 
     // ---- init: r = f - K u, partials ||r||^2 (pa), ||f||^2 (pb); start of M(r)
-    for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
-        const int j0 = g * RPT;
-        double prr[RPT], pff[RPT];
-#pragma unroll
-        for (int jj = 0; jj < RPT; ++jj) prr[jj] = pff[jj] = 0;
-        if (row < B.nfree) {
-            const int ls = gsl - B.slice0, S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
-            double y[3][RPT];
-            sell_row_multi<double, RPT>(S, row & 31, W, B.scols, B.sv64,
-                                        [&](int k, int jj) {
-                                            return j0 + jj < NR ? a.u[(B.dof0 + k) * NR + j0 + jj] : 0.0;
-                                        },
-                                        y);
-#pragma unroll
-            for (int jj = 0; jj < RPT; ++jj) {
-                const int j = j0 + jj;
-                if (j >= NR) continue;
-                double rv[3];
+    for_slices([&](const BVar &B, int v, int gsl, int ls, int row, bool) {
+        const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
+        double y[3];
+        spmm_slice<double, JW>(st, S, W, B.scols, B.sv64,
+                               [&](int k, int c) { return jok ? a.u[vidx(B, NR, k, c, j)] : 0.0; }, y);
+        double prr = 0, pff = 0;
+        if (jok && row < B.nfree) {
+            double rv[3];
+            for (int c = 0; c < 3; ++c) {
+                const long d = X(B, row, c);
+                const double fv = a.f[d];
+                rv[c] = fv - y[c];
+                a.r[d] = rv[c];
+                prr += rv[c] * rv[c];
+                pff += fv * fv;
+            }
+            if (MIXED) {
+                float b[3], x[3];
+                for (int c = 0; c < 3; ++c) b[c] = (float)rv[c];
+                block3_apply(B.Dinv32 + 9L * row, b, x);
                 for (int c = 0; c < 3; ++c) {
-                    const long d = X(B, row, c) + j;
-                    const double fv = a.f[d];
-                    rv[c] = fv - y[c][jj];
-                    a.r[d] = rv[c];
-                    prr[jj] += rv[c] * rv[c];
-                    pff[jj] += fv * fv;
+                    a.b32[X(B, row, c)] = b[c];
+                    a.x32[X(B, row, c)] = B.wsm * x[c];
                 }
-                if (MIXED) {
-                    float b[3], x[3];
-                    for (int c = 0; c < 3; ++c) b[c] = (float)rv[c];
-                    block3_apply(B.Dinv32 + 9L * row, b, x);
-                    for (int c = 0; c < 3; ++c) {
-                        a.b32[X(B, row, c) + j] = b[c];
-                        a.x32[X(B, row, c) + j] = B.wsm * x[c];
-                    }
-                } else {
-                    double z[3];
-                    block3_apply(B.Dinv + 9L * row, rv, z);
-                    for (int c = 0; c < 3; ++c) a.z64[X(B, row, c) + j] = z[c];
-                }
+            } else {
+                double z[3];
+                block3_apply(B.Dinv + 9L * row, rv, z);
+                for (int c = 0; c < 3; ++c) a.z64[X(B, row, c)] = z[c];
             }
         }
-        store_partials<RPT>(a, a.pa, gsl, j0, prr);
-        store_partials<RPT>(a, a.pb, gsl, j0, pff);
+        slice_partial<JW>(st, prr, a.pa, gsl, NR);
+        slice_partial<JW>(st, pff, a.pb, gsl, NR);
     });
     if (!sync()) return;
-    for_pairs(a, true, [&](int v, int j, double rr, double ff) {
-        const int vj = v * NR + j;
+    for_pairs(a, true, [&](int v, int jj, double rr, double ff) {
+        const int vj = v * NR + jj;
         a.ff[vj] = ff;
         const double t = 0.5 * a.rtol;
         a.tol2[vj] = t * t * ff;
@@ -276,168 +326,114 @@ __global__ void __launch_bounds__(256) k_batch_solve(BArgs a) {
     });
     if (!sync()) return;
 
-    // Preconditioner application z_new = M(r) (MIXED: V-cycle from b32/x32;
-    // PCG64: z64 already written with r).  Partials r.z_new (pa), r.z_old (pb).
+    // MIXED preconditioner z_new = M(r) from b32 / x32 (pre-smoothed by the
+    // caller's phase); partials r.z_new (pa), r.z_old (pb).
     auto precondition = [&](float *znew, const float *zold) -> bool {
-        if (!MIXED) return true;
         // t = b - K32 x
-        for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
-            const int j0 = g * RPT;
-            bool lv[RPT], any;
-            live_mask<RPT>(a, v, j0, lv, any);
-            if (!any || row >= B.nfree) return;
-            const int ls = gsl - B.slice0, S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
-            float y[3][RPT];
-            sell_row_multi<float, RPT>(S, row & 31, W, B.scols, B.sv32,
-                                       [&](int k, int jj) {
-                                           return j0 + jj < NR ? a.x32[(B.dof0 + k) * NR + j0 + jj] : 0.f;
-                                       },
-                                       y);
-#pragma unroll
-            for (int jj = 0; jj < RPT; ++jj) {
-                if (!lv[jj]) continue;
-                for (int c = 0; c < 3; ++c) {
-                    const long d = X(B, row, c) + j0 + jj;
-                    a.t32[d] = a.b32[d] - y[c][jj];
-                }
-            }
+        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, bool live) {
+            const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
+            float y[3];
+            spmm_slice<float, JW>(st, S, W, B.scols, B.sv32,
+                                  [&](int k, int c) { return jok ? a.x32[vidx(B, NR, k, c, j)] : 0.f; }, y);
+            if (live && row < B.nfree)
+                for (int c = 0; c < 3; ++c) a.t32[X(B, row, c)] = a.b32[X(B, row, c)] - y[c];
         });
         if (!sync()) return false;
-        // c = Z^T t per aggregate (warp per (aggregate, group))
+        // c = Z^T t: warp per aggregate, JW lanes per load case, 32/JW nodes at a time
         {
             const int warps = blockDim.x / 32, w = threadIdx.x / 32, lane = threadIdx.x & 31;
-            const long items = (long)a.naggs * a.NG;
-            for (long it = (long)blockIdx.x * warps + w; it < items; it += (long)gridDim.x * warps) {
-                const int ga = (int)(it / a.NG), g = (int)(it % a.NG), j0 = g * RPT;
+            const int sub = lane / JW, jj = lane % JW;
+            constexpr int RPW = 32 / JW;
+            for (int ga = blockIdx.x * warps + w; ga < a.naggs; ga += gridDim.x * warps) {
                 const int v = a.agg_var[ga];
-                const BVar &B = a.var[v];
-                bool lv[RPT], any;
-                live_mask<RPT>(a, v, j0, lv, any);
-                if (!any) continue;
+                const BVar B = a.var[v];
                 const int I = ga - B.agg0;
-                float acc[6][RPT];
-#pragma unroll
-                for (int k = 0; k < 6; ++k)
-#pragma unroll
-                    for (int jj = 0; jj < RPT; ++jj) acc[k][jj] = 0.f;
+                const bool live = jj < NR && a.live[v * NR + jj] != 0;
+                float acc[6] = {0, 0, 0, 0, 0, 0};
                 const float cx = (float)B.centroid[3L * I], cy = (float)B.centroid[3L * I + 1],
                             cz = (float)B.centroid[3L * I + 2];
                 const float sc = (float)B.inv_scale;
-                for (int idx = B.agg_ptr[I] + lane; idx < B.agg_ptr[I + 1]; idx += 32) {
-                    const int r = B.agg_nodes[idx], node = B.node_of_free[r];
+                for (int idx = B.agg_ptr[I] + sub; idx < B.agg_ptr[I + 1]; idx += RPW) {
+                    if (!live) continue;
+                    const int rr = B.agg_nodes[idx], node = B.node_of_free[rr];
                     const float dx = ((float)B.xyz[3L * node] - cx) * sc;
                     const float dy = ((float)B.xyz[3L * node + 1] - cy) * sc;
                     const float dz = ((float)B.xyz[3L * node + 2] - cz) * sc;
-#pragma unroll
-                    for (int jj = 0; jj < RPT; ++jj) {
-                        if (j0 + jj >= NR) continue;
-                        const float tx = a.t32[X(B, r, 0) + j0 + jj], ty = a.t32[X(B, r, 1) + j0 + jj],
-                                    tz = a.t32[X(B, r, 2) + j0 + jj];
-                        acc[0][jj] += tx;
-                        acc[1][jj] += ty;
-                        acc[2][jj] += tz;
-                        acc[3][jj] += -dz * ty + dy * tz;
-                        acc[4][jj] += dz * tx - dx * tz;
-                        acc[5][jj] += -dy * tx + dx * ty;
-                    }
+                    const float tx = a.t32[vidx(B, NR, rr, 0, jj)], ty = a.t32[vidx(B, NR, rr, 1, jj)],
+                                tz = a.t32[vidx(B, NR, rr, 2, jj)];
+                    acc[0] += tx;
+                    acc[1] += ty;
+                    acc[2] += tz;
+                    acc[3] += -dz * ty + dy * tz;
+                    acc[4] += dz * tx - dx * tz;
+                    acc[5] += -dy * tx + dx * ty;
                 }
 #pragma unroll
-                for (int k = 0; k < 6; ++k)
+                for (int k = 0; k < 6; ++k) {
+                    float s = acc[k];
 #pragma unroll
-                    for (int jj = 0; jj < RPT; ++jj) {
-                        const float s = warp_sum(acc[k][jj]);
-                        if (lane == 0 && j0 + jj < NR) a.cvec[(B.c0 + 6L * I + k) * NR + j0 + jj] = s;
-                    }
+                    for (int off = JW; off < 32; off <<= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+                    if (sub == 0 && live) a.cvec[(B.c0 + 6L * I + k) * NR + jj] = s;
+                }
             }
         }
         if (!sync()) return false;
-        // e = E^-1 c (warp per (coarse row, group))
+        // e = E^-1 c: warp per coarse row, JW lanes per load case
         {
             const int warps = blockDim.x / 32, w = threadIdx.x / 32, lane = threadIdx.x & 31;
-            const long items = (long)a.ncrows * a.NG;
-            for (long it = (long)blockIdx.x * warps + w; it < items; it += (long)gridDim.x * warps) {
-                const int gr = (int)(it / a.NG), g = (int)(it % a.NG), j0 = g * RPT;
+            const int sub = lane / JW, jj = lane % JW;
+            constexpr int RPW = 32 / JW;
+            for (int gr = blockIdx.x * warps + w; gr < a.ncrows; gr += gridDim.x * warps) {
                 const int v = a.crow_var[gr];
-                const BVar &B = a.var[v];
-                bool lv[RPT], any;
-                live_mask<RPT>(a, v, j0, lv, any);
-                if (!any) continue;
+                const BVar B = a.var[v];
+                const bool live = jj < NR && a.live[v * NR + jj] != 0;
                 const int i = gr - B.crow0, m = B.m;
-                float acc[RPT];
-#pragma unroll
-                for (int jj = 0; jj < RPT; ++jj) acc[jj] = 0.f;
                 const float *row = B.Einv32 + (long)i * m;
-                for (int k = lane; k < m; k += 32) {
-                    const float e = __ldg(row + k);
+                float acc = 0.f;
+                if (live)
+                    for (int k = sub; k < m; k += RPW) acc = fmaf(__ldg(row + k), a.cvec[(B.c0 + k) * NR + jj], acc);
 #pragma unroll
-                    for (int jj = 0; jj < RPT; ++jj)
-                        if (j0 + jj < NR) acc[jj] = fmaf(e, a.cvec[(B.c0 + k) * NR + j0 + jj], acc[jj]);
-                }
-#pragma unroll
-                for (int jj = 0; jj < RPT; ++jj) {
-                    const float s = warp_sum(acc[jj]);
-                    if (lane == 0 && j0 + jj < NR) a.evec[(B.c0 + i) * NR + j0 + jj] = s;
-                }
+                for (int off = JW; off < 32; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+                if (sub == 0 && live) a.evec[(B.c0 + i) * NR + jj] = acc;
             }
         }
         if (!sync()) return false;
         // x += Z e
-        for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
-            const int j0 = g * RPT;
-            bool lv[RPT], any;
-            live_mask<RPT>(a, v, j0, lv, any);
-            if (!any || row >= B.nfree) return;
+        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, bool live) {
+            if (!live || row >= B.nfree) return;
             const int I = B.agg_of[row], node = B.node_of_free[row];
             const float dx = (float)((B.xyz[3L * node] - B.centroid[3L * I]) * B.inv_scale);
             const float dy = (float)((B.xyz[3L * node + 1] - B.centroid[3L * I + 1]) * B.inv_scale);
             const float dz = (float)((B.xyz[3L * node + 2] - B.centroid[3L * I + 2]) * B.inv_scale);
-#pragma unroll
-            for (int jj = 0; jj < RPT; ++jj) {
-                if (!lv[jj]) continue;
-                const int j = j0 + jj;
-                float e[6];
-                for (int k = 0; k < 6; ++k) e[k] = a.evec[(B.c0 + 6L * I + k) * NR + j];
-                a.x32[X(B, row, 0) + j] += e[0] + dz * e[4] - dy * e[5];
-                a.x32[X(B, row, 1) + j] += e[1] - dz * e[3] + dx * e[5];
-                a.x32[X(B, row, 2) + j] += e[2] + dy * e[3] - dx * e[4];
-            }
+            float e[6];
+            for (int k = 0; k < 6; ++k) e[k] = a.evec[(B.c0 + 6L * I + k) * NR + j];
+            a.x32[X(B, row, 0)] += e[0] + dz * e[4] - dy * e[5];
+            a.x32[X(B, row, 1)] += e[1] - dz * e[3] + dx * e[5];
+            a.x32[X(B, row, 2)] += e[2] + dy * e[3] - dx * e[4];
         });
         if (!sync()) return false;
         // post-smoothing: z_new = x + w Dinv32 (b - K32 x); partials r.z_new, r.z_old
-        for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
-            const int j0 = g * RPT;
-            bool lv[RPT], any;
-            live_mask<RPT>(a, v, j0, lv, any);
-            double pn[RPT], po[RPT];
-#pragma unroll
-            for (int jj = 0; jj < RPT; ++jj) pn[jj] = po[jj] = 0;
-            if (any && row < B.nfree) {
-                const int ls = gsl - B.slice0, S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
-                float y[3][RPT];
-                sell_row_multi<float, RPT>(S, row & 31, W, B.scols, B.sv32,
-                                           [&](int k, int jj) {
-                                               return j0 + jj < NR ? a.x32[(B.dof0 + k) * NR + j0 + jj] : 0.f;
-                                           },
-                                           y);
-#pragma unroll
-                for (int jj = 0; jj < RPT; ++jj) {
-                    if (!lv[jj]) continue;
-                    const int j = j0 + jj;
-                    float res[3], cor[3];
-                    for (int c = 0; c < 3; ++c) res[c] = a.b32[X(B, row, c) + j] - y[c][jj];
-                    block3_apply(B.Dinv32 + 9L * row, res, cor);
-                    for (int c = 0; c < 3; ++c) {
-                        const long d = X(B, row, c) + j;
-                        const float z = a.x32[d] + B.wsm * cor[c];
-                        const double rv = a.r[d];
-                        pn[jj] += rv * (double)z;
-                        if (zold) po[jj] += rv * (double)zold[d];
-                        znew[d] = z;
-                    }
+        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, bool live) {
+            const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
+            float y[3];
+            spmm_slice<float, JW>(st, S, W, B.scols, B.sv32,
+                                  [&](int k, int c) { return jok ? a.x32[vidx(B, NR, k, c, j)] : 0.f; }, y);
+            double pn = 0, po = 0;
+            if (live && row < B.nfree) {
+                float res[3], cor[3];
+                for (int c = 0; c < 3; ++c) res[c] = a.b32[X(B, row, c)] - y[c];
+                block3_apply(B.Dinv32 + 9L * row, res, cor);
+                for (int c = 0; c < 3; ++c) {
+                    const long d = X(B, row, c);
+                    const float z = a.x32[d] + B.wsm * cor[c];
+                    const double rv = a.r[d];
+                    pn += rv * (double)z;
+                    if (zold) po += rv * (double)zold[d];
+                    znew[d] = z;
                 }
             }
-            store_partials<RPT>(a, a.pa, gsl, j0, pn);
-            store_partials<RPT>(a, a.pb, gsl, j0, po);
+            slice_partial<JW>(st, pn, a.pa, gsl, NR);
+            slice_partial<JW>(st, po, a.pb, gsl, NR);
         });
         return sync();
     };
@@ -445,23 +441,17 @@ __global__ void __launch_bounds__(256) k_batch_solve(BArgs a) {
     float *zcur = a.zA, *znext = a.zB;
     if (MIXED) {
         if (!precondition(zcur, nullptr)) return;
-        for_pairs(a, false, [&](int v, int j, double rz, double) { a.rz[v * NR + j] = rz; });
     } else {
-        // PCG64: r.z from z64 = Dinv r
-        for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
-            const int j0 = g * RPT;
-            double p[RPT];
-#pragma unroll
-            for (int jj = 0; jj < RPT; ++jj) {
-                p[jj] = 0;
-                if (row < B.nfree && j0 + jj < NR)
-                    for (int c = 0; c < 3; ++c) p[jj] += a.r[X(B, row, c) + j0 + jj] * a.z64[X(B, row, c) + j0 + jj];
-            }
-            store_partials<RPT>(a, a.pa, gsl, j0, p);
+        // PCG64: partials r.z with z64 = Dinv r
+        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, bool) {
+            double p = 0;
+            if (jok && row < B.nfree)
+                for (int c = 0; c < 3; ++c) p += a.r[X(B, row, c)] * a.z64[X(B, row, c)];
+            slice_partial<JW>(st, p, a.pa, gsl, NR);
         });
         if (!sync()) return;
-        for_pairs(a, false, [&](int v, int j, double rz, double) { a.rz[v * NR + j] = rz; });
     }
+    for_pairs(a, false, [&](int v, int jj, double rz, double) { a.rz[v * NR + jj] = rz; });
     if (!sync()) return;
 
     for (int k = 0; k < a.max_iter; ++k) {
@@ -471,44 +461,29 @@ __global__ void __launch_bounds__(256) k_batch_solve(BArgs a) {
         // slot (k + 1) % 3 was last read two barriers ago at least
         if (blockIdx.x == 0 && threadIdx.x == 0) a.live_cnt[(k + 1) % 3] = 0;
         // A: p = z + beta p_old, q = K64 p, partial p.q
-        for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
-            const int j0 = g * RPT;
-            bool lv[RPT], any;
-            live_mask<RPT>(a, v, j0, lv, any);
-            double ppq[RPT], bt[RPT];
-#pragma unroll
-            for (int jj = 0; jj < RPT; ++jj) {
-                ppq[jj] = 0;
-                bt[jj] = lv[jj] ? a.beta[v * NR + j0 + jj] : 0.0;
-            }
-            if (any && row < B.nfree) {
-                const int ls = gsl - B.slice0, S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
-                double y[3][RPT];
-                auto zval = [&](long d) -> double { return MIXED ? (double)zcur[d] : a.z64[d]; };
-                sell_row_multi<double, RPT>(S, row & 31, W, B.scols, B.sv64,
-                                            [&](int kk, int jj) {
-                                                if (!lv[jj]) return 0.0;
-                                                const long d = (B.dof0 + kk) * NR + j0 + jj;
-                                                return fma(bt[jj], pold[d], zval(d));
-                                            },
-                                            y);
-#pragma unroll
-                for (int jj = 0; jj < RPT; ++jj) {
-                    if (!lv[jj]) continue;
-                    for (int c = 0; c < 3; ++c) {
-                        const long d = X(B, row, c) + j0 + jj;
-                        const double pn = fma(bt[jj], pold[d], zval(d));
-                        pnew[d] = pn;
-                        a.q[d] = y[c][jj];
-                        ppq[jj] += pn * y[c][jj];
-                    }
+        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, bool live) {
+            const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
+            const double bt = live ? a.beta[v * NR + j] : 0.0;
+            auto pval = [&](long d) -> double {
+                return fma(bt, pold[d], MIXED ? (double)zcur[d] : a.z64[d]);
+            };
+            double y[3];
+            spmm_slice<double, JW>(st, S, W, B.scols, B.sv64,
+                                   [&](int kk, int c) { return live ? pval(vidx(B, NR, kk, c, j)) : 0.0; }, y);
+            double ppq = 0;
+            if (live && row < B.nfree)
+                for (int c = 0; c < 3; ++c) {
+                    const long d = X(B, row, c);
+                    const double pn = pval(d);
+                    pnew[d] = pn;
+                    a.q[d] = y[c];
+                    ppq += pn * y[c];
                 }
-            }
-            store_partials<RPT>(a, a.pa, gsl, j0, ppq);
+            slice_partial<JW>(st, ppq, a.pa, gsl, NR);
         });
         if (!sync()) return;
-        for_pairs(a, false, [&](int v, int j, double pq, double) {
-            const int vj = v * NR + j;
+        for_pairs(a, false, [&](int v, int jj, double pq, double) {
+            const int vj = v * NR + jj;
             if (!a.live[vj]) return;
             if (!(pq > 0.0) || !isfinite(pq)) {
                 a.live[vj] = 0;
@@ -520,51 +495,41 @@ __global__ void __launch_bounds__(256) k_batch_solve(BArgs a) {
         });
         if (!sync()) return;
         // B: u += alpha p, r -= alpha q, partial ||r||^2; start of M(r)
-        for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
-            const int j0 = g * RPT;
-            bool lv[RPT], any;
-            live_mask<RPT>(a, v, j0, lv, any);
-            double prr[RPT], prz[RPT];
-#pragma unroll
-            for (int jj = 0; jj < RPT; ++jj) prr[jj] = prz[jj] = 0;
-            if (any && row < B.nfree) {
-#pragma unroll
-                for (int jj = 0; jj < RPT; ++jj) {
-                    if (!lv[jj]) continue;
-                    const int j = j0 + jj;
-                    const double al = a.alpha[v * NR + j];
-                    double rv[3];
+        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, bool live) {
+            double prr = 0, prz = 0;
+            if (live && row < B.nfree) {
+                const double al = a.alpha[v * NR + j];
+                double rv[3];
+                for (int c = 0; c < 3; ++c) {
+                    const long d = X(B, row, c);
+                    a.u[d] = fma(al, pnew[d], a.u[d]);
+                    rv[c] = fma(-al, a.q[d], a.r[d]);
+                    a.r[d] = rv[c];
+                    prr += rv[c] * rv[c];
+                }
+                if (MIXED) {
+                    float b[3], x[3];
+                    for (int c = 0; c < 3; ++c) b[c] = (float)rv[c];
+                    block3_apply(B.Dinv32 + 9L * row, b, x);
                     for (int c = 0; c < 3; ++c) {
-                        const long d = X(B, row, c) + j;
-                        a.u[d] = fma(al, pnew[d], a.u[d]);
-                        rv[c] = fma(-al, a.q[d], a.r[d]);
-                        a.r[d] = rv[c];
-                        prr[jj] += rv[c] * rv[c];
+                        a.b32[X(B, row, c)] = b[c];
+                        a.x32[X(B, row, c)] = B.wsm * x[c];
                     }
-                    if (MIXED) {
-                        float b[3], x[3];
-                        for (int c = 0; c < 3; ++c) b[c] = (float)rv[c];
-                        block3_apply(B.Dinv32 + 9L * row, b, x);
-                        for (int c = 0; c < 3; ++c) {
-                            a.b32[X(B, row, c) + j] = b[c];
-                            a.x32[X(B, row, c) + j] = B.wsm * x[c];
-                        }
-                    } else {
-                        double z[3];
-                        block3_apply(B.Dinv + 9L * row, rv, z);
-                        for (int c = 0; c < 3; ++c) {
-                            a.z64[X(B, row, c) + j] = z[c];
-                            prz[jj] += rv[c] * z[c];
-                        }
+                } else {
+                    double z[3];
+                    block3_apply(B.Dinv + 9L * row, rv, z);
+                    for (int c = 0; c < 3; ++c) {
+                        a.z64[X(B, row, c)] = z[c];
+                        prz += rv[c] * z[c];
                     }
                 }
             }
-            store_partials<RPT>(a, a.pa, gsl, j0, prr);
-            if (!MIXED) store_partials<RPT>(a, a.pb, gsl, j0, prz);
+            slice_partial<JW>(st, prr, a.pa, gsl, NR);
+            if (!MIXED) slice_partial<JW>(st, prz, a.pb, gsl, NR);
         });
         if (!sync()) return;
-        for_pairs(a, !MIXED, [&](int v, int j, double rr, double rz) {
-            const int vj = v * NR + j;
+        for_pairs(a, !MIXED, [&](int v, int jj, double rr, double rz) {
+            const int vj = v * NR + jj;
             if (!a.live[vj]) return;
             a.iters[vj] = k + 1;
             if (!isfinite(rr)) {
@@ -591,8 +556,8 @@ __global__ void __launch_bounds__(256) k_batch_solve(BArgs a) {
         if (*(volatile int *)&a.live_cnt[k % 3] == 0) break;
         if (MIXED) {
             if (!precondition(znext, zcur)) return;
-            for_pairs(a, true, [&](int v, int j, double rzn, double rzo) {
-                const int vj = v * NR + j;
+            for_pairs(a, true, [&](int v, int jj, double rzn, double rzo) {
+                const int vj = v * NR + jj;
                 if (!a.live[vj]) return;
                 a.beta[vj] = (rzn - rzo) / a.rz[vj];
                 a.rz[vj] = rzn;
@@ -605,57 +570,48 @@ __global__ void __launch_bounds__(256) k_batch_solve(BArgs a) {
     }
 }
 
-// Load-case interleaving of the host-ordered right-hand sides / solutions:
-// dst[(dof0 + i) * NR + j] = src[j * n + i] (and back).
-__global__ void k_interleave(long n, int nrhs, int NR, long dof0, const double *__restrict__ src,
-                             double *__restrict__ dst) {
+// Host order (load case j at j * n, DOF 3 i + c) to the batch's interleaved
+// order (dof0 * NR + (3 i + c) * NR + j), for one variant (and back).
+__global__ void k_interleave(long n, int nrhs, const double *__restrict__ src, double *__restrict__ dst) {
     for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < n * nrhs; g += (long)gridDim.x * blockDim.x) {
-        const long j = g / n, i = g % n;
-        dst[(dof0 + i) * NR + j] = src[g];
+        const long j = g / n, d = g % n;
+        dst[d * nrhs + j] = src[g];
     }
 }
-__global__ void k_deinterleave(long n, int nrhs, int NR, long dof0, const double *__restrict__ src,
-                               double *__restrict__ dst) {
+__global__ void k_deinterleave(long n, int nrhs, const double *__restrict__ src, double *__restrict__ dst) {
     for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < n * nrhs; g += (long)gridDim.x * blockDim.x) {
-        const long j = g / n, i = g % n;
-        dst[g] = src[(dof0 + i) * NR + j];
+        const long j = g / n, d = g % n;
+        dst[g] = src[d * nrhs + j];
     }
 }
 
 // True FP64 residual partials per (slice, load case): ||f - K u||^2 (pa), ||f||^2 (pb).
-template <int RPT>
-__global__ void __launch_bounds__(256) k_batch_residual(BArgs a) {
-    const int NR = a.NR;
-    for_slices(a, [&](const BVar &B, int v, int gsl, int row, int g) {
-        const int j0 = g * RPT;
-        double prr[RPT], pff[RPT];
-#pragma unroll
-        for (int jj = 0; jj < RPT; ++jj) prr[jj] = pff[jj] = 0;
-        if (row < B.nfree) {
-            const int ls = gsl - B.slice0, S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
-            double y[3][RPT];
-            sell_row_multi<double, RPT>(S, row & 31, W, B.scols, B.sv64,
-                                        [&](int k, int jj) {
-                                            return j0 + jj < NR ? a.u[(B.dof0 + k) * NR + j0 + jj] : 0.0;
-                                        },
-                                        y);
-#pragma unroll
-            for (int jj = 0; jj < RPT; ++jj) {
-                if (j0 + jj >= NR) continue;
-                for (int c = 0; c < 3; ++c) {
-                    const double fv = a.f[(B.dof0 + 3L * row + c) * NR + j0 + jj];
-                    const double rv = fv - y[c][jj];
-                    prr[jj] += rv * rv;
-                    pff[jj] += fv * fv;
-                }
+template <int JW>
+__global__ void __launch_bounds__(32 * JW) k_batch_residual(BArgs a) {
+    __shared__ Stage st;
+    const int NR = a.NR, j = Lanes<JW>::rhs(), r = Lanes<JW>::row();
+    const bool jok = j < NR;
+    for (int gsl = blockIdx.x; gsl < a.nslices; gsl += gridDim.x) {
+        const BVar B = a.var[a.slice_var[gsl]];
+        const int ls = gsl - B.slice0, row = ls * kSlice + r;
+        const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
+        double y[3];
+        spmm_slice<double, JW>(st, S, W, B.scols, B.sv64,
+                               [&](int k, int c) { return jok ? a.u[vidx(B, NR, k, c, j)] : 0.0; }, y);
+        double prr = 0, pff = 0;
+        if (jok && row < B.nfree)
+            for (int c = 0; c < 3; ++c) {
+                const double fv = a.f[vidx(B, NR, row, c, j)];
+                const double rv = fv - y[c];
+                prr += rv * rv;
+                pff += fv * fv;
             }
-        }
-        store_partials<RPT>(a, a.pa, gsl, j0, prr);
-        store_partials<RPT>(a, a.pb, gsl, j0, pff);
-    });
+        slice_partial<JW>(st, prr, a.pa, gsl, NR);
+        slice_partial<JW>(st, pff, a.pb, gsl, NR);
+    }
 }
 
-// Per (variant, load case): rel = sqrt(rr / ff) into alpha (reused as output).
+// Per (variant, load case): rel = sqrt(rr / ff).
 __global__ void k_batch_rel(BArgs a, double *rel) {
     for_pairs(a, true, [&](int v, int j, double rr, double ff) {
         rel[v * a.NR + j] = ff > 0.0 ? sqrt(rr / ff) : 0.0;
@@ -670,34 +626,36 @@ __global__ void k_barrier_probe(GridSync *gs, unsigned extra, unsigned long long
     if (blockIdx.x == 0 && threadIdx.x == 0) *out = ok ? 1 : 0;
 }
 
-
 // ------------------------------------------------------------------ host --
 
 namespace {
 
 struct TuneCfg {
-    int rpt = 4, threads = 256, ctas_per_sm = 1;
+    int kc = 4, ctas_per_sm = 1;
     double ms_per_iter = 0.0;
 };
 
-// Kernel instance for (rpt, mixed).
-const void *solve_kernel(int rpt, bool mixed) {
-    switch (rpt) {
-        case 1: return mixed ? (const void *)k_batch_solve<1, true> : (const void *)k_batch_solve<1, false>;
-        case 2: return mixed ? (const void *)k_batch_solve<2, true> : (const void *)k_batch_solve<2, false>;
+// Lanes per block row for NR load cases.
+int jw_for(int NR) { return NR <= 4 ? 4 : NR <= 8 ? 8 : NR <= 16 ? 16 : 32; }
+
+// Kernel instance for (JW, mixed).
+const void *solve_kernel(int jw, bool mixed) {
+    switch (jw) {
         case 4: return mixed ? (const void *)k_batch_solve<4, true> : (const void *)k_batch_solve<4, false>;
         case 8: return mixed ? (const void *)k_batch_solve<8, true> : (const void *)k_batch_solve<8, false>;
+        case 16: return mixed ? (const void *)k_batch_solve<16, true> : (const void *)k_batch_solve<16, false>;
+        case 32: return mixed ? (const void *)k_batch_solve<32, true> : (const void *)k_batch_solve<32, false>;
     }
-    fail(OFEA_ERR_INVALID_ARG, "unsupported load cases per thread");
+    fail(OFEA_ERR_INVALID_ARG, "unsupported lanes per row");
 }
-const void *residual_kernel(int rpt) {
-    switch (rpt) {
-        case 1: return (const void *)k_batch_residual<1>;
-        case 2: return (const void *)k_batch_residual<2>;
+const void *residual_kernel(int jw) {
+    switch (jw) {
         case 4: return (const void *)k_batch_residual<4>;
         case 8: return (const void *)k_batch_residual<8>;
+        case 16: return (const void *)k_batch_residual<16>;
+        case 32: return (const void *)k_batch_residual<32>;
     }
-    fail(OFEA_ERR_INVALID_ARG, "unsupported load cases per thread");
+    fail(OFEA_ERR_INVALID_ARG, "unsupported lanes per row");
 }
 
 // ---- the on-disk tuning cache: one JSON object per line inside "entries"
@@ -724,8 +682,7 @@ std::map<std::string, TuneCfg> tune_load(const std::string &path) {
         const size_t b = p + 8, e = line.find('"', b);
         if (e == std::string::npos) continue;
         TuneCfg t;
-        t.rpt = (int)num(line, "rpt", 4);
-        t.threads = (int)num(line, "threads", 256);
+        t.kc = (int)num(line, "kc", 4);
         t.ctas_per_sm = (int)num(line, "ctas_per_sm", 1);
         t.ms_per_iter = num(line, "ms_per_iter", 0);
         out[line.substr(b, e - b)] = t;
@@ -746,8 +703,8 @@ void tune_store(const std::string &path, const std::string &key, const TuneCfg &
     for (const auto &kv : all) {
         char buf[512];
         std::snprintf(buf, sizeof(buf),
-                      "    {\"key\": \"%s\", \"rpt\": %d, \"threads\": %d, \"ctas_per_sm\": %d, \"ms_per_iter\": %.6f}%s\n",
-                      kv.first.c_str(), kv.second.rpt, kv.second.threads, kv.second.ctas_per_sm,
+                      "    {\"key\": \"%s\", \"kc\": %d, \"ctas_per_sm\": %d, \"ms_per_iter\": %.6f}%s\n",
+                      kv.first.c_str(), kv.second.kc, kv.second.ctas_per_sm,
                       kv.second.ms_per_iter, ++i < all.size() ? "," : "");
         o << buf;
     }
@@ -805,6 +762,7 @@ void build_desc(ofea_batch *b, bool mixed) {
         BVar &B = d[v];
         std::memset(&B, 0, sizeof(B));
         B.nfree = c->nfree;
+        B.n = c->n;
         B.nslice = (c->nfree + kSlice - 1) / kSlice;
         B.slice0 = slice0;
         B.dof0 = b->dof0[v];
@@ -881,7 +839,7 @@ BArgs make_args(ofea_batch *b, bool mixed, const TuneCfg &t, int max_iter, doubl
     BArgs a{};
     a.V = b->V;
     a.NR = b->NR;
-    a.NG = (b->NR + t.rpt - 1) / t.rpt;
+    a.kc = t.kc;
     a.nslices = b->nslices;
     a.naggs = mixed ? b->naggs : 0;
     a.ncrows = mixed ? b->ncrows : 0;
@@ -924,7 +882,7 @@ BArgs make_args(ofea_batch *b, bool mixed, const TuneCfg &t, int max_iter, doubl
 
 int grid_of(ofea_batch *b, const void *fn, const TuneCfg &t) {
     int occ = 0;
-    OFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, t.threads, 0));
+    OFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * jw_for(b->NR), 0));
     if (occ < 1) fail(OFEA_ERR_CAPACITY, "batched solver kernel does not fit on an SM");
     return b->num_sms * std::min(occ, t.ctas_per_sm);
 }
@@ -937,10 +895,10 @@ void enqueue(ofea_batch *b, const BArgs &a, const TuneCfg &t, bool mixed) {
     OFEA_CUDA(cudaMemsetAsync(b->p1.p, 0, sizeof(double) * n, s));
     OFEA_CUDA(cudaMemsetAsync(b->gs.p, 0, sizeof(GridSync), s));
     OFEA_CUDA(cudaMemsetAsync(b->live_cnt.p, 0, sizeof(int) * 3, s));
-    const void *fn = solve_kernel(t.rpt, mixed);
+    const void *fn = solve_kernel(jw_for(b->NR), mixed);
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(grid_of(b, fn, t));
-    cfg.blockDim = dim3(t.threads);
+    cfg.blockDim = dim3(32 * jw_for(b->NR));
     cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -956,10 +914,10 @@ void enqueue(ofea_batch *b, const BArgs &a, const TuneCfg &t, bool mixed) {
 void residuals(ofea_batch *b, const TuneCfg &t) {
     BArgs a = make_args(b, false, t, 0, 0.0);
     cudaStream_t s = b->stream;
-    const void *fn = residual_kernel(t.rpt);
-    const int G = std::min(kMaxGrid, b->num_sms * 8);
+    const void *fn = residual_kernel(jw_for(b->NR));
+    const int G = std::min(kMaxGrid, b->num_sms * 4);
     void *args[] = {(void *)&a};
-    OFEA_CUDA(cudaLaunchKernel(fn, dim3(G), dim3(256), args, 0, s));
+    OFEA_CUDA(cudaLaunchKernel(fn, dim3(G), dim3(32 * jw_for(b->NR)), args, 0, s));
     k_batch_rel<<<std::max(1, std::min(kMaxGrid, (b->V * b->NR + 7) / 8)), 256, 0, s>>>(a, b->rel.p);
     OFEA_CHECK_LAUNCH();
 }
@@ -987,24 +945,18 @@ TuneCfg autotune(ofea_batch *b, bool mixed, double rtol) {
         auto it = all.find(key);
         if (it != all.end()) {
             TuneCfg t = it->second;
-            if ((t.rpt == 1 || t.rpt == 2 || t.rpt == 4 || t.rpt == 8) && (t.threads == 128 || t.threads == 256) &&
-                t.ctas_per_sm >= 1 && t.ctas_per_sm <= 16)
-                return t;
+            if (t.ctas_per_sm >= 1 && t.ctas_per_sm <= 32) return t;
         }
     }
     std::vector<TuneCfg> cand;
-    for (int rpt : {1, 2, 4, 8}) {
-        if (rpt > 1 && rpt / 2 >= b->NR) continue;  // groups wider than the load cases
-        for (int th : {128, 256}) {
-            int occ = 0;
-            OFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_kernel(rpt, mixed), th, 0));
-            std::vector<int> cps{1, 2, occ};
-            std::sort(cps.begin(), cps.end());
-            cps.erase(std::unique(cps.begin(), cps.end()), cps.end());
-            for (int c : cps)
-                if (c >= 1 && c <= occ) cand.push_back(TuneCfg{rpt, th, c, 0.0});
-        }
-    }
+    int occ = 0;
+    OFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_kernel(jw_for(b->NR), mixed),
+                                                            32 * jw_for(b->NR), 0));
+    std::vector<int> cps{1, 2, occ};
+    std::sort(cps.begin(), cps.end());
+    cps.erase(std::unique(cps.begin(), cps.end()), cps.end());
+    for (int c : cps)
+        if (c >= 1 && c <= occ) cand.push_back(TuneCfg{kKC, c, 0.0});
     const int iters = 6;
     cudaEvent_t e0, e1;
     OFEA_CUDA(cudaEventCreate(&e0));
@@ -1096,7 +1048,7 @@ void batch_set_rhs(ofea_batch *b, const double *const *f) {
         b->stage.ensure((size_t)n * b->NR);
         OFEA_CUDA(cudaMemcpyAsync(b->stage.p, f[v], sizeof(double) * n * b->NR, cudaMemcpyHostToDevice, s));
         k_interleave<<<std::max(1, std::min(kMaxGrid, (int)((n * b->NR + 255) / 256))), 256, 0, s>>>(
-            n, b->NR, b->NR, b->dof0[v], b->stage.p, b->f.p);
+            n, b->NR, b->stage.p, b->f.p + b->dof0[v] * b->NR);
         OFEA_CHECK_LAUNCH();
     }
     OFEA_CUDA(cudaStreamSynchronize(s));
@@ -1111,22 +1063,22 @@ void batch_get_solution(ofea_batch *b, double *const *u) {
         if (!u[v]) fail(OFEA_ERR_INVALID_ARG, "batch: NULL solution array");
         b->stage.ensure((size_t)n * b->NR);
         k_deinterleave<<<std::max(1, std::min(kMaxGrid, (int)((n * b->NR + 255) / 256))), 256, 0, s>>>(
-            n, b->NR, b->NR, b->dof0[v], b->u.p, b->stage.p);
+            n, b->NR, b->u.p + b->dof0[v] * b->NR, b->stage.p);
         OFEA_CHECK_LAUNCH();
         OFEA_CUDA(cudaMemcpyAsync(u[v], b->stage.p, sizeof(double) * n * b->NR, cudaMemcpyDeviceToHost, s));
         OFEA_CUDA(cudaStreamSynchronize(s));
     }
 }
 
-void batch_tuning(ofea_batch *b, int method, int *rpt, int *threads, int *ctas_per_sm, double *ms_per_iter) {
+void batch_tuning(ofea_batch *b, int method, int *kc, int *threads, int *ctas_per_sm, double *ms_per_iter) {
     const bool mixed = method == OFEA_SOLVER_MIXED;
     OFEA_CUDA(cudaSetDevice(b->device));
     prepare(b, mixed);
     auto it = b->tuned.find(method);
     if (it == b->tuned.end()) it = b->tuned.emplace(method, autotune(b, mixed, 1e-8)).first;
     const TuneCfg &t = it->second;
-    if (rpt) *rpt = t.rpt;
-    if (threads) *threads = t.threads;
+    if (kc) *kc = t.kc;
+    if (threads) *threads = 32 * jw_for(b->NR);
     if (ctas_per_sm) *ctas_per_sm = t.ctas_per_sm;
     if (ms_per_iter) *ms_per_iter = t.ms_per_iter;
 }
@@ -1143,8 +1095,7 @@ void batch_solve(ofea_batch *b, const ofea_solve_opts &o, ofea_solve_stats *stat
     const bool mixed = o.method == OFEA_SOLVER_MIXED;
     OFEA_CUDA(cudaSetDevice(b->device));
     prepare(b, mixed);
-    int rpt = 0;
-    batch_tuning(b, o.method, &rpt, nullptr, nullptr, nullptr);
+    batch_tuning(b, o.method, nullptr, nullptr, nullptr, nullptr);
     const TuneCfg t = b->tuned[o.method];
     cudaStream_t s = b->stream;
     const int VJ = b->V * b->NR;
@@ -1160,7 +1111,7 @@ void batch_solve(ofea_batch *b, const ofea_solve_opts &o, ofea_solve_stats *stat
     for (; attempts < 4 && remaining > 0; ++attempts) {
         BArgs a = make_args(b, mixed, t, remaining, o.rtol);
         std::ostringstream k;
-        k << o.method << "/" << t.rpt << "/" << t.threads << "/" << t.ctas_per_sm << "/" << remaining << "/"
+        k << o.method << "/" << t.kc << "/" << t.ctas_per_sm << "/" << remaining << "/"
           << o.rtol;
         if (o.use_graph) {
             if (!b->exec || b->exec_key != k.str()) {
