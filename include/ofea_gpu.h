@@ -215,10 +215,9 @@ OFEA_API int ofea_learned_gradient(ofea_ctx *ctx, const float *x, int batch, dou
  * cases each, solved together by one persistent cooperative kernel launched
  * from a CUDA graph.  Methods OFEA_SOLVER_MIXED (FP64 flexible CG + FP32
  * two-level V-cycle per variant) and OFEA_SOLVER_PCG64.  Its tile sizes
- * (matrix slots staged in shared memory per step, CTAs per SM; the CTA size
- * follows from nrhs) are chosen by timing candidates on the first solve of a
- * problem class and kept in a JSON file (OFEA_TUNE_FILE, default
- * ~/.cache/openfea_b200_tune.json).  The batch borrows the contexts:
+ * (load cases per lane, hence the CTA size, and CTAs per SM) are chosen by
+ * timing candidates on the first solve of a problem class and kept in a JSON
+ * file (OFEA_TUNE_FILE, default ~/.cache/openfea_b200_tune.json).  The batch borrows the contexts:
  * keep them alive and unchanged until ofea_batch_destroy. */
 typedef struct ofea_batch ofea_batch;
 #define OFEA_BATCH_MAX_RHS 32
@@ -236,7 +235,7 @@ OFEA_API int ofea_batch_get_solution(ofea_batch *batch, double *const *u);
 OFEA_API int ofea_batch_solve(ofea_batch *batch, const double *const *f, double *const *u,
                               const ofea_solve_opts *opts, ofea_solve_stats *stats);
 /* The tile configuration used for `method` (tuning it now if needed). */
-OFEA_API int ofea_batch_tuning(ofea_batch *batch, int method, int *slots_per_stage, int *threads,
+OFEA_API int ofea_batch_tuning(ofea_batch *batch, int method, int *rhs_per_lane, int *threads,
                                int *ctas_per_sm, double *ms_per_iteration);
 /* One-call form: create, solve, destroy. */
 OFEA_API int ofea_solve_batched(ofea_ctx *const *ctxs, int n_variants, const double *const *f,

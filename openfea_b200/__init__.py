@@ -205,7 +205,7 @@ class Batch:
         r, t, c, ms = _I(), _I(), _I(), _D()
         _check(lib().ofea_batch_tuning(self.h, SOLVERS[method], ctypes.byref(r), ctypes.byref(t), ctypes.byref(c),
                                        ctypes.byref(ms)), "ofea_batch_tuning")
-        return {"slots_per_stage": r.value, "threads": t.value, "ctas_per_sm": c.value, "ms_per_iteration": ms.value}
+        return {"rhs_per_lane": r.value, "threads": t.value, "ctas_per_sm": c.value, "ms_per_iteration": ms.value}
 
 
 def solve_batched(contexts, loads, method="GPU_MIXED", rtol=1e-8, **kw):

@@ -42,6 +42,7 @@
 #include <mutex>
 #include <sstream>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "precond.cuh"
@@ -127,19 +128,66 @@ __device__ bool grid_barrier(GridSync *gs, unsigned nblocks, unsigned long long 
     return s_ok != 0;
 }
 
-// Entry (node i, component c, load case j) of a variant in a batch vector.
-__device__ __forceinline__ long vidx(const BVar &B, int NR, long i, int c, int j) {
-    return (B.dof0 + 3 * i + c) * NR + j;
+// Entry (node i, component c, load case j) of a variant in a batch vector
+// whose load-case stride is NP (NR rounded up; padding entries stay zero).
+template <int NP>
+__device__ __forceinline__ long vidx(const BVar &B, long i, int c, int j) {
+    return (B.dof0 + 3 * i + c) * NP + j;
 }
 
-// Thread roles inside the CTA that owns one slice: JW lanes per block row
-// (one load case each), 32 / JW rows per warp, 32 rows per CTA.
-template <int JW>
+// RL consecutive load cases of one DOF as one vector access (the offset is
+// a multiple of RL: aligned).
+template <class V, int RL>
+__device__ __forceinline__ void ldv(const V *p, V (&o)[RL]) {
+    if constexpr (sizeof(V) * RL == 32) {
+        using T = typename std::conditional<sizeof(V) == 8, double2, float4>::type;
+        const T a = reinterpret_cast<const T *>(p)[0], b = reinterpret_cast<const T *>(p)[1];
+        std::memcpy(&o[0], &a, 16);
+        std::memcpy(&o[RL / 2], &b, 16);
+    } else if constexpr (sizeof(V) * RL == 16) {
+        using T = typename std::conditional<sizeof(V) == 8, double2, float4>::type;
+        const T a = *reinterpret_cast<const T *>(p);
+        std::memcpy(&o[0], &a, 16);
+    } else if constexpr (sizeof(V) * RL == 8 && sizeof(V) == 4) {
+        const float2 a = *reinterpret_cast<const float2 *>(p);
+        o[0] = a.x;
+        o[1] = a.y;
+    } else {
+#pragma unroll
+        for (int q = 0; q < RL; ++q) o[q] = p[q];
+    }
+}
+template <class V, int RL>
+__device__ __forceinline__ void stv(V *p, const V (&o)[RL]) {
+    if constexpr (sizeof(V) * RL == 32) {
+        using T = typename std::conditional<sizeof(V) == 8, double2, float4>::type;
+        T a, b;
+        std::memcpy(&a, &o[0], 16);
+        std::memcpy(&b, &o[RL / 2], 16);
+        reinterpret_cast<T *>(p)[0] = a;
+        reinterpret_cast<T *>(p)[1] = b;
+    } else if constexpr (sizeof(V) * RL == 16) {
+        using T = typename std::conditional<sizeof(V) == 8, double2, float4>::type;
+        T a;
+        std::memcpy(&a, &o[0], 16);
+        *reinterpret_cast<T *>(p) = a;
+    } else if constexpr (sizeof(V) * RL == 8 && sizeof(V) == 4) {
+        *reinterpret_cast<float2 *>(p) = make_float2(o[0], o[1]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < RL; ++q) p[q] = o[q];
+    }
+}
+
+// Thread roles in the CTA that owns one slice: LW = NP / RL lanes per block
+// row, each carrying RL consecutive load cases; 32 / LW rows per warp.
+template <int NP, int RL>
 struct Lanes {
-    static constexpr int kRowsPerWarp = 32 / JW;
-    static constexpr int kWarps = 32 / kRowsPerWarp;  // = JW
-    __device__ static int row() { return (threadIdx.x >> 5) * kRowsPerWarp + (threadIdx.x & 31) / JW; }
-    __device__ static int rhs() { return threadIdx.x & (JW - 1); }
+    static constexpr int kLW = NP / RL;
+    static constexpr int kRowsPerWarp = 32 / kLW;
+    static constexpr int kWarps = kSlice / kRowsPerWarp;
+    __device__ static int row() { return (threadIdx.x >> 5) * kRowsPerWarp + (threadIdx.x & 31) / kLW; }
+    __device__ static int j0() { return (threadIdx.x & (kLW - 1)) * RL; }
 };
 
 // Shared-memory stage of a slice's BSELL slots: two buffers of kKC slots
@@ -149,7 +197,7 @@ constexpr int kKC = 4;
 struct __align__(128) Stage {
     double v[2][kKC * 9 * kSlice];  // FP32 values use the first half of each buffer
     int col[2][kKC * kSlice];
-    double red[32][32];             // [warp][lane] partial sums
+    double red[32][32];             // [warp][load case] partial sums
 };
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
@@ -176,15 +224,19 @@ __device__ __forceinline__ void stage_chunk(Stage &st, int b, long S, int k0, in
     cp_async_commit();
 }
 
-// y[c] = (K x)_row for this thread's load case.  The slice's slots stream
-// through shared memory kKC at a time, double-buffered, shared by every load
-// case; a chunk's gathers are all issued before its FMAs.  Called by all
-// threads of the CTA (rows beyond nfree read padding: column 0, value 0).
-template <class V, int JW, class XF>
+// y[c][q] = (K x)_(row, c) for this thread's RL load cases.  The slice's
+// slots stream through shared memory kKC at a time, double-buffered, shared
+// by every load case; each staged value feeds RL FMAs.  xf(col, c, out[RL])
+// loads the operand.  Called by all threads of the CTA (rows beyond nfree
+// read padding: column 0, value 0).
+template <class V, int NP, int RL, class XF>
 __device__ __forceinline__ void spmm_slice(Stage &st, long S, int W, const int *__restrict__ scols,
-                                           const V *__restrict__ svals, XF xf, V (&y)[3]) {
-    const int r = Lanes<JW>::row();
-    y[0] = y[1] = y[2] = 0;
+                                           const V *__restrict__ svals, XF xf, V (&y)[3][RL]) {
+    const int r = Lanes<NP, RL>::row();
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int q = 0; q < RL; ++q) y[c][q] = 0;
     const int nch = (W + kKC - 1) / kKC;
     __syncthreads();  // both buffers are free
     if (nch > 0) stage_chunk<V>(st, 0, S, 0, min(kKC, W), scols, svals);
@@ -198,40 +250,52 @@ __device__ __forceinline__ void spmm_slice(Stage &st, long S, int W, const int *
         }
         __syncthreads();
         const V *sv = reinterpret_cast<const V *>(st.v[b]);
-        V x[kKC][3];
 #pragma unroll
-        for (int kk = 0; kk < kKC; ++kk)
-            if (kk < kc) {
-                const int col = st.col[b][kk * kSlice + r];
-                x[kk][0] = xf(col, 0);
-                x[kk][1] = xf(col, 1);
-                x[kk][2] = xf(col, 2);
-            }
+        for (int k2 = 0; k2 < kKC; k2 += 2) {
+            V x[2][3][RL];
 #pragma unroll
-        for (int kk = 0; kk < kKC; ++kk)
-            if (kk < kc) {
-                const V *v = sv + kk * 9 * kSlice + r;
-                y[0] = fma(v[0 * kSlice], x[kk][0], fma(v[1 * kSlice], x[kk][1], fma(v[2 * kSlice], x[kk][2], y[0])));
-                y[1] = fma(v[3 * kSlice], x[kk][0], fma(v[4 * kSlice], x[kk][1], fma(v[5 * kSlice], x[kk][2], y[1])));
-                y[2] = fma(v[6 * kSlice], x[kk][0], fma(v[7 * kSlice], x[kk][1], fma(v[8 * kSlice], x[kk][2], y[2])));
-            }
+            for (int u = 0; u < 2; ++u)
+                if (k2 + u < kc) {
+                    const int col = st.col[b][(k2 + u) * kSlice + r];
+                    xf(col, 0, x[u][0]);
+                    xf(col, 1, x[u][1]);
+                    xf(col, 2, x[u][2]);
+                }
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+                if (k2 + u < kc) {
+                    const V *v = sv + (k2 + u) * 9 * kSlice + r;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const V a0 = v[(3 * c) * kSlice], a1 = v[(3 * c + 1) * kSlice], a2 = v[(3 * c + 2) * kSlice];
+#pragma unroll
+                        for (int q = 0; q < RL; ++q)
+                            y[c][q] = fma(a0, x[u][0][q], fma(a1, x[u][1][q], fma(a2, x[u][2][q], y[c][q])));
+                    }
+                }
+        }
         __syncthreads();  // buffer b is consumed before it is refilled
     }
 }
 
-// Sum of p over the CTA's 32 rows for this thread's load case, stored as
-// P[gsl * NR + j] (fixed order: lanes, then warps).
-template <int JW>
-__device__ __forceinline__ void slice_partial(Stage &st, double p, double *P, int gsl, int NR) {
+// Sums of p[q] over the CTA's 32 rows for each of this thread's load cases,
+// stored as P[gsl * NR + j] for j < NR (fixed order: lanes, then warps).
+template <int NP, int RL>
+__device__ __forceinline__ void slice_partial(Stage &st, double (&p)[RL], double *P, int gsl, int NR) {
+    constexpr int LW = Lanes<NP, RL>::kLW;
 #pragma unroll
-    for (int off = JW; off < 32; off <<= 1) p += __shfl_xor_sync(0xffffffffu, p, off);
+    for (int q = 0; q < RL; ++q)
+#pragma unroll
+        for (int off = LW; off < 32; off <<= 1) p[q] += __shfl_xor_sync(0xffffffffu, p[q], off);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     __syncthreads();
-    if (lane < JW) st.red[w][lane] = p;
+    if (lane < LW)
+#pragma unroll
+        for (int q = 0; q < RL; ++q) st.red[w][lane * RL + q] = p[q];
     __syncthreads();
-    if (threadIdx.x < JW && (int)threadIdx.x < NR) {
+    if ((int)threadIdx.x < NR) {
         double s = 0;
-        for (int q = 0; q < Lanes<JW>::kWarps; ++q) s += st.red[q][threadIdx.x];
+        for (int ww = 0; ww < Lanes<NP, RL>::kWarps; ++ww) s += st.red[ww][threadIdx.x];
         P[(long)gsl * NR + threadIdx.x] = s;
     }
 }
@@ -257,61 +321,85 @@ __device__ __forceinline__ void for_pairs(const BArgs &a, bool two, F f) {
 }  // namespace
 
 // The persistent batched solver.  MIXED: FP64 FCG + FP32 V-cycle; else PCG64.
-// One CTA per slice item (grid-stride), JW lanes per block row.
-template <int JW, bool MIXED>
-__global__ void __launch_bounds__(32 * JW) k_batch_solve(BArgs a) {
+// One CTA per slice item (grid-stride); NP / RL lanes per block row, RL load
+// cases per lane.
+template <int NP, int RL, bool MIXED>
+__global__ void __launch_bounds__(32 * (NP / RL)) k_batch_solve(BArgs a) {
     __shared__ Stage st;
+    using LN = Lanes<NP, RL>;
     const unsigned nb = gridDim.x + a.extra_arrivals;
     const int NR = a.NR;
-    const int r = Lanes<JW>::row(), j = Lanes<JW>::rhs();
-    const bool jok = j < NR;
+    const int r = LN::row(), j0 = LN::j0();
     auto sync = [&]() { return grid_barrier(a.gs, nb, a.limit_ns); };
-    auto X = [&](const BVar &B, int row, int c) { return vidx(B, NR, row, c, j); };
-    // CTA-level loop over slices: f(B, v, gsl, ls, row, live)
+    auto X = [&](const BVar &B, int row, int c) { return vidx<NP>(B, row, c, j0); };
+    // CTA-level loop over slices: f(B, v, gsl, ls, row, live[RL], any)
     auto for_slices = [&](auto f) {
         for (int gsl = blockIdx.x; gsl < a.nslices; gsl += gridDim.x) {
             const int v = a.slice_var[gsl];
             const BVar B = a.var[v];
             const int ls = gsl - B.slice0;
             const int row = ls * kSlice + r;
-            const bool live = jok && a.live[v * NR + j] != 0;
-            f(B, v, gsl, ls, row, live);
+            bool live[RL];
+            bool any = false;
+#pragma unroll
+            for (int q = 0; q < RL; ++q) {
+                live[q] = j0 + q < NR && a.live[v * NR + j0 + q] != 0;
+                any |= live[q];
+            }
+            f(B, v, gsl, ls, row, live, any);
         }
     };
 
     // ---- init: r = f - K u, partials ||r||^2 (pa), ||f||^2 (pb); start of M(r)
-    for_slices([&](const BVar &B, int v, int gsl, int ls, int row, bool) {
+    for_slices([&](const BVar &B, int v, int gsl, int ls, int row, const bool (&)[RL], bool) {
         const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
-        double y[3];
-        spmm_slice<double, JW>(st, S, W, B.scols, B.sv64,
-                               [&](int k, int c) { return jok ? a.u[vidx(B, NR, k, c, j)] : 0.0; }, y);
-        double prr = 0, pff = 0;
-        if (jok && row < B.nfree) {
-            double rv[3];
+        double y[3][RL];
+        spmm_slice<double, NP, RL>(st, S, W, B.scols, B.sv64,
+                                   [&](int k, int c, double (&o)[RL]) { ldv<double, RL>(a.u + vidx<NP>(B, k, c, j0), o); }, y);
+        double prr[RL] = {}, pff[RL] = {};
+        if (row < B.nfree) {
+            double rv[3][RL];
             for (int c = 0; c < 3; ++c) {
-                const long d = X(B, row, c);
-                const double fv = a.f[d];
-                rv[c] = fv - y[c];
-                a.r[d] = rv[c];
-                prr += rv[c] * rv[c];
-                pff += fv * fv;
+                double fv[RL];
+                ldv<double, RL>(a.f + X(B, row, c), fv);
+#pragma unroll
+                for (int q = 0; q < RL; ++q) {
+                    rv[c][q] = fv[q] - y[c][q];
+                    prr[q] += rv[c][q] * rv[c][q];
+                    pff[q] += fv[q] * fv[q];
+                }
+                stv<double, RL>(a.r + X(B, row, c), rv[c]);
             }
             if (MIXED) {
-                float b[3], x[3];
-                for (int c = 0; c < 3; ++c) b[c] = (float)rv[c];
-                block3_apply(B.Dinv32 + 9L * row, b, x);
+                float b[3][RL], x[3][RL];
+#pragma unroll
+                for (int q = 0; q < RL; ++q) {
+                    float bb[3], xx[3];
+                    for (int c = 0; c < 3; ++c) bb[c] = (float)rv[c][q];
+                    block3_apply(B.Dinv32 + 9L * row, bb, xx);
+                    for (int c = 0; c < 3; ++c) {
+                        b[c][q] = bb[c];
+                        x[c][q] = B.wsm * xx[c];
+                    }
+                }
                 for (int c = 0; c < 3; ++c) {
-                    a.b32[X(B, row, c)] = b[c];
-                    a.x32[X(B, row, c)] = B.wsm * x[c];
+                    stv<float, RL>(a.b32 + X(B, row, c), b[c]);
+                    stv<float, RL>(a.x32 + X(B, row, c), x[c]);
                 }
             } else {
-                double z[3];
-                block3_apply(B.Dinv + 9L * row, rv, z);
-                for (int c = 0; c < 3; ++c) a.z64[X(B, row, c)] = z[c];
+                double z[3][RL];
+#pragma unroll
+                for (int q = 0; q < RL; ++q) {
+                    double rr[3], zz[3];
+                    for (int c = 0; c < 3; ++c) rr[c] = rv[c][q];
+                    block3_apply(B.Dinv + 9L * row, rr, zz);
+                    for (int c = 0; c < 3; ++c) z[c][q] = zz[c];
+                }
+                for (int c = 0; c < 3; ++c) stv<double, RL>(a.z64 + X(B, row, c), z[c]);
             }
         }
-        slice_partial<JW>(st, prr, a.pa, gsl, NR);
-        slice_partial<JW>(st, pff, a.pb, gsl, NR);
+        slice_partial<NP, RL>(st, prr, a.pa, gsl, NR);
+        slice_partial<NP, RL>(st, pff, a.pb, gsl, NR);
     });
     if (!sync()) return;
     for_pairs(a, true, [&](int v, int jj, double rr, double ff) {
@@ -327,23 +415,29 @@ __global__ void __launch_bounds__(32 * JW) k_batch_solve(BArgs a) {
     if (!sync()) return;
 
     // MIXED preconditioner z_new = M(r) from b32 / x32 (pre-smoothed by the
-    // caller's phase); partials r.z_new (pa), r.z_old (pb).
+    // phase before); partials r.z_new (pa), r.z_old (pb).
     auto precondition = [&](float *znew, const float *zold) -> bool {
         // t = b - K32 x
-        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, bool live) {
+        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, const bool (&live)[RL], bool any) {
             const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
-            float y[3];
-            spmm_slice<float, JW>(st, S, W, B.scols, B.sv32,
-                                  [&](int k, int c) { return jok ? a.x32[vidx(B, NR, k, c, j)] : 0.f; }, y);
-            if (live && row < B.nfree)
-                for (int c = 0; c < 3; ++c) a.t32[X(B, row, c)] = a.b32[X(B, row, c)] - y[c];
+            float y[3][RL];
+            spmm_slice<float, NP, RL>(st, S, W, B.scols, B.sv32,
+                                      [&](int k, int c, float (&o)[RL]) { ldv<float, RL>(a.x32 + vidx<NP>(B, k, c, j0), o); }, y);
+            if (any && row < B.nfree)
+                for (int c = 0; c < 3; ++c) {
+                    float bv[RL], t[RL];
+                    ldv<float, RL>(a.b32 + X(B, row, c), bv);
+#pragma unroll
+                    for (int q = 0; q < RL; ++q) t[q] = bv[q] - y[c][q];
+                    stv<float, RL>(a.t32 + X(B, row, c), t);
+                }
         });
         if (!sync()) return false;
-        // c = Z^T t: warp per aggregate, JW lanes per load case, 32/JW nodes at a time
+        // c = Z^T t: warp per aggregate, NP lanes per node (one load case each)
         {
+            constexpr int JW = NP, RPW = 32 / NP;
             const int warps = blockDim.x / 32, w = threadIdx.x / 32, lane = threadIdx.x & 31;
             const int sub = lane / JW, jj = lane % JW;
-            constexpr int RPW = 32 / JW;
             for (int ga = blockIdx.x * warps + w; ga < a.naggs; ga += gridDim.x * warps) {
                 const int v = a.agg_var[ga];
                 const BVar B = a.var[v];
@@ -359,8 +453,8 @@ __global__ void __launch_bounds__(32 * JW) k_batch_solve(BArgs a) {
                     const float dx = ((float)B.xyz[3L * node] - cx) * sc;
                     const float dy = ((float)B.xyz[3L * node + 1] - cy) * sc;
                     const float dz = ((float)B.xyz[3L * node + 2] - cz) * sc;
-                    const float tx = a.t32[vidx(B, NR, rr, 0, jj)], ty = a.t32[vidx(B, NR, rr, 1, jj)],
-                                tz = a.t32[vidx(B, NR, rr, 2, jj)];
+                    const float tx = a.t32[vidx<NP>(B, rr, 0, jj)], ty = a.t32[vidx<NP>(B, rr, 1, jj)],
+                                tz = a.t32[vidx<NP>(B, rr, 2, jj)];
                     acc[0] += tx;
                     acc[1] += ty;
                     acc[2] += tz;
@@ -373,16 +467,16 @@ __global__ void __launch_bounds__(32 * JW) k_batch_solve(BArgs a) {
                     float s = acc[k];
 #pragma unroll
                     for (int off = JW; off < 32; off <<= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-                    if (sub == 0 && live) a.cvec[(B.c0 + 6L * I + k) * NR + jj] = s;
+                    if (sub == 0 && live) a.cvec[(B.c0 + 6L * I + k) * NP + jj] = s;
                 }
             }
         }
         if (!sync()) return false;
-        // e = E^-1 c: warp per coarse row, JW lanes per load case
+        // e = E^-1 c: warp per coarse row, NP lanes per load case group
         {
+            constexpr int JW = NP, RPW = 32 / NP;
             const int warps = blockDim.x / 32, w = threadIdx.x / 32, lane = threadIdx.x & 31;
             const int sub = lane / JW, jj = lane % JW;
-            constexpr int RPW = 32 / JW;
             for (int gr = blockIdx.x * warps + w; gr < a.ncrows; gr += gridDim.x * warps) {
                 const int v = a.crow_var[gr];
                 const BVar B = a.var[v];
@@ -391,49 +485,68 @@ __global__ void __launch_bounds__(32 * JW) k_batch_solve(BArgs a) {
                 const float *row = B.Einv32 + (long)i * m;
                 float acc = 0.f;
                 if (live)
-                    for (int k = sub; k < m; k += RPW) acc = fmaf(__ldg(row + k), a.cvec[(B.c0 + k) * NR + jj], acc);
+                    for (int k = sub; k < m; k += RPW) acc = fmaf(__ldg(row + k), a.cvec[(B.c0 + k) * NP + jj], acc);
 #pragma unroll
                 for (int off = JW; off < 32; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-                if (sub == 0 && live) a.evec[(B.c0 + i) * NR + jj] = acc;
+                if (sub == 0 && live) a.evec[(B.c0 + i) * NP + jj] = acc;
             }
         }
         if (!sync()) return false;
         // x += Z e
-        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, bool live) {
-            if (!live || row >= B.nfree) return;
+        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, const bool (&live)[RL], bool any) {
+            if (!any || row >= B.nfree) return;
             const int I = B.agg_of[row], node = B.node_of_free[row];
             const float dx = (float)((B.xyz[3L * node] - B.centroid[3L * I]) * B.inv_scale);
             const float dy = (float)((B.xyz[3L * node + 1] - B.centroid[3L * I + 1]) * B.inv_scale);
             const float dz = (float)((B.xyz[3L * node + 2] - B.centroid[3L * I + 2]) * B.inv_scale);
-            float e[6];
-            for (int k = 0; k < 6; ++k) e[k] = a.evec[(B.c0 + 6L * I + k) * NR + j];
-            a.x32[X(B, row, 0)] += e[0] + dz * e[4] - dy * e[5];
-            a.x32[X(B, row, 1)] += e[1] - dz * e[3] + dx * e[5];
-            a.x32[X(B, row, 2)] += e[2] + dy * e[3] - dx * e[4];
+            float e[6][RL], x[3][RL];
+            for (int k = 0; k < 6; ++k) ldv<float, RL>(a.evec + (B.c0 + 6L * I + k) * NP + j0, e[k]);
+            for (int c = 0; c < 3; ++c) ldv<float, RL>(a.x32 + X(B, row, c), x[c]);
+#pragma unroll
+            for (int q = 0; q < RL; ++q) {
+                x[0][q] += e[0][q] + dz * e[4][q] - dy * e[5][q];
+                x[1][q] += e[1][q] - dz * e[3][q] + dx * e[5][q];
+                x[2][q] += e[2][q] + dy * e[3][q] - dx * e[4][q];
+            }
+            for (int c = 0; c < 3; ++c) stv<float, RL>(a.x32 + X(B, row, c), x[c]);
         });
         if (!sync()) return false;
         // post-smoothing: z_new = x + w Dinv32 (b - K32 x); partials r.z_new, r.z_old
-        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, bool live) {
+        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, const bool (&live)[RL], bool any) {
             const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
-            float y[3];
-            spmm_slice<float, JW>(st, S, W, B.scols, B.sv32,
-                                  [&](int k, int c) { return jok ? a.x32[vidx(B, NR, k, c, j)] : 0.f; }, y);
-            double pn = 0, po = 0;
-            if (live && row < B.nfree) {
-                float res[3], cor[3];
-                for (int c = 0; c < 3; ++c) res[c] = a.b32[X(B, row, c)] - y[c];
-                block3_apply(B.Dinv32 + 9L * row, res, cor);
+            float y[3][RL];
+            spmm_slice<float, NP, RL>(st, S, W, B.scols, B.sv32,
+                                      [&](int k, int c, float (&o)[RL]) { ldv<float, RL>(a.x32 + vidx<NP>(B, k, c, j0), o); }, y);
+            double pn[RL] = {}, po[RL] = {};
+            if (any && row < B.nfree) {
+                float res[3][RL], xv[3][RL], zn[3][RL], zo[3][RL];
+                double rv[3][RL];
                 for (int c = 0; c < 3; ++c) {
-                    const long d = X(B, row, c);
-                    const float z = a.x32[d] + B.wsm * cor[c];
-                    const double rv = a.r[d];
-                    pn += rv * (double)z;
-                    if (zold) po += rv * (double)zold[d];
-                    znew[d] = z;
+                    float bv[RL];
+                    ldv<float, RL>(a.b32 + X(B, row, c), bv);
+                    ldv<float, RL>(a.x32 + X(B, row, c), xv[c]);
+                    ldv<double, RL>(a.r + X(B, row, c), rv[c]);
+                    if (zold) ldv<float, RL>(zold + X(B, row, c), zo[c]);
+#pragma unroll
+                    for (int q = 0; q < RL; ++q) res[c][q] = bv[q] - y[c][q];
                 }
+#pragma unroll
+                for (int q = 0; q < RL; ++q) {
+                    float rr[3], cor[3];
+                    for (int c = 0; c < 3; ++c) rr[c] = res[c][q];
+                    block3_apply(B.Dinv32 + 9L * row, rr, cor);
+                    for (int c = 0; c < 3; ++c) {
+                        zn[c][q] = xv[c][q] + B.wsm * cor[c];
+                        if (live[q]) {
+                            pn[q] += rv[c][q] * (double)zn[c][q];
+                            if (zold) po[q] += rv[c][q] * (double)zo[c][q];
+                        }
+                    }
+                }
+                for (int c = 0; c < 3; ++c) stv<float, RL>(znew + X(B, row, c), zn[c]);
             }
-            slice_partial<JW>(st, pn, a.pa, gsl, NR);
-            slice_partial<JW>(st, po, a.pb, gsl, NR);
+            slice_partial<NP, RL>(st, pn, a.pa, gsl, NR);
+            slice_partial<NP, RL>(st, po, a.pb, gsl, NR);
         });
         return sync();
     };
@@ -443,11 +556,17 @@ __global__ void __launch_bounds__(32 * JW) k_batch_solve(BArgs a) {
         if (!precondition(zcur, nullptr)) return;
     } else {
         // PCG64: partials r.z with z64 = Dinv r
-        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, bool) {
-            double p = 0;
-            if (jok && row < B.nfree)
-                for (int c = 0; c < 3; ++c) p += a.r[X(B, row, c)] * a.z64[X(B, row, c)];
-            slice_partial<JW>(st, p, a.pa, gsl, NR);
+        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, const bool (&)[RL], bool) {
+            double p[RL] = {};
+            if (row < B.nfree)
+                for (int c = 0; c < 3; ++c) {
+                    double rv[RL], zv[RL];
+                    ldv<double, RL>(a.r + X(B, row, c), rv);
+                    ldv<double, RL>(a.z64 + X(B, row, c), zv);
+#pragma unroll
+                    for (int q = 0; q < RL; ++q) p[q] += rv[q] * zv[q];
+                }
+            slice_partial<NP, RL>(st, p, a.pa, gsl, NR);
         });
         if (!sync()) return;
     }
@@ -461,25 +580,42 @@ __global__ void __launch_bounds__(32 * JW) k_batch_solve(BArgs a) {
         // slot (k + 1) % 3 was last read two barriers ago at least
         if (blockIdx.x == 0 && threadIdx.x == 0) a.live_cnt[(k + 1) % 3] = 0;
         // A: p = z + beta p_old, q = K64 p, partial p.q
-        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, bool live) {
+        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, const bool (&live)[RL], bool any) {
             const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
-            const double bt = live ? a.beta[v * NR + j] : 0.0;
-            auto pval = [&](long d) -> double {
-                return fma(bt, pold[d], MIXED ? (double)zcur[d] : a.z64[d]);
+            double bt[RL];
+#pragma unroll
+            for (int q = 0; q < RL; ++q) bt[q] = live[q] ? a.beta[v * NR + j0 + q] : 0.0;
+            auto pval = [&](long d, double (&o)[RL]) {
+                double po[RL];
+                ldv<double, RL>(pold + d, po);
+                if (MIXED) {
+                    float zf[RL];
+                    ldv<float, RL>(zcur + d, zf);
+#pragma unroll
+                    for (int q = 0; q < RL; ++q) o[q] = fma(bt[q], po[q], (double)zf[q]);
+                } else {
+                    double zd[RL];
+                    ldv<double, RL>(a.z64 + d, zd);
+#pragma unroll
+                    for (int q = 0; q < RL; ++q) o[q] = fma(bt[q], po[q], zd[q]);
+                }
             };
-            double y[3];
-            spmm_slice<double, JW>(st, S, W, B.scols, B.sv64,
-                                   [&](int kk, int c) { return live ? pval(vidx(B, NR, kk, c, j)) : 0.0; }, y);
-            double ppq = 0;
-            if (live && row < B.nfree)
+            double y[3][RL];
+            spmm_slice<double, NP, RL>(st, S, W, B.scols, B.sv64,
+                                       [&](int kk, int c, double (&o)[RL]) { pval(vidx<NP>(B, kk, c, j0), o); }, y);
+            double ppq[RL] = {};
+            if (any && row < B.nfree)
                 for (int c = 0; c < 3; ++c) {
                     const long d = X(B, row, c);
-                    const double pn = pval(d);
-                    pnew[d] = pn;
-                    a.q[d] = y[c];
-                    ppq += pn * y[c];
+                    double pn[RL];
+                    pval(d, pn);
+                    stv<double, RL>(pnew + d, pn);
+                    stv<double, RL>(a.q + d, y[c]);
+#pragma unroll
+                    for (int q = 0; q < RL; ++q)
+                        if (live[q]) ppq[q] += pn[q] * y[c][q];
                 }
-            slice_partial<JW>(st, ppq, a.pa, gsl, NR);
+            slice_partial<NP, RL>(st, ppq, a.pa, gsl, NR);
         });
         if (!sync()) return;
         for_pairs(a, false, [&](int v, int jj, double pq, double) {
@@ -495,37 +631,63 @@ __global__ void __launch_bounds__(32 * JW) k_batch_solve(BArgs a) {
         });
         if (!sync()) return;
         // B: u += alpha p, r -= alpha q, partial ||r||^2; start of M(r)
-        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, bool live) {
-            double prr = 0, prz = 0;
-            if (live && row < B.nfree) {
-                const double al = a.alpha[v * NR + j];
-                double rv[3];
+        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, const bool (&live)[RL], bool any) {
+            double prr[RL] = {}, prz[RL] = {};
+            if (any && row < B.nfree) {
+                double al[RL];
+#pragma unroll
+                for (int q = 0; q < RL; ++q) al[q] = live[q] ? a.alpha[v * NR + j0 + q] : 0.0;
+                double rv[3][RL];
                 for (int c = 0; c < 3; ++c) {
                     const long d = X(B, row, c);
-                    a.u[d] = fma(al, pnew[d], a.u[d]);
-                    rv[c] = fma(-al, a.q[d], a.r[d]);
-                    a.r[d] = rv[c];
-                    prr += rv[c] * rv[c];
+                    double uu[RL], pp[RL], qq[RL];
+                    ldv<double, RL>(a.u + d, uu);
+                    ldv<double, RL>(pnew + d, pp);
+                    ldv<double, RL>(a.q + d, qq);
+                    ldv<double, RL>(a.r + d, rv[c]);
+#pragma unroll
+                    for (int q = 0; q < RL; ++q)
+                        if (live[q]) {
+                            uu[q] = fma(al[q], pp[q], uu[q]);
+                            rv[c][q] = fma(-al[q], qq[q], rv[c][q]);
+                            prr[q] += rv[c][q] * rv[c][q];
+                        }
+                    stv<double, RL>(a.u + d, uu);
+                    stv<double, RL>(a.r + d, rv[c]);
                 }
                 if (MIXED) {
-                    float b[3], x[3];
-                    for (int c = 0; c < 3; ++c) b[c] = (float)rv[c];
-                    block3_apply(B.Dinv32 + 9L * row, b, x);
+                    float b[3][RL], x[3][RL];
+#pragma unroll
+                    for (int q = 0; q < RL; ++q) {
+                        float bb[3], xx[3];
+                        for (int c = 0; c < 3; ++c) bb[c] = (float)rv[c][q];
+                        block3_apply(B.Dinv32 + 9L * row, bb, xx);
+                        for (int c = 0; c < 3; ++c) {
+                            b[c][q] = bb[c];
+                            x[c][q] = B.wsm * xx[c];
+                        }
+                    }
                     for (int c = 0; c < 3; ++c) {
-                        a.b32[X(B, row, c)] = b[c];
-                        a.x32[X(B, row, c)] = B.wsm * x[c];
+                        stv<float, RL>(a.b32 + X(B, row, c), b[c]);
+                        stv<float, RL>(a.x32 + X(B, row, c), x[c]);
                     }
                 } else {
-                    double z[3];
-                    block3_apply(B.Dinv + 9L * row, rv, z);
-                    for (int c = 0; c < 3; ++c) {
-                        a.z64[X(B, row, c)] = z[c];
-                        prz += rv[c] * z[c];
+                    double z[3][RL];
+#pragma unroll
+                    for (int q = 0; q < RL; ++q) {
+                        double rr[3], zz[3];
+                        for (int c = 0; c < 3; ++c) rr[c] = rv[c][q];
+                        block3_apply(B.Dinv + 9L * row, rr, zz);
+                        for (int c = 0; c < 3; ++c) {
+                            z[c][q] = zz[c];
+                            if (live[q]) prz[q] += rr[c] * zz[c];
+                        }
                     }
+                    for (int c = 0; c < 3; ++c) stv<double, RL>(a.z64 + X(B, row, c), z[c]);
                 }
             }
-            slice_partial<JW>(st, prr, a.pa, gsl, NR);
-            if (!MIXED) slice_partial<JW>(st, prz, a.pb, gsl, NR);
+            slice_partial<NP, RL>(st, prr, a.pa, gsl, NR);
+            if (!MIXED) slice_partial<NP, RL>(st, prz, a.pb, gsl, NR);
         });
         if (!sync()) return;
         for_pairs(a, !MIXED, [&](int v, int jj, double rr, double rz) {
@@ -570,44 +732,48 @@ __global__ void __launch_bounds__(32 * JW) k_batch_solve(BArgs a) {
     }
 }
 
-// Host order (load case j at j * n, DOF 3 i + c) to the batch's interleaved
-// order (dof0 * NR + (3 i + c) * NR + j), for one variant (and back).
-__global__ void k_interleave(long n, int nrhs, const double *__restrict__ src, double *__restrict__ dst) {
+// Host order (load case j at j * n, DOF d) to the batch's interleaved order
+// (d * NP + j) for one variant (and back); padding load cases stay zero.
+__global__ void k_interleave(long n, int nrhs, int NP, const double *__restrict__ src, double *__restrict__ dst) {
     for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < n * nrhs; g += (long)gridDim.x * blockDim.x) {
         const long j = g / n, d = g % n;
-        dst[d * nrhs + j] = src[g];
+        dst[d * NP + j] = src[g];
     }
 }
-__global__ void k_deinterleave(long n, int nrhs, const double *__restrict__ src, double *__restrict__ dst) {
+__global__ void k_deinterleave(long n, int nrhs, int NP, const double *__restrict__ src, double *__restrict__ dst) {
     for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < n * nrhs; g += (long)gridDim.x * blockDim.x) {
         const long j = g / n, d = g % n;
-        dst[g] = src[d * nrhs + j];
+        dst[g] = src[d * NP + j];
     }
 }
 
 // True FP64 residual partials per (slice, load case): ||f - K u||^2 (pa), ||f||^2 (pb).
-template <int JW>
-__global__ void __launch_bounds__(32 * JW) k_batch_residual(BArgs a) {
+template <int NP, int RL>
+__global__ void __launch_bounds__(32 * (NP / RL)) k_batch_residual(BArgs a) {
     __shared__ Stage st;
-    const int NR = a.NR, j = Lanes<JW>::rhs(), r = Lanes<JW>::row();
-    const bool jok = j < NR;
+    using LN = Lanes<NP, RL>;
+    const int NR = a.NR, j0 = LN::j0(), r = LN::row();
     for (int gsl = blockIdx.x; gsl < a.nslices; gsl += gridDim.x) {
         const BVar B = a.var[a.slice_var[gsl]];
         const int ls = gsl - B.slice0, row = ls * kSlice + r;
         const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
-        double y[3];
-        spmm_slice<double, JW>(st, S, W, B.scols, B.sv64,
-                               [&](int k, int c) { return jok ? a.u[vidx(B, NR, k, c, j)] : 0.0; }, y);
-        double prr = 0, pff = 0;
-        if (jok && row < B.nfree)
+        double y[3][RL];
+        spmm_slice<double, NP, RL>(st, S, W, B.scols, B.sv64,
+                                   [&](int k, int c, double (&o)[RL]) { ldv<double, RL>(a.u + vidx<NP>(B, k, c, j0), o); }, y);
+        double prr[RL] = {}, pff[RL] = {};
+        if (row < B.nfree)
             for (int c = 0; c < 3; ++c) {
-                const double fv = a.f[vidx(B, NR, row, c, j)];
-                const double rv = fv - y[c];
-                prr += rv * rv;
-                pff += fv * fv;
+                double fv[RL];
+                ldv<double, RL>(a.f + vidx<NP>(B, row, c, j0), fv);
+#pragma unroll
+                for (int q = 0; q < RL; ++q) {
+                    const double rv = fv[q] - y[c][q];
+                    prr[q] += rv * rv;
+                    pff[q] += fv[q] * fv[q];
+                }
             }
-        slice_partial<JW>(st, prr, a.pa, gsl, NR);
-        slice_partial<JW>(st, pff, a.pb, gsl, NR);
+        slice_partial<NP, RL>(st, prr, a.pa, gsl, NR);
+        slice_partial<NP, RL>(st, pff, a.pb, gsl, NR);
     }
 }
 
@@ -631,31 +797,54 @@ __global__ void k_barrier_probe(GridSync *gs, unsigned extra, unsigned long long
 namespace {
 
 struct TuneCfg {
-    int kc = 4, ctas_per_sm = 1;
+    int rl = 2, ctas_per_sm = 1;
     double ms_per_iter = 0.0;
 };
 
-// Lanes per block row for NR load cases.
-int jw_for(int NR) { return NR <= 4 ? 4 : NR <= 8 ? 8 : NR <= 16 ? 16 : 32; }
+// Load-case stride of the batch vectors: NR rounded up to a power of two >= 4.
+int np_for(int NR) { return NR <= 4 ? 4 : NR <= 8 ? 8 : NR <= 16 ? 16 : 32; }
+int threads_for(int np, int rl) { return 32 * (np / rl); }
 
-// Kernel instance for (JW, mixed).
-const void *solve_kernel(int jw, bool mixed) {
-    switch (jw) {
-        case 4: return mixed ? (const void *)k_batch_solve<4, true> : (const void *)k_batch_solve<4, false>;
-        case 8: return mixed ? (const void *)k_batch_solve<8, true> : (const void *)k_batch_solve<8, false>;
-        case 16: return mixed ? (const void *)k_batch_solve<16, true> : (const void *)k_batch_solve<16, false>;
-        case 32: return mixed ? (const void *)k_batch_solve<32, true> : (const void *)k_batch_solve<32, false>;
-    }
-    fail(OFEA_ERR_INVALID_ARG, "unsupported lanes per row");
+template <int NP, int RL>
+const void *solve_inst(bool mixed) {
+    return mixed ? (const void *)k_batch_solve<NP, RL, true> : (const void *)k_batch_solve<NP, RL, false>;
 }
-const void *residual_kernel(int jw) {
-    switch (jw) {
-        case 4: return (const void *)k_batch_residual<4>;
-        case 8: return (const void *)k_batch_residual<8>;
-        case 16: return (const void *)k_batch_residual<16>;
-        case 32: return (const void *)k_batch_residual<32>;
+template <int NP>
+const void *solve_np(int rl, bool mixed) {
+    switch (rl) {
+        case 1: return solve_inst<NP, 1>(mixed);
+        case 2: return solve_inst<NP, 2>(mixed);
+        case 4: return solve_inst<NP, 4>(mixed);
     }
-    fail(OFEA_ERR_INVALID_ARG, "unsupported lanes per row");
+    fail(OFEA_ERR_INVALID_ARG, "unsupported load cases per lane");
+}
+// Kernel instance for (NP, RL, mixed).
+const void *solve_kernel(int np, int rl, bool mixed) {
+    switch (np) {
+        case 4: return solve_np<4>(rl, mixed);
+        case 8: return solve_np<8>(rl, mixed);
+        case 16: return solve_np<16>(rl, mixed);
+        case 32: return solve_np<32>(rl, mixed);
+    }
+    fail(OFEA_ERR_INVALID_ARG, "unsupported load-case stride");
+}
+template <int NP>
+const void *residual_np(int rl) {
+    switch (rl) {
+        case 1: return (const void *)k_batch_residual<NP, 1>;
+        case 2: return (const void *)k_batch_residual<NP, 2>;
+        case 4: return (const void *)k_batch_residual<NP, 4>;
+    }
+    fail(OFEA_ERR_INVALID_ARG, "unsupported load cases per lane");
+}
+const void *residual_kernel(int np, int rl) {
+    switch (np) {
+        case 4: return residual_np<4>(rl);
+        case 8: return residual_np<8>(rl);
+        case 16: return residual_np<16>(rl);
+        case 32: return residual_np<32>(rl);
+    }
+    fail(OFEA_ERR_INVALID_ARG, "unsupported load-case stride");
 }
 
 // ---- the on-disk tuning cache: one JSON object per line inside "entries"
@@ -682,7 +871,7 @@ std::map<std::string, TuneCfg> tune_load(const std::string &path) {
         const size_t b = p + 8, e = line.find('"', b);
         if (e == std::string::npos) continue;
         TuneCfg t;
-        t.kc = (int)num(line, "kc", 4);
+        t.rl = (int)num(line, "rl", 2);
         t.ctas_per_sm = (int)num(line, "ctas_per_sm", 1);
         t.ms_per_iter = num(line, "ms_per_iter", 0);
         out[line.substr(b, e - b)] = t;
@@ -703,8 +892,8 @@ void tune_store(const std::string &path, const std::string &key, const TuneCfg &
     for (const auto &kv : all) {
         char buf[512];
         std::snprintf(buf, sizeof(buf),
-                      "    {\"key\": \"%s\", \"kc\": %d, \"ctas_per_sm\": %d, \"ms_per_iter\": %.6f}%s\n",
-                      kv.first.c_str(), kv.second.kc, kv.second.ctas_per_sm,
+                      "    {\"key\": \"%s\", \"rl\": %d, \"ctas_per_sm\": %d, \"ms_per_iter\": %.6f}%s\n",
+                      kv.first.c_str(), kv.second.rl, kv.second.ctas_per_sm,
                       kv.second.ms_per_iter, ++i < all.size() ? "," : "");
         o << buf;
     }
@@ -718,7 +907,7 @@ void tune_store(const std::string &path, const std::string &key, const TuneCfg &
 }  // namespace ofea
 
 struct ofea_batch {
-    int device = 0, V = 0, NR = 0, num_sms = 148;
+    int device = 0, V = 0, NR = 0, NP = 4, num_sms = 148;
     cudaStream_t stream = nullptr;
     std::vector<ofea_ctx *> ctx;
     std::vector<long> dof0, c0;
@@ -822,7 +1011,7 @@ void prepare(ofea_batch *b, bool mixed) {
             OFEA_CUDA(cudaStreamSynchronize(c->stream));
         }
         build_desc(b, true);
-        const size_t n = (size_t)b->ndof * b->NR, nc = std::max<size_t>(1, (size_t)b->ncoarse * b->NR);
+        const size_t n = (size_t)b->ndof * b->NP, nc = std::max<size_t>(1, (size_t)b->ncoarse * b->NP);
         b->b32.ensure(n);
         b->x32.ensure(n);
         b->t32.ensure(n);
@@ -830,16 +1019,23 @@ void prepare(ofea_batch *b, bool mixed) {
         b->zB.ensure(n);
         b->cvec.ensure(nc);
         b->evec.ensure(nc);
+        for (auto *buf : {&b->b32, &b->x32, &b->t32, &b->zA, &b->zB})
+            OFEA_CUDA(cudaMemsetAsync(buf->p, 0, sizeof(float) * n, b->stream));
+        OFEA_CUDA(cudaMemsetAsync(b->cvec.p, 0, sizeof(float) * nc, b->stream));
+        OFEA_CUDA(cudaMemsetAsync(b->evec.p, 0, sizeof(float) * nc, b->stream));
         b->mixed_ready = true;
     }
-    if (!mixed) b->z64.ensure((size_t)b->ndof * b->NR);
+    if (!mixed && !b->z64.p) {
+        b->z64.ensure((size_t)b->ndof * b->NP);
+        OFEA_CUDA(cudaMemsetAsync(b->z64.p, 0, sizeof(double) * b->ndof * b->NP, b->stream));
+    }
 }
 
 BArgs make_args(ofea_batch *b, bool mixed, const TuneCfg &t, int max_iter, double rtol) {
     BArgs a{};
     a.V = b->V;
     a.NR = b->NR;
-    a.kc = t.kc;
+    a.kc = t.rl;
     a.nslices = b->nslices;
     a.naggs = mixed ? b->naggs : 0;
     a.ncrows = mixed ? b->ncrows : 0;
@@ -882,7 +1078,7 @@ BArgs make_args(ofea_batch *b, bool mixed, const TuneCfg &t, int max_iter, doubl
 
 int grid_of(ofea_batch *b, const void *fn, const TuneCfg &t) {
     int occ = 0;
-    OFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * jw_for(b->NR), 0));
+    OFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads_for(b->NP, t.rl), 0));
     if (occ < 1) fail(OFEA_ERR_CAPACITY, "batched solver kernel does not fit on an SM");
     return b->num_sms * std::min(occ, t.ctas_per_sm);
 }
@@ -890,15 +1086,15 @@ int grid_of(ofea_batch *b, const void *fn, const TuneCfg &t) {
 // Enqueue one launch: reset of the per-launch state + the cooperative kernel.
 void enqueue(ofea_batch *b, const BArgs &a, const TuneCfg &t, bool mixed) {
     cudaStream_t s = b->stream;
-    const size_t n = (size_t)b->ndof * b->NR;
+    const size_t n = (size_t)b->ndof * b->NP;
     OFEA_CUDA(cudaMemsetAsync(b->p0.p, 0, sizeof(double) * n, s));
     OFEA_CUDA(cudaMemsetAsync(b->p1.p, 0, sizeof(double) * n, s));
     OFEA_CUDA(cudaMemsetAsync(b->gs.p, 0, sizeof(GridSync), s));
     OFEA_CUDA(cudaMemsetAsync(b->live_cnt.p, 0, sizeof(int) * 3, s));
-    const void *fn = solve_kernel(jw_for(b->NR), mixed);
+    const void *fn = solve_kernel(b->NP, t.rl, mixed);
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(grid_of(b, fn, t));
-    cfg.blockDim = dim3(32 * jw_for(b->NR));
+    cfg.blockDim = dim3(threads_for(b->NP, t.rl));
     cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -914,10 +1110,10 @@ void enqueue(ofea_batch *b, const BArgs &a, const TuneCfg &t, bool mixed) {
 void residuals(ofea_batch *b, const TuneCfg &t) {
     BArgs a = make_args(b, false, t, 0, 0.0);
     cudaStream_t s = b->stream;
-    const void *fn = residual_kernel(jw_for(b->NR));
+    const void *fn = residual_kernel(b->NP, t.rl);
     const int G = std::min(kMaxGrid, b->num_sms * 4);
     void *args[] = {(void *)&a};
-    OFEA_CUDA(cudaLaunchKernel(fn, dim3(G), dim3(32 * jw_for(b->NR)), args, 0, s));
+    OFEA_CUDA(cudaLaunchKernel(fn, dim3(G), dim3(threads_for(b->NP, t.rl)), args, 0, s));
     k_batch_rel<<<std::max(1, std::min(kMaxGrid, (b->V * b->NR + 7) / 8)), 256, 0, s>>>(a, b->rel.p);
     OFEA_CHECK_LAUNCH();
 }
@@ -945,18 +1141,21 @@ TuneCfg autotune(ofea_batch *b, bool mixed, double rtol) {
         auto it = all.find(key);
         if (it != all.end()) {
             TuneCfg t = it->second;
-            if (t.ctas_per_sm >= 1 && t.ctas_per_sm <= 32) return t;
+            if ((t.rl == 1 || t.rl == 2 || t.rl == 4) && t.rl <= b->NP && t.ctas_per_sm >= 1 && t.ctas_per_sm <= 32)
+                return t;
         }
     }
     std::vector<TuneCfg> cand;
-    int occ = 0;
-    OFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_kernel(jw_for(b->NR), mixed),
-                                                            32 * jw_for(b->NR), 0));
-    std::vector<int> cps{1, 2, occ};
-    std::sort(cps.begin(), cps.end());
-    cps.erase(std::unique(cps.begin(), cps.end()), cps.end());
-    for (int c : cps)
-        if (c >= 1 && c <= occ) cand.push_back(TuneCfg{kKC, c, 0.0});
+    for (int rl : {1, 2, 4}) {
+        int occ = 0;
+        OFEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_kernel(b->NP, rl, mixed),
+                                                                threads_for(b->NP, rl), 0));
+        std::vector<int> cps{1, 2, 4, occ};
+        std::sort(cps.begin(), cps.end());
+        cps.erase(std::unique(cps.begin(), cps.end()), cps.end());
+        for (int c : cps)
+            if (c >= 1 && c <= occ) cand.push_back(TuneCfg{rl, c, 0.0});
+    }
     const int iters = 6;
     cudaEvent_t e0, e1;
     OFEA_CUDA(cudaEventCreate(&e0));
@@ -967,7 +1166,7 @@ TuneCfg autotune(ofea_batch *b, bool mixed, double rtol) {
     for (TuneCfg &t : cand) {
         double ms_min = 1e300;
         for (int rep = 0; rep < 2; ++rep) {
-            OFEA_CUDA(cudaMemsetAsync(b->u.p, 0, sizeof(double) * b->ndof * b->NR, s));
+            OFEA_CUDA(cudaMemsetAsync(b->u.p, 0, sizeof(double) * b->ndof * b->NP, s));
             BArgs a = make_args(b, mixed, t, iters, rtol);
             OFEA_CUDA(cudaEventRecord(e0, s));
             enqueue(b, a, t, mixed);
@@ -1001,6 +1200,7 @@ ofea_batch *batch_create(ofea_ctx *const *ctxs, int nv, int nrhs) {
     auto b = std::make_unique<ofea_batch>();
     b->V = nv;
     b->NR = nrhs;
+    b->NP = np_for(nrhs);
     for (int v = 0; v < nv; ++v) {
         ofea_ctx *c = ctxs[v];
         if (!c) fail(OFEA_ERR_INVALID_ARG, "batch: NULL context");
@@ -1021,7 +1221,7 @@ ofea_batch *batch_create(ofea_ctx *const *ctxs, int nv, int nrhs) {
         d0 += c->n;
     }
     b->ndof = d0;
-    const size_t n = std::max<size_t>(1, (size_t)b->ndof * nrhs), vj = (size_t)nv * nrhs;
+    const size_t n = std::max<size_t>(1, (size_t)b->ndof * b->NP), vj = (size_t)nv * nrhs;
     for (auto *buf : {&b->f, &b->u, &b->r, &b->p0, &b->p1, &b->q}) buf->ensure(n);
     for (auto *buf : {&b->ff, &b->tol2, &b->rz, &b->alpha, &b->beta, &b->rel}) buf->ensure(vj);
     for (auto *buf : {&b->live, &b->iters, &b->status}) buf->ensure(vj);
@@ -1048,7 +1248,7 @@ void batch_set_rhs(ofea_batch *b, const double *const *f) {
         b->stage.ensure((size_t)n * b->NR);
         OFEA_CUDA(cudaMemcpyAsync(b->stage.p, f[v], sizeof(double) * n * b->NR, cudaMemcpyHostToDevice, s));
         k_interleave<<<std::max(1, std::min(kMaxGrid, (int)((n * b->NR + 255) / 256))), 256, 0, s>>>(
-            n, b->NR, b->stage.p, b->f.p + b->dof0[v] * b->NR);
+            n, b->NR, b->NP, b->stage.p, b->f.p + b->dof0[v] * b->NP);
         OFEA_CHECK_LAUNCH();
     }
     OFEA_CUDA(cudaStreamSynchronize(s));
@@ -1063,7 +1263,7 @@ void batch_get_solution(ofea_batch *b, double *const *u) {
         if (!u[v]) fail(OFEA_ERR_INVALID_ARG, "batch: NULL solution array");
         b->stage.ensure((size_t)n * b->NR);
         k_deinterleave<<<std::max(1, std::min(kMaxGrid, (int)((n * b->NR + 255) / 256))), 256, 0, s>>>(
-            n, b->NR, b->u.p + b->dof0[v] * b->NR, b->stage.p);
+            n, b->NR, b->NP, b->u.p + b->dof0[v] * b->NP, b->stage.p);
         OFEA_CHECK_LAUNCH();
         OFEA_CUDA(cudaMemcpyAsync(u[v], b->stage.p, sizeof(double) * n * b->NR, cudaMemcpyDeviceToHost, s));
         OFEA_CUDA(cudaStreamSynchronize(s));
@@ -1077,8 +1277,8 @@ void batch_tuning(ofea_batch *b, int method, int *kc, int *threads, int *ctas_pe
     auto it = b->tuned.find(method);
     if (it == b->tuned.end()) it = b->tuned.emplace(method, autotune(b, mixed, 1e-8)).first;
     const TuneCfg &t = it->second;
-    if (kc) *kc = t.kc;
-    if (threads) *threads = 32 * jw_for(b->NR);
+    if (kc) *kc = t.rl;
+    if (threads) *threads = threads_for(b->NP, t.rl);
     if (ctas_per_sm) *ctas_per_sm = t.ctas_per_sm;
     if (ms_per_iter) *ms_per_iter = t.ms_per_iter;
 }
@@ -1104,14 +1304,14 @@ void batch_solve(ofea_batch *b, const ofea_solve_opts &o, ofea_solve_stats *stat
     cudaEvent_t e0, e1;
     OFEA_CUDA(cudaEventCreate(&e0));
     OFEA_CUDA(cudaEventCreate(&e1));
-    OFEA_CUDA(cudaMemsetAsync(b->u.p, 0, sizeof(double) * b->ndof * b->NR, s));
+    OFEA_CUDA(cudaMemsetAsync(b->u.p, 0, sizeof(double) * b->ndof * b->NP, s));
     OFEA_CUDA(cudaEventRecord(e0, s));
     int attempts = 0, launches = 0, remaining = o.max_iter;
     bool failed_barrier = false;
     for (; attempts < 4 && remaining > 0; ++attempts) {
         BArgs a = make_args(b, mixed, t, remaining, o.rtol);
         std::ostringstream k;
-        k << o.method << "/" << t.kc << "/" << t.ctas_per_sm << "/" << remaining << "/"
+        k << o.method << "/" << t.rl << "/" << t.ctas_per_sm << "/" << remaining << "/"
           << o.rtol;
         if (o.use_graph) {
             if (!b->exec || b->exec_key != k.str()) {
