@@ -54,6 +54,7 @@ def parse():
     p.add_argument("--shape", default="200x50x50", help="cantilever elements nx x ny x nz")
     p.add_argument("--rtol", type=float, default=1e-8)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-batched", action="store_true", help="skip the batched-reanalysis measurement")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--mode", default="full", choices=["full", "solve-only"],
                    help="solve-only: assemble, one MIXED and one plain solve, nothing else "
@@ -134,6 +135,72 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+# ------------------------------------------------------ batched reanalysis --
+
+# Algorithmic bytes per (DOF, load case) of one MIXED batched iteration,
+# vectors only (each array counted once per phase): A 28, B 56, residual 12,
+# restriction 4, prolongation 8, post-smoothing 24.
+BATCH_VEC_BYTES_MIXED = 132
+BATCH_VEC_BYTES_PCG64 = 28 + 64  # A (z, p_old, p, q); B (u, p, q, r, z)
+
+
+def run_batched(ob, mg, local, hbm, steps=2, count=64, nrhs=16, rtol=1e-8):
+    """The batched reanalysis workload: `count` SIMP variants n x 20 x 20 (n ~
+    U{20..60}), `nrhs` load cases each, solved by one persistent kernel."""
+    variants = mg.design_variants(count=count, nrhs=nrhs)
+    ctxs, loads, meshes = [], [], []
+    for m, F in variants:
+        c = ob.Context(local)
+        fm = c.upload_mesh(m)
+        c.assemble_pattern()
+        c.assemble_linear()
+        ctxs.append(c)
+        meshes.append((m, fm))
+        loads.append(np.stack([mg.to_free(F[j], fm) for j in range(nrhs)]))
+    n_tot = sum(c.n for c in ctxs)
+    nnz_tot = sum(c.nnz for c in ctxs)
+    b = ob.Batch(ctxs, nrhs)
+    b.set_rhs(loads)
+    out = {}
+    for meth, vec_b in (("GPU_PCG", BATCH_VEC_BYTES_PCG64), ("GPU_MIXED", BATCH_VEC_BYTES_MIXED)):
+        b.solve_resident(meth, rtol=rtol)  # warm-up (tunes on first use, cached on disk)
+        runs = [b.solve_resident(meth, rtol=rtol) for _ in range(steps if meth == "GPU_MIXED" else 1)]
+        st = runs[-1]
+        sec = min(r[0]["seconds"] for r in runs)
+        iters = max(s_["iterations"] for s_ in st)
+        assert all(s_["status"] == 0 and s_["rel_residual"] <= rtol for s_ in st), st
+        # matrix bytes per iteration: FP64 BSELL once (+ FP32 twice for MIXED), 76/9 resp. 40/9 B per nnz
+        mat = 76 * nnz_tot / 9 + (2 * 40 * nnz_tot / 9 if meth == "GPU_MIXED" else 0)
+        per_iter = mat + vec_b * n_tot * nrhs
+        out[meth] = {"seconds": sec, "iterations_max": iters,
+                     "iterations_min": min(s_["iterations"] for s_ in st),
+                     "worst_rel_residual": max(s_["rel_residual"] for s_ in st),
+                     "solves_per_s": count * nrhs / sec, "tuning": b.tuning(meth),
+                     "bytes_per_iteration": per_iter, "achieved_gbs": per_iter * iters / sec / 1e9,
+                     "frac_of_hbm": per_iter * iters / sec / 1e9 / hbm}
+    u_dev = b.solution()  # of the MIXED solve (the last one)
+    # end to end through the one-call C ABI with host buffers (create, upload, solve, download)
+    t0 = time.perf_counter()
+    U, st = ob.solve_batched(ctxs, loads, method="GPU_MIXED", rtol=rtol)
+    e2e = time.perf_counter() - t0
+    diff = max(float(np.linalg.norm(a - c) / max(np.linalg.norm(c), 1e-300)) for a, c in zip(U, u_dev))
+    b.close()
+    for c in ctxs:
+        c.close()
+    mixed = out["GPU_MIXED"]
+    return {
+        "workload": (f"{count} C3D8 SIMP variants n x 20 x 20 (n ~ U{{20..60}}, rho ~ U[0.1,1], E = 210 GPa rho^3), "
+                     f"{nrhs} random load cases each on the x=L face, rtol {rtol:g}; one persistent cooperative "
+                     f"kernel per solve, graph-launched"),
+        "n_dof_total": n_tot, "nnz_total": nnz_tot, "load_cases": count * nrhs,
+        "value": mixed["seconds"], "unit": "s per batch (all load cases of all variants)",
+        "mixed": mixed, "plain_pcg64": out["GPU_PCG"],
+        "speedup_vs_plain_pcg64": out["GPU_PCG"]["seconds"] / mixed["seconds"],
+        "e2e": {"value": e2e, "unit": "s", "h2d_bytes": int(8 * n_tot * nrhs), "d2h_bytes": int(8 * n_tot * nrhs),
+                "max_rel_diff_vs_resident": diff},
+    }
 
 
 # --------------------------------------------------------- reference (CPU) --
@@ -361,6 +428,9 @@ def run_ours(args):
                            "precond_setup_s": st["setup_seconds"]})
         assert st["status"] == 0
     e2e_s = statistics.mean(e2e) if e2e else None
+    batched = None
+    if not args.no_batched:
+        batched = run_batched(ob, mg, local, hbm)
 
     line = {
         "metric": METRIC, "value": sec, "unit": "s", "n_gpus": world, "steps": args.steps,
@@ -397,6 +467,7 @@ def run_ours(args):
                 "phases": phases[-1] if phases else None},
         "clocks": clk.summary(),
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
+        "batched": batched,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
