@@ -463,8 +463,7 @@ void ofea_learn_opts_default(ofea_learn_opts *o) {
 static void prepare_learned_level(ofea_ctx *c) {
     need(c->K_ok, OFEA_ERR_STATE, "K not assembled");
     use_device(c);
-    setup_coarse(c, c->coarse_nodes);
-    setup_learned_level(c);
+    setup_learned_levels(c);
 }
 
 int ofea_learned_train(ofea_ctx *c, const double *f, const ofea_learn_opts *opts, ofea_learn_stats *stats) {

@@ -443,6 +443,59 @@ __global__ void k_f64_to_f32(long n, const double *__restrict__ a, float *__rest
 
 
 
+// ------------------------------------------------ coarse level from level 2 --
+
+// E1 = P^T E2 P: the coarse Galerkin matrix from the nested level's blocks
+// (Z1 = Z2 P exactly, P the map of a parent's rigid modes into its
+// children's).  36 threads per (parent I, neighbour slot S), one per entry of
+// the 6 x 6 block; sums over child pairs in a fixed order.
+__device__ __forceinline__ double pmat(const float *pd, int p, int k) {
+    // P[p][k] of a child with (delta, ratio) = pd
+    const double dx = pd[0], dy = pd[1], dz = pd[2], ro = pd[3];
+    if (p < 3) {
+        if (k < 3) return p == k ? 1.0 : 0.0;
+        // translation rows: T2 = T1 + theta1 x delta
+        const int t = k - 3;  // theta component
+        if (p == 0) return t == 1 ? dz : t == 2 ? -dy : 0.0;
+        if (p == 1) return t == 2 ? dx : t == 0 ? -dz : 0.0;
+        return t == 0 ? dy : t == 1 ? -dx : 0.0;
+    }
+    return k == p ? ro : 0.0;
+}
+
+__global__ void k_e1_from_e2(int na1, int m1, const int *__restrict__ nbr1, const int *__restrict__ children,
+                             const int *__restrict__ cell2, const float *__restrict__ pdel,
+                             const double *__restrict__ Eb, double *__restrict__ E1) {
+    const int k = threadIdx.x / 6, l = threadIdx.x % 6;
+    for (int item = blockIdx.x; item < na1 * 27; item += gridDim.x) {
+        const int I = item / 27, S = item % 27;
+        const int J = nbr1[27L * I + S];
+        if (J < 0 || threadIdx.x >= 36) continue;
+        double acc = 0.0;
+        for (int ca = 0; ca < 8; ++ca) {
+            const int a = children[8L * I + ca];
+            if (a < 0) continue;
+            for (int cb = 0; cb < 8; ++cb) {
+                const int b = children[8L * J + cb];
+                if (b < 0) continue;
+                const int dx = cell2[3 * b] - cell2[3 * a], dy = cell2[3 * b + 1] - cell2[3 * a + 1],
+                          dz = cell2[3 * b + 2] - cell2[3 * a + 2];
+                if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) continue;
+                const double *E = Eb + ((long)a * 27 + (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1)) * 36;
+                const float *pa = pdel + 4L * a, *pb = pdel + 4L * b;
+                for (int p = 0; p < 6; ++p) {
+                    const double pak = pmat(pa, p, k);
+                    if (pak == 0.0) continue;
+                    double t = 0.0;
+                    for (int q = 0; q < 6; ++q) t += E[6 * p + q] * pmat(pb, q, l);
+                    acc += pak * t;
+                }
+            }
+        }
+        E1[(6L * I + k) * m1 + 6L * J + l] = acc;
+    }
+}
+
 // -------------------------------------------------------- the stage M --
 
 // Rows r = b * na + I of a batch of coarse vectors (6 floats per row).
@@ -683,7 +736,14 @@ void setup_learned_level(ofea_ctx *c) {
                 pd[4L * J + d] = (float)((C2.centroid_h[3L * J + d] - C1.centroid_h[3L * P + d]) * C1.inv_scale);
             pd[4L * J + 3] = (float)ratio;
         }
+        std::vector<int> ch(8L * C1.na, -1), nch(C1.na, 0);
+        for (int J = 0; J < na2; ++J) {
+            const int P = par[J];
+            if (nch[P] >= 8) fail(OFEA_ERR_STATE, "learned level: more than 8 children in a coarse cell");
+            ch[8L * P + nch[P]++] = J;
+        }
         N.parent.upload(par.data(), na2, c->stream);
+        N.children.upload(ch.data(), ch.size(), c->stream);
         N.pdel.upload(pd.data(), pd.size(), c->stream);
         N.invdeg.ensure(na2);
         k_invdeg<<<grid_for(c, na2, kBlock), kBlock, 0, c->stream>>>(na2, C2.nbr.p, N.invdeg.p);
@@ -728,6 +788,24 @@ void setup_learned_level(ofea_ctx *c) {
     C2.K_ok = true;
 }
 
+
+// Both coarse levels for the LEARNED solver: the nested level's Galerkin
+// blocks are assembled from K, and, when the coarse level's E is missing, it
+// is formed from them (E1 = P^T E2 P) instead of a second pass over K.
+void setup_learned_levels(ofea_ctx *c) {
+    setup_coarse_geometry(c, c->coarse_nodes);
+    const bool need_e1 = !c->coarse.K_ok;
+    setup_learned_level(c);
+    if (need_e1) {
+        Coarse &C1 = c->coarse;
+        double *E = coarse_begin_E(c);
+        k_e1_from_e2<<<std::min(C1.na * 27, c->num_sms * 16), 64, 0, c->stream>>>(
+            C1.na, C1.m, C1.nbr.p, c->learned.children.p, c->coarse2.agg_cell.p, c->learned.pdel.p,
+            c->learned.Eb.p, E);
+        OFEA_CHECK_LAUNCH();
+        coarse_finish(c);
+    }
+}
 
 static void ensure_rows(ofea_ctx *c, long Rp) {
     Learned &N = c->learned;

@@ -145,7 +145,7 @@ struct Learned {
     DevBuf<float> w, g, m, v, part;              // weights, gradient, Adam moments, wgrad partials
     DevBuf<double> Eb, sigma, lossp, cpart;      // E2 blocks, sample RMS, loss / coefficient partials
     DevBuf<float> Ehat, dsq, feat, pdel, shifted, invdeg, Binv, X0, scale;
-    DevBuf<int> parent;
+    DevBuf<int> parent, children;
     DevBuf<float> Z0, H[5], A[4], Zl[4], Y, dY, dH, dZ, dA;  // network activations (one row per aggregate)
     DevBuf<float> pv[9];                                      // stage vectors (rows of a batch)
     DevBuf<float> batch_src, r32, data;
@@ -212,6 +212,7 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
 void profile_kernels(ofea_ctx *c, int method, int reps, double *ms, double *bytes);
 // learned.cu
 void setup_learned_level(ofea_ctx *c);
+void setup_learned_levels(ofea_ctx *c);
 void learned_prepare_inference(ofea_ctx *c);
 void learned_apply(ofea_ctx *c, const float *t, float *x);
 // Batched persistent solver (batched.cu).

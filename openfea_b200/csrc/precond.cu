@@ -570,20 +570,43 @@ void coarse_E_partials(ofea_ctx *c, Coarse &C, int nchunk) {
     OFEA_CHECK_LAUNCH();
 }
 
-void setup_coarse(ofea_ctx *c, int target_nodes) {
+void setup_coarse_geometry(ofea_ctx *c, int target_nodes) {
     Coarse &C = c->coarse;
     if (!C.geom_ok || C.target != target_nodes) {
         C.target = target_nodes;
         build_aggregation(c, target_nodes);
     }
-    if (C.K_ok) return;
-    cudaStream_t s = c->stream;
+}
+
+double *coarse_begin_E(ofea_ctx *c) {
+    Coarse &C = c->coarse;
     const int m = C.m;
     C.E.ensure((size_t)m * m);
     C.Einv32.ensure((size_t)m * m);
     C.cvec.ensure(std::max(m, 1));
     C.evec.ensure(std::max(m, 1));
-    OFEA_CUDA(cudaMemsetAsync(C.E.p, 0, sizeof(double) * m * m, s));
+    OFEA_CUDA(cudaMemsetAsync(C.E.p, 0, sizeof(double) * m * m, c->stream));
+    return C.E.p;
+}
+
+void coarse_finish(ofea_ctx *c) {
+    Coarse &C = c->coarse;
+    cudaStream_t s = c->stream;
+    const int m = C.m;
+    invert_spd(c, C.E.p, m);
+    k_round_f32<<<grid_for(c, (long)m * m, kBlock), kBlock, 0, s>>>((long)m * m, C.E.p, C.Einv32.p);
+    OFEA_CHECK_LAUNCH();
+    C.lmax = estimate_lambda_max(c, 10);
+    C.K_ok = true;
+}
+
+void setup_coarse(ofea_ctx *c, int target_nodes) {
+    Coarse &C = c->coarse;
+    setup_coarse_geometry(c, target_nodes);
+    if (C.K_ok) return;
+    cudaStream_t s = c->stream;
+    const int m = C.m;
+    coarse_begin_E(c);
     OFEA_CUDA(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), s));
     const int nchunk = (C.max_agg + kChunkNodes - 1) / kChunkNodes;
     C.part.ensure((size_t)C.na * nchunk * 27 * 36);
@@ -594,11 +617,7 @@ void setup_coarse(ofea_ctx *c, int target_nodes) {
     OFEA_CUDA(cudaMemcpyAsync(c->herr.p, c->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     OFEA_CUDA(cudaStreamSynchronize(s));
     if (c->herr.p[0]) fail(OFEA_ERR_CAPACITY, "coarse cells smaller than the element couplings");
-    invert_spd(c, C.E.p, m);
-    k_round_f32<<<grid_for(c, (long)m * m, kBlock), kBlock, 0, s>>>((long)m * m, C.E.p, C.Einv32.p);
-    OFEA_CHECK_LAUNCH();
-    C.lmax = estimate_lambda_max(c, 10);
-    C.K_ok = true;
+    coarse_finish(c);
 }
 
 // ---------------------------------------------------------- V-cycle kernels --

@@ -9,6 +9,11 @@ void build_aggregation_fine(ofea_ctx *c);
 // Aggregation (once per mesh), E = Z^T K Z, its inverse and lambda_max(D^-1 K)
 // (once per K).
 void setup_coarse(ofea_ctx *c, int target_nodes);
+// The same in parts: the aggregation only; a zeroed dense E to fill (returns
+// it); inversion, FP32 copy and lambda_max of a filled E.
+void setup_coarse_geometry(ofea_ctx *c, int target_nodes);
+double *coarse_begin_E(ofea_ctx *c);
+void coarse_finish(ofea_ctx *c);
 // Damping weight of the block-Jacobi smoother (needs setup_coarse's lmax).
 float smoother_weight(const ofea_ctx *c);
 // x += Z E^-1 Z^T t  (FP32 vectors of n entries)

@@ -495,11 +495,12 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
         const bool had = c->coarse.K_ok;
         cudaEvent_t es;
         OFEA_CUDA(cudaEventCreate(&es));
-        setup_coarse(c, c->coarse_nodes);
         if (learned) {
             if (!c->learned.have_weights) fail(OFEA_ERR_STATE, "train or load the learned stage first");
-            setup_learned_level(c);
+            setup_learned_levels(c);
             learned_prepare_inference(c);
+        } else {
+            setup_coarse(c, c->coarse_nodes);
         }
         OFEA_CUDA(cudaEventRecord(es, s));
         OFEA_CUDA(cudaEventSynchronize(es));

@@ -69,3 +69,19 @@ def test_learned_solve_needs_weights(gpu_ctx_factory):
     with pytest.raises(ob.OfeaError) as e:
         ctx.solve(f, method="GPU_LEARNED")
     assert e.value.code == -6
+
+
+def test_coarse_matrix_from_nested_level_matches_direct_assembly(gpu_ctx_factory):
+    """A LEARNED solve forms the coarse Galerkin matrix from the nested level's
+    blocks (E1 = P^T E2 P); a MIXED solve that reuses it must behave like one
+    whose E1 was assembled from K directly."""
+    ctx, f = cantilever_ctx(gpu_ctx_factory, 40, 10, 10)
+    ctx.learned_train(sample_iters=64, sample_every=4, steps=5, batch=4)
+    ctx.precond_reset()
+    u1, s1 = ctx.solve(f, method="GPU_MIXED", rtol=1e-10)  # E1 from K
+    ctx.precond_reset()
+    _, sl = ctx.solve(f, method="GPU_LEARNED", rtol=1e-10)  # E1 from E2
+    assert sl["status"] == 0 and sl["rejected_learned"] == 0
+    u2, s2 = ctx.solve(f, method="GPU_MIXED", rtol=1e-10)  # reuses that E1
+    assert abs(s1["iterations"] - s2["iterations"]) <= 1
+    assert np.linalg.norm(u1 - u2) / np.linalg.norm(u1) < 1e-8
