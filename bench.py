@@ -55,6 +55,7 @@ def parse():
     p.add_argument("--rtol", type=float, default=1e-8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-batched", action="store_true", help="skip the batched-reanalysis measurement")
+    p.add_argument("--no-simp", action="store_true", help="skip the learned-preconditioner SIMP measurement")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--mode", default="full", choices=["full", "solve-only"],
                    help="solve-only: assemble, one MIXED and one plain solve, nothing else "
@@ -200,6 +201,60 @@ def run_batched(ob, mg, local, hbm, steps=2, count=64, nrhs=16, rtol=1e-8):
         "speedup_vs_plain_pcg64": out["GPU_PCG"]["seconds"] / mixed["seconds"],
         "e2e": {"value": e2e, "unit": "s", "h2d_bytes": int(8 * n_tot * nrhs), "d2h_bytes": int(8 * n_tot * nrhs),
                 "max_rel_diff_vs_resident": diff},
+    }
+
+
+# ------------------------------------------------ learned preconditioner (cfg5) --
+
+def run_learned_simp(ob, mg, local, shape, rtol=1e-8, steps=2):
+    """The learned-preconditioner configuration: the cantilever mesh with a
+    SIMP density field (rho ~ U[0.1, 1] per element, 3x3x3 box filter, E =
+    210 GPa rho^3).  The stage is trained on the plain-PCG residuals of one
+    seeded density sample (2,000 samples) and applied, unchanged, to another
+    density sample; plain PCG64 and MIXED are timed on the same test matrix."""
+    nx, ny, nz = shape
+
+    def make(seed):
+        m, ff = mg.cantilever_large(nx, ny, nz)
+        m.E = 210e9 * mg.simp_density((nx, ny, nz), seed, smooth=True) ** 3
+        c = ob.Context(local)
+        fm = c.upload_mesh(m)
+        c.assemble_pattern()
+        c.assemble_linear()
+        return c, mg.to_free(ff, fm)
+
+    ctr, _ = make(11)
+    cte, f = make(12)
+    t0 = time.perf_counter()
+    train = ctr.learned_train(None, sample_iters=2000, sample_every=1, steps=400, batch=16, lr=1e-3, seed=1234)
+    train["wall_s"] = time.perf_counter() - t0
+    cte.set_learned_weights(ctr.learned_weights())
+
+    def timed(method, reps):
+        out = []
+        for _ in range(reps):
+            cte.precond_reset()
+            u, st = cte.solve(f, method=method, rtol=rtol)
+            assert st["status"] == 0 and st["rel_residual"] <= rtol, st
+            out.append(st)
+        return min(out, key=lambda s_: s_["seconds"])
+
+    plain = timed("GPU_PCG", 1)
+    mixed = timed("GPU_MIXED", steps + 1)
+    learned = timed("GPU_LEARNED", steps + 1)
+    ctr.close()
+    cte.close()
+    return {
+        "workload": (f"C3D8 cantilever {nx}x{ny}x{nz}, SIMP density (rho ~ U[0.1,1], 3x3x3 box filter, seed 12), "
+                     f"E = 210 GPa rho^3; stage trained on density seed 11 (2,000 plain-PCG residual samples); "
+                     f"rel. residual {rtol:g}; set-up included"),
+        "learned_s": learned["seconds"], "learned_iterations": learned["iterations"],
+        "learned_rejected": learned["rejected_learned"], "learned_setup_s": learned["setup_seconds"],
+        "mixed_s": mixed["seconds"], "mixed_iterations": mixed["iterations"],
+        "plain_pcg64_s": plain["seconds"], "plain_pcg64_iterations": plain["iterations"],
+        "speedup_learned_vs_plain": plain["seconds"] / learned["seconds"],
+        "gain_learned_vs_mixed": mixed["seconds"] / learned["seconds"],
+        "training": train,
     }
 
 
@@ -431,6 +486,9 @@ def run_ours(args):
     batched = None
     if not args.no_batched:
         batched = run_batched(ob, mg, local, hbm)
+    learned_simp = None
+    if not args.no_simp:
+        learned_simp = run_learned_simp(ob, mg, local, (nx, ny, nz), rtol=args.rtol)
 
     line = {
         "metric": METRIC, "value": sec, "unit": "s", "n_gpus": world, "steps": args.steps,
@@ -468,6 +526,7 @@ def run_ours(args):
         "clocks": clk.summary(),
         "gpu_launches": int(sum(s["kernel_launches"] for s in stats)),
         "batched": batched,
+        "learned_simp": learned_simp,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

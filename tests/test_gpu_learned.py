@@ -85,3 +85,25 @@ def test_coarse_matrix_from_nested_level_matches_direct_assembly(gpu_ctx_factory
     u2, s2 = ctx.solve(f, method="GPU_MIXED", rtol=1e-10)  # reuses that E1
     assert abs(s1["iterations"] - s2["iterations"]) <= 1
     assert np.linalg.norm(u1 - u2) / np.linalg.norm(u1) < 1e-8
+
+
+def test_stage_trained_on_one_density_field_helps_on_another(gpu_ctx_factory):
+    """What the trained stage gains on a heterogeneous SIMP material, with
+    weights trained on a different density sample than the one solved."""
+    def make(seed):
+        m, ffull = mg.cantilever_large(60, 16, 16)
+        m.E = 210e9 * mg.simp_density((60, 16, 16), seed, smooth=True) ** 3
+        ctx = gpu_ctx_factory()
+        fm = ctx.upload_mesh(m)
+        ctx.assemble_pattern()
+        ctx.assemble_linear()
+        return ctx, mg.to_free(ffull, fm)
+    ctr, _ = make(21)
+    cte, f = make(22)
+    ctr.learned_train(sample_iters=800, sample_every=2, steps=300, batch=16)
+    cte.set_learned_weights(ctr.learned_weights())
+    um, sm = cte.solve(f, method="GPU_MIXED", rtol=1e-8)
+    ul, sl = cte.solve(f, method="GPU_LEARNED", rtol=1e-8)
+    assert sl["status"] == 0 and sl["rejected_learned"] == 0 and sl["rel_residual"] <= 1e-8
+    assert np.linalg.norm(ul - um) / np.linalg.norm(um) < 1e-6
+    assert sl["iterations"] < sm["iterations"], (sl["iterations"], sm["iterations"])
