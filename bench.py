@@ -57,9 +57,13 @@ def parse():
     p.add_argument("--no-batched", action="store_true", help="skip the batched-reanalysis measurement")
     p.add_argument("--no-simp", action="store_true", help="skip the learned-preconditioner SIMP measurement")
     p.add_argument("--e2e-steps", type=int, default=2)
-    p.add_argument("--mode", default="full", choices=["full", "solve-only"],
-                   help="solve-only: assemble, one MIXED and one plain solve, nothing else "
-                        "(a short launch list for profilers)")
+    p.add_argument("--batch-count", type=int, default=16, help="variants of --mode batched-only")
+    p.add_argument("--batch-max-iter", type=int, default=12, help="iterations of --mode batched-only")
+    p.add_argument("--mode", default="full", choices=["full", "solve-only", "batched-only"],
+                   help="solve-only: assemble, a short training, one LEARNED, one MIXED and one "
+                        "plain solve, nothing else (a short launch list for profilers); batched-only: "
+                        "--batch-count variants of the batched workload, one MIXED batched solve capped "
+                        "at --batch-max-iter iterations (a small case for a kernel profile)")
     return p.parse_args()
 
 
@@ -355,6 +359,31 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    if args.mode == "batched-only":
+        variants = mg.design_variants(count=args.batch_count, nrhs=16)
+        ctxs, loads = [], []
+        for m, F in variants:
+            c = ob.Context(local)
+            fm = c.upload_mesh(m)
+            c.assemble_pattern()
+            c.assemble_linear()
+            ctxs.append(c)
+            loads.append(np.stack([mg.to_free(F[j], fm) for j in range(F.shape[0])]))
+        b = ob.Batch(ctxs, 16)
+        b.set_rhs(loads)
+        tune = b.tuning("GPU_MIXED")
+        st = b.solve_resident("GPU_MIXED", rtol=args.rtol, max_iter=args.batch_max_iter, raise_on_error=False)
+        if rank == 0:
+            print(json.dumps({"mode": "batched-only", "variants": args.batch_count,
+                              "n_dof_total": sum(c.n for c in ctxs), "tuning": tune,
+                              "seconds": st[0]["seconds"], "iterations": st[0]["iterations"]}), flush=True)
+        b.close()
+        for c in ctxs:
+            c.close()
+        if dist:
+            dist.destroy_process_group()
+        return 0
+
     nx, ny, nz = shape_of(args.shape)
     mesh, ffull = mg.cantilever_large(nx, ny, nz)
     fm = mg.free_map(mesh.nd, mesh.fix)
@@ -384,12 +413,16 @@ def run_ours(args):
         return st
 
     if args.mode == "solve-only":
+        # a short launch list for profilers: a brief training (20 steps), then
+        # one LEARNED, one MIXED and one plain solve
+        ctx.learned_train(None, sample_iters=200, sample_every=4, steps=20, batch=16)
+        st_l = solve("GPU_LEARNED")
         st_m = solve("GPU_MIXED")
         st_p = solve("GPU_PCG")
         torch.cuda.synchronize()
         if rank == 0:
             print(json.dumps({"mode": "solve-only", "shape": args.shape, "n": n, "nnz": nnz,
-                              "mixed": st_m, "plain": st_p}), flush=True)
+                              "learned": st_l, "mixed": st_m, "plain": st_p}), flush=True)
         ctx.close()
         if dist:
             dist.destroy_process_group()

@@ -153,6 +153,13 @@ OFEA_API int ofea_solve_device(ofea_ctx *ctx, const double *d_f, double *d_u, co
 OFEA_API int ofea_residual_norms_noalloc(ofea_ctx *ctx, int nrhs, const double *d_f,
                                          const double *d_u, double *d_norms);
 
+/* No counterpart in the reference: the target number of free nodes per
+ * aggregate of the MIXED / LEARNED coarse level (default 1000; the learned
+ * level's aggregates are 8 times smaller).  Larger aggregates make the
+ * per-matrix set-up cheaper (its dense inverse is cubic in their count) and
+ * the iterations more numerous.  Invalidates the coarse levels. */
+OFEA_API int ofea_set_coarse_nodes(ofea_ctx *ctx, int nodes);
+
 /* ---- learned coarse-correction stage -------------------------------------- */
 /* No counterpart in the reference.  OFEA_SOLVER_LEARNED adds a second coarse
  * stage to the mixed V-cycle, on nested aggregates (cells half as wide as the

@@ -107,6 +107,7 @@ def lib():
         "ofea_write_vtk": (_I, [ctypes.c_char_p, _I, _P, _I, _P, _P, _P, _D]),
         "ofea_profile_solver_kernels": (_I, [_P, _I, _I, _P, _P]),
         "ofea_precond_reset": (_I, [_P]),
+        "ofea_set_coarse_nodes": (_I, [_P, _I]),
         "ofea_learn_opts_default": (None, [_P]),
         "ofea_batch_create": (_I, [ctypes.POINTER(_P), _P, _I, _I]),
         "ofea_batch_destroy": (_I, [_P]),
@@ -327,6 +328,10 @@ class Context:
             _check(rc, "ofea_solve")
         st = [s.as_dict() for s in stats]
         return (U[:, 0] if F.ndim == 1 else U), (st[0] if F.ndim == 1 else st)
+
+    def set_coarse_nodes(self, nodes):
+        """Target free nodes per coarse aggregate (default 1000)."""
+        _check(lib().ofea_set_coarse_nodes(self.h, int(nodes)), "ofea_set_coarse_nodes")
 
     def precond_reset(self):
         """Rebuild the preconditioner at the next solve (as after a new assembly)."""

@@ -379,6 +379,18 @@ static void check_solve_ready(ofea_ctx *c, const ofea_solve_opts &o) {
     if (!c->jacobi_ok) fail(OFEA_ERR_BREAKDOWN, "a diagonal block of K is not positive definite");
 }
 
+int ofea_set_coarse_nodes(ofea_ctx *c, int nodes) {
+    return guarded([&] {
+        need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
+        need(nodes >= 8 && nodes <= 1000000, OFEA_ERR_INVALID_ARG, "nodes per aggregate must be 8..1e6");
+        if (nodes != c->coarse_nodes) {
+            c->coarse_nodes = nodes;
+            c->coarse.geom_ok = c->coarse.K_ok = false;
+            c->coarse2.geom_ok = c->coarse2.K_ok = false;
+        }
+    });
+}
+
 int ofea_precond_reset(ofea_ctx *c) {
     return guarded([&] {
         need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");

@@ -753,8 +753,7 @@ void setup_learned_level(ofea_ctx *c) {
     if (C2.K_ok) return;
     cudaStream_t s = c->stream;
     const int na = C2.na;
-    const int nchunk = (C2.max_agg + 63) / 64;
-    C2.part.ensure((size_t)na * nchunk * 27 * 36);
+    const int nchunk = 1;
     OFEA_CUDA(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), s));
     coarse_E_partials(c, C2, nchunk);
     N.Eb.ensure((size_t)na * 27 * 36);

@@ -291,6 +291,129 @@ __global__ void __launch_bounds__(kEThreads) k_coarse_E_chunks(
 }
 
 // Stage 2: E entries from the chunk partials, fixed chunk order.
+// Galerkin blocks E[I][s] = sum over nodes i of I and row blocks K_ij with
+// aggregate(j) in neighbour slot s of Z_i^T K_ij Z_j (6 x 6, row-major), for
+// every aggregate I of a level.  One CTA per aggregate; warp w takes the
+// aggregate's nodes w, w + kGW, ... in order; lane t takes block t of the
+// node's row (32 at a time) and forms W = K_ij Z_j (3 x 6).  Lanes whose
+// blocks land in the same slot are summed in lane order (match_any, then 32
+// broadcast shuffles, or a shuffle tree when the whole warp shares one slot),
+// the group's first lane adds Z_i^T W to its warp's accumulator, and the
+// warps' accumulators are summed in warp order: deterministic.
+constexpr int kGW = 4;  // warps per CTA
+
+__device__ __forceinline__ void cross_e(int t, const double d[3], double z[3]) {
+    // e_t x d
+    if (t == 0) { z[0] = 0.0; z[1] = -d[2]; z[2] = d[1]; }
+    else if (t == 1) { z[0] = d[2]; z[1] = 0.0; z[2] = -d[0]; }
+    else { z[0] = -d[1]; z[1] = d[0]; z[2] = 0.0; }
+}
+
+__global__ void __launch_bounds__(kGW * 32) k_galerkin_blocks(
+    int na, const int *__restrict__ agg_ptr, const int *__restrict__ agg_nodes, const int *__restrict__ agg_of,
+    const int *__restrict__ agg_cell, const int *__restrict__ node_of_free, const double *__restrict__ xyz,
+    const double *__restrict__ centroid, double inv_scale, const int *__restrict__ rowptr,
+    const int *__restrict__ cols, const double *__restrict__ Kb, double *__restrict__ Eb, int *__restrict__ err) {
+    __shared__ double acc[kGW][27 * 36];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int I = blockIdx.x; I < na; I += gridDim.x) {
+        for (int v = threadIdx.x; v < kGW * 27 * 36; v += blockDim.x) (&acc[0][0])[v] = 0.0;
+        __syncthreads();
+        const int cx = agg_cell[3 * I], cy = agg_cell[3 * I + 1], cz = agg_cell[3 * I + 2];
+        const double cI[3] = {centroid[3L * I], centroid[3L * I + 1], centroid[3L * I + 2]};
+        for (int idx = agg_ptr[I] + w; idx < agg_ptr[I + 1]; idx += kGW) {
+            const int i = agg_nodes[idx], ni = node_of_free[i];
+            double di[3];
+            for (int d = 0; d < 3; ++d) di[d] = (xyz[3L * ni + d] - cI[d]) * inv_scale;
+            const int rb = rowptr[i], deg = rowptr[i + 1] - rb;
+            for (int c0 = 0; c0 < deg; c0 += 32) {
+                const int k = c0 + lane;
+                double v[18];
+#pragma unroll
+                for (int e = 0; e < 18; ++e) v[e] = 0.0;
+                int slot = -2;  // lanes past the row form their own group
+                if (k < deg) {
+                    const int j = cols[rb + k], J = agg_of[j];
+                    const int dx = agg_cell[3 * J] - cx, dy = agg_cell[3 * J + 1] - cy, dz = agg_cell[3 * J + 2] - cz;
+                    if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1) {
+                        slot = (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
+                    } else {
+                        atomicExch(err, 1);
+                        slot = -1;
+                    }
+                    const int nj = node_of_free[j];
+                    double dj[3];
+                    for (int d = 0; d < 3; ++d) dj[d] = (xyz[3L * nj + d] - centroid[3L * J + d]) * inv_scale;
+                    double K[9];
+#pragma unroll
+                    for (int e = 0; e < 9; ++e) K[e] = Kb[9L * (rb + k) + e];
+                    // W[:, l] = K e_l (l < 3), K (e_(l-3) x dj) (l >= 3); v[r * 6 + l]
+#pragma unroll
+                    for (int r = 0; r < 3; ++r)
+#pragma unroll
+                        for (int l = 0; l < 3; ++l) v[r * 6 + l] = K[3 * r + l];
+#pragma unroll
+                    for (int t = 0; t < 3; ++t) {
+                        double z[3];
+                        cross_e(t, dj, z);
+#pragma unroll
+                        for (int r = 0; r < 3; ++r) v[r * 6 + 3 + t] = K[3 * r] * z[0] + K[3 * r + 1] * z[1] + K[3 * r + 2] * z[2];
+                    }
+                }
+                const unsigned mask = __match_any_sync(0xffffffffu, slot);
+                const int leader = __ffs(mask) - 1;
+                double W[18];
+                if (__all_sync(0xffffffffu, mask == 0xffffffffu)) {
+                    // one slot for the whole warp: tree sum
+#pragma unroll
+                    for (int e = 0; e < 18; ++e) {
+                        double x = v[e];
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+                        W[e] = x;
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 18; ++e) W[e] = 0.0;
+                    for (int t = 0; t < 32; ++t) {
+                        const bool mine = (mask >> t) & 1u;
+#pragma unroll
+                        for (int e = 0; e < 18; ++e) {
+                            const double x = __shfl_sync(0xffffffffu, v[e], t);
+                            if (mine) W[e] += x;
+                        }
+                    }
+                }
+                if (lane == leader && slot >= 0) {
+                    // E[k][l] += Z_i[:, k] . W[:, l]
+                    double *a = acc[w] + slot * 36;
+#pragma unroll
+                    for (int kk = 0; kk < 3; ++kk)
+#pragma unroll
+                        for (int l = 0; l < 6; ++l) a[kk * 6 + l] += W[kk * 6 + l];
+#pragma unroll
+                    for (int t = 0; t < 3; ++t) {
+                        double z[3];
+                        cross_e(t, di, z);
+#pragma unroll
+                        for (int l = 0; l < 6; ++l)
+                            a[(3 + t) * 6 + l] += z[0] * W[l] + z[1] * W[6 + l] + z[2] * W[12 + l];
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int v = threadIdx.x; v < 27 * 36; v += blockDim.x) {
+            double sum = 0.0;
+#pragma unroll
+            for (int q = 0; q < kGW; ++q) sum += acc[q][v];
+            Eb[(long)I * 27 * 36 + v] = sum;
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void k_coarse_E_sum(int na, int nchunk_max, const int *__restrict__ agg_cell,
                                const int *__restrict__ cell_agg, int ncx, int ncy, int ncz, int m,
                                const double *__restrict__ part, double *__restrict__ E) {
@@ -563,10 +686,11 @@ static double estimate_lambda_max(ofea_ctx *c, int steps) {
 // ------------------------------------------------------------ setup entry --
 
 void coarse_E_partials(ofea_ctx *c, Coarse &C, int nchunk) {
-    k_coarse_E_chunks<<<(int)std::min<long>((long)C.na * nchunk, (long)c->num_sms * 32), kEThreads, 0,
-                        c->stream>>>(C.na, nchunk, C.agg_ptr.p, C.agg_nodes.p, C.agg_of.p, C.agg_cell.p,
-                                     c->node_of_free.p, c->xyz.p, C.centroid.p, C.inv_scale, c->rowptr.p,
-                                     c->cols.p, c->Kb.p, C.part.p, c->err_flag.p);
+    if (nchunk != 1) fail(OFEA_ERR_STATE, "Galerkin blocks are assembled in one pass");
+    C.part.ensure((size_t)C.na * 27 * 36);
+    k_galerkin_blocks<<<std::max(1, C.na), kGW * 32, 0, c->stream>>>(
+        C.na, C.agg_ptr.p, C.agg_nodes.p, C.agg_of.p, C.agg_cell.p, c->node_of_free.p, c->xyz.p, C.centroid.p,
+        C.inv_scale, c->rowptr.p, c->cols.p, c->Kb.p, C.part.p, c->err_flag.p);
     OFEA_CHECK_LAUNCH();
 }
 
@@ -608,8 +732,7 @@ void setup_coarse(ofea_ctx *c, int target_nodes) {
     const int m = C.m;
     coarse_begin_E(c);
     OFEA_CUDA(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), s));
-    const int nchunk = (C.max_agg + kChunkNodes - 1) / kChunkNodes;
-    C.part.ensure((size_t)C.na * nchunk * 27 * 36);
+    const int nchunk = 1;
     coarse_E_partials(c, C, nchunk);
     k_coarse_E_sum<<<grid_for(c, (long)C.na * 27 * 36, kBlock), kBlock, 0, s>>>(
         C.na, nchunk, C.agg_cell.p, C.cell_agg.p, C.nc[0], C.nc[1], C.nc[2], m, C.part.p, C.E.p);

@@ -23,7 +23,8 @@ void coarse_correct(ofea_ctx *c, const float *t, float *x);
 // t = b - K32 x
 void vc_resid(ofea_ctx *c, const float *b, const float *x, float *t);
 // Level-generic pieces (also used by the learned level):
-// cvec = Z^T t, x += Z g, and the chunk partials of Z^T K Z into C.part.
+// cvec = Z^T t, x += Z g, and the Galerkin blocks of Z^T K Z into C.part
+// ([aggregate][27 neighbour slots][6 x 6]; nchunk must be 1).
 void restrict_level(ofea_ctx *c, const Coarse &C, const float *t, float *cvec);
 void prolong_level(ofea_ctx *c, const Coarse &C, const float *g, float *x);
 void coarse_E_partials(ofea_ctx *c, Coarse &C, int nchunk);
