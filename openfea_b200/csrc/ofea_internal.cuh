@@ -120,7 +120,7 @@ constexpr int kMaxGrid = 4096;  // upper bound on CTAs of any reducing kernel
 // Coarse space of the two-level preconditioner (precond.cu).
 struct Coarse {
     bool geom_ok = false, K_ok = false;
-    int target = 0, na = 0, m = 0, max_agg = 0;
+    int target = 0, na = 0, m = 0, max_agg = 0, band = 0;  // band: max |J - I| of neighbouring aggregates
     int nc[3] = {1, 1, 1};
     double lo[3] = {0, 0, 0}, ext[3] = {0, 0, 0};
     double inv_scale = 1.0, lmax = 0.0;

@@ -82,13 +82,17 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
     for (int a = 0; a < na; ++a) C.max_agg = std::max(C.max_agg, ptr[a + 1] - ptr[a]);
     // neighbour table: slot (dx+1)*9 + (dy+1)*3 + (dz+1), -1 where the cell is empty/outside
     std::vector<int> nbr(27L * na, -1);
+    int band = 0;  // largest |J - I| over neighbouring aggregates
     for (int a = 0; a < na; ++a)
         for (int sl = 0; sl < 27; ++sl) {
             const int x = agg_cell3[3 * a] + sl / 9 - 1, y = agg_cell3[3 * a + 1] + (sl / 3) % 3 - 1,
                       z = agg_cell3[3 * a + 2] + sl % 3 - 1;
             if (x < 0 || y < 0 || z < 0 || x >= nc[0] || y >= nc[1] || z >= nc[2]) continue;
-            nbr[27L * a + sl] = cell_agg[((long)x * nc[1] + y) * nc[2] + z];
+            const int J = cell_agg[((long)x * nc[1] + y) * nc[2] + z];
+            nbr[27L * a + sl] = J;
+            if (J >= 0) band = std::max(band, std::abs(J - a));
         }
+    C.band = band;
     cudaStream_t st = c->stream;
     C.agg_of.upload(agg_of.data(), nf, st);
     C.agg_ptr.upload(ptr.data(), na + 1, st);
@@ -488,13 +492,13 @@ __global__ void __launch_bounds__(1024) k_gj_diag(int m, int j0, int bb, const d
 
 // Column panel, one warp per row i: P_i = A_{i,J} (saved for the update),
 // A_{i,J} <- -P_i S (i outside J) or S (i inside J).
-__global__ void __launch_bounds__(256) k_gj_panel(int m, int j0, int bb, double *__restrict__ A,
+__global__ void __launch_bounds__(256) k_gj_panel(int m, int lim, int j0, int bb, double *__restrict__ A,
                                                   const double *__restrict__ S, double *__restrict__ P) {
     __shared__ double sS[kGJ][kGJ];
     for (int v = threadIdx.x; v < kGJ * kGJ; v += blockDim.x) sS[v / kGJ][v % kGJ] = S[v];
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32; i < m; i += gridDim.x * blockDim.x / 32) {
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32; i < lim; i += gridDim.x * blockDim.x / 32) {
         const bool in = i >= j0 && i < j0 + bb;
         double p0 = lane < bb ? A[(long)i * m + j0 + lane] : 0.0;
         double p1 = lane + 32 < bb ? A[(long)i * m + j0 + lane + 32] : 0.0;
@@ -522,21 +526,21 @@ __global__ void __launch_bounds__(256) k_gj_panel(int m, int j0, int bb, double 
 }
 
 // Row panel: A_{J,k} <- S A_{J,k} for k outside J; one CTA per 32 columns.
-__global__ void __launch_bounds__(256) k_gj_rows(int m, int j0, int bb, double *__restrict__ A,
+__global__ void __launch_bounds__(256) k_gj_rows(int m, int lim, int j0, int bb, double *__restrict__ A,
                                                  const double *__restrict__ S) {
     __shared__ double sS[kGJ][kGJ];  // read as broadcasts: no padding needed
     __shared__ double sR[kGJ][32];
     for (int v = threadIdx.x; v < kGJ * kGJ; v += blockDim.x) sS[v / kGJ][v % kGJ] = S[v];
-    for (int k0 = blockIdx.x * 32; k0 < m; k0 += gridDim.x * 32) {
+    for (int k0 = blockIdx.x * 32; k0 < lim; k0 += gridDim.x * 32) {
         __syncthreads();
         for (int v = threadIdx.x; v < kGJ * 32; v += blockDim.x) {
             const int j = v / 32, kk = v % 32, k = k0 + kk;
-            sR[j][kk] = (j < bb && k < m) ? A[(long)(j0 + j) * m + k] : 0.0;
+            sR[j][kk] = (j < bb && k < lim) ? A[(long)(j0 + j) * m + k] : 0.0;
         }
         __syncthreads();
         // thread: column kk = tid % 32, rows i = tid / 32 + 8 q
         const int kk = threadIdx.x % 32, k = k0 + kk;
-        const bool skip = k >= m || (k >= j0 && k < j0 + bb);
+        const bool skip = k >= lim || (k >= j0 && k < j0 + bb);
         for (int q = 0; q < kGJ / 8; ++q) {
             const int i = threadIdx.x / 32 + 8 * q;
             if (i >= bb || skip) continue;
@@ -549,7 +553,7 @@ __global__ void __launch_bounds__(256) k_gj_rows(int m, int j0, int bb, double *
 
 // Rank-bb update of the outside block: A_ik -= P_i . A_{J,k}, 64 x 64 tiles,
 // 256 threads with 4 x 4 outputs each; dynamic shared memory (66 KB).
-__global__ void __launch_bounds__(256) k_gj_update(int m, int j0, int bb, double *__restrict__ A,
+__global__ void __launch_bounds__(256) k_gj_update(int m, int lim, int j0, int bb, double *__restrict__ A,
                                                    const double *__restrict__ P) {
     extern __shared__ double smem[];
     double (*sP)[kGJ + 1] = reinterpret_cast<double (*)[kGJ + 1]>(smem);             // [64][65]
@@ -559,9 +563,9 @@ __global__ void __launch_bounds__(256) k_gj_update(int m, int j0, int bb, double
     const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
     for (int v = threadIdx.x; v < 64 * kGJ; v += 256) {
         const int ii = v / kGJ, jj = v % kGJ;
-        sP[ii][jj] = (i0 + ii < m && jj < bb) ? P[(long)(i0 + ii) * kGJ + jj] : 0.0;
+        sP[ii][jj] = (i0 + ii < lim && jj < bb) ? P[(long)(i0 + ii) * kGJ + jj] : 0.0;
         const int jr = v / 64, kk = v % 64;
-        sR[jr][kk] = (jr < bb && k0 + kk < m) ? A[(long)(j0 + jr) * m + k0 + kk] : 0.0;
+        sR[jr][kk] = (jr < bb && k0 + kk < lim) ? A[(long)(j0 + jr) * m + k0 + kk] : 0.0;
     }
     __syncthreads();
     double acc[4][4] = {};
@@ -579,11 +583,11 @@ __global__ void __launch_bounds__(256) k_gj_update(int m, int j0, int bb, double
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
         const int i = i0 + tr * 4 + a;
-        if (i >= m || (i >= j0 && i < j0 + bb)) continue;
+        if (i >= lim || (i >= j0 && i < j0 + bb)) continue;
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             const int k = k0 + tc * 4 + b;
-            if (k >= m || (k >= j0 && k < j0 + bb)) continue;
+            if (k >= lim || (k >= j0 && k < j0 + bb)) continue;
             A[(long)i * m + k] -= acc[a][b];
         }
     }
@@ -599,7 +603,12 @@ __global__ void k_round_f32(long n, const double *__restrict__ a, float *__restr
         b[i] = (float)a[i];
 }
 
-static void invert_spd(ofea_ctx *c, double *A, int m) {
+// hb: half-bandwidth of A (A_ik = 0 for |i - k| > hb).  Before panel J is
+// processed, rows and columns beyond j0 + bb + hb are still untouched band
+// (their entries in the panel's rows and columns are zero), so every step
+// works on the leading (j0 + bb + hb)^2 window only: about a third of the
+// dense work for a narrow band.
+static void invert_spd(ofea_ctx *c, double *A, int m, int hb) {
     Coarse &C = c->coarse;
     cudaStream_t s = c->stream;
     C.S.ensure(kGJ * kGJ);
@@ -609,13 +618,14 @@ static void invert_spd(ofea_ctx *c, double *A, int m) {
     OFEA_CHECK_LAUNCH();
     const size_t upd_smem = sizeof(double) * (64 * (kGJ + 1) + kGJ * 65);
     OFEA_CUDA(cudaFuncSetAttribute(k_gj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem));
-    dim3 tiles((m + 63) / 64, (m + 63) / 64);
     for (int j0 = 0; j0 < m; j0 += kGJ) {
         const int bb = std::min(kGJ, m - j0);
+        const int lim = (int)std::min<long>(m, (long)j0 + bb + hb);
+        dim3 tiles((lim + 63) / 64, (lim + 63) / 64);
         k_gj_diag<<<1, 1024, 0, s>>>(m, j0, bb, A, C.S.p, C.diag0.p);
-        k_gj_panel<<<grid_for(c, (long)m * 32, 256), 256, 0, s>>>(m, j0, bb, A, C.S.p, C.P.p);
-        k_gj_rows<<<std::max(1, std::min((m + 31) / 32, c->num_sms * 4)), 256, 0, s>>>(m, j0, bb, A, C.S.p);
-        k_gj_update<<<tiles, 256, upd_smem, s>>>(m, j0, bb, A, C.P.p);
+        k_gj_panel<<<grid_for(c, (long)lim * 32, 256), 256, 0, s>>>(m, lim, j0, bb, A, C.S.p, C.P.p);
+        k_gj_rows<<<std::max(1, std::min((lim + 31) / 32, c->num_sms * 4)), 256, 0, s>>>(m, lim, j0, bb, A, C.S.p);
+        k_gj_update<<<tiles, 256, upd_smem, s>>>(m, lim, j0, bb, A, C.P.p);
     }
     OFEA_CHECK_LAUNCH();
 }
@@ -717,7 +727,7 @@ void coarse_finish(ofea_ctx *c) {
     Coarse &C = c->coarse;
     cudaStream_t s = c->stream;
     const int m = C.m;
-    invert_spd(c, C.E.p, m);
+    invert_spd(c, C.E.p, m, 6 * C.band + 5);
     k_round_f32<<<grid_for(c, (long)m * m, kBlock), kBlock, 0, s>>>((long)m * m, C.E.p, C.Einv32.p);
     OFEA_CHECK_LAUNCH();
     C.lmax = estimate_lambda_max(c, 10);
