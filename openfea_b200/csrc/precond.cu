@@ -633,7 +633,7 @@ static void invert_spd(ofea_ctx *c, double *A, int m, int hb) {
 // ----------------------------------------------------- lambda_max(D^-1 K) --
 
 // w = Dinv32 K32 (v * sc), sc = 1/||v|| from the previous partials.
-__global__ void __launch_bounds__(kBlock) k_power(int nfree, const int *__restrict__ sl_ptr,
+__global__ void __launch_bounds__(kBlock, 2048 / kBlock) k_power(int nfree, const int *__restrict__ sl_ptr,
                                                   const int *__restrict__ scols,
                                                   const float *__restrict__ sv32,
                                                   const float *__restrict__ Dinv32,
@@ -756,7 +756,7 @@ void setup_coarse(ofea_ctx *c, int target_nodes) {
 // ---------------------------------------------------------- V-cycle kernels --
 
 // t = b - K32 x (x complete), per row.
-__global__ void __launch_bounds__(kBlock) k_vc_resid(int nfree, const int *__restrict__ sl_ptr,
+__global__ void __launch_bounds__(kBlock, 2048 / kBlock) k_vc_resid(int nfree, const int *__restrict__ sl_ptr,
                                                      const int *__restrict__ scols,
                                                      const float *__restrict__ sv32,
                                                      const float *__restrict__ b,
