@@ -151,10 +151,17 @@ BATCH_VEC_BYTES_MIXED = 132
 BATCH_VEC_BYTES_PCG64 = 28 + 64  # A (z, p_old, p, q); B (u, p, q, r, z)
 
 
-def run_batched(ob, mg, local, hbm, steps=2, count=64, nrhs=16, rtol=1e-8):
+def run_batched(ob, mg, local, hbm, steps=2, count=64, nrhs=16, rtol=1e-8, dist=None):
     """The batched reanalysis workload: `count` SIMP variants n x 20 x 20 (n ~
-    U{20..60}), `nrhs` load cases each, solved by one persistent kernel."""
-    variants = mg.design_variants(count=count, nrhs=nrhs)
+    U{20..60}), `nrhs` load cases each, solved by one persistent kernel per
+    rank.  With several ranks the variants are partitioned (longest first onto
+    the least-loaded rank); ranks exchange only timings and statistics."""
+    from openfea_b200.multirank import gather_by_variant, max_over_ranks, partition_variants
+    world = dist.get_world_size() if dist is not None and dist.is_initialized() else 1
+    rank = dist.get_rank() if world > 1 else 0
+    all_variants = mg.design_variants(count=count, nrhs=nrhs)
+    mine = partition_variants([3 * m.nd * nrhs for m, _ in all_variants], world)[rank]
+    variants = [all_variants[i] for i in mine]
     ctxs, loads, meshes = [], [], []
     for m, F in variants:
         c = ob.Context(local)
@@ -164,8 +171,9 @@ def run_batched(ob, mg, local, hbm, steps=2, count=64, nrhs=16, rtol=1e-8):
         ctxs.append(c)
         meshes.append((m, fm))
         loads.append(np.stack([mg.to_free(F[j], fm) for j in range(nrhs)]))
-    n_tot = sum(c.n for c in ctxs)
-    nnz_tot = sum(c.nnz for c in ctxs)
+    sizes = gather_by_variant({i: (c.n, c.nnz) for i, c in zip(mine, ctxs)}, dist)
+    n_tot = sum(v[0] for v in sizes.values())      # all ranks' variants
+    nnz_tot = sum(v[1] for v in sizes.values())
     b = ob.Batch(ctxs, nrhs)
     b.set_rhs(loads)
     out = {}
@@ -173,9 +181,10 @@ def run_batched(ob, mg, local, hbm, steps=2, count=64, nrhs=16, rtol=1e-8):
         b.solve_resident(meth, rtol=rtol)  # warm-up (tunes on first use, cached on disk)
         runs = [b.solve_resident(meth, rtol=rtol) for _ in range(steps if meth == "GPU_MIXED" else 1)]
         st = runs[-1]
-        sec = min(r[0]["seconds"] for r in runs)
-        iters = max(s_["iterations"] for s_ in st)
         assert all(s_["status"] == 0 and s_["rel_residual"] <= rtol for s_ in st), st
+        sec = max_over_ranks(min(r[0]["seconds"] for r in runs), dist)
+        st = list(gather_by_variant(dict(zip(mine, st)), dist).values())
+        iters = max(s_["iterations"] for s_ in st)
         # matrix bytes per iteration: FP64 BSELL once (+ FP32 twice for MIXED), 76/9 resp. 40/9 B per nnz
         mat = 76 * nnz_tot / 9 + (2 * 40 * nnz_tot / 9 if meth == "GPU_MIXED" else 0)
         per_iter = mat + vec_b * n_tot * nrhs
@@ -184,13 +193,14 @@ def run_batched(ob, mg, local, hbm, steps=2, count=64, nrhs=16, rtol=1e-8):
                      "worst_rel_residual": max(s_["rel_residual"] for s_ in st),
                      "solves_per_s": count * nrhs / sec, "tuning": b.tuning(meth),
                      "bytes_per_iteration": per_iter, "achieved_gbs": per_iter * iters / sec / 1e9,
-                     "frac_of_hbm": per_iter * iters / sec / 1e9 / hbm}
+                     "frac_of_hbm": per_iter * iters / sec / 1e9 / (hbm * world)}
     u_dev = b.solution()  # of the MIXED solve (the last one)
     # end to end through the one-call C ABI with host buffers (create, upload, solve, download)
     t0 = time.perf_counter()
     U, st = ob.solve_batched(ctxs, loads, method="GPU_MIXED", rtol=rtol)
-    e2e = time.perf_counter() - t0
-    diff = max(float(np.linalg.norm(a - c) / max(np.linalg.norm(c), 1e-300)) for a, c in zip(U, u_dev))
+    e2e = max_over_ranks(time.perf_counter() - t0, dist)
+    diff = max_over_ranks(max(float(np.linalg.norm(a - c) / max(np.linalg.norm(c), 1e-300))
+                              for a, c in zip(U, u_dev)), dist)
     b.close()
     for c in ctxs:
         c.close()
@@ -200,6 +210,7 @@ def run_batched(ob, mg, local, hbm, steps=2, count=64, nrhs=16, rtol=1e-8):
                      f"{nrhs} random load cases each on the x=L face, rtol {rtol:g}; one persistent cooperative "
                      f"kernel per solve, graph-launched"),
         "n_dof_total": n_tot, "nnz_total": nnz_tot, "load_cases": count * nrhs,
+        "ranks": world, "scaling": "strong (the variants are partitioned over the ranks)",
         "value": mixed["seconds"], "unit": "s per batch (all load cases of all variants)",
         "mixed": mixed, "plain_pcg64": out["GPU_PCG"],
         "speedup_vs_plain_pcg64": out["GPU_PCG"]["seconds"] / mixed["seconds"],
@@ -518,7 +529,7 @@ def run_ours(args):
     e2e_s = statistics.mean(e2e) if e2e else None
     batched = None
     if not args.no_batched:
-        batched = run_batched(ob, mg, local, hbm)
+        batched = run_batched(ob, mg, local, hbm, dist=dist)
     learned_simp = None
     if not args.no_simp:
         learned_simp = run_learned_simp(ob, mg, local, (nx, ny, nz), rtol=args.rtol)
