@@ -2,8 +2,12 @@
 // implict_analysis, src/cae.cpp:18-301) with the assembly and the linear
 // solves running on the GPU through the C ABI.
 //
-//   ofea_cli -i model.inp [-o out.vtk] [-imp] [-nl] [-solver GPU_PCG|GPU_MIXED]
-//            [-rtol 1e-8] [-E <Young> -nu <Poisson>]
+//   ofea_cli -i model.inp [-o out.vtk] [-imp] [-nl] [-solver GPU_PCG|GPU_MIXED|GPU_LEARNED]
+//            [-weights gnn.bin] [-save-weights gnn.bin] [-rtol 1e-8] [-E <Young> -nu <Poisson>]
+//
+// GPU_LEARNED loads the learned stage's weights from -weights, or trains it
+// on the model's own K (plain-PCG residuals of a seeded random load) when no
+// file is given; -save-weights keeps the trained weights for later runs.
 //
 // -E/-nu override the file's material (the reference's code_test cases set it
 // in code for models without *Elastic, src/main.cpp:121-135).  The output VTK
@@ -33,7 +37,7 @@ int die(const char *what, int rc) {
 }  // namespace
 
 int main(int argc, char **argv) {
-    std::string in, out, solver = "GPU_PCG";
+    std::string in, out, solver = "GPU_PCG", weights, save_weights;
     bool nl = false;
     double rtol = 1e-8, E_over = -1, nu_over = -1;
     for (int i = 1; i < argc; ++i) {
@@ -44,6 +48,8 @@ int main(int argc, char **argv) {
         else if (a == "-imp") {}
         else if (a == "-solver" && i + 1 < argc) solver = argv[++i];
         else if (a == "-rtol" && i + 1 < argc) rtol = std::atof(argv[++i]);
+        else if (a == "-weights" && i + 1 < argc) weights = argv[++i];
+        else if (a == "-save-weights" && i + 1 < argc) save_weights = argv[++i];
         else if (a == "-E" && i + 1 < argc) E_over = std::atof(argv[++i]);
         else if (a == "-nu" && i + 1 < argc) nu_over = std::atof(argv[++i]);
         else if (argc == 2) in = a;
@@ -62,6 +68,7 @@ int main(int argc, char **argv) {
     opts.rtol = rtol;
     if (solver == "GPU_PCG") opts.method = OFEA_SOLVER_PCG64;
     else if (solver == "GPU_MIXED") opts.method = OFEA_SOLVER_MIXED;
+    else if (solver == "GPU_LEARNED") opts.method = OFEA_SOLVER_LEARNED;
     else {
         std::fprintf(stderr, "Please check your flag of solver !!!\n");
         return 2;
@@ -107,8 +114,25 @@ int main(int argc, char **argv) {
     if ((rc = ofea_assemble_pattern(ctx, &n_chk, &nnz))) return die("ofea_assemble_pattern", rc);
     std::printf("The CSR index has been built (n = %d, nnz = %lld)\n", n_chk, nnz);
     ofea_solve_stats st{};
+    // the learned stage needs weights before its first solve
+    auto prepare_learned = [&]() -> int {
+        if (opts.method != OFEA_SOLVER_LEARNED) return OFEA_OK;
+        int r;
+        if (!weights.empty()) {
+            if ((r = ofea_learned_load(ctx, weights.c_str()))) return die("ofea_learned_load", r);
+        } else {
+            ofea_learn_stats ls{};
+            if ((r = ofea_learned_train(ctx, nullptr, nullptr, &ls))) return die("ofea_learned_train", r);
+            std::printf("learned stage trained: %d samples, %d steps, %.3f s\n", ls.samples, ls.steps, ls.seconds);
+            weights = "(trained)";
+        }
+        if (!save_weights.empty() && (r = ofea_learned_save(ctx, save_weights.c_str())))
+            return die("ofea_learned_save", r);
+        return OFEA_OK;
+    };
     if (!nl) {
         if ((rc = ofea_assemble_linear(ctx))) return die("ofea_assemble_linear", rc);
+        if ((rc = prepare_learned())) return rc;
         rc = ofea_solve(ctx, f.data(), u.data(), 1, &opts, &st);
         std::printf("solve: %s, %d iterations, relative residual %.3e, %.4f s on the GPU\n",
                     ofea_status_string(st.status), st.iterations, st.rel_residual, st.seconds);
@@ -121,6 +145,7 @@ int main(int argc, char **argv) {
         int loop = 0;
         while (res > 1.0e-6 && loop < 100) {
             if ((rc = ofea_assemble_nl(ctx, u.data(), fint.data()))) return die("ofea_assemble_nl", rc);
+            if (loop == 0 && (rc = prepare_learned())) return rc;
             for (int i = 0; i < n; ++i) r[i] = f[i] - fint[i];
             rc = ofea_solve(ctx, r.data(), du.data(), 1, &opts, &st);
             if (rc) return die("ofea_solve", rc);

@@ -5,6 +5,7 @@ Bars: integer pattern data bit-exact; K entries and element matrices within
 (relative L2) of the reference's SuperLU solution for the FP64 PCG;
 mixed precision within 1e-8.
 """
+import os
 import numpy as np
 import pytest
 
@@ -279,3 +280,29 @@ def test_bad_uploads_rejected(gpu_ctx_factory):
     fm2[fm2 == 3] = 4
     with pytest.raises(ob.OfeaError):
         ctx.upload(m.xyz, m.topo, m.etype, fm2, m.E0, m.nu)
+
+
+@pytest.mark.parametrize("solver", ["GPU_PCG", "GPU_MIXED", "GPU_LEARNED"])
+def test_cli_drives_the_gpu_path(golden, inp_file, tmp_path, solver):
+    """The command-line driver: .inp in, .vtk out (the reference's
+    OpenFEA -i ... -o ...), the GPU solver picked by -solver; the written
+    u_z field matches the reference's golden result to its print precision.
+    GPU_LEARNED trains on the model once, saves the weights and a second
+    run reuses them."""
+    import subprocess
+    cli = os.path.join(os.path.dirname(ob.__file__), "ofea_cli")
+    inp = inp_file("mesh_o.inp")
+    out = tmp_path / "o.vtk"
+    args = [cli, "-i", inp, "-o", str(out), "-solver", solver, "-rtol", "1e-10", "-E", "2.1e5", "-nu", "0.3"]
+    runs = [args]
+    if solver == "GPU_LEARNED":
+        w = str(tmp_path / "gnn.bin")
+        runs = [args + ["-save-weights", w], args + ["-weights", w]]
+    ug = golden("cadcae_o_u.npz")["u"].ravel()
+    for a in runs:
+        r = subprocess.run(a, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+        lines = out.read_text().split("\n")
+        j = lines.index("SCALARS u_z double 1")
+        uz = np.array([float(x) for x in lines[j + 2:j + 2 + 625]])
+        assert np.abs(uz - ug[2::3]).max() <= 3e-6 * np.abs(ug[2::3]).max()
