@@ -193,7 +193,7 @@ struct Lanes {
 // Shared-memory stage of a slice's BSELL slots: two buffers of kKC slots
 // (values in FP64 or FP32, then columns), filled with cp.async while the
 // other buffer is consumed.
-constexpr int kKC = 4;
+constexpr int kKC = 8;
 struct __align__(128) Stage {
     double v[2][kKC * 9 * kSlice];  // FP32 values use the first half of each buffer
     int col[2][kKC * kSlice];
@@ -322,9 +322,15 @@ __device__ __forceinline__ void for_pairs(const BArgs &a, bool two, F f) {
 
 // The persistent batched solver.  MIXED: FP64 FCG + FP32 V-cycle; else PCG64.
 // One CTA per slice item (grid-stride); NP / RL lanes per block row, RL load
-// cases per lane.
+// cases per lane.  The PCG64 instances are held to 3 (RL <= 2) or 2 CTAs per
+// SM worth of registers and MIXED with RL = 2 to 2 (measured faster than the
+// compiler's choice); the other MIXED ones keep theirs (bounds spill and
+// measured slower).
+constexpr int batch_min_ctas(int threads, int rl, bool mixed) {
+    return mixed ? (rl == 2 ? 2 : 1) : ((rl <= 2 ? 3 : 2) * threads <= 2048 ? (rl <= 2 ? 3 : 2) : 2048 / threads);
+}
 template <int NP, int RL, bool MIXED>
-__global__ void __launch_bounds__(32 * (NP / RL)) k_batch_solve(BArgs a) {
+__global__ void __launch_bounds__(32 * (NP / RL), batch_min_ctas(32 * (NP / RL), RL, MIXED)) k_batch_solve(BArgs a) {
     __shared__ Stage st;
     using LN = Lanes<NP, RL>;
     const unsigned nb = gridDim.x + a.extra_arrivals;
@@ -818,8 +824,7 @@ const void *solve_np(int rl, bool mixed) {
     }
     fail(OFEA_ERR_INVALID_ARG, "unsupported load cases per lane");
 }
-// Kernel instance for (NP, RL, mixed).
-const void *solve_kernel(int np, int rl, bool mixed) {
+const void *solve_kernel_raw(int np, int rl, bool mixed) {
     switch (np) {
         case 4: return solve_np<4>(rl, mixed);
         case 8: return solve_np<8>(rl, mixed);
@@ -827,6 +832,14 @@ const void *solve_kernel(int np, int rl, bool mixed) {
         case 32: return solve_np<32>(rl, mixed);
     }
     fail(OFEA_ERR_INVALID_ARG, "unsupported load-case stride");
+}
+// Kernel instance for (NP, RL, mixed), with the shared-memory carveout at its
+// maximum so that several CTAs' slot stages fit on an SM.
+const void *solve_kernel(int np, int rl, bool mixed) {
+    const void *fn = solve_kernel_raw(np, rl, mixed);
+    OFEA_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   (int)cudaSharedmemCarveoutMaxShared));
+    return fn;
 }
 template <int NP>
 const void *residual_np(int rl) {
@@ -1156,16 +1169,18 @@ TuneCfg autotune(ofea_batch *b, bool mixed, double rtol) {
         for (int c : cps)
             if (c >= 1 && c <= occ) cand.push_back(TuneCfg{rl, c, 0.0});
     }
-    const int iters = 6;
+    // per-iteration time = (t(long) - t(short)) / (long - short): the init
+    // phases and the launch cancel out
+    const int it_short = 4, it_long = 20;
     cudaEvent_t e0, e1;
     OFEA_CUDA(cudaEventCreate(&e0));
     OFEA_CUDA(cudaEventCreate(&e1));
     TuneCfg best;
     double best_ms = 1e300;
     cudaStream_t s = b->stream;
-    for (TuneCfg &t : cand) {
+    auto time_launch = [&](const TuneCfg &t, int iters) {
         double ms_min = 1e300;
-        for (int rep = 0; rep < 2; ++rep) {
+        for (int rep = 0; rep < 3; ++rep) {
             OFEA_CUDA(cudaMemsetAsync(b->u.p, 0, sizeof(double) * b->ndof * b->NP, s));
             BArgs a = make_args(b, mixed, t, iters, rtol);
             OFEA_CUDA(cudaEventRecord(e0, s));
@@ -1179,9 +1194,16 @@ TuneCfg autotune(ofea_batch *b, bool mixed, double rtol) {
             if (g.err) fail(OFEA_ERR_TIMEOUT, "batched solver: a grid-barrier wait ran out while tuning");
             ms_min = std::min(ms_min, (double)ms);
         }
-        t.ms_per_iter = ms_min / iters;
-        if (ms_min < best_ms) {
-            best_ms = ms_min;
+        return ms_min;
+    };
+    const bool verbose = std::getenv("OFEA_TUNE_VERBOSE") != nullptr;
+    for (TuneCfg &t : cand) {
+        t.ms_per_iter = std::max(0.0, time_launch(t, it_long) - time_launch(t, it_short)) / (it_long - it_short);
+        if (verbose)
+            std::fprintf(stderr, "ofea tune %s: rl %d ctas/SM %d -> %.4f ms per iteration\n", key.c_str(), t.rl,
+                         t.ctas_per_sm, t.ms_per_iter);
+        if (t.ms_per_iter < best_ms) {
+            best_ms = t.ms_per_iter;
             best = t;
         }
     }
