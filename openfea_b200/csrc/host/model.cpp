@@ -1,13 +1,16 @@
 // Host-side model I/O and DOF numbering (include/ofea_host.h): the .inp subset
 // OpenFEA reads, set_BCs numbering / load vector, legacy-VTK output.
 #include <algorithm>
+#include <charconv>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <iomanip>
 #include <sstream>
 #include <string>
+#include <string_view>
 #include <vector>
 
 #include "../../../include/ofea_gpu.h"
@@ -29,40 +32,90 @@ struct IoError {
     std::string msg;
 };
 
-// Lines with '\r' removed (the reference's safeGetline accepts \n, \r\n, \r).
-std::vector<std::string> read_lines(const char *path) {
-    std::ifstream in(path, std::ios::binary);
-    if (!in) throw IoError{std::string("cannot open ") + path};
-    std::stringstream ss;
-    ss << in.rdbuf();
-    std::string all = ss.str();
-    std::vector<std::string> lines;
-    std::string cur;
+// The whole file in one buffer and the [begin, end) of every line, line
+// breaks \n, \r\n and \r as the reference's safeGetline accepts them.  The
+// lines are parsed in place (no per-line strings): a 1.56M-DOF model reads
+// in a fraction of a second.
+struct Lines {
+    std::string buf;
+    std::vector<std::pair<size_t, size_t>> ln;
+    size_t size() const { return ln.size(); }
+    std::string_view operator[](size_t i) const {
+        return std::string_view(buf.data() + ln[i].first, ln[i].second - ln[i].first);
+    }
+};
+
+Lines read_lines(const char *path) {
+    Lines L;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) throw IoError{std::string("cannot open ") + path};
+    std::fseek(f, 0, SEEK_END);
+    const long size = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    L.buf.resize(size > 0 ? (size_t)size : 0);
+    const size_t got = size > 0 ? std::fread(&L.buf[0], 1, (size_t)size, f) : 0;
+    std::fclose(f);
+    if (size < 0 || got != (size_t)size) throw IoError{std::string("cannot read ") + path};
+    const std::string &all = L.buf;
+    size_t b = 0;
     for (size_t i = 0; i < all.size(); ++i) {
-        char ch = all[i];
+        const char ch = all[i];
         if (ch == '\n' || ch == '\r') {
-            lines.push_back(cur);
-            cur.clear();
+            L.ln.emplace_back(b, i);
             if (ch == '\r' && i + 1 < all.size() && all[i + 1] == '\n') ++i;
-        } else {
-            cur.push_back(ch);
+            b = i + 1;
         }
     }
-    if (!cur.empty()) lines.push_back(cur);
-    return lines;
+    if (b < all.size()) L.ln.emplace_back(b, all.size());
+    return L;
 }
 
-bool has(const std::string &s, const char *key) { return s.find(key) != std::string::npos; }
+bool has(std::string_view s, const char *key) { return s.find(key) != std::string_view::npos; }
 
-std::string strip(const std::string &s) {
+std::string_view strip(std::string_view s) {
     size_t b = s.find_first_not_of(" \t"), e = s.find_last_not_of(" \t");
-    return b == std::string::npos ? std::string() : s.substr(b, e - b + 1);
+    return b == std::string_view::npos ? std::string_view() : s.substr(b, e - b + 1);
+}
+
+// The numbers of a "*Node" line: whitespace and commas separate them (the
+// reference replaces ',' by ' ' and reads with >>, src/data2cae.cpp:103-115).
+bool parse_doubles(std::string_view s, double *v, int count) {
+    const char *p = s.data(), *e = p + s.size();
+    for (int k = 0; k < count; ++k) {
+        while (p < e && (*p == ' ' || *p == '\t' || *p == ',')) ++p;
+        if (p < e && *p == '+') ++p;
+        const auto r = std::from_chars(p, e, v[k]);
+        if (r.ec != std::errc()) return false;
+        p = r.ptr;
+    }
+    return true;
+}
+
+// The comma-separated integers of an "*Element" line (each token stripped).
+int parse_ints(std::string_view s, int *v, int cap) {
+    int n = 0;
+    size_t pos = 0;
+    while (pos <= s.size()) {
+        size_t c = s.find(',', pos);
+        if (c == std::string_view::npos) c = s.size();
+        std::string_view t = strip(s.substr(pos, c - pos));
+        if (!t.empty()) {
+            if (n >= cap) return -1;
+            const char *p = t.data(), *e = p + t.size();
+            if (*p == '+') ++p;
+            const auto r = std::from_chars(p, e, v[n]);
+            if (r.ec != std::errc()) return -1;
+            ++n;
+        }
+        pos = c + 1;
+    }
+    return n;
 }
 
 // Whitespace tokens with one trailing comma removed, as the reference's
 // "iss >> node_id; erase last ','" (src/data2cae.cpp:334-341).
-std::vector<int> id_list(const std::string &line) {
-    std::istringstream iss(line);
+std::vector<int> id_list(std::string_view line) {
+    std::istringstream iss{std::string(line)};
     std::string tok;
     std::vector<int> out;
     while (iss >> tok) {
@@ -73,14 +126,14 @@ std::vector<int> id_list(const std::string &line) {
 }
 
 // Value of the second token of a "a, b, c" generate line (read_ele_node_num).
-int generate_count(const std::string &line) {
-    std::istringstream iss(line);
+int generate_count(std::string_view line) {
+    std::istringstream iss{std::string(line)};
     std::string t1, t2;
     iss >> t1 >> t2;
     return std::atoi(t2.c_str());
 }
 
-void parse(const std::vector<std::string> &L, ofea_model &m) {
+void parse(const Lines &L, ofea_model &m) {
     // counts from the first *Nset / *Elset generate lines (src/data2cae.cpp:28-47)
     int nd_gen = -1, ne_gen = -1;
     for (size_t i = 0; i + 1 < L.size(); ++i) {
@@ -94,46 +147,37 @@ void parse(const std::vector<std::string> &L, ofea_model &m) {
     bool in_node = false, in_elem = false;
     int etype = -1;
     for (size_t i = 0; i < L.size(); ++i) {
-        const std::string &s = L[i];
+        const std::string_view s = L[i];
         if (has(s, "*End Assembly")) break;
         if (has(s, "*")) {
             in_node = has(s, "*Node") && !has(s, "*Nset") && !has(s, "*Node Output");
             in_elem = false;
             if (has(s, "*Element") && !has(s, "*Element Output")) {
                 size_t eq = s.find('=');
-                std::string t = eq == std::string::npos ? "" : strip(s.substr(eq + 1));
+                std::string_view t = eq == std::string_view::npos ? std::string_view() : strip(s.substr(eq + 1));
                 size_t comma = t.find(',');
-                if (comma != std::string::npos) t = strip(t.substr(0, comma));
+                if (comma != std::string_view::npos) t = strip(t.substr(0, comma));
                 if (t == "C3D4")
                     etype = 0;
                 else if (t == "C3D8")
                     etype = 1;
                 else
-                    throw IoError{"unsupported element type '" + t + "' (C3D4, C3D8 only)"};
+                    throw IoError{"unsupported element type '" + std::string(t) + "' (C3D4, C3D8 only)"};
                 in_elem = true;
             }
             continue;
         }
         if (in_node) {
-            std::string t = s;
-            std::replace(t.begin(), t.end(), ',', ' ');
-            std::istringstream iss(t);
-            double id, x, y, z;
-            if (!(iss >> id >> x >> y >> z)) throw IoError{"bad *Node line: " + s};
+            double v[4];  // id, x, y, z
+            if (!parse_doubles(s, v, 4)) throw IoError{"bad *Node line: " + std::string(s)};
             // stored in file order, ids not used (src/data2cae.cpp:103-115)
-            m.xyz.push_back(x);
-            m.xyz.push_back(y);
-            m.xyz.push_back(z);
+            m.xyz.push_back(v[1]);
+            m.xyz.push_back(v[2]);
+            m.xyz.push_back(v[3]);
         } else if (in_elem) {
-            std::istringstream iss(s);
-            std::string tok;
-            std::vector<int> v;
-            while (std::getline(iss, tok, ',')) {
-                tok = strip(tok);
-                if (!tok.empty()) v.push_back(std::atoi(tok.c_str()));
-            }
-            int npe = etype == 1 ? 8 : 4;
-            if ((int)v.size() != npe + 1) throw IoError{"bad *Element line: " + s};
+            int v[10];
+            const int npe = etype == 1 ? 8 : 4;
+            if (parse_ints(s, v, 10) != npe + 1) throw IoError{"bad *Element line: " + std::string(s)};
             for (int a = 0; a < 8; ++a) m.topo.push_back(a < npe ? v[1 + a] : 0);
             m.etype.push_back(etype);
         }
@@ -166,7 +210,7 @@ void parse(const std::vector<std::string> &L, ofea_model &m) {
     for (size_t i = 0; i < L.size(); ++i) {
         if (has(L[i], "*End Assembly")) after = true;
         if (after && has(L[i], "Cload") && i + 1 < L.size()) {
-            std::istringstream iss(L[i + 1]);
+            std::istringstream iss{std::string(L[i + 1])};
             std::string name, dof, val;
             iss >> name >> dof >> val;
             if (!dof.empty() && dof.back() == ',') dof.pop_back();
@@ -178,14 +222,14 @@ void parse(const std::vector<std::string> &L, ofea_model &m) {
     // *Density, *Elastic (last occurrence wins, src/data2cae.cpp:422-442)
     for (size_t i = 0; i + 1 < L.size(); ++i) {
         if (has(L[i], "*Density")) {
-            std::istringstream iss(L[i + 1]);
+            std::istringstream iss{std::string(L[i + 1])};
             std::string d;
             iss >> d;
             if (!d.empty() && d.back() == ',') d.pop_back();
             m.density = std::strtod(d.c_str(), nullptr);
         }
         if (has(L[i], "*Elastic")) {
-            std::istringstream iss(L[i + 1]);
+            std::istringstream iss{std::string(L[i + 1])};
             std::string e, nu;
             iss >> e >> nu;
             if (!e.empty() && e.back() == ',') e.pop_back();
