@@ -352,48 +352,92 @@ int ofea_full_displacement(int nd, const int *free_map, const double *u, double 
 int ofea_write_vtk(const char *path, int nd, const double *xyz, int ne, const int *topo,
                    const int *etype, const double *u_full, double scale) {
     if (!path || nd <= 0 || ne < 0 || !xyz || !topo || !etype || !u_full) return OFEA_ERR_INVALID_ARG;
-    std::ofstream fout(path);
-    if (!fout) return OFEA_ERR_IO;
     // same header, separators and default 6-significant-digit formatting as
-    // the reference writer (src/data2vtk.cpp:56-100, 143-196)
-    fout << "# vtk DataFile Version 3.0\n";
-    fout << "The density field of the optimized results\n";
-    fout << "ASCII\n";
-    fout << "DATASET UNSTRUCTURED_GRID\n\n";
-    fout << "POINTS\t" << nd << "\tdouble\n";
-    for (int i = 0; i < nd; ++i)
-        fout << xyz[3L * i] + scale * u_full[3L * i] << "\t\t" << xyz[3L * i + 1] + scale * u_full[3L * i + 1]
-             << "\t\t" << xyz[3L * i + 2] + scale * u_full[3L * i + 2] << "\n";
+    // the reference writer (src/data2vtk.cpp:56-100, 143-196); the text is
+    // built in one buffer with std::to_chars (general format, precision 6 is
+    // what an ostream prints by default) and written once
+    std::string out;
+    out.reserve((size_t)nd * 120 + (size_t)ne * 64 + 1024);
+    char tmp[64];
+    auto put = [&](const char *str) { out.append(str); };
+    auto put_d = [&](double v) {
+        const auto r = std::to_chars(tmp, tmp + sizeof(tmp), v, std::chars_format::general, 6);
+        out.append(tmp, r.ptr);
+    };
+    auto put_i = [&](long v) {
+        const auto r = std::to_chars(tmp, tmp + sizeof(tmp), v);
+        out.append(tmp, r.ptr);
+    };
+    put("# vtk DataFile Version 3.0\n");
+    put("The density field of the optimized results\n");
+    put("ASCII\n");
+    put("DATASET UNSTRUCTURED_GRID\n\n");
+    put("POINTS\t");
+    put_i(nd);
+    put("\tdouble\n");
+    for (int i = 0; i < nd; ++i) {
+        put_d(xyz[3L * i] + scale * u_full[3L * i]);
+        put("\t\t");
+        put_d(xyz[3L * i + 1] + scale * u_full[3L * i + 1]);
+        put("\t\t");
+        put_d(xyz[3L * i + 2] + scale * u_full[3L * i + 2]);
+        put("\n");
+    }
     long n4 = 0, n8 = 0;
     for (int e = 0; e < ne; ++e) (etype[e] == 1 ? n8 : n4)++;
-    fout << "CELLS\t" << ne << "\t" << n8 * 9 + n4 * 5 << "\n";
+    put("CELLS\t");
+    put_i(ne);
+    put("\t");
+    put_i(n8 * 9 + n4 * 5);
+    put("\n");
     for (int e = 0; e < ne; ++e) {
         const int *t = topo + 8L * e;
         if (etype[e] == 1) {
             static const int ord[8] = {0, 1, 3, 2, 4, 5, 7, 6};  // VTK_VOXEL order
-            fout << 8;
-            for (int a = 0; a < 8; ++a) fout << "\t" << t[ord[a]] - 1;
-            fout << "\n";
+            put("8");
+            for (int a = 0; a < 8; ++a) {
+                put("\t");
+                put_i(t[ord[a]] - 1);
+            }
         } else {
-            fout << 4 << "\t" << t[0] - 1 << "\t" << t[2] - 1 << "\t" << t[1] - 1 << "\t" << t[3] - 1 << "\n";
+            static const int ord[4] = {0, 2, 1, 3};
+            put("4");
+            for (int a = 0; a < 4; ++a) {
+                put("\t");
+                put_i(t[ord[a]] - 1);
+            }
+        }
+        put("\n");
+    }
+    put("CELL_TYPES\t\t");
+    put_i(ne);
+    put("\n");
+    for (int e = 0; e < ne; ++e) put(etype[e] == 1 ? "11\n" : "10\n");
+    const char *names[3] = {"u_x", "u_y", "u_z"};
+    put("\nPOINT_DATA\t");
+    put_i(nd);
+    for (int c = 0; c < 3; ++c) {
+        put("\nSCALARS ");
+        put(names[c]);
+        put(" double 1\nLOOKUP_TABLE  table");
+        put_i(c + 1);
+        put("\n");
+        for (int i = 0; i < nd; ++i) {
+            put_d(u_full[3L * i + c]);
+            put("\n");
         }
     }
-    fout << "CELL_TYPES\t\t" << ne << "\n";
-    for (int e = 0; e < ne; ++e) fout << (etype[e] == 1 ? 11 : 10) << "\n";
-    const char *names[3] = {"u_x", "u_y", "u_z"};
-    fout << "\nPOINT_DATA\t" << nd;
-    for (int c = 0; c < 3; ++c) {
-        fout << "\nSCALARS " << names[c] << " double 1\n"
-             << "LOOKUP_TABLE  table" << c + 1 << "\n";
-        for (int i = 0; i < nd; ++i) fout << u_full[3L * i + c] << "\n";
-    }
-    fout << "\nSCALARS u_magnitude double 1\n"
-         << "LOOKUP_TABLE  table4\n";
+    put("\nSCALARS u_magnitude double 1\nLOOKUP_TABLE  table4\n");
     for (int i = 0; i < nd; ++i) {
         const double *u = u_full + 3L * i;
-        fout << std::sqrt(u[2] * u[2] + u[1] * u[1] + u[0] * u[0]) << "\n";
+        put_d(std::sqrt(u[2] * u[2] + u[1] * u[1] + u[0] * u[0]));
+        put("\n");
     }
-    return fout.good() ? OFEA_OK : OFEA_ERR_IO;
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return OFEA_ERR_IO;
+    const size_t w = std::fwrite(out.data(), 1, out.size(), f);
+    const int rc = std::fclose(f);
+    return (w == out.size() && rc == 0) ? OFEA_OK : OFEA_ERR_IO;
 }
 
 }  // extern "C"
