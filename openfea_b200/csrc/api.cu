@@ -664,11 +664,11 @@ int ofea_batch_solve(ofea_batch *b, const double *const *f, double *const *u, co
     return ofea_batch_get_solution(b, u);
 }
 
-int ofea_batch_tuning(ofea_batch *b, int method, int *kc, int *threads, int *ctas_per_sm, double *ms) {
+int ofea_batch_tuning(ofea_batch *b, int method, int *rl, int *threads, int *ctas_per_sm, double *ms) {
     return guarded([&] {
         need(b != nullptr, OFEA_ERR_INVALID_ARG, "NULL batch");
         need(method == OFEA_SOLVER_PCG64 || method == OFEA_SOLVER_MIXED, OFEA_ERR_UNKNOWN_SOLVER, "method");
-        batch_tuning(b, method, kc, threads, ctas_per_sm, ms);
+        batch_tuning(b, method, rl, threads, ctas_per_sm, ms);
     });
 }
 

@@ -74,7 +74,7 @@ struct GridSync {
 };
 
 struct BArgs {
-    int V, NR, kc, nslices, naggs, ncrows, max_iter, extra_arrivals;
+    int V, NR, nslices, naggs, ncrows, max_iter, extra_arrivals;
     unsigned long long limit_ns;
     double rtol;
     const BVar *var;
@@ -1048,7 +1048,6 @@ BArgs make_args(ofea_batch *b, bool mixed, const TuneCfg &t, int max_iter, doubl
     BArgs a{};
     a.V = b->V;
     a.NR = b->NR;
-    a.kc = t.rl;
     a.nslices = b->nslices;
     a.naggs = mixed ? b->naggs : 0;
     a.ncrows = mixed ? b->ncrows : 0;
@@ -1292,14 +1291,14 @@ void batch_get_solution(ofea_batch *b, double *const *u) {
     }
 }
 
-void batch_tuning(ofea_batch *b, int method, int *kc, int *threads, int *ctas_per_sm, double *ms_per_iter) {
+void batch_tuning(ofea_batch *b, int method, int *rl, int *threads, int *ctas_per_sm, double *ms_per_iter) {
     const bool mixed = method == OFEA_SOLVER_MIXED;
     OFEA_CUDA(cudaSetDevice(b->device));
     prepare(b, mixed);
     auto it = b->tuned.find(method);
     if (it == b->tuned.end()) it = b->tuned.emplace(method, autotune(b, mixed, 1e-8)).first;
     const TuneCfg &t = it->second;
-    if (kc) *kc = t.rl;
+    if (rl) *rl = t.rl;
     if (threads) *threads = threads_for(b->NP, t.rl);
     if (ctas_per_sm) *ctas_per_sm = t.ctas_per_sm;
     if (ms_per_iter) *ms_per_iter = t.ms_per_iter;

@@ -79,7 +79,7 @@ __device__ __forceinline__ int slot_dz(int s) { return s % 3 - 1; }
 
 // ------------------------------------------------------------ level data --
 
-// Eb[I][slot][36] from the chunk partials of k_coarse_E_chunks (fixed order).
+// Eb[I][slot][36] from the Galerkin blocks (nchunk = 1: a masked copy).
 __global__ void k_e2_blocks(int na, int nchunk, const int *__restrict__ nbr, const double *__restrict__ part,
                             double *__restrict__ Eb) {
     const long total = (long)na * 27 * 36;

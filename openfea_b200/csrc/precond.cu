@@ -173,126 +173,7 @@ void build_aggregation_fine(ofea_ctx *c) {
 
 // ------------------------------------------------------- coarse matrix --
 
-constexpr int kEGroups = 4;             // node groups per CTA
-constexpr int kEThreads = 36 * kEGroups;  // one thread per (k,l) entry of a 6x6 block
 
-__device__ __forceinline__ void rigid_col(int k, const double *d, double *z) {
-    // column k of Z_a: translations e_k, rotations e_(k-3) x d
-    z[0] = z[1] = z[2] = 0.0;
-    if (k < 3) {
-        z[k] = 1.0;
-    } else if (k == 3) {
-        z[1] = -d[2];
-        z[2] = d[1];
-    } else if (k == 4) {
-        z[0] = d[2];
-        z[2] = -d[0];
-    } else {
-        z[0] = -d[1];
-        z[1] = d[0];
-    }
-}
-
-// E[6I+k][6J+l] = sum_{a in I} sum_b Z_a^T K_ab Z_b, in two deterministic
-// stages.  Stage 1: one CTA per (aggregate I, chunk of kChunkNodes of I's
-// nodes); each group of 36 threads walks its share of the chunk's nodes in
-// ascending order, stages a block row (kStage blocks at a time) in shared
-// memory, and every thread accumulates its (k,l) entry per neighbour cell
-// slot; the groups are summed in a fixed order into the chunk's partial.
-// Stage 2: per (I, slot, k, l), the chunks are summed in order into E.
-constexpr int kStage = 32;
-constexpr int kChunkNodes = 64;
-__global__ void __launch_bounds__(kEThreads) k_coarse_E_chunks(
-    int na, int nchunk_max, const int *__restrict__ agg_ptr, const int *__restrict__ agg_nodes,
-    const int *__restrict__ agg_of, const int *__restrict__ agg_cell,
-    const int *__restrict__ node_of_free, const double *__restrict__ xyz,
-    const double *__restrict__ centroid, double inv_scale, const int *__restrict__ rowptr,
-    const int *__restrict__ cols, const double *__restrict__ Kb, double *__restrict__ part,
-    int *__restrict__ err) {
-    __shared__ double acc[kEGroups][27][36];
-    __shared__ double sK[kEGroups][kStage][9];
-    __shared__ double sD[kEGroups][kStage][3];
-    __shared__ int sSlot[kEGroups][kStage];
-    __shared__ int s_chunks[kEGroups];
-    const int g = threadIdx.x / 36, kl = threadIdx.x % 36, k = kl / 6, l = kl % 6;
-    const long nwork = (long)na * nchunk_max;
-    for (long wi = blockIdx.x; wi < nwork; wi += gridDim.x) {
-        const int I = (int)(wi / nchunk_max), ch = (int)(wi % nchunk_max);
-        for (int v = threadIdx.x; v < kEGroups * 27 * 36; v += blockDim.x) (&acc[0][0][0])[v] = 0.0;
-        __syncthreads();
-        const int cx = agg_cell[3 * I], cy = agg_cell[3 * I + 1], cz = agg_cell[3 * I + 2];
-        const double ci[3] = {centroid[3L * I], centroid[3L * I + 1], centroid[3L * I + 2]};
-        const int b0 = agg_ptr[I] + ch * kChunkNodes;
-        const int b1 = min(agg_ptr[I + 1], b0 + kChunkNodes);
-        // groups take nodes round-robin; a uniform trip count keeps every
-        // thread of the CTA at the same barriers
-        const int per = b1 > b0 ? (b1 - b0 + kEGroups - 1) / kEGroups : 0;
-        for (int it = 0; it < per; ++it) {
-            const int idx = b0 + it * kEGroups + g;
-            const bool live = idx < b1;
-            int rb = 0, deg = 0;
-            double da[3] = {0, 0, 0};
-            if (live) {
-                const int r = agg_nodes[idx];
-                rb = rowptr[r];
-                deg = rowptr[r + 1] - rb;
-                const int node = node_of_free[r];
-                for (int d = 0; d < 3; ++d) da[d] = (xyz[3L * node + d] - ci[d]) * inv_scale;
-            }
-            double za[3];
-            rigid_col(k, da, za);
-            const int nchunks = (deg + kStage - 1) / kStage;
-            __syncthreads();
-            if (kl == 0) s_chunks[g] = nchunks;
-            __syncthreads();
-            int maxchunks = 0;
-            for (int q = 0; q < kEGroups; ++q) maxchunks = max(maxchunks, s_chunks[q]);
-            for (int cc = 0; cc < maxchunks; ++cc) {
-                const int p0 = cc * kStage;
-                const int cnt = live ? min(kStage, deg - p0) : 0;
-                if (kl < cnt) {
-                    const int p = rb + p0 + kl;
-                    const int s = cols[p];
-                    const int J = agg_of[s];
-                    const int dx = agg_cell[3 * J] - cx, dy = agg_cell[3 * J + 1] - cy,
-                              dz = agg_cell[3 * J + 2] - cz;
-                    int slot = -1;
-                    if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1)
-                        slot = (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
-                    else
-                        atomicExch(err, 1);
-                    sSlot[g][kl] = slot;
-                    const int nb = node_of_free[s];
-                    for (int d = 0; d < 3; ++d)
-                        sD[g][kl][d] = (xyz[3L * nb + d] - centroid[3L * J + d]) * inv_scale;
-                    for (int e = 0; e < 9; ++e) sK[g][kl][e] = Kb[9L * p + e];
-                }
-                __syncthreads();
-                for (int q = 0; q < cnt; ++q) {
-                    const int slot = sSlot[g][q];
-                    if (slot < 0) continue;
-                    double zb[3];
-                    rigid_col(l, sD[g][q], zb);
-                    const double *K = sK[g][q];
-                    double v = 0.0;
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-                        v += za[i] * (K[3 * i] * zb[0] + K[3 * i + 1] * zb[1] + K[3 * i + 2] * zb[2]);
-                    acc[g][slot][kl] += v;
-                }
-                __syncthreads();
-            }
-        }
-        __syncthreads();
-        double *out = part + wi * (27L * 36);
-        for (int v = threadIdx.x; v < 27 * 36; v += blockDim.x) {
-            double s = 0.0;
-            for (int q = 0; q < kEGroups; ++q) s += (&acc[q][0][0])[v];
-            out[v] = s;
-        }
-        __syncthreads();
-    }
-}
 
 // Stage 2: E entries from the chunk partials, fixed chunk order.
 // Galerkin blocks E[I][s] = sum over nodes i of I and row blocks K_ij with
