@@ -108,6 +108,7 @@ def lib():
         "ofea_profile_solver_kernels": (_I, [_P, _I, _I, _P, _P]),
         "ofea_precond_reset": (_I, [_P]),
         "ofea_set_coarse_nodes": (_I, [_P, _I]),
+        "ofea_trim_device_memory": (_I, []),
         "ofea_learn_opts_default": (None, [_P]),
         "ofea_batch_create": (_I, [ctypes.POINTER(_P), _P, _I, _I]),
         "ofea_batch_destroy": (_I, [_P]),
@@ -150,6 +151,11 @@ def _f64(a):
 
 def _i32(a):
     return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def trim_device_memory():
+    """Return the library's cached device memory to the driver."""
+    _check(lib().ofea_trim_device_memory(), "ofea_trim_device_memory")
 
 
 class Batch:

@@ -391,6 +391,10 @@ int ofea_set_coarse_nodes(ofea_ctx *c, int nodes) {
     });
 }
 
+int ofea_trim_device_memory(void) {
+    return guarded([&] { dev_trim(); });
+}
+
 int ofea_precond_reset(ofea_ctx *c) {
     return guarded([&] {
         need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");

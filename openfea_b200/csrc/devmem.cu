@@ -1,0 +1,120 @@
+// Device-memory cache behind every DevBuf of the library.
+//
+// A context allocates a few dozen buffers (solver vectors, the coarse levels'
+// matrices, the learned level, batch vectors) the first time it needs them;
+// cudaMalloc / cudaFree of each cost up to milliseconds, which dominated the
+// first solve of a fresh context.  Freed blocks are therefore kept per device
+// (up to kCacheCap bytes) and handed to later requests of a fitting size;
+// a block is cached only after the device has finished every queued use of it
+// (cudaDeviceSynchronize, the wait cudaFree itself implies).  Sizes are
+// rounded (256 B, or 2 MB from 1 MB up) so that contexts of the same problem
+// reuse each other's blocks exactly.  ofea_trim_device_memory returns the
+// cached blocks to the driver.
+#include <map>
+#include <mutex>
+
+#include "ofea_internal.cuh"
+
+namespace ofea {
+namespace {
+
+constexpr size_t kCacheCap = size_t(8) << 30;  // bytes cached per device
+
+struct DeviceCache {
+    std::multimap<size_t, void *> free;  // size -> block
+    size_t cached = 0;
+};
+
+// never destroyed: contexts may be freed during process teardown
+struct State {
+    std::mutex mu;
+    std::map<int, DeviceCache> cache;
+};
+State &state() {
+    static State *s = new State();
+    return *s;
+}
+
+size_t round_size(size_t bytes) {
+    const size_t big = size_t(1) << 20, step = bytes >= big ? (size_t(2) << 20) : 256;
+    return (bytes + step - 1) / step * step;
+}
+
+}  // namespace
+
+void *dev_alloc(size_t bytes, size_t *got, int *device) {
+    const size_t want = round_size(bytes == 0 ? 1 : bytes);
+    int dev = 0;
+    OFEA_CUDA(cudaGetDevice(&dev));
+    *device = dev;
+    {
+        std::lock_guard<std::mutex> lock(state().mu);
+        DeviceCache &c = state().cache[dev];
+        auto it = c.free.lower_bound(want);
+        if (it != c.free.end() && it->first <= 2 * want) {
+            void *p = it->second;
+            *got = it->first;
+            c.cached -= it->first;
+            c.free.erase(it);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        // give the cached blocks back and try once more
+        dev_trim();
+        e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            fail(OFEA_ERR_OOM, "cudaMalloc of " + std::to_string(want) + " bytes failed");
+        }
+    }
+    *got = want;
+    return p;
+}
+
+void dev_free(void *p, size_t bytes, int dev) {
+    if (!p) return;
+    // the block belongs to `dev`: wait for that device, whichever is current
+    int cur = 0;
+    const bool have_cur = cudaGetDevice(&cur) == cudaSuccess;
+    const bool ok = cudaSetDevice(dev) == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        cudaFree(p);
+        if (have_cur) cudaSetDevice(cur);
+        return;
+    }
+    if (have_cur) cudaSetDevice(cur);
+    std::lock_guard<std::mutex> lock(state().mu);
+    DeviceCache &c = state().cache[dev];
+    if (c.cached + bytes > kCacheCap) {
+        cudaSetDevice(dev);
+        cudaFree(p);
+        if (have_cur) cudaSetDevice(cur);
+        return;
+    }
+    c.free.emplace(bytes, p);
+    c.cached += bytes;
+}
+
+void dev_trim() {
+    std::lock_guard<std::mutex> lock(state().mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (auto &kv : state().cache) {
+        if (cudaSetDevice(kv.first) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        cudaDeviceSynchronize();
+        for (auto &b : kv.second.free) cudaFree(b.second);
+        kv.second.free.clear();
+        kv.second.cached = 0;
+    }
+    cudaSetDevice(cur);
+}
+
+}  // namespace ofea

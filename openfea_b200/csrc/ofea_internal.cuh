@@ -22,6 +22,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -51,31 +52,36 @@ void set_last_error(const std::string &msg);
 
 #define OFEA_CHECK_LAUNCH() OFEA_CUDA(cudaGetLastError())
 
+// Device memory of the library's buffers comes from a per-device cache
+// (devmem.cu): dev_free waits for the device and keeps the block, dev_alloc
+// reuses a fitting one or calls cudaMalloc; dev_trim frees the cached blocks.
+void *dev_alloc(size_t bytes, size_t *got, int *device);
+void dev_free(void *p, size_t bytes, int device);
+void dev_trim();
+
 template <class T>
 struct DevBuf {
     T *p = nullptr;
     size_t n = 0;
+    size_t bytes = 0;  // size of the block held
+    int dev = 0;       // the GPU it lives on
     DevBuf() = default;
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) dev_free(p, bytes, dev);
         p = nullptr;
         n = 0;
+        bytes = 0;
     }
     // Grow-only allocation; contents are not preserved on growth.
     void ensure(size_t count) {
         if (count <= n && p) return;
         release();
-        size_t bytes = count * sizeof(T);
-        if (bytes == 0) bytes = sizeof(T);
-        cudaError_t e = cudaMalloc((void **)&p, bytes);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            p = nullptr;
-            fail(OFEA_ERR_OOM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
-        }
+        const size_t want = std::max(count, size_t(1)) * sizeof(T);
+        if (want / sizeof(T) < count) fail(OFEA_ERR_OOM, "allocation size overflows");
+        p = static_cast<T *>(dev_alloc(want, &bytes, &dev));
         n = count;
     }
     void upload(const T *h, size_t count, cudaStream_t s) {
