@@ -577,7 +577,7 @@ def run_ours(args):
                      "achieved": gbsA, "peak": hbm, "unit": "GB/s", "frac": gbsA / hbm,
                      "peak_kind": peak_kind, "traffic": traffic,
                      "bytes_per_launch": byM[0], "ms_per_launch": msM[0]},
-        "spmv32_smoother": {"kernel": "k_fcg_post (FP32 BSELL SpMV + block-Jacobi + dots)",
+        "spmv32_smoother": {"kernel": "k_fcg_post (BSELL SpMV with BF16 K and FP32 arithmetic + block-Jacobi + dots)",
                             "achieved_gbs": gbs32, "frac": gbs32 / hbm, "bytes_per_launch": byM[1],
                             "ms_per_launch": msM[1]},
         "spmv64_plain": {"kernel": "k_pcg64_A (FP64 BSELL SpMV, plain PCG)", "achieved_gbs": gbs64,

@@ -20,6 +20,7 @@
 //   Dinv       double[9*nfree]         inverted diagonal blocks (block-Jacobi), + FP32 copy
 //   coarse                             aggregates, E = Z^T K Z and its FP32 inverse (precond.cu)
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -190,6 +191,7 @@ struct ofea_ctx {
     ofea::DevBuf<int> sl_ptr, scols;
     ofea::DevBuf<double> sv64;
     ofea::DevBuf<float> sv32;
+    ofea::DevBuf<__nv_bfloat16> sv16;  // BF16 copy for the smoother SpMVs
     long long sell_len = 0;
     bool sell_ok = false;
     ofea::Coarse coarse;      // exact coarse level

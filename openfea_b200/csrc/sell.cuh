@@ -10,22 +10,31 @@
 // 9 planes of a slot and several slots are in flight at once, and for
 // structured node orderings neighbouring threads gather neighbouring x.
 #pragma once
+#include <type_traits>
+
 #include "ofea_internal.cuh"
 
 namespace ofea {
 
 constexpr int kSlice = 32;
 
+// Matrix values are stored as ST and used as V (BF16 storage, FP32 arithmetic).
+template <class V, class ST>
+__device__ __forceinline__ V sell_val(const ST *p) {
+    if constexpr (std::is_same<ST, __nv_bfloat16>::value) return (V)__bfloat162float(__ldg(p));
+    else return (V)__ldg(p);
+}
+
 // y_i (i = 0..2) of block row (slice base S, lane t, width W); x(k) returns
 // entry k of the operand vector.
-template <class V, int UNROLL, class XF>
+template <class V, int UNROLL, class XF, class ST = V>
 __device__ __forceinline__ void sell_row(long S, int t, int W, const int *__restrict__ scols,
-                                         const V *__restrict__ svals, XF x, V &y0, V &y1, V &y2) {
+                                         const ST *__restrict__ svals, XF x, V &y0, V &y1, V &y2) {
     y0 = 0;
     y1 = 0;
     y2 = 0;
     const int *cp = scols + S * kSlice + t;
-    const V *vp = svals + S * 9 * kSlice + t;
+    const ST *vp = svals + S * 9 * kSlice + t;
     int k = 0;
     for (; k + UNROLL <= W; k += UNROLL) {
         int c[UNROLL];
@@ -34,7 +43,7 @@ __device__ __forceinline__ void sell_row(long S, int t, int W, const int *__rest
         for (int u = 0; u < UNROLL; ++u) {
             c[u] = __ldg(cp + (long)(k + u) * kSlice);
 #pragma unroll
-            for (int e = 0; e < 9; ++e) v[u][e] = __ldg(vp + ((long)(k + u) * 9 + e) * kSlice);
+            for (int e = 0; e < 9; ++e) v[u][e] = sell_val<V>(vp + ((long)(k + u) * 9 + e) * kSlice);
         }
 #pragma unroll
         for (int u = 0; u < UNROLL; ++u) {
@@ -48,7 +57,7 @@ __device__ __forceinline__ void sell_row(long S, int t, int W, const int *__rest
         int c = __ldg(cp + (long)k * kSlice);
         V v[9];
 #pragma unroll
-        for (int e = 0; e < 9; ++e) v[e] = __ldg(vp + ((long)k * 9 + e) * kSlice);
+        for (int e = 0; e < 9; ++e) v[e] = sell_val<V>(vp + ((long)k * 9 + e) * kSlice);
         V x0 = x(3 * c), x1 = x(3 * c + 1), x2 = x(3 * c + 2);
         y0 = fma(v[0], x0, fma(v[1], x1, fma(v[2], x2, y0)));
         y1 = fma(v[3], x0, fma(v[4], x1, fma(v[5], x2, y1)));
