@@ -88,3 +88,24 @@ def test_grid_barrier_wait_runs_out_and_context_stays_usable(gpu_ctx_factory):
     U, st = b.solve([vs[0][3]], method="GPU_MIXED", rtol=1e-9)
     assert st[0]["status"] == 0
     b.close()
+
+
+def test_batched_mixes_element_types(gpu_ctx_factory, oracle):
+    """A batch holding a C3D4 tet block (per-element E) beside C3D8 variants:
+    each variant is solved against its own K (checked with the oracle's)."""
+    vs = variants(gpu_ctx_factory, count=2, nrhs=4)
+    m, ffull = mg.tet_block(8, 4, 4)
+    ctx = gpu_ctx_factory()
+    fm = ctx.upload_mesh(m)
+    ctx.assemble_pattern()
+    ctx.assemble_linear()
+    rng = np.random.default_rng(3)
+    Ft = np.stack([mg.to_free(ffull * rng.uniform(0.5, 2.0), fm) for _ in range(4)])
+    items = vs + [(ctx, m, fm, Ft)]
+    U, st = ob.solve_batched([v[0] for v in items], [v[3] for v in items], method="GPU_MIXED", rtol=1e-10)
+    for (c, mm, ff, F), u, s in zip(items, U, st):
+        assert s["status"] == 0
+        cp, ri, val = oracle.assemble(mm, ff)
+        K = sp.csc_matrix((val, ri, cp), shape=(c.n, c.n))
+        for j in range(F.shape[0]):
+            assert np.linalg.norm(F[j] - K @ u[j]) <= 1.0001e-10 * np.linalg.norm(F[j])

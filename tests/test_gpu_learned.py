@@ -107,3 +107,22 @@ def test_stage_trained_on_one_density_field_helps_on_another(gpu_ctx_factory):
     assert sl["status"] == 0 and sl["rejected_learned"] == 0 and sl["rel_residual"] <= 1e-8
     assert np.linalg.norm(ul - um) / np.linalg.norm(um) < 1e-6
     assert sl["iterations"] < sm["iterations"], (sl["iterations"], sm["iterations"])
+
+
+def test_learned_on_tetrahedra_with_per_element_modulus(gpu_ctx_factory, oracle):
+    """The learned stage on a jittered C3D4 block with lognormal per-element E
+    (the config-2 mesh type): trained on the GPU, accepted by the FP64 judge,
+    and the solution satisfies the oracle's K to the tolerance."""
+    import scipy.sparse as sp
+    m, ffull = mg.tet_block(24, 8, 8)
+    ctx = gpu_ctx_factory()
+    fm = ctx.upload_mesh(m)
+    ctx.assemble_pattern()
+    ctx.assemble_linear()
+    f = mg.to_free(ffull, fm)
+    ctx.learned_train(sample_iters=400, sample_every=4, steps=100, batch=16)
+    u, st = ctx.solve(f, method="GPU_LEARNED", rtol=1e-10)
+    assert st["status"] == 0 and st["rejected_learned"] == 0
+    cp, ri, val = oracle.assemble(m, fm)
+    K = sp.csc_matrix((val, ri, cp), shape=(ctx.n, ctx.n))
+    assert np.linalg.norm(f - K @ u) <= 1e-10 * np.linalg.norm(f) * 1.0001
