@@ -186,8 +186,8 @@ def run_batched(ob, mg, local, hbm, steps=2, count=64, nrhs=16, rtol=1e-8, dist=
         sec = max_over_ranks(min(r[0]["seconds"] for r in runs), dist)
         st = list(gather_by_variant(dict(zip(mine, st)), dist).values())
         iters = max(s_["iterations"] for s_ in st)
-        # matrix bytes per iteration: FP64 BSELL once (+ FP32 twice for MIXED), 76/9 resp. 40/9 B per nnz
-        mat = 76 * nnz_tot / 9 + (2 * 40 * nnz_tot / 9 if meth == "GPU_MIXED" else 0)
+        # matrix bytes per iteration: FP64 BSELL once (+ BF16 twice for MIXED), 76/9 resp. 22/9 B per nnz
+        mat = 76 * nnz_tot / 9 + (2 * 22 * nnz_tot / 9 if meth == "GPU_MIXED" else 0)
         per_iter = mat + vec_b * n_tot * nrhs
         out[meth] = {"seconds": sec, "iterations_max": iters,
                      "iterations_min": min(s_["iterations"] for s_ in st),
@@ -571,7 +571,7 @@ def run_ours(args):
                          f"two-level V-cycle preconditioner and the learned coarse stage, to FP64 rel. "
                          f"residual {args.rtol:g}"),
             "n_dof": n, "nnz": nnz, "parallelism": f"replicas x{world}",
-            "l2": "inputs larger than L2 (FP64 K ~1 GB and FP32 K ~0.5 GB streamed per SpMV)",
+            "l2": "inputs larger than L2 (FP64 K ~1 GB and BF16 K ~0.25 GB streamed per SpMV)",
         },
         "roofline": {"bound": "hbm", "kernel": "k_fcg_A (FP64 BSELL SpMV + p update + p.q)",
                      "achieved": gbsA, "peak": hbm, "unit": "GB/s", "frac": gbsA / hbm,

@@ -6,9 +6,10 @@
 // src/ca_analysis.cpp:148-248).
 //
 // Layout in HBM: the variants' DOF are concatenated (variant v starts at
-// dof0[v]) and every vector is load-case interleaved, x[(dof0 + d) * NR + j]:
-// the NR load cases of one DOF are one contiguous run.  Matrices stay where their contexts
-// keep them (BSELL-32, FP64 and FP32 copies); a table of per-variant
+// dof0[v]) and every vector is load-case interleaved, x[(dof0 + d) * NP + j]
+// (NP = the NR load cases padded to a power of two >= 4): the load cases of
+// one DOF are one contiguous run.  Matrices stay where their contexts keep
+// them (BSELL-32, FP64 and BF16 copies); a table of per-variant
 // descriptors points at them.
 //
 // Algorithm per (variant, load case): the MIXED method of solve.cu, FP64
@@ -60,7 +61,8 @@ struct BVar {
     long c0;    // first coarse entry of the variant (times NR)
     const int *sl_ptr, *scols;
     const double *sv64, *Dinv;
-    const float *sv32, *Dinv32;
+    const __nv_bfloat16 *sv16;
+    const float *Dinv32;
     const int *agg_of, *agg_ptr, *agg_nodes, *node_of_free;
     const double *xyz, *centroid;
     const float *Einv32;
@@ -191,11 +193,11 @@ struct Lanes {
 };
 
 // Shared-memory stage of a slice's BSELL slots: two buffers of kKC slots
-// (values in FP64 or FP32, then columns), filled with cp.async while the
+// (values in FP64 or BF16, then columns), filled with cp.async while the
 // other buffer is consumed.
 constexpr int kKC = 8;
 struct __align__(128) Stage {
-    double v[2][kKC * 9 * kSlice];  // FP32 values use the first half of each buffer
+    double v[2][kKC * 9 * kSlice];  // BF16 values use the first quarter of each buffer
     int col[2][kKC * kSlice];
     double red[32][32];             // [warp][load case] partial sums
 };
@@ -210,12 +212,12 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 // Start copying slots [k0, k0 + kc) of the slice at S into buffer b (16-byte
 // pieces: every chunk is a multiple of 16 bytes at a 16-byte-aligned offset).
-template <class V>
+template <class ST>
 __device__ __forceinline__ void stage_chunk(Stage &st, int b, long S, int k0, int kc, const int *__restrict__ scols,
-                                            const V *__restrict__ svals) {
+                                            const ST *__restrict__ svals) {
     const char *gv = reinterpret_cast<const char *>(svals + (S + k0) * 9L * kSlice);
     char *sv = reinterpret_cast<char *>(st.v[b]);
-    const int nv = kc * 9 * kSlice * (int)sizeof(V) / 16;
+    const int nv = kc * 9 * kSlice * (int)sizeof(ST) / 16;
     for (int i = threadIdx.x; i < nv; i += blockDim.x) cp_async16(sv + 16 * i, gv + 16 * i);
     const char *gc = reinterpret_cast<const char *>(scols + (S + k0) * (long)kSlice);
     char *sc = reinterpret_cast<char *>(st.col[b]);
@@ -224,14 +226,22 @@ __device__ __forceinline__ void stage_chunk(Stage &st, int b, long S, int k0, in
     cp_async_commit();
 }
 
+// A staged matrix value in the arithmetic type V.
+template <class V, class ST>
+__device__ __forceinline__ V staged_val(const ST &a) {
+    if constexpr (std::is_same<ST, __nv_bfloat16>::value) return (V)__bfloat162float(a);
+    else return (V)a;
+}
+
 // y[c][q] = (K x)_(row, c) for this thread's RL load cases.  The slice's
-// slots stream through shared memory kKC at a time, double-buffered, shared
-// by every load case; each staged value feeds RL FMAs.  xf(col, c, out[RL])
-// loads the operand.  Called by all threads of the CTA (rows beyond nfree
-// read padding: column 0, value 0).
-template <class V, int NP, int RL, class XF>
+// slots (stored as ST: FP64, or BF16 read into FP32 arithmetic) stream
+// through shared memory kKC at a time, double-buffered, shared by every load
+// case; each staged value feeds RL FMAs.  xf(col, c, out[RL]) loads the
+// operand.  Called by all threads of the CTA (rows beyond nfree read
+// padding: column 0, value 0).
+template <class V, class ST, int NP, int RL, class XF>
 __device__ __forceinline__ void spmm_slice(Stage &st, long S, int W, const int *__restrict__ scols,
-                                           const V *__restrict__ svals, XF xf, V (&y)[3][RL]) {
+                                           const ST *__restrict__ svals, XF xf, V (&y)[3][RL]) {
     const int r = Lanes<NP, RL>::row();
 #pragma unroll
     for (int c = 0; c < 3; ++c)
@@ -239,17 +249,17 @@ __device__ __forceinline__ void spmm_slice(Stage &st, long S, int W, const int *
         for (int q = 0; q < RL; ++q) y[c][q] = 0;
     const int nch = (W + kKC - 1) / kKC;
     __syncthreads();  // both buffers are free
-    if (nch > 0) stage_chunk<V>(st, 0, S, 0, min(kKC, W), scols, svals);
+    if (nch > 0) stage_chunk<ST>(st, 0, S, 0, min(kKC, W), scols, svals);
     for (int ch = 0; ch < nch; ++ch) {
         const int b = ch & 1, k0 = ch * kKC, kc = min(kKC, W - k0);
         if (ch + 1 < nch) {
-            stage_chunk<V>(st, b ^ 1, S, k0 + kKC, min(kKC, W - k0 - kKC), scols, svals);
+            stage_chunk<ST>(st, b ^ 1, S, k0 + kKC, min(kKC, W - k0 - kKC), scols, svals);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
         }
         __syncthreads();
-        const V *sv = reinterpret_cast<const V *>(st.v[b]);
+        const ST *sv = reinterpret_cast<const ST *>(st.v[b]);
 #pragma unroll
         for (int k2 = 0; k2 < kKC; k2 += 2) {
             V x[2][3][RL];
@@ -264,10 +274,11 @@ __device__ __forceinline__ void spmm_slice(Stage &st, long S, int W, const int *
 #pragma unroll
             for (int u = 0; u < 2; ++u)
                 if (k2 + u < kc) {
-                    const V *v = sv + (k2 + u) * 9 * kSlice + r;
+                    const ST *v = sv + (k2 + u) * 9 * kSlice + r;
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
-                        const V a0 = v[(3 * c) * kSlice], a1 = v[(3 * c + 1) * kSlice], a2 = v[(3 * c + 2) * kSlice];
+                        const V a0 = staged_val<V>(v[(3 * c) * kSlice]), a1 = staged_val<V>(v[(3 * c + 1) * kSlice]),
+                                a2 = staged_val<V>(v[(3 * c + 2) * kSlice]);
 #pragma unroll
                         for (int q = 0; q < RL; ++q)
                             y[c][q] = fma(a0, x[u][0][q], fma(a1, x[u][1][q], fma(a2, x[u][2][q], y[c][q])));
@@ -360,7 +371,7 @@ __global__ void __launch_bounds__(32 * (NP / RL), batch_min_ctas(32 * (NP / RL),
     for_slices([&](const BVar &B, int v, int gsl, int ls, int row, const bool (&)[RL], bool) {
         const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
         double y[3][RL];
-        spmm_slice<double, NP, RL>(st, S, W, B.scols, B.sv64,
+        spmm_slice<double, double, NP, RL>(st, S, W, B.scols, B.sv64,
                                    [&](int k, int c, double (&o)[RL]) { ldv<double, RL>(a.u + vidx<NP>(B, k, c, j0), o); }, y);
         double prr[RL] = {}, pff[RL] = {};
         if (row < B.nfree) {
@@ -427,7 +438,7 @@ __global__ void __launch_bounds__(32 * (NP / RL), batch_min_ctas(32 * (NP / RL),
         for_slices([&](const BVar &B, int v, int gsl, int ls, int row, const bool (&live)[RL], bool any) {
             const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
             float y[3][RL];
-            spmm_slice<float, NP, RL>(st, S, W, B.scols, B.sv32,
+            spmm_slice<float, __nv_bfloat16, NP, RL>(st, S, W, B.scols, B.sv16,
                                       [&](int k, int c, float (&o)[RL]) { ldv<float, RL>(a.x32 + vidx<NP>(B, k, c, j0), o); }, y);
             if (any && row < B.nfree)
                 for (int c = 0; c < 3; ++c) {
@@ -521,7 +532,7 @@ __global__ void __launch_bounds__(32 * (NP / RL), batch_min_ctas(32 * (NP / RL),
         for_slices([&](const BVar &B, int v, int gsl, int ls, int row, const bool (&live)[RL], bool any) {
             const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
             float y[3][RL];
-            spmm_slice<float, NP, RL>(st, S, W, B.scols, B.sv32,
+            spmm_slice<float, __nv_bfloat16, NP, RL>(st, S, W, B.scols, B.sv16,
                                       [&](int k, int c, float (&o)[RL]) { ldv<float, RL>(a.x32 + vidx<NP>(B, k, c, j0), o); }, y);
             double pn[RL] = {}, po[RL] = {};
             if (any && row < B.nfree) {
@@ -607,7 +618,7 @@ __global__ void __launch_bounds__(32 * (NP / RL), batch_min_ctas(32 * (NP / RL),
                 }
             };
             double y[3][RL];
-            spmm_slice<double, NP, RL>(st, S, W, B.scols, B.sv64,
+            spmm_slice<double, double, NP, RL>(st, S, W, B.scols, B.sv64,
                                        [&](int kk, int c, double (&o)[RL]) { pval(vidx<NP>(B, kk, c, j0), o); }, y);
             double ppq[RL] = {};
             if (any && row < B.nfree)
@@ -764,7 +775,7 @@ __global__ void __launch_bounds__(32 * (NP / RL)) k_batch_residual(BArgs a) {
         const int ls = gsl - B.slice0, row = ls * kSlice + r;
         const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
         double y[3][RL];
-        spmm_slice<double, NP, RL>(st, S, W, B.scols, B.sv64,
+        spmm_slice<double, double, NP, RL>(st, S, W, B.scols, B.sv64,
                                    [&](int k, int c, double (&o)[RL]) { ldv<double, RL>(a.u + vidx<NP>(B, k, c, j0), o); }, y);
         double prr[RL] = {}, pff[RL] = {};
         if (row < B.nfree)
@@ -972,7 +983,7 @@ void build_desc(ofea_batch *b, bool mixed) {
         B.scols = c->scols.p;
         B.sv64 = c->sv64.p;
         B.Dinv = c->Dinv.p;
-        B.sv32 = c->sv32.p;
+        B.sv16 = c->sv16.p;
         B.Dinv32 = c->Dinv32.p;
         for (int s = 0; s < B.nslice; ++s) sv.push_back(v);
         slice0 += B.nslice;

@@ -13,8 +13,8 @@
 //   slot       uint16[8*len(inc)]      for incidence k and local node b: block
 //                                      position within the row, 0xFFFF if b is fixed
 //   Kb         double[9*nnzb]          K values, block-row-major, 3x3 blocks row-major
-//   sl_ptr, scols, sv64, sv32          the solver's copy of K in BSELL-32 (sell.cuh),
-//                                      FP64 values and an FP32 rounding
+//   sl_ptr, scols, sv64, sv16          the solver's copy of K in BSELL-32 (sell.cuh),
+//                                      FP64 values and a BF16 rounding
 //   Ke         double[576*ne8 + 144*ne4]  element matrices (scratch of the assembly):
 //                                      element g, block (a,b), entries 3x3 row-major
 //   Dinv       double[9*nfree]         inverted diagonal blocks (block-Jacobi), + FP32 copy
@@ -187,11 +187,10 @@ struct ofea_ctx {
     ofea::DevBuf<double> Kb, Ke, Fe, Dinv, u_nl, f_int;
     ofea::DevBuf<float> Dinv32;
     bool K_ok = false, jacobi_ok = false;
-    // solver layout of K (sell.cuh): BSELL-32, FP64 and FP32 values
+    // solver layout of K (sell.cuh): BSELL-32, FP64 and BF16 values
     ofea::DevBuf<int> sl_ptr, scols;
     ofea::DevBuf<double> sv64;
-    ofea::DevBuf<float> sv32;
-    ofea::DevBuf<__nv_bfloat16> sv16;  // BF16 copy for the smoother SpMVs
+    ofea::DevBuf<__nv_bfloat16> sv16;  // BF16 copy for the FP32 preconditioner SpMVs
     long long sell_len = 0;
     bool sell_ok = false;
     ofea::Coarse coarse;      // exact coarse level

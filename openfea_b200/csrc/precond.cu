@@ -12,8 +12,9 @@
 // cell size).  E = Z^T K Z (FP64, 6 x 6 blocks between neighbouring cells) is
 // inverted on the device by blocked Gauss-Jordan and applied as an FP32 GEMV.
 //
-// The FP32 SpMV is accurate for the high-frequency error the smoother damps;
-// the smooth modes that FP32 rounding of K would corrupt are carried by the
+// The smoother's SpMV reads a BF16 rounding of K into FP32 arithmetic; that
+// is accurate for the high-frequency error the smoother damps, and the smooth
+// modes that the rounding of K would corrupt are carried by the
 // exact FP64 coarse operator, so the FP64 outer iteration keeps the iteration
 // count of an all-FP64 preconditioner.
 #include <algorithm>

@@ -22,7 +22,7 @@ __global__ void k_slice_width(int nfree, const int *__restrict__ rowptr, int *__
 __global__ void k_fill_sell(int nfree, const int *__restrict__ rowptr, const int *__restrict__ cols,
                             const double *__restrict__ Kb, const int *__restrict__ sl_ptr,
                             int *__restrict__ scols, double *__restrict__ sv64,
-                            float *__restrict__ sv32, __nv_bfloat16 *__restrict__ sv16) {
+                            __nv_bfloat16 *__restrict__ sv16) {
     const int nslice = (nfree + kSlice - 1) / kSlice;
     for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < (long)nslice * kSlice;
          g += (long)gridDim.x * blockDim.x) {
@@ -39,7 +39,6 @@ __global__ void k_fill_sell(int nfree, const int *__restrict__ rowptr, const int
             for (int e = 0; e < 9; ++e) {
                 double v = real ? Kb[9L * (rb + k) + e] : 0.0;
                 sv64[((S + k) * 9 + e) * kSlice + t] = v;
-                sv32[((S + k) * 9 + e) * kSlice + t] = (float)v;
                 sv16[((S + k) * 9 + e) * kSlice + t] = __double2bfloat16(v);
             }
         }
@@ -60,10 +59,9 @@ void build_sell(ofea_ctx *c) {
     size_t slots = (size_t)std::max<long long>(tot, 1) * kSlice;
     c->scols.ensure(slots);
     c->sv64.ensure(9 * slots);
-    c->sv32.ensure(9 * slots);
     c->sv16.ensure(9 * slots);
     k_fill_sell<<<grid_for(c, (long)nslice * kSlice, kBlock), kBlock, 0, s>>>(
-        c->nfree, c->rowptr.p, c->cols.p, c->Kb.p, c->sl_ptr.p, c->scols.p, c->sv64.p, c->sv32.p, c->sv16.p);
+        c->nfree, c->rowptr.p, c->cols.p, c->Kb.p, c->sl_ptr.p, c->scols.p, c->sv64.p, c->sv16.p);
     OFEA_CHECK_LAUNCH();
     c->sell_ok = true;
 }

@@ -684,7 +684,7 @@ void profile_kernels(ofea_ctx *c, int method, int reps, double *ms, double *byte
         OFEA_CUDA(cudaEventRecord(e2, s));
         // FP64 K + columns + slice pointers, z (FP32) and p_old read, p_new and q written
         bytes[0] = 8 * nnzv + 4 * nblk + 4.0 * ((nf + 31) / 32 + 1) + 4.0 * n + 8.0 * n * 3;
-        // FP32 K + columns, x32 and b32 read, Dinv32, r (FP64) and z_old read, z_new written
+        // BF16 K + columns, x32 and b32 read, Dinv32, r (FP64) and z_old read, z_new written
         bytes[1] = 2 * nnzv + 4 * nblk + 4.0 * n * 2 + 36.0 * nf + 8.0 * n + 4.0 * n * 2;
     }
     OFEA_CHECK_LAUNCH();
