@@ -250,6 +250,18 @@ OFEA_API int ofea_batch_solve(ofea_batch *batch, const double *const *f, double 
 /* The tile configuration used for `method` (tuning it now if needed). */
 OFEA_API int ofea_batch_tuning(ofea_batch *batch, int method, int *rhs_per_lane, int *threads,
                                int *ctas_per_sm, double *ms_per_iteration);
+/* Phase trace (no counterpart in the reference, which prints clock() spans):
+ * with max_phases > 0 every later solve launch records the device clock
+ * (%globaltimer, CTA 0) at its start and after each of its grid barriers, at
+ * most max_phases of them; 0 turns it off.  ofea_batch_phase_times returns
+ * the durations in milliseconds between consecutive records of the last
+ * launch, in barrier order (MIXED: init, init pairs, then the V-cycle's five
+ * phases and its pair step, then per iteration A, pairs, B, pairs, the
+ * V-cycle's five and its pair step; PCG64: init, init pairs, r.z, pairs,
+ * then A, pairs, B, pairs per iteration); *count = how many exist, up to cap
+ * are written (ms may be NULL to query). */
+OFEA_API int ofea_batch_set_trace(ofea_batch *batch, int max_phases);
+OFEA_API int ofea_batch_phase_times(ofea_batch *batch, double *ms, int cap, int *count);
 /* One-call form: create, solve, destroy. */
 OFEA_API int ofea_solve_batched(ofea_ctx *const *ctxs, int n_variants, const double *const *f,
                                 double *const *u, int nrhs, const ofea_solve_opts *opts,

@@ -118,6 +118,8 @@ def lib():
         "ofea_batch_solve": (_I, [_P, _P, _P, _P, _P]),
         "ofea_batch_tuning": (_I, [_P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I),
                                    ctypes.POINTER(_D)]),
+        "ofea_batch_set_trace": (_I, [_P, _I]),
+        "ofea_batch_phase_times": (_I, [_P, _P, _I, ctypes.POINTER(_I)]),
         "ofea_solve_batched": (_I, [_P, _I, _P, _P, _I, _P, _P]),
         "ofea_check_barrier_timeout": (_I, [_P, _I, ctypes.POINTER(_I)]),
         "ofea_learned_train": (_I, [_P, _P, _P, _P]),
@@ -213,6 +215,20 @@ class Batch:
         _check(lib().ofea_batch_tuning(self.h, SOLVERS[method], ctypes.byref(r), ctypes.byref(t), ctypes.byref(c),
                                        ctypes.byref(ms)), "ofea_batch_tuning")
         return {"rhs_per_lane": r.value, "threads": t.value, "ctas_per_sm": c.value, "ms_per_iteration": ms.value}
+
+    def set_trace(self, max_phases):
+        """Record the device clock after each grid barrier of later solves
+        (up to max_phases barriers per launch; 0 turns it off)."""
+        _check(lib().ofea_batch_set_trace(self.h, int(max_phases)), "ofea_batch_set_trace")
+
+    def phase_times(self):
+        """Milliseconds between consecutive barriers of the last traced launch."""
+        n = _I()
+        _check(lib().ofea_batch_phase_times(self.h, None, 0, ctypes.byref(n)), "ofea_batch_phase_times")
+        out = np.zeros(n.value)
+        _check(lib().ofea_batch_phase_times(self.h, out.ctypes.data, n.value, ctypes.byref(n)),
+               "ofea_batch_phase_times")
+        return out
 
 
 def solve_batched(contexts, loads, method="GPU_MIXED", rtol=1e-8, **kw):

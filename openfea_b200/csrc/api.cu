@@ -676,6 +676,20 @@ int ofea_batch_tuning(ofea_batch *b, int method, int *rl, int *threads, int *cta
     });
 }
 
+int ofea_batch_set_trace(ofea_batch *b, int max_phases) {
+    return guarded([&] {
+        need(b != nullptr, OFEA_ERR_INVALID_ARG, "NULL batch");
+        batch_set_trace(b, max_phases);
+    });
+}
+
+int ofea_batch_phase_times(ofea_batch *b, double *ms, int cap, int *count) {
+    return guarded([&] {
+        need(b != nullptr && count != nullptr && cap >= 0, OFEA_ERR_INVALID_ARG, "bad argument");
+        batch_phase_times(b, ms, cap, count);
+    });
+}
+
 int ofea_solve_batched(ofea_ctx *const *ctxs, int n_variants, const double *const *f, double *const *u, int nrhs,
                        const ofea_solve_opts *opts, ofea_solve_stats *stats) {
     ofea_batch *b = nullptr;

@@ -88,6 +88,8 @@ struct BArgs {
     double *ff, *tol2, *rz, *alpha, *beta;              // [V * NR]
     int *live, *iters, *status, *live_cnt;              // [V * NR], live_cnt[3]
     GridSync *gs;
+    unsigned long long *trace;  // NULL, or %globaltimer at the start and after each grid barrier (CTA 0)
+    int trace_cap;
 };
 
 namespace {
@@ -201,6 +203,7 @@ struct __align__(128) Stage {
     int col[2][kKC * kSlice];
     double red[32][32];             // [warp][load case] partial sums
 };
+static_assert(sizeof(Stage::v) >= 6 * 32 * 32 * sizeof(float), "the restriction's per-warp sums fit in the stage");
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -347,7 +350,14 @@ __global__ void __launch_bounds__(32 * (NP / RL), batch_min_ctas(32 * (NP / RL),
     const unsigned nb = gridDim.x + a.extra_arrivals;
     const int NR = a.NR;
     const int r = LN::row(), j0 = LN::j0();
-    auto sync = [&]() { return grid_barrier(a.gs, nb, a.limit_ns); };
+    const bool tracer = a.trace != nullptr && blockIdx.x == 0 && threadIdx.x == 0;
+    int tn = 0;
+    if (tracer && tn < a.trace_cap) a.trace[tn++] = global_ns();
+    auto sync = [&]() {
+        const bool ok = grid_barrier(a.gs, nb, a.limit_ns);
+        if (tracer && tn < a.trace_cap) a.trace[tn++] = global_ns();
+        return ok;
+    };
     auto X = [&](const BVar &B, int row, int c) { return vidx<NP>(B, row, c, j0); };
     // CTA-level loop over slices: f(B, v, gsl, ls, row, live[RL], any)
     auto for_slices = [&](auto f) {
@@ -432,8 +442,9 @@ __global__ void __launch_bounds__(32 * (NP / RL), batch_min_ctas(32 * (NP / RL),
     if (!sync()) return;
 
     // MIXED preconditioner z_new = M(r) from b32 / x32 (pre-smoothed by the
-    // phase before); partials r.z_new (pa), r.z_old (pb).
-    auto precondition = [&](float *znew, const float *zold) -> bool {
+    // phase before); partials r.z_new (pa), r.z_old (pb).  Inlined at both
+    // call sites: a call would put every captured local on the stack.
+    auto precondition = [&](float *znew, const float *zold) __attribute__((always_inline)) -> bool {
         // t = b - K32 x
         for_slices([&](const BVar &B, int v, int gsl, int ls, int row, const bool (&live)[RL], bool any) {
             const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
@@ -450,42 +461,73 @@ __global__ void __launch_bounds__(32 * (NP / RL), batch_min_ctas(32 * (NP / RL),
                 }
         });
         if (!sync()) return false;
-        // c = Z^T t: warp per aggregate, NP lanes per node (one load case each)
+        // c = Z^T t: CTA per aggregate, NP lanes per node (one load case
+        // each), G = threads / NP nodes side by side and 4 nodes per thread in
+        // flight; per-warp sums, then a fixed-order sum over the warps.
         {
-            constexpr int JW = NP, RPW = 32 / NP;
-            const int warps = blockDim.x / 32, w = threadIdx.x / 32, lane = threadIdx.x & 31;
-            const int sub = lane / JW, jj = lane % JW;
-            for (int ga = blockIdx.x * warps + w; ga < a.naggs; ga += gridDim.x * warps) {
+            constexpr int JW = NP, kU = 4;
+            const int G = blockDim.x / JW, sub = threadIdx.x / JW, jj = threadIdx.x % JW;
+            const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+            float *red = reinterpret_cast<float *>(st.v);  // [warp][6][JW]: 6 * 32 * 32 floats at most
+            for (int ga = blockIdx.x; ga < a.naggs; ga += gridDim.x) {
                 const int v = a.agg_var[ga];
                 const BVar B = a.var[v];
                 const int I = ga - B.agg0;
                 const bool live = jj < NR && a.live[v * NR + jj] != 0;
                 float acc[6] = {0, 0, 0, 0, 0, 0};
-                const float cx = (float)B.centroid[3L * I], cy = (float)B.centroid[3L * I + 1],
-                            cz = (float)B.centroid[3L * I + 2];
-                const float sc = (float)B.inv_scale;
-                for (int idx = B.agg_ptr[I] + sub; idx < B.agg_ptr[I + 1]; idx += RPW) {
-                    if (!live) continue;
-                    const int rr = B.agg_nodes[idx], node = B.node_of_free[rr];
-                    const float dx = ((float)B.xyz[3L * node] - cx) * sc;
-                    const float dy = ((float)B.xyz[3L * node + 1] - cy) * sc;
-                    const float dz = ((float)B.xyz[3L * node + 2] - cz) * sc;
-                    const float tx = a.t32[vidx<NP>(B, rr, 0, jj)], ty = a.t32[vidx<NP>(B, rr, 1, jj)],
-                                tz = a.t32[vidx<NP>(B, rr, 2, jj)];
-                    acc[0] += tx;
-                    acc[1] += ty;
-                    acc[2] += tz;
-                    acc[3] += -dz * ty + dy * tz;
-                    acc[4] += dz * tx - dx * tz;
-                    acc[5] += -dy * tx + dx * ty;
+                if (live) {
+                    const float cx = (float)B.centroid[3L * I], cy = (float)B.centroid[3L * I + 1],
+                                cz = (float)B.centroid[3L * I + 2];
+                    const float sc = (float)B.inv_scale;
+                    auto add = [&](int node, float tx, float ty, float tz) {
+                        const float dx = ((float)B.xyz[3L * node] - cx) * sc;
+                        const float dy = ((float)B.xyz[3L * node + 1] - cy) * sc;
+                        const float dz = ((float)B.xyz[3L * node + 2] - cz) * sc;
+                        acc[0] += tx;
+                        acc[1] += ty;
+                        acc[2] += tz;
+                        acc[3] += -dz * ty + dy * tz;
+                        acc[4] += dz * tx - dx * tz;
+                        acc[5] += -dy * tx + dx * ty;
+                    };
+                    const int e = B.agg_ptr[I + 1];
+                    int idx = B.agg_ptr[I] + sub;
+                    for (; idx + (kU - 1) * G < e; idx += kU * G) {
+                        int rr[kU], node[kU];
+                        float t[kU][3];
+#pragma unroll
+                        for (int u = 0; u < kU; ++u) rr[u] = B.agg_nodes[idx + u * G];
+#pragma unroll
+                        for (int u = 0; u < kU; ++u) {
+                            node[u] = B.node_of_free[rr[u]];
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) t[u][c] = a.t32[vidx<NP>(B, rr[u], c, jj)];
+                        }
+#pragma unroll
+                        for (int u = 0; u < kU; ++u) add(node[u], t[u][0], t[u][1], t[u][2]);
+                    }
+                    for (; idx < e; idx += G) {
+                        const int rr = B.agg_nodes[idx];
+                        add(B.node_of_free[rr], a.t32[vidx<NP>(B, rr, 0, jj)], a.t32[vidx<NP>(B, rr, 1, jj)],
+                            a.t32[vidx<NP>(B, rr, 2, jj)]);
+                    }
                 }
 #pragma unroll
                 for (int k = 0; k < 6; ++k) {
-                    float s = acc[k];
 #pragma unroll
-                    for (int off = JW; off < 32; off <<= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-                    if (sub == 0 && live) a.cvec[(B.c0 + 6L * I + k) * NP + jj] = s;
+                    for (int off = JW; off < 32; off <<= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], off);
                 }
+                if (lane < JW)
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) red[(w * 6 + k) * JW + lane] = acc[k];
+                __syncthreads();
+                if ((int)threadIdx.x < 6 * JW) {
+                    const int k = threadIdx.x / JW, j = threadIdx.x % JW;
+                    float sum = 0.f;
+                    for (int ww = 0; ww < nw; ++ww) sum += red[(ww * 6 + k) * JW + j];
+                    if (j < NR && a.live[v * NR + j] != 0) a.cvec[(B.c0 + 6L * I + k) * NP + j] = sum;
+                }
+                __syncthreads();
             }
         }
         if (!sync()) return false;
@@ -944,6 +986,8 @@ struct ofea_batch {
     ofea::DevBuf<float> b32, x32, t32, zA, zB, cvec, evec;
     ofea::DevBuf<int> live, iters, status, live_cnt;
     ofea::DevBuf<ofea::GridSync> gs;
+    ofea::DevBuf<unsigned long long> trace;  // per-phase timestamps when tracing (trace_cap > 0)
+    int trace_cap = 0;
     std::map<int, ofea::TuneCfg> tuned;  // by method
     // the captured graph of one launch and what it was captured for
     cudaGraphExec_t exec = nullptr;
@@ -1096,6 +1140,8 @@ BArgs make_args(ofea_batch *b, bool mixed, const TuneCfg &t, int max_iter, doubl
     a.status = b->status.p;
     a.live_cnt = b->live_cnt.p;
     a.gs = b->gs.p;
+    a.trace = b->trace_cap > 0 ? b->trace.p : nullptr;
+    a.trace_cap = b->trace_cap;
     return a;
 }
 
@@ -1114,6 +1160,7 @@ void enqueue(ofea_batch *b, const BArgs &a, const TuneCfg &t, bool mixed) {
     OFEA_CUDA(cudaMemsetAsync(b->p1.p, 0, sizeof(double) * n, s));
     OFEA_CUDA(cudaMemsetAsync(b->gs.p, 0, sizeof(GridSync), s));
     OFEA_CUDA(cudaMemsetAsync(b->live_cnt.p, 0, sizeof(int) * 3, s));
+    if (a.trace) OFEA_CUDA(cudaMemsetAsync(a.trace, 0, sizeof(unsigned long long) * a.trace_cap, s));
     const void *fn = solve_kernel(b->NP, t.rl, mixed);
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(grid_of(b, fn, t));
@@ -1344,7 +1391,7 @@ void batch_solve(ofea_batch *b, const ofea_solve_opts &o, ofea_solve_stats *stat
         BArgs a = make_args(b, mixed, t, remaining, o.rtol);
         std::ostringstream k;
         k << o.method << "/" << t.rl << "/" << t.ctas_per_sm << "/" << remaining << "/"
-          << o.rtol;
+          << o.rtol << "/" << b->trace_cap;
         if (o.use_graph) {
             if (!b->exec || b->exec_key != k.str()) {
                 if (b->exec) {
@@ -1423,6 +1470,37 @@ void batch_solve(ofea_batch *b, const ofea_solve_opts &o, ofea_solve_stats *stat
 
 // A cooperative launch whose barrier expects one CTA more than it has: every
 // wait runs out after limit_ms and the kernel reports it (*released = 0).
+// Phase trace of the solver kernel: with max_phases > 0 every later launch
+// records %globaltimer at its start and after each grid barrier (CTA 0,
+// thread 0; at most max_phases barriers); 0 turns it off.
+void batch_set_trace(ofea_batch *b, int max_phases) {
+    if (max_phases < 0 || max_phases > (1 << 20)) fail(OFEA_ERR_INVALID_ARG, "batch: max_phases must be 0..2^20");
+    OFEA_CUDA(cudaSetDevice(b->device));
+    if (max_phases > 0) {
+        b->trace.ensure((size_t)max_phases + 1);
+        OFEA_CUDA(cudaMemsetAsync(b->trace.p, 0, sizeof(unsigned long long) * (max_phases + 1), b->stream));
+    }
+    b->trace_cap = max_phases > 0 ? max_phases + 1 : 0;
+}
+
+// Durations (ms) between consecutive records of the last traced launch, in
+// barrier order; *count = how many there are (up to cap are written).
+void batch_phase_times(ofea_batch *b, double *ms, int cap, int *count) {
+    *count = 0;
+    if (b->trace_cap == 0) fail(OFEA_ERR_STATE, "batch: tracing is off (ofea_batch_set_trace)");
+    OFEA_CUDA(cudaSetDevice(b->device));
+    std::vector<unsigned long long> t(b->trace_cap);
+    OFEA_CUDA(cudaMemcpyAsync(t.data(), b->trace.p, sizeof(unsigned long long) * t.size(), cudaMemcpyDeviceToHost,
+                              b->stream));
+    OFEA_CUDA(cudaStreamSynchronize(b->stream));
+    int n = 0;
+    while (n + 1 < (int)t.size() && t[n] != 0 && t[n + 1] != 0) {
+        if (ms && n < cap) ms[n] = (double)(t[n + 1] - t[n]) * 1e-6;
+        ++n;
+    }
+    *count = n;
+}
+
 void barrier_probe(ofea_ctx *c, int limit_ms, int *released) {
     DevBuf<GridSync> gs;
     DevBuf<int> out;

@@ -229,6 +229,8 @@ void batch_set_rhs(ofea_batch *b, const double *const *f);
 void batch_get_solution(ofea_batch *b, double *const *u);
 void batch_solve(ofea_batch *b, const ofea_solve_opts &o, ofea_solve_stats *stats);
 void batch_tuning(ofea_batch *b, int method, int *rl, int *threads, int *ctas_per_sm, double *ms_per_iter);
+void batch_set_trace(ofea_batch *b, int max_phases);
+void batch_phase_times(ofea_batch *b, double *ms, int cap, int *count);
 void barrier_probe(ofea_ctx *c, int limit_ms, int *released);
 void learned_begin_dataset(ofea_ctx *c, int max_samples);
 void learned_add_sample(ofea_ctx *c, const double *d_r);

@@ -109,3 +109,30 @@ def test_batched_mixes_element_types(gpu_ctx_factory, oracle):
         K = sp.csc_matrix((val, ri, cp), shape=(c.n, c.n))
         for j in range(F.shape[0]):
             assert np.linalg.norm(F[j] - K @ u[j]) <= 1.0001e-10 * np.linalg.norm(F[j])
+
+
+@pytest.mark.parametrize("method,init,per_iter", [("GPU_MIXED", 8, 10), ("GPU_PCG", 4, 4)])
+def test_batched_phase_trace(gpu_ctx_factory, tmp_path, monkeypatch, method, init, per_iter):
+    # one launch: the init phases, then per iteration every phase but the
+    # last iteration's V-cycle (the loop ends after the convergence check)
+    monkeypatch.setenv("OFEA_TUNE_FILE", str(tmp_path / "tune.json"))
+    vs = variants(gpu_ctx_factory, count=2, nrhs=3)
+    b = ob.Batch([v[0] for v in vs], 3)
+    with pytest.raises(ob.OfeaError):
+        b.phase_times()  # tracing is off
+    b.set_trace(100000)
+    _, st = b.solve([v[3] for v in vs], method=method, rtol=1e-9)
+    assert all(s["status"] == 0 and s["refinements"] == 0 for s in st), st
+    it = max(s["iterations"] for s in st)
+    t = b.phase_times()
+    expect = init + per_iter * it if method == "GPU_PCG" else init + per_iter * (it - 1) + 4
+    assert len(t) == expect
+    assert np.all(t > 0) and t.sum() <= 1e3 * st[0]["seconds"]
+    # a short trace keeps the first phases only
+    b.set_trace(5)
+    b.solve([v[3] for v in vs], method=method, rtol=1e-9)
+    assert len(b.phase_times()) == 5
+    b.set_trace(0)
+    with pytest.raises(ob.OfeaError):
+        b.phase_times()
+    b.close()
