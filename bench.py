@@ -145,11 +145,14 @@ class ClockSampler:
 
 # ------------------------------------------------------ batched reanalysis --
 
-# Algorithmic bytes per (DOF, load case) of one MIXED batched iteration,
-# vectors only (each array counted once per phase): A 28, B 56, residual 12,
-# restriction 4, prolongation 8, post-smoothing 24.
-BATCH_VEC_BYTES_MIXED = 132
-BATCH_VEC_BYTES_PCG64 = 28 + 64  # A (z, p_old, p, q); B (u, p, q, r, z)
+# Algorithmic bytes per (DOF, load case) of one batched iteration, vectors
+# only (each array counted once per phase).  MIXED: A 36 (z FP32, p_old,
+# q_old read; p, q written), B 56 (u, p, q, r read; u, r, b32, x32 written),
+# residual 12, restriction 4, prolongation 8, post-smoothing 24.  PCG64: A 40
+# (z, p_old, q_old read; p, q written), B 56 (u, p, q, r read; u, r, z
+# written).
+BATCH_VEC_BYTES_MIXED = 36 + 56 + 12 + 4 + 8 + 24
+BATCH_VEC_BYTES_PCG64 = 40 + 56
 
 
 def run_batched(ob, mg, local, hbm, steps=2, count=64, nrhs=16, rtol=1e-8, dist=None):

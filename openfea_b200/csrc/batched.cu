@@ -20,8 +20,13 @@
 // BSELL slots in shared memory (cp.async, double-buffered), and its
 // threads take (block row, load case) pairs, JW lanes per row, so each matrix
 // value is read from HBM once for all load cases and every gather of x is one
-// contiguous run of load cases.  Other phases take (aggregate), (coarse row)
-// or (variant, load case) items per warp.
+// contiguous run of load cases.  The restriction takes one aggregate per
+// CTA; other phases take (coarse row) or (variant, load case) items per warp.
+// The outer SpMM multiplies the preconditioned residual z, not p: q = K z +
+// beta q_old equals K p (p = z + beta p_old), and gathering z (FP32 for
+// MIXED) instead of p_old and z cuts the gathered bytes by 3x (MIXED) or 2x
+// (PCG64).  Any drift of q from K p is caught by the true FP64 residual that
+// the host checks after the kernel.
 // Per-(variant, load case) scalars come from per-slice partial sums reduced
 // in a fixed order: results are bitwise reproducible.  Converged load cases
 // stop updating; the kernel ends when none is left or at max_iter.
@@ -647,41 +652,41 @@ __global__ void __launch_bounds__(32 * (NP / RL), batch_min_ctas(32 * (NP / RL),
         // live_cnt[k % 3] counts the load cases still running after iteration k;
         // slot (k + 1) % 3 was last read two barriers ago at least
         if (blockIdx.x == 0 && threadIdx.x == 0) a.live_cnt[(k + 1) % 3] = 0;
-        // A: p = z + beta p_old, q = K64 p, partial p.q
+        // A: p = z + beta p_old, q = K64 z + beta q_old (= K64 p), partial p.q
         for_slices([&](const BVar &B, int v, int gsl, int ls, int row, const bool (&live)[RL], bool any) {
             const int S = B.sl_ptr[ls], W = B.sl_ptr[ls + 1] - S;
             double bt[RL];
 #pragma unroll
             for (int q = 0; q < RL; ++q) bt[q] = live[q] ? a.beta[v * NR + j0 + q] : 0.0;
-            auto pval = [&](long d, double (&o)[RL]) {
-                double po[RL];
-                ldv<double, RL>(pold + d, po);
+            auto zval = [&](long d, double (&o)[RL]) {
                 if (MIXED) {
                     float zf[RL];
                     ldv<float, RL>(zcur + d, zf);
 #pragma unroll
-                    for (int q = 0; q < RL; ++q) o[q] = fma(bt[q], po[q], (double)zf[q]);
+                    for (int q = 0; q < RL; ++q) o[q] = (double)zf[q];
                 } else {
-                    double zd[RL];
-                    ldv<double, RL>(a.z64 + d, zd);
-#pragma unroll
-                    for (int q = 0; q < RL; ++q) o[q] = fma(bt[q], po[q], zd[q]);
+                    ldv<double, RL>(a.z64 + d, o);
                 }
             };
             double y[3][RL];
             spmm_slice<double, double, NP, RL>(st, S, W, B.scols, B.sv64,
-                                       [&](int kk, int c, double (&o)[RL]) { pval(vidx<NP>(B, kk, c, j0), o); }, y);
+                                       [&](int kk, int c, double (&o)[RL]) { zval(vidx<NP>(B, kk, c, j0), o); }, y);
             double ppq[RL] = {};
             if (any && row < B.nfree)
                 for (int c = 0; c < 3; ++c) {
                     const long d = X(B, row, c);
-                    double pn[RL];
-                    pval(d, pn);
-                    stv<double, RL>(pnew + d, pn);
-                    stv<double, RL>(a.q + d, y[c]);
+                    double zn[RL], po[RL], qo[RL], pn[RL], qn[RL];
+                    zval(d, zn);
+                    ldv<double, RL>(pold + d, po);
+                    ldv<double, RL>(a.q + d, qo);
 #pragma unroll
-                    for (int q = 0; q < RL; ++q)
-                        if (live[q]) ppq[q] += pn[q] * y[c][q];
+                    for (int q = 0; q < RL; ++q) {
+                        pn[q] = fma(bt[q], po[q], zn[q]);
+                        qn[q] = bt[q] != 0.0 ? fma(bt[q], qo[q], y[c][q]) : y[c][q];
+                        if (live[q]) ppq[q] += pn[q] * qn[q];
+                    }
+                    stv<double, RL>(pnew + d, pn);
+                    stv<double, RL>(a.q + d, qn);
                 }
             slice_partial<NP, RL>(st, ppq, a.pa, gsl, NR);
         });
