@@ -272,6 +272,36 @@ OFEA_API int ofea_solve_batched(ofea_ctx *const *ctxs, int n_variants, const dou
  * barrier opened).  The context stays usable. */
 OFEA_API int ofea_check_barrier_timeout(ofea_ctx *ctx, int limit_ms, int *released);
 
+/* ---- CA reanalysis -------------------------------------------------------- */
+/* Replaces the combined-approximations reanalysis of the reference:
+ * ca_get_delt_stiffness / ca_build_rom / ca_SVD / ca_solve
+ * (src/ca_analysis.cpp:18-30, 146-250), driven by CAE_process::CA_ReAnalysis
+ * (src/cae.cpp:317-375).  base: the original model, K0 assembled.  modified:
+ * the modified model on the SAME nodes, element list and free numbering, K
+ * assembled: a deleted element has E = 0 there (an added one is in both
+ * meshes, with E = 0 in the base), moved nodes carry their new coordinates.
+ * Then ΔK x = K x - K0 x.  Basis r_0 = u0 (host [n], the base solution; NULL:
+ * solved here), r_i = -K0^-1 ΔK r_(i-1) for 0 < i < n_basis (device solves
+ * with opts), made orthonormal in FP64 (directions whose Gram eigenvalue is
+ * below 1e-13 of the largest are dropped); the reduced system
+ * V^T K V y = V^T f is solved on the host and u = V y.  f: the load (host
+ * [n]; the reference uses the original model's), u: host [n] out.
+ * Differences from the reference: its basis SVD runs in FP32 (here FP64, the
+ * same span), and its moved-element branch reads the old coordinates into
+ * the wrong row (src/ca_analysis.cpp:103-105); here a moved node changes
+ * every element on it, through the modified model's assembly. */
+#define OFEA_CA_MAX_BASIS 32
+typedef struct {
+    int status;
+    int basis_requested;
+    int basis_used;        /* after dropping dependent directions */
+    int solve_iterations;  /* summed over the solves with K0 */
+    double rel_residual;   /* ||f - K u|| / ||f|| of the CA solution on the modified K */
+    double seconds;        /* wall time of the call */
+} ofea_ca_stats;
+OFEA_API int ofea_ca_reanalysis(ofea_ctx *base, ofea_ctx *modified, const double *f, const double *u0,
+                                int n_basis, const ofea_solve_opts *opts, double *u, ofea_ca_stats *stats);
+
 /* ---- measurement ------------------------------------------------------- */
 /* No counterpart in the reference (it only prints clock() spans): times the
  * solver's two per-iteration kernels (A: p update + SpMV + p.q, B: vector

@@ -35,6 +35,17 @@ OFEA_API int ofea_model_material(const ofea_model *m, double *E, double *nu, dou
                         int *has_elastic);
 OFEA_API int ofea_model_cload(const ofea_model *m, int *dof, double *value);
 
+/* The CA change file of the reanalysis (ReadInfo::CA_read_change,
+ * src/data2cae.cpp:520-661): every node of the original model with its
+ * modified coordinates (*nodes_all), the changed elements (*eles_change:
+ * kind 0 deleted, 1 moved, 2 added; etype 0 = C3D4, 1 = C3D8; topo 8 0-based
+ * node ids per change, -1 padded), and each node's id in the modified model
+ * or -1 (*idref2new).  Sizes are always returned; arrays may be NULL (call
+ * once for the sizes, then with arrays of n_nodes*3, n_changes, n_changes,
+ * n_changes*8 and n_nodes entries).  OFEA_ERR_IO on a malformed file. */
+OFEA_API int ofea_ca_info_read(const char *path, int *n_nodes, int *n_changes, double *xyz, int *kind,
+                               int *etype, int *topo, int *node_map);
+
 /* set_BCs::build_free_index (src/set_bc.cpp:20-43): free_map (nd) and the
  * number of free nodes.  Rejects an empty, duplicated or out-of-range fixed
  * set (the reference's loop is undefined there). */

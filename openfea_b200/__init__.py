@@ -54,6 +54,14 @@ class SolveStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class CaStats(ctypes.Structure):
+    _fields_ = [("status", _I), ("basis_requested", _I), ("basis_used", _I), ("solve_iterations", _I),
+                ("rel_residual", _D), ("seconds", _D)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class LearnOpts(ctypes.Structure):
     _fields_ = [("sample_iters", _I), ("sample_every", _I), ("steps", _I), ("batch", _I),
                 ("lr", ctypes.c_float), ("seed", ctypes.c_uint), ("reset", _I)]
@@ -96,6 +104,8 @@ def lib():
         "ofea_solve": (_I, [_P, _P, _P, _I, _P, _P]),
         "ofea_solve_device": (_I, [_P, _P, _P, _P, _P]),
         "ofea_inp_read": (_I, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+        "ofea_ca_info_read": (_I, [ctypes.c_char_p, ctypes.POINTER(_I), ctypes.POINTER(_I), _P, _P, _P, _P, _P]),
+        "ofea_ca_reanalysis": (_I, [_P, _P, _P, _P, _I, _P, _P, _P]),
         "ofea_model_free": (None, [_P]),
         "ofea_model_sizes": (_I, [_P, _P, _P, _P, _P]),
         "ofea_model_arrays": (_I, [_P, _P, _P, _P, _P, _P]),
@@ -451,6 +461,42 @@ def inp_read(path):
                     load_value=val.value)
     finally:
         L.ofea_model_free(m)
+
+
+def ca_info_read(path):
+    """The CA change file (ReadInfo::CA_read_change, src/data2cae.cpp:520-661):
+    modified coordinates of every original node, the changed elements (kind 0
+    deleted, 1 moved, 2 added; etype; 0-based topology, -1 padded) and the
+    original-to-modified node map (-1: removed)."""
+    L = lib()
+    nd, nc = _I(), _I()
+    _check(L.ofea_ca_info_read(str(path).encode(), ctypes.byref(nd), ctypes.byref(nc), None, None, None, None, None),
+           "ofea_ca_info_read")
+    xyz = np.zeros((nd.value, 3))
+    kind = np.zeros(nc.value, dtype=np.int32)
+    et = np.zeros(nc.value, dtype=np.int32)
+    topo = np.zeros((nc.value, 8), dtype=np.int32)
+    nmap = np.zeros(nd.value, dtype=np.int32)
+    _check(L.ofea_ca_info_read(str(path).encode(), ctypes.byref(nd), ctypes.byref(nc), _ptr(xyz), _ptr(kind),
+                               _ptr(et), _ptr(topo), _ptr(nmap)), "ofea_ca_info_read")
+    return dict(xyz=xyz, kind=kind, etype=et, topo=topo, node_map=nmap)
+
+
+def ca_reanalysis(base, modified, f, u0=None, n_basis=4, method="GPU_PCG", rtol=1e-10, **kw):
+    """Combined-approximations reanalysis (ofea_ca_reanalysis): the CA
+    solution of the modified model from n_basis basis vectors built with the
+    base model's K.  Returns (u, stats)."""
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    u = np.zeros(base.n)
+    u0p = None
+    if u0 is not None:
+        u0 = np.ascontiguousarray(u0, dtype=np.float64)
+        u0p = u0.ctypes.data
+    o = solve_opts(method, rtol, **kw)
+    st = CaStats()
+    _check(lib().ofea_ca_reanalysis(base.h, modified.h, f.ctypes.data, u0p, int(n_basis), ctypes.byref(o),
+                                    u.ctypes.data, ctypes.byref(st)), "ofea_ca_reanalysis")
+    return u, st.as_dict()
 
 
 def build_free_index(nd, fix):

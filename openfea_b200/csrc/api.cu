@@ -709,6 +709,29 @@ int ofea_check_barrier_timeout(ofea_ctx *c, int limit_ms, int *released) {
     });
 }
 
+int ofea_ca_reanalysis(ofea_ctx *base, ofea_ctx *mod, const double *f, const double *u0, int n_basis,
+                       const ofea_solve_opts *opts, double *u, ofea_ca_stats *stats) {
+    int rc = guarded([&] {
+        need(base != nullptr && mod != nullptr && f != nullptr && u != nullptr, OFEA_ERR_INVALID_ARG,
+             "NULL argument");
+        need(n_basis >= 1 && n_basis <= OFEA_CA_MAX_BASIS, OFEA_ERR_INVALID_ARG, "n_basis must be 1..32");
+        need(base != mod, OFEA_ERR_INVALID_ARG, "base and modified are the same context");
+        need(base->device == mod->device, OFEA_ERR_INVALID_ARG, "base and modified are on different GPUs");
+        need(base->K_ok && base->sell_ok && mod->K_ok && mod->sell_ok, OFEA_ERR_STATE, "K not assembled");
+        need(base->n == mod->n && base->nnzb == mod->nnzb && base->fm_h == mod->fm_h &&
+                 base->topo_h == mod->topo_h && base->elem_type == mod->elem_type,
+             OFEA_ERR_INVALID_ARG, "base and modified differ in nodes, elements or free numbering");
+        ofea_solve_opts o;
+        if (opts) o = *opts;
+        else ofea_solve_opts_default(&o);
+        check_solve_ready(base, o);
+        use_device(base);
+        ca_reanalysis(base, mod, f, u0, n_basis, o, u, stats);
+    });
+    if (rc != OFEA_OK && stats) stats->status = rc;
+    return rc;
+}
+
 int ofea_profile_solver_kernels(ofea_ctx *c, int method, int reps, double *ms, double *bytes) {
     return guarded([&] {
         need(c != nullptr && ms && bytes && reps > 0, OFEA_ERR_INVALID_ARG, "bad argument");

@@ -240,9 +240,101 @@ void parse(const Lines &L, ofea_model &m) {
     }
 }
 
+// The CA change file (ReadInfo::CA_read_change, src/data2cae.cpp:520-661):
+// "*nodes_all, N" then N lines "x, y, z" (every node of the original model,
+// modified coordinates); "*eles_change, M, type=C3D4|C3D8" then M lines
+// "kind, n1, .., nk" (kind 0 deleted, 1 moved, 2 added; node ids 0-based into
+// the node list), several such blocks allowed; "*End Assembly";
+// "*idref2new, N" then N lines: the node's id in the modified model, or -1.
+struct CaInfo {
+    std::vector<double> xyz;
+    std::vector<int> kind, etype, topo, map;
+};
+
+void parse_ca_info(const Lines &L, CaInfo &ci) {
+    size_t i = 0;
+    auto count_after_comma = [](std::string_view line) {
+        const size_t c = line.find(',');
+        if (c == std::string_view::npos) throw IoError{"missing count"};
+        std::string_view t = line.substr(c + 1);
+        const size_t e = t.find(',');
+        if (e != std::string_view::npos) t = t.substr(0, e);
+        t = strip(t);
+        int v = 0;
+        const auto r = std::from_chars(t.data(), t.data() + t.size(), v);
+        if (r.ec != std::errc() || v < 0) throw IoError{"bad count"};
+        return v;
+    };
+    int nd = -1;
+    for (; i < L.size(); ++i) {
+        std::string_view line = L[i];
+        if (has(line, "*nodes_all")) {
+            nd = count_after_comma(line);
+            ci.xyz.resize(3 * (size_t)nd);
+            for (int k = 0; k < nd; ++k) {
+                if (++i >= L.size() || !parse_doubles(L[i], &ci.xyz[3 * (size_t)k], 3))
+                    throw IoError{"bad node line in *nodes_all"};
+            }
+        } else if (has(line, "*eles_change")) {
+            if (nd < 0) throw IoError{"*eles_change before *nodes_all"};
+            const int m = count_after_comma(line);
+            const size_t eq = line.find('=');
+            if (eq == std::string_view::npos) throw IoError{"*eles_change without type="};
+            std::string_view ty = strip(line.substr(eq + 1));
+            int et, nn;
+            if (ty == "C3D4") et = 0, nn = 4;
+            else if (ty == "C3D8" || ty == "C3D8R") et = 1, nn = 8;
+            else throw IoError{"unknown element type in *eles_change"};
+            for (int k = 0; k < m; ++k) {
+                if (++i >= L.size()) throw IoError{"truncated *eles_change"};
+                int v[9];
+                if (parse_ints(L[i], v, 9) != nn + 1) throw IoError{"bad line in *eles_change"};
+                if (v[0] < 0 || v[0] > 2) throw IoError{"change kind must be 0, 1 or 2"};
+                ci.kind.push_back(v[0]);
+                ci.etype.push_back(et);
+                for (int j = 0; j < 8; ++j) {
+                    const int node = j < nn ? v[j + 1] : -1;
+                    if (j < nn && (node < 0 || node >= nd)) throw IoError{"node id out of range in *eles_change"};
+                    ci.topo.push_back(node);
+                }
+            }
+        } else if (has(line, "*idref2new")) {
+            if (nd < 0) throw IoError{"*idref2new before *nodes_all"};
+            const int m = count_after_comma(line);
+            if (m != nd) throw IoError{"*idref2new count differs from *nodes_all"};
+            ci.map.resize(nd);
+            for (int k = 0; k < nd; ++k) {
+                if (++i >= L.size() || parse_ints(L[i], &ci.map[k], 1) != 1 || ci.map[k] < -1)
+                    throw IoError{"bad line in *idref2new"};
+            }
+        }
+    }
+    if (nd < 0) throw IoError{"no *nodes_all section"};
+    if (ci.map.empty() && nd > 0) throw IoError{"no *idref2new section"};
+}
+
 }  // namespace
 
 extern "C" {
+
+int ofea_ca_info_read(const char *path, int *n_nodes, int *n_changes, double *xyz, int *kind, int *etype,
+                      int *topo, int *node_map) {
+    if (!path || !n_nodes || !n_changes) return OFEA_ERR_INVALID_ARG;
+    try {
+        CaInfo ci;
+        parse_ca_info(read_lines(path), ci);
+        *n_nodes = (int)ci.map.size();
+        *n_changes = (int)ci.kind.size();
+        if (xyz) std::copy(ci.xyz.begin(), ci.xyz.end(), xyz);
+        if (kind) std::copy(ci.kind.begin(), ci.kind.end(), kind);
+        if (etype) std::copy(ci.etype.begin(), ci.etype.end(), etype);
+        if (topo) std::copy(ci.topo.begin(), ci.topo.end(), topo);
+        if (node_map) std::copy(ci.map.begin(), ci.map.end(), node_map);
+        return OFEA_OK;
+    } catch (...) {
+        return OFEA_ERR_IO;
+    }
+}
 
 int ofea_inp_read(const char *path, ofea_model **out) {
     if (!path || !out) return OFEA_ERR_INVALID_ARG;

@@ -236,6 +236,10 @@ void learned_begin_dataset(ofea_ctx *c, int max_samples);
 void learned_add_sample(ofea_ctx *c, const double *d_r);
 void learned_train(ofea_ctx *c, int steps, int batch, float lr, unsigned seed, double *loss0, double *loss1);
 void learned_gradient(ofea_ctx *c, const float *h_x, int B, double *loss, float *h_grad);
+// ca.cu
+constexpr int kCaMaxBasis = OFEA_CA_MAX_BASIS;
+void ca_reanalysis(ofea_ctx *base, ofea_ctx *mod, const double *h_f, const double *h_u0, int nb,
+                   const ofea_solve_opts &o, double *h_u, ofea_ca_stats *stats);
 // noalloc.cu
 void residual_norms_noalloc(ofea_ctx *c, int nrhs, const double *d_f, const double *d_u,
                             double *d_norms);

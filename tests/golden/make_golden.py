@@ -11,6 +11,14 @@ Writes:
                         sample_model/test/implicite_test_C3D4_C3D8.inp)
   cadcae_o_u.npz        u_x, u_y, u_z of the reference's shipped output
                         sample_model/CA/cadcae_o.vtk (E = 2.1e5, nu = 0.3)
+  CA_info.txt.gz        the CA change file of that sample (384 deleted C3D4)
+  cadcae_ca_u.npz       u_x, u_y, u_z of the shipped CA reanalysis output
+                        sample_model/CA/cadcae_ca.vtk (525 nodes of the
+                        modified model)
+
+    python tests/golden/make_golden.py --ca-only [/path/to/OpenFEA]
+
+writes only the two CA fixtures (no oracle/_ref needed).
   ref_elements.npz      element matrices from the reference's element routines
   ref_models.npz        K (CSC) and SuperLU displacements from the reference's
                         own build_CSR / fill_CSR_sparse_mat / solution_api
@@ -49,7 +57,16 @@ def vtk_displacement(path, nd):
     return np.stack(out, axis=1)
 
 
+def ca_fixtures(ref_root):
+    with open(os.path.join(ref_root, "sample_model/CA/CA_info.txt"), "rb") as fi, \
+            gzip.GzipFile(os.path.join(HERE, "CA_info.txt.gz"), "wb", mtime=0) as fo:
+        shutil.copyfileobj(fi, fo)
+    u = vtk_displacement(os.path.join(ref_root, "sample_model/CA/cadcae_ca.vtk"), 525)
+    np.savez_compressed(os.path.join(HERE, "cadcae_ca_u.npz"), u=u, E=2.1e5, nu=0.3, n_basis=4)
+
+
 def main(ref_root):
+    ca_fixtures(ref_root)
     R = Reference()
     for name, rel in SAMPLES.items():
         with open(os.path.join(ref_root, rel), "rb") as fi, gzip.open(os.path.join(HERE, name + ".gz"), "wb") as fo:
@@ -128,4 +145,9 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if a != "--ca-only"]
+    root = args[0] if args else "/root/reference"
+    if "--ca-only" in sys.argv:
+        ca_fixtures(root)
+    else:
+        main(root)
