@@ -4,6 +4,13 @@
 //
 //   ofea_cli -i model.inp [-o out.vtk] [-imp] [-nl] [-solver GPU_PCG|GPU_MIXED|GPU_LEARNED]
 //            [-weights gnn.bin] [-save-weights gnn.bin] [-rtol 1e-8] [-E <Young> -nu <Poisson>]
+//            [-ca CA_info.txt -mesh-m mesh_m.inp [-nbasis 4] [-o-ca out_ca.vtk]]
+//
+// -ca runs the combined-approximations reanalysis after the linear analysis
+// (CAE_process::CA_pre_process + CA_ReAnalysis, src/cae.cpp:303-375): the
+// change file's deleted elements get E = 0 and its coordinates are used for
+// the modified model, which is assembled as a second context; the CA
+// solution goes to the modified model's nodes (mesh_m.inp) and its VTK.
 //
 // GPU_LEARNED loads the learned stage's weights from -weights, or trains it
 // on the model's own K (plain-PCG residuals of a seeded random load) when no
@@ -12,11 +19,13 @@
 // -E/-nu override the file's material (the reference's code_test cases set it
 // in code for models without *Elastic, src/main.cpp:121-135).  The output VTK
 // name defaults to the input name with .vtk (src/cae.cpp:108-110).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -34,10 +43,94 @@ int die(const char *what, int rc) {
     return 2;
 }
 
+// The CA reanalysis of the analysed model (ctx, u) from the change file:
+// the modified model on the same elements and numbering (deleted elements
+// E = 0, the change file's coordinates), assembled as a second context.
+int reanalyse(const std::string &info, const std::string &mesh_m, const std::string &out_ca, int nbasis,
+              ofea_ctx *ctx, int nd, int ne, const std::vector<int> &topo, const std::vector<int> &etype,
+              double E, double nu, const std::vector<int> &fm, const std::vector<double> &f,
+              const std::vector<double> &u, const ofea_solve_opts &opts) {
+    int rc, ndc = 0, nc = 0;
+    if ((rc = ofea_ca_info_read(info.c_str(), &ndc, &nc, nullptr, nullptr, nullptr, nullptr, nullptr)))
+        return die("reading the CA change file", rc);
+    if (ndc != nd) {
+        std::fprintf(stderr, "ofea_cli: the change file has %d nodes, the model %d\n", ndc, nd);
+        return 2;
+    }
+    std::vector<double> xyz_m(3L * nd);
+    std::vector<int> kind(nc), cet(nc), ctopo(8L * nc), node_map(nd);
+    ofea_ca_info_read(info.c_str(), &ndc, &nc, xyz_m.data(), kind.data(), cet.data(), ctopo.data(),
+                      node_map.data());
+    std::printf("the number node set after modifying is: %d\nthe number of changed element is: %d\n", nd, nc);
+    // each changed element among the model's elements (same node set)
+    std::map<std::vector<int>, int> by_nodes;
+    for (int e = 0; e < ne; ++e) {
+        std::vector<int> k;
+        for (int j = 0; j < 8; ++j)
+            if (topo[8L * e + j] > 0) k.push_back(topo[8L * e + j] - 1);
+        std::sort(k.begin(), k.end());
+        by_nodes.emplace(k, e);
+    }
+    std::vector<double> E_m(ne, E);
+    for (int c = 0; c < nc; ++c) {
+        std::vector<int> k;
+        for (int j = 0; j < 8; ++j)
+            if (ctopo[8L * c + j] >= 0) k.push_back(ctopo[8L * c + j]);
+        std::sort(k.begin(), k.end());
+        auto it = by_nodes.find(k);
+        if (it == by_nodes.end()) {
+            std::fprintf(stderr, "ofea_cli: changed element %d is not an element of the model (added elements "
+                                 "must be in the model's mesh)\n", c);
+            return 2;
+        }
+        if (kind[c] == 0) E_m[it->second] = 0.0;
+    }
+    ofea_ctx *cm = nullptr;
+    if ((rc = ofea_ctx_create(&cm, 0))) return die("ofea_ctx_create", rc);
+    if ((rc = ofea_mesh_upload(cm, nd, xyz_m.data(), ne, topo.data(), etype.data(), E_m.data(), E, nu, fm.data())))
+        return die("ofea_mesh_upload (modified model)", rc);
+    int n_chk;
+    long long nnz;
+    if ((rc = ofea_assemble_pattern(cm, &n_chk, &nnz))) return die("ofea_assemble_pattern (modified model)", rc);
+    if ((rc = ofea_assemble_linear(cm))) return die("ofea_assemble_linear (modified model)", rc);
+    std::vector<double> uca(f.size());
+    ofea_ca_stats cs{};
+    if ((rc = ofea_ca_reanalysis(ctx, cm, f.data(), u.data(), nbasis, &opts, uca.data(), &cs)))
+        return die("ofea_ca_reanalysis", rc);
+    std::printf("CA reanalysis: %d of %d basis vectors, %d solver iterations, relative residual %.3e, %.4f s\n",
+                cs.basis_used, cs.basis_requested, cs.solve_iterations, cs.rel_residual, cs.seconds);
+    ofea_ctx_destroy(cm);
+    // reset_ca_displacement (src/post_process.cpp:42-75): onto the modified model's nodes
+    std::vector<double> uf(3L * nd);
+    ofea_full_displacement(nd, fm.data(), uca.data(), uf.data());
+    ofea_model *mm = nullptr;
+    if ((rc = ofea_inp_read(mesh_m.c_str(), &mm))) return die("reading the modified mesh", rc);
+    int ndm, nem, nfm, nlm;
+    ofea_model_sizes(mm, &ndm, &nem, &nfm, &nlm);
+    std::vector<double> xm(3L * ndm);
+    std::vector<int> tm(8L * nem), em(nem), fxm(nfm), lm(nlm);
+    ofea_model_arrays(mm, xm.data(), tm.data(), em.data(), fxm.data(), lm.data());
+    ofea_model_free(mm);
+    std::vector<double> un(3L * ndm, 0.0);
+    for (int i = 0; i < nd; ++i) {
+        const int j = node_map[i];
+        if (j < 0) continue;
+        if (j >= ndm) {
+            std::fprintf(stderr, "ofea_cli: the node map points past the modified mesh's %d nodes\n", ndm);
+            return 2;
+        }
+        for (int c = 0; c < 3; ++c) un[3L * j + c] = uf[3L * i + c];
+    }
+    if ((rc = ofea_write_vtk(out_ca.c_str(), ndm, xm.data(), nem, tm.data(), em.data(), un.data(), 1.0)))
+        return die("writing the CA VTK file", rc);
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
-    std::string in, out, solver = "GPU_PCG", weights, save_weights;
+    std::string in, out, solver = "GPU_PCG", weights, save_weights, ca_info, mesh_m, out_ca;
+    int nbasis = 4;
     bool nl = false;
     double rtol = 1e-8, E_over = -1, nu_over = -1;
     for (int i = 1; i < argc; ++i) {
@@ -52,6 +145,10 @@ int main(int argc, char **argv) {
         else if (a == "-save-weights" && i + 1 < argc) save_weights = argv[++i];
         else if (a == "-E" && i + 1 < argc) E_over = std::atof(argv[++i]);
         else if (a == "-nu" && i + 1 < argc) nu_over = std::atof(argv[++i]);
+        else if (a == "-ca" && i + 1 < argc) ca_info = argv[++i];
+        else if (a == "-mesh-m" && i + 1 < argc) mesh_m = argv[++i];
+        else if (a == "-nbasis" && i + 1 < argc) nbasis = std::atoi(argv[++i]);
+        else if (a == "-o-ca" && i + 1 < argc) out_ca = argv[++i];
         else if (argc == 2) in = a;
         else if (a == "-exp" || a == "-sfem" || a == "-re") {
             std::fprintf(stderr, "ofea_cli: %s is not part of the GPU implicit-static path\n", a.c_str());
@@ -63,6 +160,11 @@ int main(int argc, char **argv) {
         return 2;
     }
     if (out.empty()) out = in.substr(0, in.size() - 4) + ".vtk";
+    if (!ca_info.empty() && (nl || mesh_m.empty())) {
+        std::fprintf(stderr, "ofea_cli: -ca needs -mesh-m and the linear analysis (no -nl)\n");
+        return 2;
+    }
+    if (out_ca.empty()) out_ca = in.substr(0, in.size() - 4) + "_ca.vtk";
     ofea_solve_opts opts;
     ofea_solve_opts_default(&opts);
     opts.rtol = rtol;
@@ -165,6 +267,10 @@ int main(int argc, char **argv) {
     ofea_full_displacement(nd, fm.data(), u.data(), uf.data());
     if ((rc = ofea_write_vtk(out.c_str(), nd, xyz.data(), ne, topo.data(), etype.data(), uf.data(), 1.0)))
         return die("writing the VTK file", rc);
+    if (!ca_info.empty()) {
+        if ((rc = reanalyse(ca_info, mesh_m, out_ca, nbasis, ctx, nd, ne, topo, etype, E, nu, fm, f, u, opts)))
+            return rc;
+    }
     ofea_ctx_destroy(ctx);
     return 0;
 }

@@ -12,13 +12,14 @@ Writes:
   cadcae_o_u.npz        u_x, u_y, u_z of the reference's shipped output
                         sample_model/CA/cadcae_o.vtk (E = 2.1e5, nu = 0.3)
   CA_info.txt.gz        the CA change file of that sample (384 deleted C3D4)
+  mesh_m.inp.gz         the sample's modified mesh (525 nodes, 1,920 C3D4)
   cadcae_ca_u.npz       u_x, u_y, u_z of the shipped CA reanalysis output
                         sample_model/CA/cadcae_ca.vtk (525 nodes of the
                         modified model)
 
     python tests/golden/make_golden.py --ca-only [/path/to/OpenFEA]
 
-writes only the two CA fixtures (no oracle/_ref needed).
+writes only the three CA fixtures (no oracle/_ref needed).
   ref_elements.npz      element matrices from the reference's element routines
   ref_models.npz        K (CSC) and SuperLU displacements from the reference's
                         own build_CSR / fill_CSR_sparse_mat / solution_api
@@ -60,6 +61,9 @@ def vtk_displacement(path, nd):
 def ca_fixtures(ref_root):
     with open(os.path.join(ref_root, "sample_model/CA/CA_info.txt"), "rb") as fi, \
             gzip.GzipFile(os.path.join(HERE, "CA_info.txt.gz"), "wb", mtime=0) as fo:
+        shutil.copyfileobj(fi, fo)
+    with open(os.path.join(ref_root, "sample_model/CA/mesh_m.inp"), "rb") as fi, \
+            gzip.GzipFile(os.path.join(HERE, "mesh_m.inp.gz"), "wb", mtime=0) as fo:
         shutil.copyfileobj(fi, fo)
     u = vtk_displacement(os.path.join(ref_root, "sample_model/CA/cadcae_ca.vtk"), 525)
     np.savez_compressed(os.path.join(HERE, "cadcae_ca_u.npz"), u=u, E=2.1e5, nu=0.3, n_basis=4)

@@ -132,3 +132,27 @@ def test_ca_rejects_bad_arguments(gpu_ctx_factory):
     with pytest.raises(ob.OfeaError) as e:
         ob.ca_reanalysis(base, c3, f, None, n_basis=2)
     assert e.value.code == -1
+
+
+def test_cli_ca_mode_writes_the_modified_model(golden, inp_file, tmp_path):
+    """ofea_cli -ca: the analysis of mesh_o.inp, then the reanalysis from the
+    change file onto mesh_m.inp's nodes; with one basis vector the written
+    field is the reference's shipped cadcae_ca.vtk to its print precision."""
+    import os
+    import subprocess
+    cli = os.path.join(os.path.dirname(ob.__file__), "ofea_cli")
+    ug = golden("cadcae_ca_u.npz")["u"]
+    for nb in (1, 4):
+        out, out_ca = tmp_path / f"o{nb}.vtk", tmp_path / f"ca{nb}.vtk"
+        args = [cli, "-i", inp_file("mesh_o.inp"), "-o", str(out), "-rtol", "1e-10", "-E", "2.1e5", "-nu", "0.3",
+                "-ca", inp_file("CA_info.txt"), "-mesh-m", inp_file("mesh_m.inp"), "-nbasis", str(nb),
+                "-o-ca", str(out_ca)]
+        r = subprocess.run(args, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stdout + r.stderr
+        lines = out_ca.read_text().split("\n")
+        assert "POINTS\t525\tdouble" in lines and any(s_.startswith("CELLS\t1920") for s_ in lines)
+        u = np.stack([np.array([float(x) for x in lines[lines.index(f"SCALARS {c} double 1") + 2:][:525]])
+                      for c in ("u_x", "u_y", "u_z")], axis=1)
+        assert np.all(np.isfinite(u))
+        if nb == 1:
+            assert np.linalg.norm(u - ug) / np.linalg.norm(ug) < 1e-5
