@@ -18,8 +18,15 @@
 // exact FP64 coarse operator, so the FP64 outer iteration keeps the iteration
 // count of an all-FP64 preconditioner.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <numeric>
+#include <thread>
+
+#include <unistd.h>
 
 #include "precond.cuh"
 #include "sell.cuh"
@@ -28,6 +35,81 @@
 namespace ofea {
 
 // ---------------------------------------------------------- aggregation --
+
+// The host geometry below splits its loops into kGeoChunks fixed chunks that
+// run on up to that many threads; partial results are combined in chunk
+// order, so the result does not depend on the number of cores.
+constexpr int kGeoChunks = 16;
+
+// Worker threads for those loops, started on first use and kept (never torn
+// down: process exit ends them).  run(w) calls w on every worker and on the
+// caller and returns when all have returned; calls are serialised.
+class GeoPool {
+public:
+    explicit GeoPool(int workers) : workers_(workers) {
+        for (int t = 0; t < workers; ++t) std::thread([this] { loop(); }).detach();
+    }
+    void run(const std::function<void()> &w) {
+        std::lock_guard<std::mutex> serial(run_mu_);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            work_ = &w;
+            busy_ = workers_;
+            ++gen_;
+        }
+        go_.notify_all();
+        w();
+        std::unique_lock<std::mutex> lk(mu_);
+        done_.wait(lk, [&] { return busy_ == 0; });
+    }
+
+private:
+    void loop() {
+        unsigned seen = 0;
+        for (;;) {
+            const std::function<void()> *w;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                go_.wait(lk, [&] { return gen_ != seen; });
+                seen = gen_;
+                w = work_;
+            }
+            (*w)();
+            std::lock_guard<std::mutex> lk(mu_);
+            if (--busy_ == 0) done_.notify_all();
+        }
+    }
+    std::mutex run_mu_, mu_;
+    std::condition_variable go_, done_;
+    const std::function<void()> *work_ = nullptr;
+    unsigned gen_ = 0;
+    int busy_ = 0, workers_;
+};
+
+// The pool of this process (a forked child inherits the object but not the
+// threads, so it starts its own).
+static GeoPool &geo_pool() {
+    static std::mutex mu;
+    static GeoPool *p = nullptr;
+    static pid_t owner = 0;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!p || owner != getpid()) {
+        p = new GeoPool((int)std::min<unsigned>(kGeoChunks, std::max(1u, std::thread::hardware_concurrency())) - 1);
+        owner = getpid();
+    }
+    return *p;
+}
+
+template <class F>
+static void for_chunks(F f) {
+    std::atomic<int> next(0);
+    const std::function<void()> work = [&] {
+        for (int k; (k = next.fetch_add(1)) < kGeoChunks;) f(k);
+    };
+    geo_pool().run(work);
+}
+
+static inline long chunk_begin(long n, int k) { return n * k / kGeoChunks; }
 
 // Bins the free nodes into the nc[0] x nc[1] x nc[2] cell grid over [lo, lo+ext]
 // and fills C's aggregate arrays (non-empty cells in cell order, nodes in
@@ -38,40 +120,70 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
     const std::vector<double> &X = c->xyz_h;
     const std::vector<int> &fm = c->fm_h;
     std::vector<int> nof(nf);
-    for (int i = 0; i < nd; ++i)
-        if (fm[i] >= 0) nof[fm[i]] = i;
+    for_chunks([&](int k) {
+        for (long i = chunk_begin(nd, k); i < chunk_begin(nd, k + 1); ++i)
+            if (fm[i] >= 0) nof[fm[i]] = (int)i;
+    });
     for (int d = 0; d < 3; ++d) C.nc[d] = nc[d];
     const long ncell = (long)nc[0] * nc[1] * nc[2];
-    std::vector<int> cell_of(nf), cnt(ncell, 0);
-    for (int r = 0; r < nf; ++r) {
-        int node = nof[r], ci[3];
-        for (int d = 0; d < 3; ++d) {
-            ci[d] = ext[d] > 0 ? (int)std::floor((X[3L * node + d] - lo[d]) / ext[d] * nc[d]) : 0;
-            ci[d] = std::min(std::max(ci[d], 0), nc[d] - 1);
+    // cell of every free row and per-chunk counts per cell
+    std::vector<int> cell_of(nf);
+    std::vector<std::vector<int>> ccnt(kGeoChunks);
+    for_chunks([&](int k) {
+        std::vector<int> &cnt = ccnt[k];
+        cnt.assign(ncell, 0);
+        for (long r = chunk_begin(nf, k); r < chunk_begin(nf, k + 1); ++r) {
+            const int node = nof[r];
+            int ci[3];
+            for (int d = 0; d < 3; ++d) {
+                ci[d] = ext[d] > 0 ? (int)std::floor((X[3L * node + d] - lo[d]) / ext[d] * nc[d]) : 0;
+                ci[d] = std::min(std::max(ci[d], 0), nc[d] - 1);
+            }
+            cell_of[r] = (ci[0] * nc[1] + ci[1]) * nc[2] + ci[2];
+            cnt[cell_of[r]]++;
         }
-        cell_of[r] = (ci[0] * nc[1] + ci[1]) * nc[2] + ci[2];
-        cnt[cell_of[r]]++;
-    }
+    });
     std::vector<int> cell_agg(ncell, -1), agg_cell3;
+    std::vector<int> ptr(1, 0);
     int na = 0;
-    for (long k = 0; k < ncell; ++k)
-        if (cnt[k] > 0) {
-            cell_agg[k] = na++;
-            agg_cell3.push_back((int)(k / ((long)nc[1] * nc[2])));
-            agg_cell3.push_back((int)((k / nc[2]) % nc[1]));
-            agg_cell3.push_back((int)(k % nc[2]));
+    for (long cl = 0; cl < ncell; ++cl) {
+        int tot = 0;
+        for (int k = 0; k < kGeoChunks; ++k) tot += ccnt[k][cl];
+        if (tot > 0) {
+            cell_agg[cl] = na++;
+            agg_cell3.push_back((int)(cl / ((long)nc[1] * nc[2])));
+            agg_cell3.push_back((int)((cl / nc[2]) % nc[1]));
+            agg_cell3.push_back((int)(cl % nc[2]));
+            ptr.push_back(ptr.back() + tot);
         }
-    std::vector<int> agg_of(nf), ptr(na + 1, 0), nodes(nf);
-    for (int r = 0; r < nf; ++r) {
-        agg_of[r] = cell_agg[cell_of[r]];
-        ptr[agg_of[r] + 1]++;
     }
-    for (int a = 0; a < na; ++a) ptr[a + 1] += ptr[a];
-    std::vector<int> cur(ptr.begin(), ptr.end() - 1);
-    for (int r = 0; r < nf; ++r) nodes[cur[agg_of[r]]++] = r;  // ascending within each aggregate
+    // chunk k's first slot in aggregate a: ptr[a] + rows of a in chunks < k
+    // (rows stay in ascending order within each aggregate)
+    std::vector<std::vector<int>> cur(kGeoChunks, std::vector<int>(na));
+    for (int a = 0; a < na; ++a) {
+        const long cl = ((long)agg_cell3[3 * a] * nc[1] + agg_cell3[3 * a + 1]) * nc[2] + agg_cell3[3 * a + 2];
+        int o = ptr[a];
+        for (int k = 0; k < kGeoChunks; ++k) {
+            cur[k][a] = o;
+            o += ccnt[k][cl];
+        }
+    }
+    std::vector<int> agg_of(nf), nodes(nf);
+    std::vector<std::vector<double>> csum(kGeoChunks);
+    for_chunks([&](int k) {
+        std::vector<int> &pos = cur[k];
+        std::vector<double> &cs = csum[k];
+        cs.assign(3L * na, 0.0);
+        for (long r = chunk_begin(nf, k); r < chunk_begin(nf, k + 1); ++r) {
+            const int a = cell_agg[cell_of[r]];
+            agg_of[r] = a;
+            nodes[pos[a]++] = (int)r;
+            for (int d = 0; d < 3; ++d) cs[3L * a + d] += X[3L * nof[r] + d];
+        }
+    });
     std::vector<double> cen(3L * na, 0.0);
-    for (int r = 0; r < nf; ++r)
-        for (int d = 0; d < 3; ++d) cen[3L * agg_of[r] + d] += X[3L * nof[r] + d];
+    for (int k = 0; k < kGeoChunks; ++k)
+        for (long j = 0; j < 3L * na; ++j) cen[j] += csum[k][j];
     for (int a = 0; a < na; ++a)
         for (int d = 0; d < 3; ++d) cen[3L * a + d] /= (ptr[a + 1] - ptr[a]);
     double scale = 0;
@@ -115,29 +227,44 @@ void build_aggregation(ofea_ctx *c, int target_nodes) {
     const int nd = c->nd, nf = c->nfree;
     const std::vector<double> &X = c->xyz_h;
     const std::vector<int> &fm = c->fm_h;
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    for (int i = 0; i < nd; ++i)
-        if (fm[i] >= 0)
+    // box of the free nodes and the largest element extent per direction
+    // (cells must be at least 2.5x wider so that every K coupling stays
+    // between neighbouring cells; the nested level, half as wide, then still
+    // spans an element); min and max do not depend on the combining order
+    double clo[kGeoChunks][3], chi[kGeoChunks][3], cem[kGeoChunks][3];
+    for_chunks([&](int k) {
+        double l[3] = {1e300, 1e300, 1e300}, h[3] = {-1e300, -1e300, -1e300}, em[3] = {0, 0, 0};
+        for (long i = chunk_begin(nd, k); i < chunk_begin(nd, k + 1); ++i)
+            if (fm[i] >= 0)
+                for (int d = 0; d < 3; ++d) {
+                    l[d] = std::min(l[d], X[3L * i + d]);
+                    h[d] = std::max(h[d], X[3L * i + d]);
+                }
+        for (long e = chunk_begin(c->ne, k); e < chunk_begin(c->ne, k + 1); ++e) {
+            const int *t = &c->topo_h[8L * e];
+            const int npe = c->elem_type[e] == 1 ? 8 : 4;
             for (int d = 0; d < 3; ++d) {
-                lo[d] = std::min(lo[d], X[3L * i + d]);
-                hi[d] = std::max(hi[d], X[3L * i + d]);
+                double a = 1e300, b = -1e300;
+                for (int q = 0; q < npe; ++q) {
+                    a = std::min(a, X[3L * t[q] + d]);
+                    b = std::max(b, X[3L * t[q] + d]);
+                }
+                em[d] = std::max(em[d], b - a);
             }
-    // largest element extent per direction: cells must be at least 2.5x wider
-    // so that every K coupling stays between neighbouring cells (the nested
-    // level, half as wide, then still spans an element)
-    double emax[3] = {0, 0, 0};
-    for (int e = 0; e < c->ne; ++e) {
-        const int *t = &c->topo_h[8L * e];
-        int npe = c->elem_type[e] == 1 ? 8 : 4;
-        for (int d = 0; d < 3; ++d) {
-            double a = 1e300, b = -1e300;
-            for (int k = 0; k < npe; ++k) {
-                a = std::min(a, X[3L * t[k] + d]);
-                b = std::max(b, X[3L * t[k] + d]);
-            }
-            emax[d] = std::max(emax[d], b - a);
         }
-    }
+        for (int d = 0; d < 3; ++d) {  // written once per chunk (no shared cache lines in the loops)
+            clo[k][d] = l[d];
+            chi[k][d] = h[d];
+            cem[k][d] = em[d];
+        }
+    });
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300}, emax[3] = {0, 0, 0};
+    for (int k = 0; k < kGeoChunks; ++k)
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = std::min(lo[d], clo[k][d]);
+            hi[d] = std::max(hi[d], chi[k][d]);
+            emax[d] = std::max(emax[d], cem[k][d]);
+        }
     double ext[3], vol = 1.0;
     int flat = 0;
     for (int d = 0; d < 3; ++d) {
