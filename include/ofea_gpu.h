@@ -90,9 +90,11 @@ OFEA_API int ofea_ctx_create(ofea_ctx **out, int device);
 OFEA_API int ofea_ctx_destroy(ofea_ctx *ctx);
 /* No counterpart in the reference.  Device memory the library frees is kept
  * per GPU (up to 8 GB) and reused by later allocations of a fitting size, so
- * that a fresh context does not pay cudaMalloc for every buffer again.  This
- * returns the kept blocks to the driver (e.g. before handing the GPU to
- * another allocator). */
+ * that a fresh context does not pay cudaMalloc for every buffer again; large
+ * host blocks (the mesh's host copies, set-up scratch; up to 1 GB) are kept
+ * the same way so that a new context does not fault in fresh pages.  This
+ * returns both to the driver / the C allocator (e.g. before handing the GPU
+ * to another allocator). */
 OFEA_API int ofea_trim_device_memory(void);
 /* Run this context's work on an existing cudaStream_t (NULL: library-owned stream). */
 OFEA_API int ofea_ctx_set_stream(ofea_ctx *ctx, void *cuda_stream);

@@ -8,6 +8,7 @@
 #include <mutex>
 #include <random>
 
+#include "host_pool.cuh"
 #include "ofea_internal.cuh"
 #include "precond.cuh"
 
@@ -146,8 +147,8 @@ int ofea_ctx_set_stream(ofea_ctx *c, void *stream) {
     });
 }
 
-static void split_modulus(ofea_ctx *c, const double *E_elem, double E0, std::vector<double> &E8,
-                          std::vector<double> &E4) {
+static void split_modulus(ofea_ctx *c, const double *E_elem, double E0, HVec<double> &E8,
+                          HVec<double> &E4) {
     E8.assign(c->ne8, E0);
     E4.assign(c->ne4, E0);
     if (E_elem)
@@ -178,26 +179,60 @@ int ofea_mesh_upload(ofea_ctx *c, int nd, const double *xyz, int ne, const int *
         c->nu = nu;
         c->elem_type.assign(etype, etype + ne);
         c->elem_local.resize(ne);
-        std::vector<int> t8, t4;
-        t8.reserve(8L * ne);
-        for (int e = 0; e < ne; ++e) {
-            int t = etype[e];
-            need(t == 0 || t == 1, OFEA_ERR_INVALID_ARG, "element type must be 0 (C3D4) or 1 (C3D8)");
-            int npe = t == 1 ? 8 : 4;
-            auto &dst = t == 1 ? t8 : t4;
-            c->elem_local[e] = (int)(dst.size() / npe);
-            for (int a = 0; a < npe; ++a) {
-                int v = topo[8L * e + a];
-                need(v >= 1 && v <= nd, OFEA_ERR_INVALID_ARG, "node id out of range 1..nd in topo");
-                for (int b = 0; b < a; ++b)
-                    need(topo[8L * e + b] != v, OFEA_ERR_INVALID_ARG, "element repeats a node");
-                dst.push_back(v - 1);  // device connectivity is 0-based
+        // pass 1 (chunks of elements): checks and per-chunk counts by type; the
+        // error reported is the first one in element order
+        struct Scan {
+            long n8 = 0, n4 = 0;
+            const char *why = nullptr;
+        };
+        std::vector<Scan> sc(kHostChunks);
+        host_for_chunks([&](int k) {
+            Scan &r = sc[k];
+            for (long e = chunk_begin(ne, k); e < chunk_begin(ne, k + 1); ++e) {
+                const int t = etype[e];
+                if (t != 0 && t != 1) {
+                    r.why = "element type must be 0 (C3D4) or 1 (C3D8)";
+                    return;
+                }
+                const int npe = t == 1 ? 8 : 4;
+                for (int a = 0; a < npe; ++a) {
+                    const int v = topo[8L * e + a];
+                    if (v < 1 || v > nd) {
+                        r.why = "node id out of range 1..nd in topo";
+                        return;
+                    }
+                    for (int b = 0; b < a; ++b)
+                        if (topo[8L * e + b] == v) {
+                            r.why = "element repeats a node";
+                            return;
+                        }
+                }
+                (t == 1 ? r.n8 : r.n4)++;
             }
+        });
+        std::vector<long> o8(kHostChunks + 1, 0), o4(kHostChunks + 1, 0);
+        for (int k = 0; k < kHostChunks; ++k) {
+            need(sc[k].why == nullptr, OFEA_ERR_INVALID_ARG, sc[k].why);
+            o8[k + 1] = o8[k] + sc[k].n8;
+            o4[k + 1] = o4[k] + sc[k].n4;
         }
-        c->ne8 = (int)(t8.size() / 8);
-        c->ne4 = (int)(t4.size() / 4);
+        // pass 2: 0-based device connectivity per type, element -> position, host copy
+        HVec<int> t8(8L * o8[kHostChunks]), t4(4L * o4[kHostChunks]);
+        c->topo_h.resize(8L * ne);
+        host_for_chunks([&](int k) {
+            long p8 = o8[k], p4 = o4[k];
+            for (long e = chunk_begin(ne, k); e < chunk_begin(ne, k + 1); ++e) {
+                const bool hex = etype[e] == 1;
+                int *dst = hex ? &t8[8 * p8] : &t4[4 * p4];
+                c->elem_local[e] = (int)(hex ? p8++ : p4++);
+                for (int a = 0; a < (hex ? 8 : 4); ++a) dst[a] = topo[8L * e + a] - 1;
+                for (int a = 0; a < 8; ++a) c->topo_h[8L * e + a] = topo[8L * e + a] > 0 ? topo[8L * e + a] - 1 : 0;
+            }
+        });
+        c->ne8 = (int)o8[kHostChunks];
+        c->ne4 = (int)o4[kHostChunks];
         int nfree = 0;
-        std::vector<char> seen(nd, 0);
+        HVec<char> seen(nd, 0);
         for (int i = 0; i < nd; ++i) {
             int f = free_map[i];
             need(f >= -1 && f < nd, OFEA_ERR_INVALID_ARG, "free_map entry out of range");
@@ -209,15 +244,20 @@ int ofea_mesh_upload(ofea_ctx *c, int nd, const double *xyz, int ne, const int *
         }
         for (int i = 0; i < nfree; ++i)
             need(seen[i], OFEA_ERR_INVALID_ARG, "free_map must number free nodes 0..nfree-1");
-        for (long i = 0; i < 3L * nd; ++i)
-            need(std::isfinite(xyz[i]), OFEA_ERR_INVALID_ARG, "non-finite coordinate");
+        std::vector<char> finite(kHostChunks, 1);
+        host_for_chunks([&](int k) {
+            for (long i = chunk_begin(3L * nd, k); i < chunk_begin(3L * nd, k + 1); ++i)
+                if (!std::isfinite(xyz[i])) {
+                    finite[k] = 0;
+                    return;
+                }
+        });
+        for (int k = 0; k < kHostChunks; ++k) need(finite[k] != 0, OFEA_ERR_INVALID_ARG, "non-finite coordinate");
         c->nfree = nfree;
         c->n = 3 * nfree;
         c->xyz_h.assign(xyz, xyz + 3L * nd);
         c->fm_h.assign(free_map, free_map + nd);
-        c->topo_h.assign(8L * ne, 0);
-        for (long i = 0; i < 8L * ne; ++i) c->topo_h[i] = topo[i] > 0 ? topo[i] - 1 : 0;
-        std::vector<double> E8, E4;
+        HVec<double> E8, E4;
         split_modulus(c, E_elem, E0, E8, E4);
         cudaStream_t s = c->stream;
         c->xyz.upload(xyz, 3L * nd, s);
@@ -236,7 +276,7 @@ int ofea_mesh_set_modulus(ofea_ctx *c, const double *E_elem, double E0) {
         need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
         need(c->mesh_ok, OFEA_ERR_STATE, "no mesh uploaded");
         use_device(c);
-        std::vector<double> E8, E4;
+        HVec<double> E8, E4;
         split_modulus(c, E_elem, E0, E8, E4);
         c->E0 = E0;
         c->E8.upload(E8.data(), E8.size(), c->stream);
@@ -392,7 +432,10 @@ int ofea_set_coarse_nodes(ofea_ctx *c, int nodes) {
 }
 
 int ofea_trim_device_memory(void) {
-    return guarded([&] { dev_trim(); });
+    return guarded([&] {
+        dev_trim();
+        host_cache_trim();
+    });
 }
 
 int ofea_precond_reset(ofea_ctx *c) {

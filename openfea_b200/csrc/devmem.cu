@@ -10,9 +10,12 @@
 // rounded (256 B, or 2 MB from 1 MB up) so that contexts of the same problem
 // reuse each other's blocks exactly.  ofea_trim_device_memory returns the
 // cached blocks to the driver.
+#include <cstdlib>
 #include <map>
 #include <mutex>
+#include <new>
 
+#include "host_pool.cuh"
 #include "ofea_internal.cuh"
 
 namespace ofea {
@@ -115,6 +118,80 @@ void dev_trim() {
         kv.second.cached = 0;
     }
     cudaSetDevice(cur);
+}
+
+}  // namespace ofea
+
+// ------------------------------------------------------ host block cache --
+// Large host blocks (host_pool.cuh): kept by rounded size, never returned to
+// the allocator until host_cache_trim(), so that the next context's vectors
+// land on pages that are already mapped.
+namespace ofea {
+namespace {
+
+constexpr std::size_t kHostSmall = 256u << 10, kHostGrain = 64u << 10, kHostCap = 1ull << 30;
+
+struct HostCache {
+    std::mutex mu;
+    std::multimap<std::size_t, void *> free;
+    std::size_t cached = 0;
+};
+
+HostCache &host_cache() {
+    static HostCache *h = new HostCache();  // never destroyed: blocks may be freed during exit
+    return *h;
+}
+
+std::size_t host_round(std::size_t bytes) { return (bytes + kHostGrain - 1) / kHostGrain * kHostGrain; }
+
+}  // namespace
+
+void *host_cache_take(std::size_t bytes) {
+    if (bytes < kHostSmall) {
+        void *p = std::malloc(bytes ? bytes : 1);
+        if (!p) throw std::bad_alloc();
+        return p;
+    }
+    const std::size_t r = host_round(bytes);
+    {
+        HostCache &h = host_cache();
+        std::lock_guard<std::mutex> lock(h.mu);
+        auto it = h.free.find(r);
+        if (it != h.free.end()) {
+            void *p = it->second;
+            h.free.erase(it);
+            h.cached -= r;
+            return p;
+        }
+    }
+    void *p = std::malloc(r);
+    if (!p) throw std::bad_alloc();
+    return p;
+}
+
+void host_cache_give(void *p, std::size_t bytes) {
+    if (!p) return;
+    if (bytes < kHostSmall) {
+        std::free(p);
+        return;
+    }
+    const std::size_t r = host_round(bytes);
+    HostCache &h = host_cache();
+    std::lock_guard<std::mutex> lock(h.mu);
+    if (h.cached + r > kHostCap) {
+        std::free(p);
+        return;
+    }
+    h.free.emplace(r, p);
+    h.cached += r;
+}
+
+void host_cache_trim() {
+    HostCache &h = host_cache();
+    std::lock_guard<std::mutex> lock(h.mu);
+    for (auto &kv : h.free) std::free(kv.second);
+    h.free.clear();
+    h.cached = 0;
 }
 
 }  // namespace ofea

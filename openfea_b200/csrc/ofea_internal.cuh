@@ -23,6 +23,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include "host_pool.cuh"
+
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -170,10 +172,10 @@ struct ofea_ctx {
     // mesh
     int nd = 0, ne = 0, ne8 = 0, ne4 = 0, nfree = 0, n = 0;
     double E0 = 0, nu = 0;
-    std::vector<int> elem_type;    // caller order
-    std::vector<int> elem_local;   // caller element -> index within its type
-    std::vector<double> xyz_h;     // host copies for the coarse-space setup
-    std::vector<int> fm_h, topo_h; // topo_h: ne x 8, 0-based
+    ofea::HVec<int> elem_type;     // caller order
+    ofea::HVec<int> elem_local;    // caller element -> index within its type
+    ofea::HVec<double> xyz_h;      // host copies for the coarse-space setup
+    ofea::HVec<int> fm_h, topo_h;  // topo_h: ne x 8, 0-based
     ofea::DevBuf<double> xyz, E8, E4;
     ofea::DevBuf<int> topo8, topo4, free_map, node_of_free;
     bool mesh_ok = false;

@@ -28,6 +28,7 @@
 
 #include <unistd.h>
 
+#include "host_pool.cuh"
 #include "precond.cuh"
 #include "sell.cuh"
 #include "solver_common.cuh"
@@ -36,17 +37,13 @@ namespace ofea {
 
 // ---------------------------------------------------------- aggregation --
 
-// The host geometry below splits its loops into kGeoChunks fixed chunks that
-// run on up to that many threads; partial results are combined in chunk
-// order, so the result does not depend on the number of cores.
-constexpr int kGeoChunks = 16;
-
-// Worker threads for those loops, started on first use and kept (never torn
-// down: process exit ends them).  run(w) calls w on every worker and on the
-// caller and returns when all have returned; calls are serialised.
-class GeoPool {
+// Worker threads of host_for_chunks (host_pool.cuh), started on first use and
+// kept (never torn down: process exit ends them).  run(w) calls w on every
+// worker and on the caller and returns when all have returned; calls are
+// serialised.
+class HostPool {
 public:
-    explicit GeoPool(int workers) : workers_(workers) {
+    explicit HostPool(int workers) : workers_(workers) {
         for (int t = 0; t < workers; ++t) std::thread([this] { loop(); }).detach();
     }
     void run(const std::function<void()> &w) {
@@ -88,28 +85,25 @@ private:
 
 // The pool of this process (a forked child inherits the object but not the
 // threads, so it starts its own).
-static GeoPool &geo_pool() {
+static HostPool &host_pool() {
     static std::mutex mu;
-    static GeoPool *p = nullptr;
+    static HostPool *p = nullptr;
     static pid_t owner = 0;
     std::lock_guard<std::mutex> lk(mu);
     if (!p || owner != getpid()) {
-        p = new GeoPool((int)std::min<unsigned>(kGeoChunks, std::max(1u, std::thread::hardware_concurrency())) - 1);
+        p = new HostPool((int)std::min<unsigned>(kHostChunks, std::max(1u, std::thread::hardware_concurrency())) - 1);
         owner = getpid();
     }
     return *p;
 }
 
-template <class F>
-static void for_chunks(F f) {
+void host_for_chunks(const std::function<void(int)> &f) {
     std::atomic<int> next(0);
     const std::function<void()> work = [&] {
-        for (int k; (k = next.fetch_add(1)) < kGeoChunks;) f(k);
+        for (int k; (k = next.fetch_add(1)) < kHostChunks;) f(k);
     };
-    geo_pool().run(work);
+    host_pool().run(work);
 }
-
-static inline long chunk_begin(long n, int k) { return n * k / kGeoChunks; }
 
 // Bins the free nodes into the nc[0] x nc[1] x nc[2] cell grid over [lo, lo+ext]
 // and fills C's aggregate arrays (non-empty cells in cell order, nodes in
@@ -117,19 +111,19 @@ static inline long chunk_begin(long n, int k) { return n * k / kGeoChunks; }
 // learned level, the 27-slot neighbour table).
 static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3], const double ext[3]) {
     const int nd = c->nd, nf = c->nfree;
-    const std::vector<double> &X = c->xyz_h;
-    const std::vector<int> &fm = c->fm_h;
-    std::vector<int> nof(nf);
-    for_chunks([&](int k) {
+    const auto &X = c->xyz_h;
+    const auto &fm = c->fm_h;
+    HVec<int> nof(nf);
+    host_for_chunks([&](int k) {
         for (long i = chunk_begin(nd, k); i < chunk_begin(nd, k + 1); ++i)
             if (fm[i] >= 0) nof[fm[i]] = (int)i;
     });
     for (int d = 0; d < 3; ++d) C.nc[d] = nc[d];
     const long ncell = (long)nc[0] * nc[1] * nc[2];
     // cell of every free row and per-chunk counts per cell
-    std::vector<int> cell_of(nf);
-    std::vector<std::vector<int>> ccnt(kGeoChunks);
-    for_chunks([&](int k) {
+    HVec<int> cell_of(nf);
+    std::vector<std::vector<int>> ccnt(kHostChunks);
+    host_for_chunks([&](int k) {
         std::vector<int> &cnt = ccnt[k];
         cnt.assign(ncell, 0);
         for (long r = chunk_begin(nf, k); r < chunk_begin(nf, k + 1); ++r) {
@@ -148,7 +142,7 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
     int na = 0;
     for (long cl = 0; cl < ncell; ++cl) {
         int tot = 0;
-        for (int k = 0; k < kGeoChunks; ++k) tot += ccnt[k][cl];
+        for (int k = 0; k < kHostChunks; ++k) tot += ccnt[k][cl];
         if (tot > 0) {
             cell_agg[cl] = na++;
             agg_cell3.push_back((int)(cl / ((long)nc[1] * nc[2])));
@@ -159,18 +153,18 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
     }
     // chunk k's first slot in aggregate a: ptr[a] + rows of a in chunks < k
     // (rows stay in ascending order within each aggregate)
-    std::vector<std::vector<int>> cur(kGeoChunks, std::vector<int>(na));
+    std::vector<std::vector<int>> cur(kHostChunks, std::vector<int>(na));
     for (int a = 0; a < na; ++a) {
         const long cl = ((long)agg_cell3[3 * a] * nc[1] + agg_cell3[3 * a + 1]) * nc[2] + agg_cell3[3 * a + 2];
         int o = ptr[a];
-        for (int k = 0; k < kGeoChunks; ++k) {
+        for (int k = 0; k < kHostChunks; ++k) {
             cur[k][a] = o;
             o += ccnt[k][cl];
         }
     }
-    std::vector<int> agg_of(nf), nodes(nf);
-    std::vector<std::vector<double>> csum(kGeoChunks);
-    for_chunks([&](int k) {
+    HVec<int> agg_of(nf), nodes(nf);
+    std::vector<std::vector<double>> csum(kHostChunks);
+    host_for_chunks([&](int k) {
         std::vector<int> &pos = cur[k];
         std::vector<double> &cs = csum[k];
         cs.assign(3L * na, 0.0);
@@ -182,7 +176,7 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
         }
     });
     std::vector<double> cen(3L * na, 0.0);
-    for (int k = 0; k < kGeoChunks; ++k)
+    for (int k = 0; k < kHostChunks; ++k)
         for (long j = 0; j < 3L * na; ++j) cen[j] += csum[k][j];
     for (int a = 0; a < na; ++a)
         for (int d = 0; d < 3; ++d) cen[3L * a + d] /= (ptr[a + 1] - ptr[a]);
@@ -225,14 +219,14 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
 void build_aggregation(ofea_ctx *c, int target_nodes) {
     Coarse &C = c->coarse;
     const int nd = c->nd, nf = c->nfree;
-    const std::vector<double> &X = c->xyz_h;
-    const std::vector<int> &fm = c->fm_h;
+    const auto &X = c->xyz_h;
+    const auto &fm = c->fm_h;
     // box of the free nodes and the largest element extent per direction
     // (cells must be at least 2.5x wider so that every K coupling stays
     // between neighbouring cells; the nested level, half as wide, then still
     // spans an element); min and max do not depend on the combining order
-    double clo[kGeoChunks][3], chi[kGeoChunks][3], cem[kGeoChunks][3];
-    for_chunks([&](int k) {
+    double clo[kHostChunks][3], chi[kHostChunks][3], cem[kHostChunks][3];
+    host_for_chunks([&](int k) {
         double l[3] = {1e300, 1e300, 1e300}, h[3] = {-1e300, -1e300, -1e300}, em[3] = {0, 0, 0};
         for (long i = chunk_begin(nd, k); i < chunk_begin(nd, k + 1); ++i)
             if (fm[i] >= 0)
@@ -259,7 +253,7 @@ void build_aggregation(ofea_ctx *c, int target_nodes) {
         }
     });
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300}, emax[3] = {0, 0, 0};
-    for (int k = 0; k < kGeoChunks; ++k)
+    for (int k = 0; k < kHostChunks; ++k)
         for (int d = 0; d < 3; ++d) {
             lo[d] = std::min(lo[d], clo[k][d]);
             hi[d] = std::max(hi[d], chi[k][d]);

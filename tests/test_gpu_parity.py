@@ -280,6 +280,27 @@ def test_bad_uploads_rejected(gpu_ctx_factory):
     fm2[fm2 == 3] = 4
     with pytest.raises(ob.OfeaError):
         ctx.upload(m.xyz, m.topo, m.etype, fm2, m.E0, m.nu)
+    # the checks run over chunks of elements in parallel; the error reported is
+    # still the first one in element order
+    topo = m.topo.copy()
+    topo[-1, 1] = topo[-1, 0]  # last element repeats a node
+    with pytest.raises(ob.OfeaError, match="repeats a node"):
+        ctx.upload(m.xyz, topo, m.etype, fm, m.E0, m.nu)
+    topo[3, 2] = 0  # an earlier element: node id out of range
+    with pytest.raises(ob.OfeaError, match="out of range"):
+        ctx.upload(m.xyz, topo, m.etype, fm, m.E0, m.nu)
+    et = m.etype.copy()
+    et[1] = 2
+    with pytest.raises(ob.OfeaError, match="element type"):
+        ctx.upload(m.xyz, topo, et, fm, m.E0, m.nu)
+    xyz = m.xyz.copy()
+    xyz[-1, 2] = np.nan
+    with pytest.raises(ob.OfeaError, match="non-finite"):
+        ctx.upload(xyz, m.topo, m.etype, fm, m.E0, m.nu)
+    # and a valid mesh after the failures uploads and solves
+    ctx.upload(m.xyz, m.topo, m.etype, fm, m.E0, m.nu)
+    ctx.assemble_pattern()
+    ctx.assemble_linear()
 
 
 @pytest.mark.parametrize("solver", ["GPU_PCG", "GPU_MIXED", "GPU_LEARNED"])
