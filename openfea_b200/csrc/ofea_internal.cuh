@@ -192,7 +192,9 @@ struct ofea_ctx {
     // solver layout of K (sell.cuh): BSELL-32, FP64 and BF16 values
     ofea::DevBuf<int> sl_ptr, scols;
     ofea::DevBuf<double> sv64;
-    ofea::DevBuf<__nv_bfloat16> sv16;  // BF16 copy for the FP32 preconditioner SpMVs
+    ofea::DevBuf<__nv_bfloat16> sv16;  // BF16 copy (plane layout) for the batched solver's V-cycle
+    ofea::DevBuf<int> sl_g;            // slot-group offsets of the grouped BF16 copy (sell.cuh)
+    ofea::DevBuf<__nv_bfloat16> sv16g; // grouped BF16 copy for the single-matrix V-cycle SpMVs
     long long sell_len = 0;
     bool sell_ok = false;
     ofea::Coarse coarse;      // exact coarse level

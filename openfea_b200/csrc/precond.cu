@@ -638,7 +638,7 @@ static void invert_spd(ofea_ctx *c, double *A, int m, int hb) {
 // w = Dinv32 K32 (v * sc), sc = 1/||v|| from the previous partials.
 __global__ void __launch_bounds__(kBlock, 2048 / kBlock) k_power(int nfree, const int *__restrict__ sl_ptr,
                                                   const int *__restrict__ scols,
-                                                  const __nv_bfloat16 *__restrict__ sv16,
+                                                  const int *__restrict__ sl_g, const __nv_bfloat16 *__restrict__ svg,
                                                   const float *__restrict__ Dinv32,
                                                   const float *__restrict__ v, float *__restrict__ w,
                                                   const double *__restrict__ Pin, int Gin,
@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(kBlock, 2048 / kBlock) k_power(int nfree, cons
     double acc = 0.0;
     for_each_sell_row(nfree, sl_ptr, [&](int r, long S, int t, int W) {
         float y[3];
-        sell_row<float, 4>(S, t, W, scols, sv16, [&](int k) { return v[k] * sc; }, y[0], y[1], y[2]);
+        sell_row_g4(S, sl_g[r / kSlice], t, W, scols, svg, [&](int k) { return v[k] * sc; }, y[0], y[1], y[2]);
         float o[3];
         block3_apply(Dinv32 + 9L * r, y, o);
         for (int i = 0; i < 3; ++i) {
@@ -682,7 +682,7 @@ static double estimate_lambda_max(ofea_ctx *c, int steps) {
     k_hash_vec<<<grid_for(c, n, kBlock), kBlock, 0, s>>>(n, v);
     for (int k = 0; k < steps; ++k) {
         double *Pin = C.pp.p + (k & 1) * kMaxGrid, *Pout = C.pp.p + ((k + 1) & 1) * kMaxGrid;
-        k_power<<<G, kBlock, 0, s>>>(c->nfree, c->sl_ptr.p, c->scols.p, c->sv16.p, c->Dinv32.p, v, w,
+        k_power<<<G, kBlock, 0, s>>>(c->nfree, c->sl_ptr.p, c->scols.p, c->sl_g.p, c->sv16g.p, c->Dinv32.p, v, w,
                                      Pin, G, Pout, k == 0);
         std::swap(v, w);
     }
@@ -761,12 +761,12 @@ void setup_coarse(ofea_ctx *c, int target_nodes) {
 // t = b - K32 x (x complete), per row.
 __global__ void __launch_bounds__(kBlock, 2048 / kBlock) k_vc_resid(int nfree, const int *__restrict__ sl_ptr,
                                                      const int *__restrict__ scols,
-                                                     const __nv_bfloat16 *__restrict__ sv16,
+                                                     const int *__restrict__ sl_g, const __nv_bfloat16 *__restrict__ svg,
                                                      const float *__restrict__ b,
                                                      const float *__restrict__ x, float *__restrict__ t) {
     for_each_sell_row(nfree, sl_ptr, [&](int r, long S, int tt, int W) {
         float y[3];
-        sell_row<float, 4>(S, tt, W, scols, sv16, [&](int k) { return x[k]; }, y[0], y[1], y[2]);
+        sell_row_g4(S, sl_g[r / kSlice], tt, W, scols, svg, [&](int k) { return x[k]; }, y[0], y[1], y[2]);
         for (int i = 0; i < 3; ++i) t[3L * r + i] = b[3L * r + i] - y[i];
     });
 }
@@ -862,7 +862,7 @@ void coarse_correct(ofea_ctx *c, const float *t, float *x) {
 
 void vc_resid(ofea_ctx *c, const float *b, const float *x, float *t) {
     k_vc_resid<<<grid_for(c, (c->nfree + 31) / 32, kWarpsPerBlock), kBlock, 0, c->stream>>>(
-        c->nfree, c->sl_ptr.p, c->scols.p, c->sv16.p, b, x, t);
+        c->nfree, c->sl_ptr.p, c->scols.p, c->sl_g.p, c->sv16g.p, b, x, t);
     OFEA_CHECK_LAUNCH();
 }
 

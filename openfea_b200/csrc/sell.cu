@@ -1,5 +1,6 @@
 // Conversion of the assembled block-CSR K into the solver's BSELL-32 layout
-// (sell.cuh), FP64 values and an FP32 copy.  Runs once per assembly.
+// (sell.cuh): FP64 values, a BF16 copy in the same plane layout and a BF16
+// copy grouped by four slots (sell_row_g4).  Runs once per assembly.
 #include <algorithm>
 
 #include "sell.cuh"
@@ -22,7 +23,8 @@ __global__ void k_slice_width(int nfree, const int *__restrict__ rowptr, int *__
 __global__ void k_fill_sell(int nfree, const int *__restrict__ rowptr, const int *__restrict__ cols,
                             const double *__restrict__ Kb, const int *__restrict__ sl_ptr,
                             int *__restrict__ scols, double *__restrict__ sv64,
-                            __nv_bfloat16 *__restrict__ sv16) {
+                            __nv_bfloat16 *__restrict__ sv16, const int *__restrict__ sl_g,
+                            __nv_bfloat16 *__restrict__ svg) {
     const int nslice = (nfree + kSlice - 1) / kSlice;
     for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < (long)nslice * kSlice;
          g += (long)gridDim.x * blockDim.x) {
@@ -32,17 +34,27 @@ __global__ void k_fill_sell(int nfree, const int *__restrict__ rowptr, const int
         const int W = sl_ptr[s + 1] - (int)S;
         const int rb = r < nfree ? rowptr[r] : 0;
         const int deg = r < nfree ? rowptr[r + 1] - rb : 0;
-        for (int k = 0; k < W; ++k) {
+        const long G = sl_g[s];
+        const int Wg = (W + 3) & ~3;
+        for (int k = 0; k < Wg; ++k) {
             const bool real = k < deg;
-            scols[(S + k) * kSlice + t] = real ? cols[rb + k] : (r < nfree ? r : 0);
+            if (k < W) scols[(S + k) * kSlice + t] = real ? cols[rb + k] : (r < nfree ? r : 0);
 #pragma unroll
             for (int e = 0; e < 9; ++e) {
                 double v = real ? Kb[9L * (rb + k) + e] : 0.0;
-                sv64[((S + k) * 9 + e) * kSlice + t] = v;
-                sv16[((S + k) * 9 + e) * kSlice + t] = __double2bfloat16(v);
+                if (k < W) {
+                    sv64[((S + k) * 9 + e) * kSlice + t] = v;
+                    sv16[((S + k) * 9 + e) * kSlice + t] = __double2bfloat16(v);
+                }
+                svg[(((G + (k >> 2)) * 9 + e) * kSlice + t) * 4 + (k & 3)] = __double2bfloat16(v);
             }
         }
     }
+}
+
+__global__ void k_group_width(int nslice, const int *__restrict__ sl_ptr, int *__restrict__ gw) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nslice; s += gridDim.x * blockDim.x)
+        gw[s] = (sl_ptr[s + 1] - sl_ptr[s] + 3) / 4;
 }
 
 void build_sell(ofea_ctx *c) {
@@ -60,8 +72,15 @@ void build_sell(ofea_ctx *c) {
     c->scols.ensure(slots);
     c->sv64.ensure(9 * slots);
     c->sv16.ensure(9 * slots);
+    // slot groups of four per slice for the grouped BF16 copy
+    c->sl_g.ensure((size_t)nslice + 1);
+    k_group_width<<<grid_for(c, nslice, kBlock), kBlock, 0, s>>>(nslice, c->sl_ptr.p, width);
+    OFEA_CHECK_LAUNCH();
+    const long long groups = exclusive_scan(width, c->sl_g.p, nslice, s, width + nslice + 1, tmp_len);
+    c->sv16g.ensure((size_t)std::max<long long>(groups, 1) * 9 * kSlice * 4);
     k_fill_sell<<<grid_for(c, (long)nslice * kSlice, kBlock), kBlock, 0, s>>>(
-        c->nfree, c->rowptr.p, c->cols.p, c->Kb.p, c->sl_ptr.p, c->scols.p, c->sv64.p, c->sv16.p);
+        c->nfree, c->rowptr.p, c->cols.p, c->Kb.p, c->sl_ptr.p, c->scols.p, c->sv64.p, c->sv16.p, c->sl_g.p,
+        c->sv16g.p);
     OFEA_CHECK_LAUNCH();
     c->sell_ok = true;
 }

@@ -65,6 +65,45 @@ __device__ __forceinline__ void sell_row(long S, int t, int W, const int *__rest
     }
 }
 
+// The same row (FP32 arithmetic) from the grouped BF16 copy: slot groups of
+// four, group g of slice s at G_s + g with G_s = sl_g[s]; for group g, plane
+// e and lane t the four slots' values are side by side,
+//   svg[(((G_s + g) * 9 + e) * 32 + t) * 4 + (k % 4)],
+// zero beyond W.  One 4-byte load per plane brings two slots (the plane
+// layout needs two 2-byte loads); the slots are summed in the same order and
+// FMA nesting as sell_row<float, 4>, so the result is the same.
+template <class XF>
+__device__ __forceinline__ void sell_row_g4(long S, long G, int t, int W, const int *__restrict__ scols,
+                                            const __nv_bfloat16 *__restrict__ svg, XF x, float &y0, float &y1,
+                                            float &y2) {
+    y0 = 0.f;
+    y1 = 0.f;
+    y2 = 0.f;
+    const int *cp = scols + S * kSlice + t;
+    const unsigned *vp = reinterpret_cast<const unsigned *>(svg) + (G * 9 * kSlice + t) * 2;
+    for (int k = 0; k < W; k += 2) {  // k even: slots k, k + 1 are half (k / 2) & 1 of group k / 4
+        const int c0 = __ldg(cp + (long)k * kSlice);
+        const bool two = k + 1 < W;
+        const int c1 = two ? __ldg(cp + (long)(k + 1) * kSlice) : 0;
+        unsigned raw[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) raw[e] = __ldg(vp + ((long)(k >> 2) * 9 + e) * kSlice * 2 + ((k >> 1) & 1));
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            if (u == 1 && !two) break;
+            float v[9];
+#pragma unroll
+            for (int e = 0; e < 9; ++e)  // BF16 -> FP32 is exact
+                v[e] = __uint_as_float(u ? (raw[e] & 0xFFFF0000u) : (raw[e] << 16));
+            const int c = u ? c1 : c0;
+            const float x0 = x(3 * c), x1 = x(3 * c + 1), x2 = x(3 * c + 2);
+            y0 = fmaf(v[0], x0, fmaf(v[1], x1, fmaf(v[2], x2, y0)));
+            y1 = fmaf(v[3], x0, fmaf(v[4], x1, fmaf(v[5], x2, y1)));
+            y2 = fmaf(v[6], x0, fmaf(v[7], x1, fmaf(v[8], x2, y2)));
+        }
+    }
+}
+
 // Iterate over this thread's block rows: f(r, S, t, W) for each row r < nfree.
 template <class F>
 __device__ __forceinline__ void for_each_sell_row(int nfree, const int *__restrict__ sl_ptr, F f) {

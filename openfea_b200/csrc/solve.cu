@@ -325,7 +325,7 @@ __global__ void __launch_bounds__(kBlock, kSpmvCtas) k_fcg_init(
 // k = itB (itB = -1 for the initial application).
 __global__ void __launch_bounds__(kBlock, kSpmvCtas) k_fcg_post(
     int nfree, const int *__restrict__ sl_ptr, const int *__restrict__ scols,
-    const __nv_bfloat16 *__restrict__ sv16, const float *__restrict__ Dinv32, float w,
+    const int *__restrict__ sl_g, const __nv_bfloat16 *__restrict__ svg, const float *__restrict__ Dinv32, float w,
     const float *__restrict__ b32, const float *__restrict__ x32, const double *__restrict__ r,
     float *__restrict__ zA, float *__restrict__ zB, Parts P, Flags *fl) {
     __shared__ double sh[kWarpsPerBlock];
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(kBlock, kSpmvCtas) k_fcg_post(
     double prz = 0, przo = 0;
     for_each_sell_row(nfree, sl_ptr, [&](int rw, long S, int t, int W) {
         float y[3], d[3], o[3];
-        sell_row<float, 4>(S, t, W, scols, sv16, [&](int kk) { return x32[kk]; }, y[0], y[1], y[2]);
+        sell_row_g4(S, sl_g[rw / kSlice], t, W, scols, svg, [&](int kk) { return x32[kk]; }, y[0], y[1], y[2]);
         for (int i = 0; i < 3; ++i) d[i] = b32[3L * rw + i] - y[i];
         block3_apply(Dinv32 + 9L * rw, d, o);
         for (int i = 0; i < 3; ++i) {
@@ -563,7 +563,7 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
             vc_resid(c, w.b32.p, w.x32.p, w.t32.p);
             coarse_correct(c, w.t32.p, w.x32.p);
             if (learned) learned_apply(c, w.t32.p, w.x32.p);
-            k_fcg_post<<<G, kBlock, 0, s>>>(nf, c->sl_ptr.p, c->scols.p, c->sv16.p, c->Dinv32.p, wsm, w.b32.p,
+            k_fcg_post<<<G, kBlock, 0, s>>>(nf, c->sl_ptr.p, c->scols.p, c->sl_g.p, c->sv16g.p, c->Dinv32.p, wsm, w.b32.p,
                                             w.x32.p, w.r.p, w.z32a.p, w.z32b.p, ws.P, ws.fl);
             OFEA_CHECK_LAUNCH();
             launches += 6;
@@ -576,7 +576,7 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
                     vc_resid(c, w.b32.p, w.x32.p, w.t32.p);
                     coarse_correct(c, w.t32.p, w.x32.p);
                     if (learned) learned_apply(c, w.t32.p, w.x32.p);
-                    k_fcg_post<<<G, kBlock, 0, s>>>(nf, c->sl_ptr.p, c->scols.p, c->sv16.p, c->Dinv32.p, wsm,
+                    k_fcg_post<<<G, kBlock, 0, s>>>(nf, c->sl_ptr.p, c->scols.p, c->sl_g.p, c->sv16g.p, c->Dinv32.p, wsm,
                                                     w.b32.p, w.x32.p, w.r.p, w.z32a.p, w.z32b.p, ws.P, ws.fl);
                 }
                 OFEA_CHECK_LAUNCH();
@@ -679,7 +679,7 @@ void profile_kernels(ofea_ctx *c, int method, int reps, double *ms, double *byte
                                          w.p1.p, w.q.p, ws.P, ws.fl, tol2);
         OFEA_CUDA(cudaEventRecord(e1, s));
         for (int i = 0; i < reps; ++i)
-            k_fcg_post<<<G, kBlock, 0, s>>>(nf, c->sl_ptr.p, c->scols.p, c->sv16.p, c->Dinv32.p, wsm, w.b32.p,
+            k_fcg_post<<<G, kBlock, 0, s>>>(nf, c->sl_ptr.p, c->scols.p, c->sl_g.p, c->sv16g.p, c->Dinv32.p, wsm, w.b32.p,
                                             w.x32.p, w.r.p, w.z32a.p, w.z32b.p, ws.P, ws.fl);
         OFEA_CUDA(cudaEventRecord(e2, s));
         // FP64 K + columns + slice pointers, z (FP32) and p_old read, p_new and q written
