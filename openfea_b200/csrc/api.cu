@@ -93,6 +93,16 @@ void ofea_solve_opts_default(ofea_solve_opts *o) {
     o->use_graph = 1;
 }
 
+// The context's own stream gets the highest priority: while the coarse
+// inversion's side stream runs a large update, the context stream's short
+// serial kernels take the next free SM instead of queueing behind it.
+static void create_ctx_stream(ofea_ctx *c) {
+    int least = 0, greatest = 0;
+    OFEA_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    OFEA_CUDA(cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, greatest));
+    c->own_stream = true;
+}
+
 int ofea_ctx_create(ofea_ctx **out, int device) {
     return guarded([&] {
         need(out != nullptr, OFEA_ERR_INVALID_ARG, "out is NULL");
@@ -109,8 +119,7 @@ int ofea_ctx_create(ofea_ctx **out, int device) {
         try {
             OFEA_CUDA(cudaSetDevice(device));
             OFEA_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
-            OFEA_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-            c->own_stream = true;
+            create_ctx_stream(c);
             c->err_flag.ensure(4);
             c->herr.ensure(4);
         } catch (...) {
@@ -126,6 +135,10 @@ int ofea_ctx_destroy(ofea_ctx *c) {
         if (!c) return;
         cudaSetDevice(c->device);
         if (c->stream) cudaStreamSynchronize(c->stream);
+        if (c->side_stream) {
+            cudaStreamSynchronize(c->side_stream);
+            cudaStreamDestroy(c->side_stream);
+        }
         if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
         delete c;
     });
@@ -141,8 +154,7 @@ int ofea_ctx_set_stream(ofea_ctx *c, void *stream) {
             c->stream = (cudaStream_t)stream;
             c->own_stream = false;
         } else {
-            OFEA_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-            c->own_stream = true;
+            create_ctx_stream(c);
         }
     });
 }

@@ -169,6 +169,7 @@ struct ofea_ctx {
     int num_sms = 148;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaStream_t side_stream = nullptr;  // second stream of the coarse inversion's lookahead (owned)
     // mesh
     int nd = 0, ne = 0, ne8 = 0, ne4 = 0, nfree = 0, n = 0;
     double E0 = 0, nu = 0;

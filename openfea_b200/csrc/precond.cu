@@ -556,12 +556,30 @@ __global__ void __launch_bounds__(256) k_gj_rows(int m, int lim, int j0, int bb,
 
 // Rank-bb update of the outside block: A_ik -= P_i . A_{J,k}, 64 x 64 tiles,
 // 256 threads with 4 x 4 outputs each; dynamic shared memory (66 KB).
+// mode 0: every tile (2D grid); 2: every tile outside tile row and column
+// `cross` (the next panel's rows and columns; 2D grid); 1: only those, on a
+// 1D grid of 2 nt - 1 blocks (nt tiles per side): row `cross` first, then
+// column `cross` without the shared tile.
 __global__ void __launch_bounds__(256) k_gj_update(int m, int lim, int j0, int bb, double *__restrict__ A,
-                                                   const double *__restrict__ P) {
+                                                   const double *__restrict__ P, int mode, int cross) {
     extern __shared__ double smem[];
     double (*sP)[kGJ + 1] = reinterpret_cast<double (*)[kGJ + 1]>(smem);             // [64][65]
     double (*sR)[64 + 1] = reinterpret_cast<double (*)[64 + 1]>(smem + 64 * (kGJ + 1));  // [64][65]
-    const int i0 = blockIdx.y * 64, k0 = blockIdx.x * 64;
+    int ty = blockIdx.y, tx = blockIdx.x;
+    if (mode == 1) {
+        const int nt = (lim + 63) / 64, b = blockIdx.x;
+        if (b < nt) {
+            ty = cross;
+            tx = b;
+        } else {
+            const int q = b - nt;
+            ty = q < cross ? q : q + 1;
+            tx = cross;
+        }
+    } else if (mode == 2 && (ty == cross || tx == cross)) {
+        return;
+    }
+    const int i0 = ty * 64, k0 = tx * 64;
     if (i0 >= j0 && i0 + 64 <= j0 + bb) return;  // every row of the tile is in J: nothing to update
     const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
     for (int v = threadIdx.x; v < 64 * kGJ; v += 256) {
@@ -611,26 +629,55 @@ __global__ void k_round_f32(long n, const double *__restrict__ a, float *__restr
 // (their entries in the panel's rows and columns are zero), so every step
 // works on the leading (j0 + bb + hb)^2 window only: about a third of the
 // dense work for a narrow band.
+//
+// Lookahead: of panel J's update only the next panel's rows and columns (the
+// "cross") are needed by the next panel's diagonal, column and row steps, and
+// those steps touch neither the rest of J's update nor its column panel P.
+// So the update runs in two launches, the cross on the context's stream and
+// the rest on a side stream, where it overlaps the next panel's three
+// serial steps; P alternates between two buffers.  Every entry gets the
+// same arithmetic as in order, so the inverse is the same.
 static void invert_spd(ofea_ctx *c, double *A, int m, int hb) {
     Coarse &C = c->coarse;
     cudaStream_t s = c->stream;
+    if (!c->side_stream) OFEA_CUDA(cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking));
+    cudaStream_t s2 = c->side_stream;
     C.S.ensure(kGJ * kGJ);
-    C.P.ensure((size_t)m * kGJ);
+    C.P.ensure(2 * (size_t)m * kGJ);
     C.diag0.ensure(m);
     k_diag_of<<<grid_for(c, m, kBlock), kBlock, 0, s>>>(m, A, C.diag0.p);
     OFEA_CHECK_LAUNCH();
     const size_t upd_smem = sizeof(double) * (64 * (kGJ + 1) + kGJ * 65);
     OFEA_CUDA(cudaFuncSetAttribute(k_gj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem));
-    for (int j0 = 0; j0 < m; j0 += kGJ) {
+    cudaEvent_t cross_done = nullptr, rest_done = nullptr;
+    OFEA_CUDA(cudaEventCreateWithFlags(&cross_done, cudaEventDisableTiming));
+    OFEA_CUDA(cudaEventCreateWithFlags(&rest_done, cudaEventDisableTiming));
+    bool rest_pending = false;
+    for (int j0 = 0, it = 0; j0 < m; j0 += kGJ, ++it) {
         const int bb = std::min(kGJ, m - j0);
         const int lim = (int)std::min<long>(m, (long)j0 + bb + hb);
         dim3 tiles((lim + 63) / 64, (lim + 63) / 64);
+        double *P = C.P.p + (size_t)(it & 1) * m * kGJ;
         k_gj_diag<<<1, 1024, 0, s>>>(m, j0, bb, A, C.S.p, C.diag0.p);
-        k_gj_panel<<<grid_for(c, (long)lim * 32, 256), 256, 0, s>>>(m, lim, j0, bb, A, C.S.p, C.P.p);
+        k_gj_panel<<<grid_for(c, (long)lim * 32, 256), 256, 0, s>>>(m, lim, j0, bb, A, C.S.p, P);
         k_gj_rows<<<std::max(1, std::min((lim + 31) / 32, c->num_sms * 4)), 256, 0, s>>>(m, lim, j0, bb, A, C.S.p);
-        k_gj_update<<<tiles, 256, upd_smem, s>>>(m, lim, j0, bb, A, C.P.p);
+        if (rest_pending) OFEA_CUDA(cudaStreamWaitEvent(s, rest_done, 0));  // the previous panel's update is complete
+        if (j0 + bb < m) {
+            const int cross = (j0 + bb) / 64;
+            k_gj_update<<<2 * tiles.x - 1, 256, upd_smem, s>>>(m, lim, j0, bb, A, P, 1, cross);
+            OFEA_CUDA(cudaEventRecord(cross_done, s));
+            OFEA_CUDA(cudaStreamWaitEvent(s2, cross_done, 0));
+            k_gj_update<<<tiles, 256, upd_smem, s2>>>(m, lim, j0, bb, A, P, 2, cross);
+            OFEA_CUDA(cudaEventRecord(rest_done, s2));
+            rest_pending = true;
+        } else {
+            k_gj_update<<<tiles, 256, upd_smem, s>>>(m, lim, j0, bb, A, P, 0, -1);
+            rest_pending = false;
+        }
     }
     OFEA_CHECK_LAUNCH();
+    cudaEventDestroy(cross_done);
+    cudaEventDestroy(rest_done);
 }
 
 // ----------------------------------------------------- lambda_max(D^-1 K) --
