@@ -98,7 +98,8 @@ __global__ void __launch_bounds__(kBlock, kSpmvCtas) k_residual64(
     }
 }
 
-// Iteration kernel A.  tol2 = (target ||r||)^2.
+// Iteration kernel A: p = z + beta p_old, q = K p as K z + beta q_old, partial
+// p.q.  tol2 = (target ||r||)^2.
 __global__ void __launch_bounds__(kBlock, kSpmvCtas) k_pcg64_A(
     int nfree, const int *__restrict__ sl_ptr, const int *__restrict__ scols,
     const double *__restrict__ sv64, const double *__restrict__ z, double *__restrict__ pA,
@@ -124,14 +125,14 @@ __global__ void __launch_bounds__(kBlock, kSpmvCtas) k_pcg64_A(
     double ppq = 0;
     for_each_sell_row(nfree, sl_ptr, [&](int rw, long S, int t, int W) {
         double y[3];
-        sell_row<double, 2>(S, t, W, scols, sv64, [&](int kk) { return fma(beta, pold[kk], z[kk]); },
-                            y[0], y[1], y[2]);
+        sell_row<double, 2>(S, t, W, scols, sv64, [&](int kk) { return z[kk]; }, y[0], y[1], y[2]);
         for (int i = 0; i < 3; ++i) {
             const long d = 3L * rw + i;
             const double pn = fma(beta, pold[d], z[d]);
+            const double qn = fma(beta, q[d], y[i]);  // K p = K z + beta K p_old
             pnew[d] = pn;
-            q[d] = y[i];
-            ppq += pn * y[i];
+            q[d] = qn;
+            ppq += pn * qn;
         }
     });
     const double s = block_sum(ppq, sh);
@@ -193,7 +194,9 @@ __global__ void __launch_bounds__(kBlock) k_pcg64_B(
 // --------------------------------------------------- MIXED: FP64 FCG --
 
 // Outer A: beta (Polak-Ribiere) from the post-smoothing partials,
-// p <- double(z_k) + beta p, q = K64 p, partial p.q.
+// p <- double(z_k) + beta p, q = K64 p as K64 z + beta q (the SpMV gathers z
+// alone; drift of q from K p is caught by the FP64 true-residual check),
+// partial p.q.
 __global__ void __launch_bounds__(kBlock, kSpmvCtas) k_fcg_A(
     int nfree, const int *__restrict__ sl_ptr, const int *__restrict__ scols,
     const double *__restrict__ sv64, const float *__restrict__ zA, const float *__restrict__ zB,
@@ -223,14 +226,14 @@ __global__ void __launch_bounds__(kBlock, kSpmvCtas) k_fcg_A(
     double ppq = 0;
     for_each_sell_row(nfree, sl_ptr, [&](int rw, long S, int t, int W) {
         double y[3];
-        sell_row<double, 2>(S, t, W, scols, sv64,
-                            [&](int kk) { return fma(beta, pold[kk], (double)z[kk]); }, y[0], y[1], y[2]);
+        sell_row<double, 2>(S, t, W, scols, sv64, [&](int kk) { return (double)z[kk]; }, y[0], y[1], y[2]);
         for (int i = 0; i < 3; ++i) {
             const long d = 3L * rw + i;
             const double pn = fma(beta, pold[d], (double)z[d]);
+            const double qn = fma(beta, q[d], y[i]);  // K p = K z + beta K p_old
             pnew[d] = pn;
-            q[d] = y[i];
-            ppq += pn * y[i];
+            q[d] = qn;
+            ppq += pn * qn;
         }
     });
     const double s = block_sum(ppq, sh);
@@ -525,6 +528,7 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
     for (int attempt = 0; attempt < 8; ++attempt) {
         OFEA_CUDA(cudaMemsetAsync(w.p0.p, 0, sizeof(double) * n, s));
         OFEA_CUDA(cudaMemsetAsync(w.p1.p, 0, sizeof(double) * n, s));
+        OFEA_CUDA(cudaMemsetAsync(w.q.p, 0, sizeof(double) * n, s));  // q = K p is kept by recurrence
         OFEA_CUDA(cudaMemsetAsync(ws.fl, 0, sizeof(Flags), s));
         if (mixed) {
             OFEA_CUDA(cudaMemsetAsync(w.z32a.p, 0, sizeof(float) * n, s));
@@ -667,8 +671,8 @@ void profile_kernels(ofea_ctx *c, int method, int reps, double *ms, double *byte
         for (int i = 0; i < reps; ++i)
             k_pcg64_B<<<G, kBlock, 0, s>>>(nf, c->Dinv.p, w.p0.p, w.p1.p, w.q.p, u, w.r.p, w.z.p, ws.P, ws.fl);
         OFEA_CUDA(cudaEventRecord(e2, s));
-        // K values + columns + slice pointers, z and p_old read, p_new and q written
-        bytes[0] = 8 * nnzv + 4 * nblk + 4.0 * ((nf + 31) / 32 + 1) + 8.0 * n * 4;
+        // K values + columns + slice pointers, z, p_old and q_old read, p_new and q written
+        bytes[0] = 8 * nnzv + 4 * nblk + 4.0 * ((nf + 31) / 32 + 1) + 8.0 * n * 5;
         bytes[1] = 72.0 * nf + 8.0 * n * 7;  // Dinv; u r/w, r r/w, p, q, z
     } else {
         if (!w.z32a.p || w.z32a.n < (size_t)n) fail(OFEA_ERR_STATE, "run a GPU_MIXED solve first");
@@ -682,8 +686,8 @@ void profile_kernels(ofea_ctx *c, int method, int reps, double *ms, double *byte
             k_fcg_post<<<G, kBlock, 0, s>>>(nf, c->sl_ptr.p, c->scols.p, c->sl_g.p, c->sv16g.p, c->Dinv32.p, wsm, w.b32.p,
                                             w.x32.p, w.r.p, w.z32a.p, w.z32b.p, ws.P, ws.fl);
         OFEA_CUDA(cudaEventRecord(e2, s));
-        // FP64 K + columns + slice pointers, z (FP32) and p_old read, p_new and q written
-        bytes[0] = 8 * nnzv + 4 * nblk + 4.0 * ((nf + 31) / 32 + 1) + 4.0 * n + 8.0 * n * 3;
+        // FP64 K + columns + slice pointers, z (FP32), p_old and q_old read, p_new and q written
+        bytes[0] = 8 * nnzv + 4 * nblk + 4.0 * ((nf + 31) / 32 + 1) + 4.0 * n + 8.0 * n * 4;
         // BF16 K + columns, x32 and b32 read, Dinv32, r (FP64) and z_old read, z_new written
         bytes[1] = 2 * nnzv + 4 * nblk + 4.0 * n * 2 + 36.0 * nf + 8.0 * n + 4.0 * n * 2;
     }
