@@ -519,7 +519,7 @@ def run_ours(args):
 
     # the learned stage: trained once on plain-PCG residuals of a seeded random load
     t_tr = time.perf_counter()
-    train = ctx.learned_train(None, sample_iters=600, sample_every=4, steps=400, batch=16, lr=1e-3, seed=1234)
+    train = ctx.learned_train(None, sample_iters=4000, sample_every=1, steps=800, batch=16, lr=1e-3, seed=1234)
     train["wall_s"] = time.perf_counter() - t_tr
     weights = ctx.learned_weights()
 
