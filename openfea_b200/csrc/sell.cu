@@ -35,19 +35,26 @@ __global__ void k_fill_sell(int nfree, const int *__restrict__ rowptr, const int
         const int rb = r < nfree ? rowptr[r] : 0;
         const int deg = r < nfree ? rowptr[r + 1] - rb : 0;
         const long G = sl_g[s];
-        const int Wg = (W + 3) & ~3;
-        for (int k = 0; k < Wg; ++k) {
-            const bool real = k < deg;
-            if (k < W) scols[(S + k) * kSlice + t] = real ? cols[rb + k] : (r < nfree ? r : 0);
+        uint2 *svg2 = reinterpret_cast<uint2 *>(svg);
+        for (int g = 0; g < (W + 3) / 4; ++g) {
+            unsigned h[9][2] = {};  // the group's four BF16 values per plane, two per word
+            for (int u = 0; u < 4; ++u) {
+                const int k = 4 * g + u;
+                const bool real = k < deg;
+                if (k < W) scols[(S + k) * kSlice + t] = real ? cols[rb + k] : (r < nfree ? r : 0);
 #pragma unroll
-            for (int e = 0; e < 9; ++e) {
-                double v = real ? Kb[9L * (rb + k) + e] : 0.0;
-                if (k < W) {
-                    sv64[((S + k) * 9 + e) * kSlice + t] = v;
-                    sv16[((S + k) * 9 + e) * kSlice + t] = __double2bfloat16(v);
+                for (int e = 0; e < 9; ++e) {
+                    const double v = real ? Kb[9L * (rb + k) + e] : 0.0;
+                    const __nv_bfloat16 bv = __double2bfloat16(v);
+                    if (k < W) {
+                        sv64[((S + k) * 9 + e) * kSlice + t] = v;
+                        sv16[((S + k) * 9 + e) * kSlice + t] = bv;
+                    }
+                    h[e][u >> 1] |= (unsigned)__bfloat16_as_ushort(bv) << (16 * (u & 1));
                 }
-                svg[(((G + (k >> 2)) * 9 + e) * kSlice + t) * 4 + (k & 3)] = __double2bfloat16(v);
             }
+#pragma unroll
+            for (int e = 0; e < 9; ++e) svg2[((G + g) * 9 + e) * kSlice + t] = make_uint2(h[e][0], h[e][1]);
         }
     }
 }
