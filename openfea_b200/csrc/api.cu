@@ -135,10 +135,11 @@ int ofea_ctx_destroy(ofea_ctx *c) {
         if (!c) return;
         cudaSetDevice(c->device);
         if (c->stream) cudaStreamSynchronize(c->stream);
-        if (c->side_stream) {
-            cudaStreamSynchronize(c->side_stream);
-            cudaStreamDestroy(c->side_stream);
-        }
+        for (cudaStream_t x : {c->side_stream, c->aux_stream})
+            if (x) {
+                cudaStreamSynchronize(x);
+                cudaStreamDestroy(x);
+            }
         if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
         delete c;
     });

@@ -170,6 +170,7 @@ struct ofea_ctx {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaStream_t side_stream = nullptr;  // second stream of the coarse inversion's lookahead (owned)
+    cudaStream_t aux_stream = nullptr;   // power iteration beside the coarse inversion (owned)
     // mesh
     int nd = 0, ne = 0, ne8 = 0, ne4 = 0, nfree = 0, n = 0;
     double E0 = 0, nu = 0;

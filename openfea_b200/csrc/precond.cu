@@ -718,26 +718,32 @@ __global__ void k_hash_vec(long n, float *v) {
     }
 }
 
-static double estimate_lambda_max(ofea_ctx *c, int steps) {
-    cudaStream_t s = c->stream;
+// lambda_max(D^-1 K) by `steps` power-iteration SpMVs, enqueued on stream a
+// (buffers allocated first, on the host); lambda_max_read returns it once
+// the context stream has waited for a.
+static void lambda_max_launch(ofea_ctx *c, int steps, cudaStream_t a) {
     const int n = c->n;
     const int G = std::min(kMaxGrid, c->num_sms * (2048 / kBlock));
     Coarse &C = c->coarse;
     C.pw.ensure(2L * std::max(n, 1));
     C.pp.ensure(2L * kMaxGrid);
     float *v = C.pw.p, *w = C.pw.p + n;
-    k_hash_vec<<<grid_for(c, n, kBlock), kBlock, 0, s>>>(n, v);
+    k_hash_vec<<<grid_for(c, n, kBlock), kBlock, 0, a>>>(n, v);
     for (int k = 0; k < steps; ++k) {
         double *Pin = C.pp.p + (k & 1) * kMaxGrid, *Pout = C.pp.p + ((k + 1) & 1) * kMaxGrid;
-        k_power<<<G, kBlock, 0, s>>>(c->nfree, c->sl_ptr.p, c->scols.p, c->sl_g.p, c->sv16g.p, c->Dinv32.p, v, w,
+        k_power<<<G, kBlock, 0, a>>>(c->nfree, c->sl_ptr.p, c->scols.p, c->sl_g.p, c->sv16g.p, c->Dinv32.p, v, w,
                                      Pin, G, Pout, k == 0);
         std::swap(v, w);
     }
     OFEA_CHECK_LAUNCH();
+}
+
+static double lambda_max_read(ofea_ctx *c, int steps) {
+    const int G = std::min(kMaxGrid, c->num_sms * (2048 / kBlock));
     std::vector<double> h(G);
-    OFEA_CUDA(cudaMemcpyAsync(h.data(), C.pp.p + (steps & 1) * kMaxGrid, sizeof(double) * G,
-                              cudaMemcpyDeviceToHost, s));
-    OFEA_CUDA(cudaStreamSynchronize(s));
+    OFEA_CUDA(cudaMemcpyAsync(h.data(), c->coarse.pp.p + (steps & 1) * kMaxGrid, sizeof(double) * G,
+                              cudaMemcpyDeviceToHost, c->stream));
+    OFEA_CUDA(cudaStreamSynchronize(c->stream));
     double nrm2 = 0;
     for (double x : h) nrm2 += x;
     return std::sqrt(nrm2);
@@ -773,14 +779,29 @@ double *coarse_begin_E(ofea_ctx *c) {
     return C.E.p;
 }
 
+// The power iteration for the smoother's interval reads only K and D^-1: it
+// runs on an auxiliary stream while the coarse inverse runs on the context
+// stream (and its side stream), and is joined before its result is read.
 void coarse_finish(ofea_ctx *c) {
     Coarse &C = c->coarse;
     cudaStream_t s = c->stream;
     const int m = C.m;
+    constexpr int kPowerSteps = 10;
+    if (!c->aux_stream) OFEA_CUDA(cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking));
+    cudaEvent_t fork = nullptr, join = nullptr;
+    OFEA_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    OFEA_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    OFEA_CUDA(cudaEventRecord(fork, s));
+    OFEA_CUDA(cudaStreamWaitEvent(c->aux_stream, fork, 0));
+    lambda_max_launch(c, kPowerSteps, c->aux_stream);
+    OFEA_CUDA(cudaEventRecord(join, c->aux_stream));
     invert_spd(c, C.E.p, m, 6 * C.band + 5);
     k_round_f32<<<grid_for(c, (long)m * m, kBlock), kBlock, 0, s>>>((long)m * m, C.E.p, C.Einv32.p);
     OFEA_CHECK_LAUNCH();
-    C.lmax = estimate_lambda_max(c, 10);
+    OFEA_CUDA(cudaStreamWaitEvent(s, join, 0));
+    C.lmax = lambda_max_read(c, kPowerSteps);
+    cudaEventDestroy(fork);
+    cudaEventDestroy(join);
     C.K_ok = true;
 }
 
