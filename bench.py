@@ -278,12 +278,14 @@ def run_learned_simp(ob, mg, local, shape, rtol=1e-8, steps=2):
     }
 
 
-def run_ca(ob, mg, local, shape, n_basis=4, rtol=1e-10):
+def run_ca(ob, mg, local, shape, n_basis=4, rtol=1e-6):
     """The CA reanalysis at full size: the cantilever and a modified model
     whose cavity (x in [0.3, 0.5] L, y and z in the middle half) is softened
     to 1e-3 E (SPD, so the modified model also has an exact solution to
     compare with).  CA from n_basis vectors (basis solves with K0 by MIXED)
-    against a full MIXED solve of the modified model."""
+    against a full MIXED solve of the modified model.  The basis solves stop
+    at rtol: CA's own approximation error (about 1e-4 here) dominates any
+    tighter basis."""
     nx, ny, nz = shape
     m0, ffull = mg.cantilever_large(nx, ny, nz)
     ex = (np.arange(m0.ne) // (ny * nz)) / nx
@@ -302,7 +304,7 @@ def run_ca(ob, mg, local, shape, n_basis=4, rtol=1e-10):
         ctxs.append(c)
     base, mod = ctxs
     f = mg.to_free(ffull, fm)
-    u0, st0 = base.solve(f, method="GPU_MIXED", rtol=rtol)
+    u0, st0 = base.solve(f, method="GPU_MIXED", rtol=1e-10)
     runs = [ob.ca_reanalysis(base, mod, f, u0, n_basis=n_basis, method="GPU_MIXED", rtol=rtol) for _ in range(3)]
     u, cs = min(runs, key=lambda r: r[1]["seconds"])
     full = []
