@@ -274,6 +274,22 @@ OFEA_API int ofea_solve_batched(ofea_ctx *const *ctxs, int n_variants, const dou
  * barrier opened).  The context stays usable. */
 OFEA_API int ofea_check_barrier_timeout(ofea_ctx *ctx, int limit_ms, int *released);
 
+/* ---- stress recovery ------------------------------------------------------ */
+/* Replaces simulation_post::get_cauchy_stress_3d (src/post_process.cpp:79-167):
+ * per element xx, yy, zz, xy, yz, xz and von Mises (the reference's expression,
+ * :103-109), and per node the mean over its incident elements.  u: host [n]
+ * (free DOF; fixed DOF are zero).  OFEA_STRESS_REFERENCE gives the reference's
+ * numbers: for C3D4 the engineering strain B u that its get_stress_node_hammer
+ * returns as stress (src/Elements/C3D4_hammer.cpp:219-226), for C3D8 zero (the
+ * reference computes nothing there and leaves the values unset).
+ * OFEA_STRESS_CAUCHY gives the Cauchy stress D B u (C3D8: the mean over its 8
+ * Gauss points).  elem: host [ne x 7] in caller element order, node: host
+ * [7 x nd] (component-major, as the reference's stress_node_mat_); either may
+ * be NULL.  Needs the pattern (node-to-element incidence). */
+#define OFEA_STRESS_REFERENCE 0
+#define OFEA_STRESS_CAUCHY 1
+OFEA_API int ofea_stress(ofea_ctx *ctx, const double *u, int mode, double *elem, double *node);
+
 /* ---- CA reanalysis -------------------------------------------------------- */
 /* Replaces the combined-approximations reanalysis of the reference:
  * ca_get_delt_stiffness / ca_build_rom / ca_SVD / ca_solve

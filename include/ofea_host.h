@@ -59,10 +59,15 @@ OFEA_API int ofea_build_single_load(int nd, const int *free_map, int nload, cons
 OFEA_API int ofea_full_displacement(int nd, const int *free_map, const double *u, double *u_full);
 /* data_process::export_dis_2_vtk (src/data2vtk.cpp:47-264): legacy ASCII VTK,
  * deformed coordinates (scale * u added), cells (C3D8 as VTK type 11 with the
- * reference's node order, C3D4 as type 10), u_x, u_y, u_z, u_magnitude.
- * Stress fields are not written. */
+ * reference's node order, C3D4 as type 10), u_x, u_y, u_z, u_magnitude. */
 OFEA_API int ofea_write_vtk(const char *path, int nd, const double *xyz, int ne, const int *topo,
                    const int *etype, const double *u_full, double scale);
+/* The same, followed by the reference's nodal stress fields S_xx, S_yy,
+ * S_zz, S_xy, S_yz, S_xz, S_Mises (src/data2vtk.cpp:211-262) from
+ * node_stress [7 x nd] (ofea_stress's node output); NULL writes none. */
+OFEA_API int ofea_write_vtk_stress(const char *path, int nd, const double *xyz, int ne, const int *topo,
+                                   const int *etype, const double *u_full, double scale,
+                                   const double *node_stress);
 
 #ifdef __cplusplus
 }

@@ -115,6 +115,8 @@ def lib():
         "ofea_build_single_load": (_I, [_I, _P, _I, _P, _I, _D, _P]),
         "ofea_full_displacement": (_I, [_I, _P, _P, _P]),
         "ofea_write_vtk": (_I, [ctypes.c_char_p, _I, _P, _I, _P, _P, _P, _D]),
+        "ofea_write_vtk_stress": (_I, [ctypes.c_char_p, _I, _P, _I, _P, _P, _P, _D, _P]),
+        "ofea_stress": (_I, [_P, _P, _I, _P, _P]),
         "ofea_profile_solver_kernels": (_I, [_P, _I, _I, _P, _P]),
         "ofea_precond_reset": (_I, [_P]),
         "ofea_set_coarse_nodes": (_I, [_P, _I]),
@@ -303,6 +305,7 @@ class Context:
         self._keep = (xyz, topo, etype, fm, E)
         _check(lib().ofea_mesh_upload(self.h, xyz.shape[0], _ptr(xyz), topo.shape[0], _ptr(topo),
                                       _ptr(etype), _ptr(E), E0, nu, _ptr(fm)), "ofea_mesh_upload")
+        self.nd, self.ne = int(xyz.shape[0]), int(topo.shape[0])
 
     def upload_mesh(self, mesh, free_map=None):
         fm = free_map if free_map is not None else build_free_index(mesh.nd, mesh.fix)
@@ -327,6 +330,18 @@ class Context:
         fint = np.zeros(self.n)
         _check(lib().ofea_assemble_nl(self.h, _ptr(u), _ptr(fint)), "ofea_assemble_nl")
         return fint
+
+    def stress(self, u, mode="reference"):
+        """Stress recovery (ofea_stress): per element (ne, 7) in caller order and
+        per node (7, nd): xx yy zz xy yz xz von Mises.  mode "reference" gives
+        the reference's numbers (C3D4: engineering strain B u; C3D8: zero),
+        "cauchy" the Cauchy stress D B u."""
+        u = _f64(u)
+        elem = np.zeros((self.ne, 7))
+        node = np.zeros((7, self.nd))
+        m = {"reference": 0, "cauchy": 1}[mode]
+        _check(lib().ofea_stress(self.h, _ptr(u), m, _ptr(elem), _ptr(node)), "ofea_stress")
+        return elem, node
 
     def get_csr(self):
         rp = np.zeros(self.n + 1, dtype=np.int32)
@@ -523,10 +538,17 @@ def full_displacement(nd, free_map, u):
     return out
 
 
-def write_vtk(path, xyz, topo, etype, u_full, scale=1.0):
+def write_vtk(path, xyz, topo, etype, u_full, scale=1.0, node_stress=None):
+    """export_dis_2_vtk (src/data2vtk.cpp:47-264); node_stress (7, nd) adds the
+    S_xx .. S_Mises fields (ofea_write_vtk_stress)."""
     xyz, topo, et, uf = _f64(xyz), _i32(topo), _i32(etype), _f64(u_full)
-    _check(lib().ofea_write_vtk(str(path).encode(), xyz.shape[0], _ptr(xyz), topo.shape[0], _ptr(topo),
-                                _ptr(et), _ptr(uf), scale), "ofea_write_vtk")
+    if node_stress is None:
+        _check(lib().ofea_write_vtk(str(path).encode(), xyz.shape[0], _ptr(xyz), topo.shape[0], _ptr(topo),
+                                    _ptr(et), _ptr(uf), scale), "ofea_write_vtk")
+    else:
+        ns = _f64(node_stress)
+        _check(lib().ofea_write_vtk_stress(str(path).encode(), xyz.shape[0], _ptr(xyz), topo.shape[0], _ptr(topo),
+                                           _ptr(et), _ptr(uf), scale, _ptr(ns)), "ofea_write_vtk_stress")
 
 
 # ------------------------------------------- reference-named entry points --

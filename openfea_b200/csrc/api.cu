@@ -765,6 +765,35 @@ int ofea_check_barrier_timeout(ofea_ctx *c, int limit_ms, int *released) {
     });
 }
 
+int ofea_stress(ofea_ctx *c, const double *u, int mode, double *elem, double *node) {
+    return guarded([&] {
+        need(c != nullptr && u != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
+        need(mode == OFEA_STRESS_REFERENCE || mode == OFEA_STRESS_CAUCHY, OFEA_ERR_INVALID_ARG,
+             "mode must be OFEA_STRESS_REFERENCE or OFEA_STRESS_CAUCHY");
+        need(c->pattern_ok, OFEA_ERR_STATE, "no pattern (ofea_assemble_pattern)");
+        use_device(c);
+        cudaStream_t s = c->stream;
+        DevBuf<double> du, de, dn;
+        du.ensure(std::max(c->n, 1));
+        de.ensure(7L * std::max(c->ne, 1));
+        dn.ensure(7L * c->nd);
+        OFEA_CUDA(cudaMemcpyAsync(du.p, u, sizeof(double) * c->n, cudaMemcpyHostToDevice, s));
+        stress_recovery(c, du.p, mode, de.p, dn.p);
+        if (node) OFEA_CUDA(cudaMemcpyAsync(node, dn.p, sizeof(double) * 7L * c->nd, cudaMemcpyDeviceToHost, s));
+        std::vector<double> h;
+        if (elem) {
+            h.resize(7L * c->ne);
+            OFEA_CUDA(cudaMemcpyAsync(h.data(), de.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s));
+        }
+        OFEA_CUDA(cudaStreamSynchronize(s));
+        if (elem)  // unified id (hexes, then tets) -> caller order
+            for (int e = 0; e < c->ne; ++e) {
+                const long g = c->elem_type[e] == 1 ? c->elem_local[e] : (long)c->ne8 + c->elem_local[e];
+                std::copy(h.begin() + 7 * g, h.begin() + 7 * g + 7, elem + 7L * e);
+            }
+    });
+}
+
 int ofea_ca_reanalysis(ofea_ctx *base, ofea_ctx *mod, const double *f, const double *u0, int n_basis,
                        const ofea_solve_opts *opts, double *u, ofea_ca_stats *stats) {
     int rc = guarded([&] {

@@ -443,6 +443,11 @@ int ofea_full_displacement(int nd, const int *free_map, const double *u, double 
 
 int ofea_write_vtk(const char *path, int nd, const double *xyz, int ne, const int *topo,
                    const int *etype, const double *u_full, double scale) {
+    return ofea_write_vtk_stress(path, nd, xyz, ne, topo, etype, u_full, scale, nullptr);
+}
+
+int ofea_write_vtk_stress(const char *path, int nd, const double *xyz, int ne, const int *topo, const int *etype,
+                          const double *u_full, double scale, const double *node_stress) {
     if (!path || nd <= 0 || ne < 0 || !xyz || !topo || !etype || !u_full) return OFEA_ERR_INVALID_ARG;
     // same header, separators and default 6-significant-digit formatting as
     // the reference writer (src/data2vtk.cpp:56-100, 143-196); the text is
@@ -524,6 +529,20 @@ int ofea_write_vtk(const char *path, int nd, const double *xyz, int ne, const in
         const double *u = u_full + 3L * i;
         put_d(std::sqrt(u[2] * u[2] + u[1] * u[1] + u[0] * u[0]));
         put("\n");
+    }
+    if (node_stress) {  // src/data2vtk.cpp:211-262
+        const char *sn[7] = {"S_xx", "S_yy", "S_zz", "S_xy", "S_yz", "S_xz", "S_Mises"};
+        for (int k = 0; k < 7; ++k) {
+            put("\nSCALARS ");
+            put(sn[k]);
+            put(" double 1\nLOOKUP_TABLE  table");
+            put_i(k + 5);
+            put("\n");
+            for (int i = 0; i < nd; ++i) {
+                put_d(node_stress[(long)k * nd + i]);
+                put("\n");
+            }
+        }
     }
     FILE *f = std::fopen(path, "wb");
     if (!f) return OFEA_ERR_IO;

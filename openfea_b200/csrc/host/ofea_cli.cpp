@@ -5,6 +5,13 @@
 //   ofea_cli -i model.inp [-o out.vtk] [-imp] [-nl] [-solver GPU_PCG|GPU_MIXED|GPU_LEARNED]
 //            [-weights gnn.bin] [-save-weights gnn.bin] [-rtol 1e-8] [-E <Young> -nu <Poisson>]
 //            [-ca CA_info.txt -mesh-m mesh_m.inp [-nbasis 4] [-o-ca out_ca.vtk]]
+//            [-stress reference|cauchy|none]
+//
+// The VTK carries the nodal stress fields S_xx .. S_Mises as the reference's
+// driver writes them (get_cauchy_stress_3d, src/cae.cpp:286-290): by default
+// its own numbers (for C3D4 the engineering strain it labels stress, for C3D8
+// zero); -stress cauchy writes the Cauchy stress instead, -stress none no
+// fields.
 //
 // -ca runs the combined-approximations reanalysis after the linear analysis
 // (CAE_process::CA_pre_process + CA_ReAnalysis, src/cae.cpp:303-375): the
@@ -131,6 +138,7 @@ int reanalyse(const std::string &info, const std::string &mesh_m, const std::str
 int main(int argc, char **argv) {
     std::string in, out, solver = "GPU_PCG", weights, save_weights, ca_info, mesh_m, out_ca;
     int nbasis = 4;
+    std::string stress = "reference";
     bool nl = false;
     double rtol = 1e-8, E_over = -1, nu_over = -1;
     for (int i = 1; i < argc; ++i) {
@@ -149,6 +157,7 @@ int main(int argc, char **argv) {
         else if (a == "-mesh-m" && i + 1 < argc) mesh_m = argv[++i];
         else if (a == "-nbasis" && i + 1 < argc) nbasis = std::atoi(argv[++i]);
         else if (a == "-o-ca" && i + 1 < argc) out_ca = argv[++i];
+        else if (a == "-stress" && i + 1 < argc) stress = argv[++i];
         else if (argc == 2) in = a;
         else if (a == "-exp" || a == "-sfem" || a == "-re") {
             std::fprintf(stderr, "ofea_cli: %s is not part of the GPU implicit-static path\n", a.c_str());
@@ -165,6 +174,10 @@ int main(int argc, char **argv) {
         return 2;
     }
     if (out_ca.empty()) out_ca = in.substr(0, in.size() - 4) + "_ca.vtk";
+    if (stress != "reference" && stress != "cauchy" && stress != "none") {
+        std::fprintf(stderr, "ofea_cli: -stress must be reference, cauchy or none\n");
+        return 2;
+    }
     ofea_solve_opts opts;
     ofea_solve_opts_default(&opts);
     opts.rtol = rtol;
@@ -265,7 +278,15 @@ int main(int argc, char **argv) {
     std::printf("It took %g s to compute full analysis\n", now() - t0);
     std::vector<double> uf(3L * nd);
     ofea_full_displacement(nd, fm.data(), u.data(), uf.data());
-    if ((rc = ofea_write_vtk(out.c_str(), nd, xyz.data(), ne, topo.data(), etype.data(), uf.data(), 1.0)))
+    std::vector<double> node_stress;
+    if (stress != "none") {
+        node_stress.resize(7L * nd);
+        const int mode = stress == "cauchy" ? OFEA_STRESS_CAUCHY : OFEA_STRESS_REFERENCE;
+        if ((rc = ofea_stress(ctx, u.data(), mode, nullptr, node_stress.data()))) return die("ofea_stress", rc);
+        std::printf("the nodal stress has been smoothed.\n");
+    }
+    if ((rc = ofea_write_vtk_stress(out.c_str(), nd, xyz.data(), ne, topo.data(), etype.data(), uf.data(), 1.0,
+                                    node_stress.empty() ? nullptr : node_stress.data())))
         return die("writing the VTK file", rc);
     if (!ca_info.empty()) {
         if ((rc = reanalyse(ca_info, mesh_m, out_ca, nbasis, ctx, nd, ne, topo, etype, E, nu, fm, f, u, opts)))

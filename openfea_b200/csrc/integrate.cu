@@ -535,4 +535,142 @@ void build_block_jacobi(ofea_ctx *c) {
 }
 
 
+// --------------------------------------------------------- stress recovery --
+// simulation_post::get_cauchy_stress_3d (src/post_process.cpp:79-167): seven
+// values per element (xx yy zz xy yz xz and the von Mises expression of
+// :103-109 applied to them), then per node the mean over its incident
+// elements.  Mode 0 is the reference's quantity: for C3D4 the engineering
+// strain B u that its get_stress_node_hammer returns as "stress"
+// (src/Elements/C3D4_hammer.cpp:219-226, the D product commented out); for
+// C3D8, which has no get_stress_node (the base-class stub leaves the values
+// unset), zero.  Mode 1 is the Cauchy stress D B u (C3D8: the mean over its
+// eight Gauss points).  Element values are stored by unified id g (hexes,
+// then tets).
+
+__device__ __forceinline__ void strain_from_grads(const double (*g)[3], const double (*U)[3], int nn, double *e) {
+    for (int k = 0; k < 6; ++k) e[k] = 0.0;
+    for (int a = 0; a < nn; ++a) {
+        e[0] += g[a][0] * U[a][0];
+        e[1] += g[a][1] * U[a][1];
+        e[2] += g[a][2] * U[a][2];
+        e[3] += g[a][1] * U[a][0] + g[a][0] * U[a][1];
+        e[4] += g[a][2] * U[a][1] + g[a][1] * U[a][2];
+        e[5] += g[a][2] * U[a][0] + g[a][0] * U[a][2];
+    }
+}
+
+__device__ __forceinline__ void stress_from_strain(const Lame &L, const double *e, double *s) {
+    const double tr = e[0] + e[1] + e[2];
+    for (int k = 0; k < 3; ++k) s[k] = L.lam * tr + 2.0 * L.mu * e[k];
+    for (int k = 3; k < 6; ++k) s[k] = L.mu * e[k];
+}
+
+__device__ __forceinline__ double mises_ref(const double *s) {
+    return sqrt(0.5 * ((s[0] - s[1]) * (s[0] - s[1]) + (s[1] - s[2]) * (s[1] - s[2]) + (s[2] - s[0]) * (s[2] - s[0]) +
+                       6.0 * (s[3] * s[3] + s[4] * s[4] + s[5] * s[5])));
+}
+
+// Gathers the element's coordinates and displacements (fixed DOF: 0).
+template <int NN>
+__device__ __forceinline__ void gather_elem(const int *t, const double *xyz, const int *free_map, const double *u,
+                                            double (*X)[3], double (*U)[3]) {
+    for (int a = 0; a < NN; ++a) {
+        const int node = t[a], f = free_map[node];
+        for (int d = 0; d < 3; ++d) {
+            X[a][d] = xyz[3L * node + d];
+            U[a][d] = f >= 0 ? u[3L * f + d] : 0.0;
+        }
+    }
+}
+
+__global__ void k_tet_stress(int ne4, int ne8, const int *__restrict__ topo4, const double *__restrict__ xyz,
+                             const double *__restrict__ E4, double nu, const int *__restrict__ free_map,
+                             const double *__restrict__ u, int mode, double *__restrict__ out) {
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < ne4; e += (long)gridDim.x * blockDim.x) {
+        double X[4][3], U[4][3];
+        gather_elem<4>(topo4 + 4 * e, xyz, free_map, u, X, U);
+        // J = dN/d(r,s,t) X with dN rows (-1 1 0 0), (-1 0 1 0), (-1 0 0 1)
+        double J[9];
+        for (int i = 0; i < 3; ++i)
+            for (int d = 0; d < 3; ++d) J[3 * i + d] = X[i + 1][d] - X[0][d];
+        double Ji[9];
+        inv3(J, Ji);
+        double g[4][3];
+        for (int i = 0; i < 3; ++i) {
+            g[0][i] = -(Ji[3 * i] + Ji[3 * i + 1] + Ji[3 * i + 2]);
+            for (int a = 1; a < 4; ++a) g[a][i] = Ji[3 * i + a - 1];
+        }
+        double eps[6], s[7];
+        strain_from_grads(g, U, 4, eps);
+        if (mode == 1) stress_from_strain(lame(E4[e], nu), eps, s);
+        else
+            for (int k = 0; k < 6; ++k) s[k] = eps[k];
+        s[6] = mises_ref(s);
+        for (int k = 0; k < 7; ++k) out[(ne8 + e) * 7 + k] = s[k];
+    }
+}
+
+__global__ void k_hex_stress(int ne8, const int *__restrict__ topo8, const double *__restrict__ xyz,
+                             const double *__restrict__ E8, double nu, const int *__restrict__ free_map,
+                             const double *__restrict__ u, int mode, double *__restrict__ out) {
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < ne8; e += (long)gridDim.x * blockDim.x) {
+        double s[7] = {0, 0, 0, 0, 0, 0, 0};
+        if (mode == 1) {
+            double X[8][3], U[8][3];
+            gather_elem<8>(topo8 + 8 * e, xyz, free_map, u, X, U);
+            const Lame L = lame(E8[e], nu);
+            for (int q = 0; q < 8; ++q) {
+                const double *dN = c_hex_dN + q * 24;
+                double J[9];
+                for (int i = 0; i < 3; ++i)
+                    for (int d = 0; d < 3; ++d) {
+                        double v = 0;
+                        for (int b = 0; b < 8; ++b) v += dN[i * 8 + b] * X[b][d];
+                        J[3 * i + d] = v;
+                    }
+                double Ji[9];
+                inv3(J, Ji);
+                double g[8][3];
+                for (int a = 0; a < 8; ++a)
+                    for (int i = 0; i < 3; ++i)
+                        g[a][i] = Ji[3 * i] * dN[a] + Ji[3 * i + 1] * dN[8 + a] + Ji[3 * i + 2] * dN[16 + a];
+                double eps[6], sq[6];
+                strain_from_grads(g, U, 8, eps);
+                stress_from_strain(L, eps, sq);
+                for (int k = 0; k < 6; ++k) s[k] += 0.125 * sq[k];
+            }
+            s[6] = mises_ref(s);
+        }
+        for (int k = 0; k < 7; ++k) out[e * 7 + k] = s[k];
+    }
+}
+
+// node[k * nd + i] = mean over node i's incident elements (ascending g) of
+// their value k; 0 for a node on no element.
+__global__ void k_node_mean(int nd, const int *__restrict__ inc_ptr, const int *__restrict__ inc,
+                            const double *__restrict__ elem, double *__restrict__ node) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nd; i += (long)gridDim.x * blockDim.x) {
+        const int b = inc_ptr[i], cnt = inc_ptr[i + 1] - b;
+        double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+        for (int j = 0; j < cnt; ++j) {
+            const long g = inc[b + j] >> 3;
+            for (int k = 0; k < 7; ++k) acc[k] += elem[g * 7 + k];
+        }
+        for (int k = 0; k < 7; ++k) node[k * (long)nd + i] = cnt > 0 ? acc[k] / cnt : 0.0;
+    }
+}
+
+void stress_recovery(ofea_ctx *c, const double *d_u, int mode, double *d_elem, double *d_node) {
+    cudaStream_t s = c->stream;
+    upload_hex_table();
+    if (c->ne8 > 0)
+        k_hex_stress<<<grid_for(c, c->ne8, kBlock), kBlock, 0, s>>>(c->ne8, c->topo8.p, c->xyz.p, c->E8.p, c->nu,
+                                                                     c->free_map.p, d_u, mode, d_elem);
+    if (c->ne4 > 0)
+        k_tet_stress<<<grid_for(c, c->ne4, kBlock), kBlock, 0, s>>>(c->ne4, c->ne8, c->topo4.p, c->xyz.p, c->E4.p,
+                                                                     c->nu, c->free_map.p, d_u, mode, d_elem);
+    k_node_mean<<<grid_for(c, c->nd, kBlock), kBlock, 0, s>>>(c->nd, c->inc_ptr.p, c->inc.p, d_elem, d_node);
+    OFEA_CHECK_LAUNCH();
+}
+
 }  // namespace ofea

@@ -216,6 +216,7 @@ void build_pattern(ofea_ctx *c);
 void assemble_linear(ofea_ctx *c);
 void assemble_nl(ofea_ctx *c, const double *d_u, double *d_fint);
 void build_block_jacobi(ofea_ctx *c);
+void stress_recovery(ofea_ctx *c, const double *d_u, int mode, double *d_elem, double *d_node);
 // sell.cu
 void build_sell(ofea_ctx *c);
 // solve.cu

@@ -13,13 +13,15 @@ Writes:
                         sample_model/CA/cadcae_o.vtk (E = 2.1e5, nu = 0.3)
   CA_info.txt.gz        the CA change file of that sample (384 deleted C3D4)
   mesh_m.inp.gz         the sample's modified mesh (525 nodes, 1,920 C3D4)
+  cadcae_o_stress.npz   S_xx .. S_Mises of the shipped sample_model/CA/cadcae_o.vtk
+                        (the reference's nodal stress recovery, 625 nodes)
   cadcae_ca_u.npz       u_x, u_y, u_z of the shipped CA reanalysis output
                         sample_model/CA/cadcae_ca.vtk (525 nodes of the
                         modified model)
 
     python tests/golden/make_golden.py --ca-only [/path/to/OpenFEA]
 
-writes only the three CA fixtures (no oracle/_ref needed).
+writes only the sample_model/CA fixtures (no oracle/_ref needed).
   ref_elements.npz      element matrices from the reference's element routines
   ref_models.npz        K (CSC) and SuperLU displacements from the reference's
                         own build_CSR / fill_CSR_sparse_mat / solution_api
@@ -58,7 +60,19 @@ def vtk_displacement(path, nd):
     return np.stack(out, axis=1)
 
 
+def vtk_fields(path, names, nd):
+    lines = open(path).read().split("\n")
+    out = []
+    for name in names:
+        i = [k for k, s in enumerate(lines) if s.startswith("SCALARS " + name + " ")][0]
+        out.append(np.array([float(x) for x in lines[i + 2:i + 2 + nd]]))
+    return np.stack(out)
+
+
 def ca_fixtures(ref_root):
+    S = vtk_fields(os.path.join(ref_root, "sample_model/CA/cadcae_o.vtk"),
+                   ["S_xx", "S_yy", "S_zz", "S_xy", "S_yz", "S_xz", "S_Mises"], 625)
+    np.savez_compressed(os.path.join(HERE, "cadcae_o_stress.npz"), S=S, E=2.1e5, nu=0.3)
     with open(os.path.join(ref_root, "sample_model/CA/CA_info.txt"), "rb") as fi, \
             gzip.GzipFile(os.path.join(HERE, "CA_info.txt.gz"), "wb", mtime=0) as fo:
         shutil.copyfileobj(fi, fo)
