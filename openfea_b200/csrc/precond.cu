@@ -321,7 +321,10 @@ __global__ void __launch_bounds__(kGW * 32) k_galerkin_blocks(
     const int *__restrict__ agg_cell, const int *__restrict__ node_of_free, const double *__restrict__ xyz,
     const double *__restrict__ centroid, double inv_scale, const int *__restrict__ rowptr,
     const int *__restrict__ cols, const double *__restrict__ Kb, double *__restrict__ Eb, int *__restrict__ err) {
-    __shared__ double acc[kGW][27 * 36];
+    extern __shared__ double gsm[];
+    double (*acc)[27 * 36] = reinterpret_cast<double (*)[27 * 36]>(gsm);                  // [kGW][27 * 36]
+    double (*stage)[32][18] = reinterpret_cast<double (*)[32][18]>(gsm + kGW * 27 * 36);  // [kGW][32][18]
+    __shared__ unsigned smask[kGW][32];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int I = blockIdx.x; I < na; I += gridDim.x) {
         for (int v = threadIdx.x; v < kGW * 27 * 36; v += blockDim.x) (&acc[0][0])[v] = 0.0;
@@ -380,16 +383,32 @@ __global__ void __launch_bounds__(kGW * 32) k_galerkin_blocks(
                         W[e] = x;
                     }
                 } else {
+                    // several slots: the lanes' values go to shared memory, the
+                    // (group, component) sums are spread over the lanes, each
+                    // summed in ascending lane order and written back into its
+                    // leader's row (groups are disjoint, so no other sum reads it)
 #pragma unroll
-                    for (int e = 0; e < 18; ++e) W[e] = 0.0;
-                    for (int t = 0; t < 32; ++t) {
-                        const bool mine = (mask >> t) & 1u;
-#pragma unroll
-                        for (int e = 0; e < 18; ++e) {
-                            const double x = __shfl_sync(0xffffffffu, v[e], t);
-                            if (mine) W[e] += x;
+                    for (int e = 0; e < 18; ++e) stage[w][lane][e] = v[e];
+                    smask[w][lane] = mask;
+                    __syncwarp();
+                    const unsigned leaders = __ballot_sync(0xffffffffu, lane == leader);
+                    const int ntask = __popc(leaders) * 18;
+                    for (int task = lane; task < ntask; task += 32) {
+                        const int gi = task / 18, e = task - 18 * gi;
+                        const int L = (int)__fns(leaders, 0, gi + 1);
+                        unsigned gm = smask[w][L];
+                        double x = 0.0;
+                        while (gm) {
+                            const int t = __ffs(gm) - 1;
+                            gm &= gm - 1;
+                            x += stage[w][t][e];
                         }
+                        stage[w][L][e] = x;
                     }
+                    __syncwarp();
+#pragma unroll
+                    for (int e = 0; e < 18; ++e) W[e] = stage[w][lane][e];
+                    __syncwarp();  // the stage is read before the next chunk overwrites it
                 }
                 if (lane == leader && slot >= 0) {
                     // E[k][l] += Z_i[:, k] . W[:, l]
@@ -754,7 +773,9 @@ static double lambda_max_read(ofea_ctx *c, int steps) {
 void coarse_E_partials(ofea_ctx *c, Coarse &C, int nchunk) {
     if (nchunk != 1) fail(OFEA_ERR_STATE, "Galerkin blocks are assembled in one pass");
     C.part.ensure((size_t)C.na * 27 * 36);
-    k_galerkin_blocks<<<std::max(1, C.na), kGW * 32, 0, c->stream>>>(
+    const int gsm_bytes = (int)(sizeof(double) * kGW * (27 * 36 + 32 * 18));
+    OFEA_CUDA(cudaFuncSetAttribute(k_galerkin_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm_bytes));
+    k_galerkin_blocks<<<std::max(1, C.na), kGW * 32, gsm_bytes, c->stream>>>(
         C.na, C.agg_ptr.p, C.agg_nodes.p, C.agg_of.p, C.agg_cell.p, c->node_of_free.p, c->xyz.p, C.centroid.p,
         C.inv_scale, c->rowptr.p, c->cols.p, c->Kb.p, C.part.p, c->err_flag.p);
     OFEA_CHECK_LAUNCH();
