@@ -134,8 +134,12 @@ int ofea_ctx_destroy(ofea_ctx *c) {
     return guarded([&] {
         if (!c) return;
         cudaSetDevice(c->device);
+        try {
+            geometry_join(c);
+        } catch (...) {  // a failed background geometry has nothing left to release
+        }
         if (c->stream) cudaStreamSynchronize(c->stream);
-        for (cudaStream_t x : {c->side_stream, c->aux_stream})
+        for (cudaStream_t x : {c->side_stream, c->aux_stream, c->geo_stream})
             if (x) {
                 cudaStreamSynchronize(x);
                 cudaStreamDestroy(x);
@@ -183,9 +187,11 @@ int ofea_mesh_upload(ofea_ctx *c, int nd, const double *xyz, int ne, const int *
         need(std::isfinite(E0) && std::isfinite(nu) && nu > -1.0 && nu < 0.5, OFEA_ERR_INVALID_ARG,
              "invalid material (nu must be in (-1, 0.5))");
         use_device(c);
+        geometry_join(c);
         c->mesh_ok = c->pattern_ok = c->K_ok = c->sell_ok = false;
         c->coarse.geom_ok = c->coarse.K_ok = false;
         c->coarse2.geom_ok = c->coarse2.K_ok = false;
+        c->learned.links_ok = false;
         c->nd = nd;
         c->ne = ne;
         c->E0 = E0;
@@ -306,7 +312,9 @@ int ofea_assemble_pattern(ofea_ctx *c, int *n, long long *nnz) {
         need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
         need(c->mesh_ok, OFEA_ERR_STATE, "no mesh uploaded");
         use_device(c);
+        geometry_join(c);
         build_pattern(c);
+        geometry_start(c);  // coarse geometry on a host thread while the caller assembles
         if (n) *n = c->n;
         if (nnz) *nnz = 9 * c->nnzb;
     });
@@ -436,10 +444,12 @@ int ofea_set_coarse_nodes(ofea_ctx *c, int nodes) {
     return guarded([&] {
         need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
         need(nodes >= 8 && nodes <= 1000000, OFEA_ERR_INVALID_ARG, "nodes per aggregate must be 8..1e6");
+        geometry_join(c);
         if (nodes != c->coarse_nodes) {
             c->coarse_nodes = nodes;
             c->coarse.geom_ok = c->coarse.K_ok = false;
             c->coarse2.geom_ok = c->coarse2.K_ok = false;
+        c->learned.links_ok = false;
         }
     });
 }
@@ -454,6 +464,7 @@ int ofea_trim_device_memory(void) {
 int ofea_precond_reset(ofea_ctx *c) {
     return guarded([&] {
         need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
+        geometry_join(c);
         c->coarse.K_ok = false;
         c->coarse2.K_ok = false;
     });

@@ -717,9 +717,13 @@ void Learned::init_weights(unsigned seed) {
 void setup_learned_level(ofea_ctx *c) {
     Coarse &C2 = c->coarse2;
     Learned &N = c->learned;
+    geometry_join(c);
     if (!c->coarse.geom_ok) fail(OFEA_ERR_STATE, "coarse level missing");
     if (!C2.geom_ok) {
         build_aggregation_fine(c);
+        N.links_ok = false;
+    }
+    if (!N.links_ok) {
         // parent aggregate of every child and the change of mode origin/scale
         const Coarse &C1 = c->coarse;
         const int na2 = C2.na;
@@ -749,6 +753,7 @@ void setup_learned_level(ofea_ctx *c) {
         k_invdeg<<<grid_for(c, na2, kBlock), kBlock, 0, c->stream>>>(na2, C2.nbr.p, N.invdeg.p);
         OFEA_CHECK_LAUNCH();
         OFEA_CUDA(cudaStreamSynchronize(c->stream));
+        N.links_ok = true;
     }
     if (C2.K_ok) return;
     cudaStream_t s = c->stream;

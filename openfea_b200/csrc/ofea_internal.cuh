@@ -30,6 +30,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <functional>
+#include <future>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -143,6 +144,7 @@ struct Coarse {
 // Learned coarse-correction stage (learned.cu): network weights, Adam state,
 // per-K data of the nested level and activation buffers.
 struct Learned {
+    bool links_ok = false;  // parent / children tables of the nested level
     struct Layout {
         size_t W0, b0, W[4], b[4], Wd, bd, c0, total;
     };
@@ -171,6 +173,8 @@ struct ofea_ctx {
     bool own_stream = false;
     cudaStream_t side_stream = nullptr;  // second stream of the coarse inversion's lookahead (owned)
     cudaStream_t aux_stream = nullptr;   // power iteration beside the coarse inversion (owned)
+    cudaStream_t geo_stream = nullptr;   // uploads of the coarse geometry (owned)
+    std::future<void> geom_job;          // coarse geometry built in the background after the pattern
     // mesh
     int nd = 0, ne = 0, ne8 = 0, ne4 = 0, nfree = 0, n = 0;
     double E0 = 0, nu = 0;
@@ -227,6 +231,8 @@ void profile_kernels(ofea_ctx *c, int method, int reps, double *ms, double *byte
 // learned.cu
 void setup_learned_level(ofea_ctx *c);
 void setup_learned_levels(ofea_ctx *c);
+void geometry_start(ofea_ctx *c);
+void geometry_join(ofea_ctx *c);
 void learned_prepare_inference(ofea_ctx *c);
 void learned_apply(ofea_ctx *c, const float *t, float *x);
 // Batched persistent solver (batched.cu).

@@ -336,6 +336,7 @@ void build_pattern(ofea_ctx *c) {
     c->coarse.K_ok = false;
     c->coarse2.geom_ok = false;
     c->coarse2.K_ok = false;
+    c->learned.links_ok = false;
 }
 
 }  // namespace ofea

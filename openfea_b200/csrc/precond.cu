@@ -22,6 +22,7 @@
 #include <cmath>
 #include <condition_variable>
 #include <functional>
+#include <future>
 #include <mutex>
 #include <numeric>
 #include <thread>
@@ -200,7 +201,8 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
             if (J >= 0) band = std::max(band, std::abs(J - a));
         }
     C.band = band;
-    cudaStream_t st = c->stream;
+    if (!c->geo_stream) OFEA_CUDA(cudaStreamCreateWithFlags(&c->geo_stream, cudaStreamNonBlocking));
+    cudaStream_t st = c->geo_stream;  // its own stream: may run beside the assembly (geometry_start)
     C.agg_of.upload(agg_of.data(), nf, st);
     C.agg_ptr.upload(ptr.data(), na + 1, st);
     C.agg_nodes.upload(nodes.data(), nf, st);
@@ -781,7 +783,26 @@ void coarse_E_partials(ofea_ctx *c, Coarse &C, int nchunk) {
     OFEA_CHECK_LAUNCH();
 }
 
+// The geometry of both levels depends on the mesh only: after the pattern it
+// is built on a background host thread while the caller assembles K; every
+// user of it joins the job first (a failure surfaces there).
+void geometry_start(ofea_ctx *c) {
+    geometry_join(c);
+    const int target = c->coarse_nodes;
+    c->geom_job = std::async(std::launch::async, [c, target] {
+        OFEA_CUDA(cudaSetDevice(c->device));
+        c->coarse.target = target;
+        build_aggregation(c, target);
+        build_aggregation_fine(c);
+    });
+}
+
+void geometry_join(ofea_ctx *c) {
+    if (c->geom_job.valid()) c->geom_job.get();
+}
+
 void setup_coarse_geometry(ofea_ctx *c, int target_nodes) {
+    geometry_join(c);
     Coarse &C = c->coarse;
     if (!C.geom_ok || C.target != target_nodes) {
         C.target = target_nodes;
