@@ -224,7 +224,7 @@ def run_batched(ob, mg, local, hbm, steps=2, count=64, nrhs=16, rtol=1e-8, dist=
     }
 
 
-# ------------------------------------------------ learned preconditioner (cfg5) --
+# ------------------------- learned preconditioner on a SIMP density field --
 
 def run_learned_simp(ob, mg, local, shape, rtol=1e-8, steps=2):
     """The learned-preconditioner configuration: the cantilever mesh with a

@@ -127,7 +127,7 @@ def main(ref_root):
         rm.set_load(f)
         models[f"{tag}_colptr"], models[f"{tag}_rowidx"], models[f"{tag}_val"] = cp, ri, val
         models[f"{tag}_f"], models[f"{tag}_u"] = f, rm.solve()
-    # config-1 cantilever: displacement only
+    # the 20x4x4 C3D8 cantilever: displacement only
     m, ffull = mg.cantilever_small()
     fm = mg.free_map(m.nd, m.fix)
     rm = R.model(m)

@@ -1,7 +1,7 @@
 """The learned coarse-correction stage on the GPU: gradients of the
 library's backward kernels against the CPU oracle (oracle/gnn_oracle.py),
 training, what the trained stage gains over the same solver without it, and
-the FP64 judge that rejects it in favour of plain PCG."""
+the FP64 residual check that rejects it in favour of plain PCG."""
 import numpy as np
 import pytest
 
@@ -111,7 +111,7 @@ def test_stage_trained_on_one_density_field_helps_on_another(gpu_ctx_factory):
 
 def test_learned_on_tetrahedra_with_per_element_modulus(gpu_ctx_factory, oracle):
     """The learned stage on a jittered C3D4 block with lognormal per-element E
-    (the config-2 mesh type): trained on the GPU, accepted by the FP64 judge,
+    (jittered Kuhn tets): trained on the GPU, accepted by the FP64 residual check,
     and the solution satisfies the oracle's K to the tolerance."""
     import scipy.sparse as sp
     m, ffull = mg.tet_block(24, 8, 8)

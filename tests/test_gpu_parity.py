@@ -193,7 +193,7 @@ def test_nl_newton_iterates_match_reference(gpu_ctx_factory, golden, inp_file):
 
 
 def test_tet_block_per_element_modulus(gpu_ctx_factory, oracle):
-    """Config-2 physics (lognormal E, jittered Kuhn tets, random top loads)
+    """The jittered Kuhn-tet block (lognormal E, random top loads)
     at a size the CPU checker solves directly."""
     import scipy.sparse as sp
     import scipy.sparse.linalg as spl
