@@ -124,6 +124,21 @@ OFEA_API int ofea_assemble_linear(ofea_ctx *ctx);
  * tangent K_T(u) replaces K on the device; f_int (n, host) receives the
  * internal force.  u: n free-DOF displacements (host). */
 OFEA_API int ofea_assemble_nl(ofea_ctx *ctx, const double *u, double *f_int);
+/* The matrix the reference has already assembled, as solution_api receives it
+ * (src/linear_solution.cpp:17-64, reading item_ass.col_idx_ / row_idx_ /
+ * nz_val_, src/include/assemble.h:41-43; solution_nl_api, :66-137, reads
+ * assamble_nl_stiffness's col_idx / row_idx / nz_val): K in 0-based CSC, n
+ * columns, col_ptr (n+1), row_idx (col_ptr[n], rows ascending in each column),
+ * val.  K must be symmetric and 3x3-block structured in the reference's DOF
+ * numbering 3*free_map[node]+c (build_CSR always stores every DOF pair of an
+ * element, so its output is); a matrix that is not block structured returns
+ * OFEA_ERR_INVALID_ARG.  The nd node coordinates (coords_) and free_map
+ * (resort_free_nodes_) give the solver's coarse levels their rigid-body
+ * modes.  Replaces any mesh or matrix of the context; then ofea_solve /
+ * ofea_solve_device / ofea_spmv / ofea_get_csr work as after an assembly,
+ * while the element-based calls (assembly, stress) return OFEA_ERR_STATE. */
+OFEA_API int ofea_matrix_upload_csc(ofea_ctx *ctx, int nd, const double *xyz, const int *free_map, int n,
+                                   const int *col_ptr, const int *row_idx, const double *val);
 /* Copy K to the host as CSR: rowptr (n+1), col (nnz), val (nnz); any may be NULL. */
 OFEA_API int ofea_get_csr(ofea_ctx *ctx, int *rowptr, int *col, double *val);
 /* Element matrices of the last assembly, for checking: Ke of element e in the
@@ -154,8 +169,11 @@ OFEA_API int ofea_solve_device(ofea_ctx *ctx, const double *d_f, double *d_u, co
  * the context's assembled matrix.  Allocates nothing: its partial sums live
  * in a 512 KB static device array that every GPU loading this library holds
  * until the process exits.  At most 16 load cases per call; more returns
- * OFEA_ERR_CAPACITY.  The first call on each device looks up that array's
- * device address; make that first call before any stream capture.  Calls
+ * OFEA_ERR_CAPACITY.  ofea_ctx_create looks up that array's device address
+ * and loads this entry point's kernels on the context's device (CUDA loads
+ * code lazily, which allocates), so the entry point itself allocates nothing
+ * from its first call on; create the context before the caller's allocator
+ * reserves the GPU.  Calls
  * share the array: calls that overlap on one GPU race and must be ordered by
  * the caller.  Enqueued on the context's stream; returns without waiting. */
 OFEA_API int ofea_residual_norms_noalloc(ofea_ctx *ctx, int nrhs, const double *d_f,

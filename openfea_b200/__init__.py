@@ -99,6 +99,7 @@ def lib():
         "ofea_assemble_linear": (_I, [_P]),
         "ofea_assemble_nl": (_I, [_P, _P, _P]),
         "ofea_get_csr": (_I, [_P, _P, _P, _P]),
+        "ofea_matrix_upload_csc": (_I, [_P, _I, _P, _P, _I, _P, _P, _P]),
         "ofea_get_element_matrices": (_I, [_P, _I, _I, _P]),
         "ofea_spmv": (_I, [_P, _P, _P]),
         "ofea_solve": (_I, [_P, _P, _P, _I, _P, _P]),
@@ -311,6 +312,18 @@ class Context:
         fm = free_map if free_map is not None else build_free_index(mesh.nd, mesh.fix)
         self.upload(mesh.xyz, mesh.topo, mesh.etype, fm, mesh.E0, mesh.nu, mesh.E)
         return fm
+
+    def upload_csc(self, xyz, free_map, col_ptr, row_idx, val):
+        """K as the reference's assembled CSC arrays (col_idx_, row_idx_,
+        nz_val_) with the model's coordinates and free numbering; replaces
+        any mesh (ofea_matrix_upload_csc)."""
+        xyz, fm = _f64(xyz), _i32(free_map)
+        cp, ri, v = _i32(col_ptr), _i32(row_idx), _f64(val)
+        n = cp.size - 1
+        _check(lib().ofea_matrix_upload_csc(self.h, xyz.shape[0], _ptr(xyz), _ptr(fm), n, _ptr(cp), _ptr(ri),
+                                            _ptr(v)), "ofea_matrix_upload_csc")
+        self.nd, self.ne = int(xyz.shape[0]), 0
+        self.n, self.nnz = n, int(cp[-1])
 
     def set_modulus(self, E_elem, E0):
         E = _f64(E_elem) if E_elem is not None else None

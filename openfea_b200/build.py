@@ -12,6 +12,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -20,7 +21,7 @@ OUT = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libofea_gpu.so")
 CLI = os.path.join(HERE, "ofea_cli")
 
-CU_SOURCES = ["api.cu", "pattern.cu", "integrate.cu", "sell.cu", "precond.cu", "solve.cu", "learned.cu", "batched.cu", "noalloc.cu", "devmem.cu", "ca.cu"]
+CU_SOURCES = ["api.cu", "pattern.cu", "integrate.cu", "sell.cu", "precond.cu", "solve.cu", "learned.cu", "batched.cu", "noalloc.cu", "devmem.cu", "ca.cu", "csc.cu"]
 HOST_SOURCES = ["host/model.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -52,7 +53,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     inc = ["-I", os.path.join(ROOT, "include")]
     headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(".cuh")]
     headers += [os.path.join(ROOT, "include", "ofea_gpu.h"), os.path.join(ROOT, "include", "ofea_host.h")]
-    objs = []
+    objs, jobs = [], []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(OUT, os.path.basename(src) + ".o")
@@ -62,7 +63,10 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
                    "-Xcompiler", "-fvisibility=hidden", *inc, "-c", s, "-o", o]
             if ptxas_info:
                 cmd.insert(1, "-Xptxas=-v")
-            out = _run(cmd)
+            jobs.append(cmd)
+    # one nvcc per translation unit, run side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        for out in pool.map(_run, jobs):
             if verbose or ptxas_info:
                 sys.stdout.write(out)
     for src in HOST_SOURCES:

@@ -52,6 +52,9 @@ static void need(bool cond, int code, const char *msg) {
     if (!cond) fail(code, msg);
 }
 
+static const char *const kNoElements =
+    "the context holds a matrix loaded by ofea_matrix_upload_csc, without elements";
+
 }  // namespace ofea
 
 using namespace ofea;
@@ -120,6 +123,7 @@ int ofea_ctx_create(ofea_ctx **out, int device) {
             OFEA_CUDA(cudaSetDevice(device));
             OFEA_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
             create_ctx_stream(c);
+            noalloc_prepare(device);
             c->err_flag.ensure(4);
             c->herr.ensure(4);
         } catch (...) {
@@ -176,6 +180,38 @@ static void split_modulus(ofea_ctx *c, const double *E_elem, double E0, HVec<dou
         }
 }
 
+// The DOF numbering and coordinates shared by both ways of loading a model:
+// free_map numbers the free nodes 0..nfree-1 (resort_free_nodes_), every
+// coordinate is finite.  Keeps the host copies the coarse levels are built from.
+static void check_nodes(ofea_ctx *c, int nd, const double *xyz, const int *free_map) {
+    int nfree = 0;
+    HVec<char> seen(nd, 0);
+    for (int i = 0; i < nd; ++i) {
+        int f = free_map[i];
+        need(f >= -1 && f < nd, OFEA_ERR_INVALID_ARG, "free_map entry out of range");
+        if (f >= 0) {
+            need(!seen[f], OFEA_ERR_INVALID_ARG, "free_map is not a numbering");
+            seen[f] = 1;
+            ++nfree;
+        }
+    }
+    for (int i = 0; i < nfree; ++i)
+        need(seen[i], OFEA_ERR_INVALID_ARG, "free_map must number free nodes 0..nfree-1");
+    std::vector<char> finite(kHostChunks, 1);
+    host_for_chunks([&](int k) {
+        for (long i = chunk_begin(3L * nd, k); i < chunk_begin(3L * nd, k + 1); ++i)
+            if (!std::isfinite(xyz[i])) {
+                finite[k] = 0;
+                return;
+            }
+    });
+    for (int k = 0; k < kHostChunks; ++k) need(finite[k] != 0, OFEA_ERR_INVALID_ARG, "non-finite coordinate");
+    c->nfree = nfree;
+    c->n = 3 * nfree;
+    c->xyz_h.assign(xyz, xyz + 3L * nd);
+    c->fm_h.assign(free_map, free_map + nd);
+}
+
 int ofea_mesh_upload(ofea_ctx *c, int nd, const double *xyz, int ne, const int *topo,
                      const int *etype, const double *E_elem, double E0, double nu,
                      const int *free_map) {
@@ -189,6 +225,7 @@ int ofea_mesh_upload(ofea_ctx *c, int nd, const double *xyz, int ne, const int *
         use_device(c);
         geometry_join(c);
         c->mesh_ok = c->pattern_ok = c->K_ok = c->sell_ok = false;
+        c->matrix_only = false;
         c->coarse.geom_ok = c->coarse.K_ok = false;
         c->coarse2.geom_ok = c->coarse2.K_ok = false;
         c->learned.links_ok = false;
@@ -250,32 +287,7 @@ int ofea_mesh_upload(ofea_ctx *c, int nd, const double *xyz, int ne, const int *
         });
         c->ne8 = (int)o8[kHostChunks];
         c->ne4 = (int)o4[kHostChunks];
-        int nfree = 0;
-        HVec<char> seen(nd, 0);
-        for (int i = 0; i < nd; ++i) {
-            int f = free_map[i];
-            need(f >= -1 && f < nd, OFEA_ERR_INVALID_ARG, "free_map entry out of range");
-            if (f >= 0) {
-                need(!seen[f], OFEA_ERR_INVALID_ARG, "free_map is not a numbering");
-                seen[f] = 1;
-                ++nfree;
-            }
-        }
-        for (int i = 0; i < nfree; ++i)
-            need(seen[i], OFEA_ERR_INVALID_ARG, "free_map must number free nodes 0..nfree-1");
-        std::vector<char> finite(kHostChunks, 1);
-        host_for_chunks([&](int k) {
-            for (long i = chunk_begin(3L * nd, k); i < chunk_begin(3L * nd, k + 1); ++i)
-                if (!std::isfinite(xyz[i])) {
-                    finite[k] = 0;
-                    return;
-                }
-        });
-        for (int k = 0; k < kHostChunks; ++k) need(finite[k] != 0, OFEA_ERR_INVALID_ARG, "non-finite coordinate");
-        c->nfree = nfree;
-        c->n = 3 * nfree;
-        c->xyz_h.assign(xyz, xyz + 3L * nd);
-        c->fm_h.assign(free_map, free_map + nd);
+        check_nodes(c, nd, xyz, free_map);
         HVec<double> E8, E4;
         split_modulus(c, E_elem, E0, E8, E4);
         cudaStream_t s = c->stream;
@@ -311,6 +323,7 @@ int ofea_assemble_pattern(ofea_ctx *c, int *n, long long *nnz) {
     return guarded([&] {
         need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
         need(c->mesh_ok, OFEA_ERR_STATE, "no mesh uploaded");
+        need(!c->matrix_only, OFEA_ERR_STATE, kNoElements);
         use_device(c);
         geometry_join(c);
         build_pattern(c);
@@ -332,6 +345,7 @@ int ofea_assemble_linear(ofea_ctx *c) {
     return guarded([&] {
         need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
         need(c->pattern_ok, OFEA_ERR_STATE, "ofea_assemble_pattern first");
+        need(!c->matrix_only, OFEA_ERR_STATE, kNoElements);
         use_device(c);
         assemble_linear(c);
         after_assembly(c);
@@ -342,6 +356,7 @@ int ofea_assemble_nl(ofea_ctx *c, const double *u, double *f_int) {
     return guarded([&] {
         need(c != nullptr && u != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
         need(c->pattern_ok, OFEA_ERR_STATE, "ofea_assemble_pattern first");
+        need(!c->matrix_only, OFEA_ERR_STATE, kNoElements);
         use_device(c);
         c->u_nl.upload(u, c->n, c->stream);
         c->f_int.ensure(std::max(c->n, 1));
@@ -350,6 +365,61 @@ int ofea_assemble_nl(ofea_ctx *c, const double *u, double *f_int) {
             OFEA_CUDA(cudaMemcpyAsync(f_int, c->f_int.p, sizeof(double) * c->n, cudaMemcpyDeviceToHost,
                                       c->stream));
         after_assembly(c);
+    });
+}
+
+int ofea_matrix_upload_csc(ofea_ctx *c, int nd, const double *xyz, const int *free_map, int n,
+                           const int *col_ptr, const int *row_idx, const double *val) {
+    return guarded([&] {
+        need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
+        need(nd > 0 && xyz && free_map && n > 0 && col_ptr && row_idx && val, OFEA_ERR_INVALID_ARG,
+             "empty model or NULL array");
+        use_device(c);
+        geometry_join(c);
+        c->mesh_ok = c->pattern_ok = c->K_ok = c->sell_ok = false;
+        c->coarse.geom_ok = c->coarse.K_ok = false;
+        c->coarse2.geom_ok = c->coarse2.K_ok = false;
+        c->learned.links_ok = false;
+        c->matrix_only = true;
+        c->nd = nd;
+        c->ne = c->ne8 = c->ne4 = 0;
+        c->elem_type.clear();
+        c->elem_local.clear();
+        c->topo_h.clear();
+        check_nodes(c, nd, xyz, free_map);
+        need(n == c->n, OFEA_ERR_INVALID_ARG, "n must be 3 x (free nodes of free_map)");
+        need(col_ptr[0] == 0, OFEA_ERR_INVALID_ARG, "col_ptr[0] must be 0");
+        for (int j = 0; j < n; ++j)
+            need(col_ptr[j + 1] >= col_ptr[j], OFEA_ERR_INVALID_ARG, "col_ptr must be non-decreasing");
+        need(col_ptr[n] % 9 == 0, OFEA_ERR_INVALID_ARG, "nnz must be a multiple of 9 (3x3 blocks)");
+        cudaStream_t s = c->stream;
+        c->xyz.upload(xyz, 3L * nd, s);
+        c->free_map.upload(free_map, nd, s);
+        upload_csc(c, n, col_ptr, row_idx, val);
+        // the widest coupling per direction (the coarse cells must be wider),
+        // over the block pattern, which the checks above have validated
+        std::vector<int> node_of(c->nfree);
+        for (int i = 0; i < nd; ++i)
+            if (free_map[i] >= 0) node_of[free_map[i]] = i;
+        double ext[kHostChunks][3] = {};
+        host_for_chunks([&](int k) {
+            for (long I = chunk_begin(c->nfree, k); I < chunk_begin(c->nfree, k + 1); ++I) {
+                const double *xi = &xyz[3L * node_of[I]];
+                for (int t = col_ptr[3 * I]; t < col_ptr[3 * I + 1]; t += 3) {
+                    const double *xj = &xyz[3L * node_of[row_idx[t] / 3]];
+                    for (int d = 0; d < 3; ++d) ext[k][d] = std::max(ext[k][d], std::fabs(xj[d] - xi[d]));
+                }
+            }
+        });
+        for (int d = 0; d < 3; ++d) {
+            c->coupling_ext[d] = 0;
+            for (int k = 0; k < kHostChunks; ++k) c->coupling_ext[d] = std::max(c->coupling_ext[d], ext[k][d]);
+        }
+        c->mesh_ok = true;
+        c->pattern_ok = true;
+        c->K_ok = true;
+        after_assembly(c);
+        geometry_start(c);
     });
 }
 
@@ -389,7 +459,7 @@ int ofea_get_csr(ofea_ctx *c, int *rowptr, int *col, double *val) {
 int ofea_get_element_matrices(ofea_ctx *c, int first, int count, double *Ke) {
     return guarded([&] {
         need(c != nullptr && Ke != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
-        need(c->K_ok && c->Ke.p, OFEA_ERR_STATE, "no assembly yet");
+        need(c->K_ok && c->Ke.p && !c->matrix_only, OFEA_ERR_STATE, "no assembly yet");
         need(first >= 0 && count >= 0 && first + count <= c->ne, OFEA_ERR_INVALID_ARG, "range");
         use_device(c);
         std::vector<double> blk(576);
@@ -684,7 +754,7 @@ int ofea_residual_norms_noalloc(ofea_ctx *c, int nrhs, const double *d_f, const 
                                 double *d_norms) {
     return guarded([&] {
         need(c != nullptr && d_f && d_u && d_norms, OFEA_ERR_INVALID_ARG, "NULL argument");
-        need(c->K_ok && c->sell_ok, OFEA_ERR_STATE, "K not assembled");
+        need(c->K_ok && c->sell_ok, OFEA_ERR_STATE, "K not assembled (or its solver copy not built)");
         OFEA_CUDA(cudaSetDevice(c->device));
         residual_norms_noalloc(c, nrhs, d_f, d_u, d_norms);
     });
@@ -782,6 +852,7 @@ int ofea_stress(ofea_ctx *c, const double *u, int mode, double *elem, double *no
         need(mode == OFEA_STRESS_REFERENCE || mode == OFEA_STRESS_CAUCHY, OFEA_ERR_INVALID_ARG,
              "mode must be OFEA_STRESS_REFERENCE or OFEA_STRESS_CAUCHY");
         need(c->pattern_ok, OFEA_ERR_STATE, "no pattern (ofea_assemble_pattern)");
+        need(!c->matrix_only, OFEA_ERR_STATE, kNoElements);
         use_device(c);
         cudaStream_t s = c->stream;
         DevBuf<double> du, de, dn;

@@ -22,6 +22,8 @@
 #include <algorithm>
 #include <cmath>
 
+#include <mutex>
+
 #include "ofea_internal.cuh"
 
 namespace ofea {
@@ -30,9 +32,18 @@ namespace ofea {
 // (node order src/Elements/C3D8_Gauss.cpp:27-52, points :84-92).
 __constant__ double c_hex_dN[8 * 3 * 8];
 
-// Per-device constant table; re-uploaded on every integration call (192
-// doubles), so contexts on several devices each see it.
+// Per-device constant table (192 doubles), uploaded once per device: the
+// first integration or stress call on a device writes it, later calls only
+// check a flag.
 static void upload_hex_table() {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static bool done[kMaxDevices] = {};
+    int dev = 0;
+    OFEA_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) fail(OFEA_ERR_INVALID_ARG, "device index too large");
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return;
     const int sr[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
     const int ss[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
     const int st[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
@@ -46,6 +57,7 @@ static void upload_hex_table() {
         }
     }
     OFEA_CUDA(cudaMemcpyToSymbol(c_hex_dN, t, sizeof(t)));
+    done[dev] = true;
 }
 
 struct Lame {

@@ -9,7 +9,9 @@
 // array below for the per-CTA partial sums.
 //
 // The scratch array (kMaxRhs * 2 * kMaxCtas doubles = 512 KB) exists on every
-// GPU that loads this library, for as long as the process lives.  Every call
+// GPU that loads this library, for as long as the process lives.  Its device
+// address is looked up, and the two kernels loaded, when a context is created
+// on a device (noalloc_prepare), so the entry point allocates nothing.  Every call
 // shares it and it keeps the last call's contents; each call overwrites every
 // partial it later reads, so nothing needs clearing.  Calls whose work
 // overlaps on the same GPU (other streams or contexts of the device) race on
@@ -86,6 +88,17 @@ __global__ void __launch_bounds__(kBlock) k_residual_final(int G, const double *
 }
 
 }  // namespace
+
+// Looks up the scratch array's address on `device` and loads the entry
+// point's two kernels there (CUDA loads modules and kernels lazily, which
+// allocates device memory); run when a context is created on that device, so
+// the entry point itself allocates nothing, from its first call on.
+void noalloc_prepare(int device) {
+    scratch_address(device);
+    cudaFuncAttributes a;
+    OFEA_CUDA(cudaFuncGetAttributes(&a, k_residual_partials));
+    OFEA_CUDA(cudaFuncGetAttributes(&a, k_residual_final));
+}
 
 void residual_norms_noalloc(ofea_ctx *c, int nrhs, const double *d_f, const double *d_u,
                             double *d_norms) {

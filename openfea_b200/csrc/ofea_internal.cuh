@@ -185,6 +185,10 @@ struct ofea_ctx {
     ofea::DevBuf<double> xyz, E8, E4;
     ofea::DevBuf<int> topo8, topo4, free_map, node_of_free;
     bool mesh_ok = false;
+    // K uploaded as CSC arrays (ofea_matrix_upload_csc): no elements, and the
+    // widest node coupling per direction stands in for the element extent
+    bool matrix_only = false;
+    double coupling_ext[3] = {0, 0, 0};
     // pattern
     ofea::DevBuf<int> inc_ptr, inc, rowptr, cols, diag_pos;
     ofea::DevBuf<uint16_t> slot;
@@ -216,6 +220,8 @@ struct ofea_ctx {
 namespace ofea {
 // pattern.cu
 void build_pattern(ofea_ctx *c);
+// csc.cu
+void upload_csc(ofea_ctx *c, int n, const int *col_ptr, const int *row_idx, const double *val);
 // integrate.cu
 void assemble_linear(ofea_ctx *c);
 void assemble_nl(ofea_ctx *c, const double *d_u, double *d_fint);
@@ -254,6 +260,7 @@ constexpr int kCaMaxBasis = OFEA_CA_MAX_BASIS;
 void ca_reanalysis(ofea_ctx *base, ofea_ctx *mod, const double *h_f, const double *h_u0, int nb,
                    const ofea_solve_opts &o, double *h_u, ofea_ca_stats *stats);
 // noalloc.cu
+void noalloc_prepare(int device);
 void residual_norms_noalloc(ofea_ctx *c, int nrhs, const double *d_f, const double *d_u,
                             double *d_norms);
 // pattern.cu (scan)

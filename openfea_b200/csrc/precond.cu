@@ -248,6 +248,8 @@ void build_aggregation(ofea_ctx *c, int target_nodes) {
                 em[d] = std::max(em[d], b - a);
             }
         }
+        if (c->matrix_only)  // no elements: the widest coupling of K
+            for (int d = 0; d < 3; ++d) em[d] = c->coupling_ext[d];
         for (int d = 0; d < 3; ++d) {  // written once per chunk (no shared cache lines in the loops)
             clo[k][d] = l[d];
             chi[k][d] = h[d];

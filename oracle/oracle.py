@@ -160,6 +160,10 @@ class Reference:
         L.ref_model_nl_get_csc.argtypes = [_P, _P, _P, _P]
         L.ref_model_nl_solve.restype = _I
         L.ref_model_nl_solve.argtypes = [_P, _P, _P]
+        L.ref_model_solve_multi.restype = _I
+        L.ref_model_solve_multi.argtypes = [_P, _I, _P, _P]
+        L.ref_model_cg_ic.restype = _I
+        L.ref_model_cg_ic.argtypes = [_P, _P, _P, _D, _I, _I, _I, _P]
         L.ref_element_ke.argtypes = [_I, _P, _D, _D, _P]
         L.ref_element_nl.argtypes = [_I, _P, _P, _D, _D, _P, _P]
         self.L = L
@@ -237,6 +241,30 @@ class RefModel:
         if st != 0:
             raise RuntimeError("reference solve failed")
         return u
+
+    def solve_multi(self, F):
+        """Load cases F (nrhs, n) on one factor: solution_api("SuperLU_class")
+        for the first, superlu_solution_next for the rest."""
+        F = np.ascontiguousarray(np.atleast_2d(F), dtype=np.float64)
+        assert F.shape[1] == self.n
+        U = np.zeros_like(F)
+        if self.r.L.ref_model_solve_multi(self.h, F.shape[0], _ptr(F), _ptr(U)) != 0:
+            raise RuntimeError("reference SuperLU_class solve failed")
+        return U
+
+    def cg_ic(self, f, rtol=1e-10, max_iter=100000, threads=1, ordering="natural", u0=None):
+        """Vendored Eigen ConjugateGradient + IncompleteCholesky (FP64) on the
+        reference-assembled K (call assemble() first).  Returns u and a dict of
+        iterations, true relative residual and set-up / CG seconds."""
+        f = _f64(f)
+        u = np.zeros(self.n) if u0 is None else _f64(u0).copy()
+        out = np.zeros(5)
+        st = self.r.L.ref_model_cg_ic(self.h, _ptr(f), _ptr(u), rtol, max_iter, threads,
+                                      1 if ordering == "amd" else 0, _ptr(out))
+        if st != 0:
+            raise RuntimeError(f"Eigen CG+IC failed ({st})")
+        return u, dict(iterations=int(out[0]), est_rel_residual=out[1], rel_residual=out[2],
+                       setup_s=out[3], cg_s=out[4], threads=threads, ordering=ordering)
 
     def full_displacement(self):
         uf = np.zeros(3 * self.nd)

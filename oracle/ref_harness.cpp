@@ -29,6 +29,9 @@
 #include "include/post_process.h"
 #include "include/set_bcs.h"
 
+#include <Eigen/IterativeLinearSolvers>
+#include <Eigen/SparseCore>
+
 using namespace CAE;
 
 namespace {
@@ -229,6 +232,101 @@ void ref_model_times(void *h, double *t3) {
     t3[0] = m->t_csr;
     t3[1] = m->t_fill;
     t3[2] = m->t_solve;
+}
+
+// Many load cases on one factor, as the reference's reanalysis does:
+// solution_api(..., "SuperLU_class") factors K and solves load case 0
+// (src/linear_solution.cpp:23-39, superlu_solution_1st keeps L and U), then
+// superlu_solution_next re-solves every further load case with that factor
+// (src/solver/solver_superlu.cpp:76-94, called so by src/ca_analysis.cpp:164);
+// the last call frees the factor.  F and U: nrhs x n, row-major.
+int ref_model_solve_multi(void *h, int nrhs, const double *F, double *U) {
+    RefModel *m = (RefModel *)h;
+    data_management &d = m->data;
+    int n = (int)d.single_load_vec_.size();
+    if (nrhs < 1) return -1;
+    std::vector<double> keep = d.single_load_vec_;
+    double t0 = now_s();
+    d.single_load_vec_.assign(F, F + n);
+    d.single_dis_vec_.assign(n, 0.0);
+    bool ok = solution_api(m->lin, d, "SuperLU_class");
+    for (int i = 0; i < n; ++i) U[i] = d.single_dis_vec_[i];
+    for (int j = 1; j < nrhs && ok; ++j) {
+        std::vector<double> b(F + (size_t)j * n, F + (size_t)(j + 1) * n), x(n, 0.0);
+        ok = d.item_superlu.superlu_solution_next(b, x, j == nrhs - 1);
+        for (int i = 0; i < n; ++i) U[(size_t)j * n + i] = x[i];
+    }
+    if (nrhs == 1 && ok) {  // free the factor that superlu_solution_1st kept
+        std::vector<double> b(n, 0.0), x(n, 0.0);
+        d.item_superlu.superlu_solution_next(b, x, true);
+    }
+    m->t_solve = now_s() - t0;
+    d.single_load_vec_ = keep;
+    return ok ? 0 : -1;
+}
+
+// The scale oracle where a direct factor does not fit in time: the vendored
+// Eigen 3.4.0 ConjugateGradient (FP64) with its IncompleteCholesky
+// preconditioner (Lin-More modified IC, externals/eigen-3.4.0/Eigen/src/
+// IterativeLinearSolvers/IncompleteCholesky.h) on the reference-assembled K.
+// K is symmetric, so the reference's CSC arrays are read as CSR, which lets
+// Eigen's SpMV use `threads` OpenMP threads (the IC triangular solves are
+// serial).  ordering: 0 natural (the reference's node-interleaved numbering),
+// 1 AMD.  u holds the start vector on entry.  Stops at ||f - K u|| <= tol ||f||
+// or after maxit iterations.  out[0..4] = iterations, Eigen's residual
+// estimate, the FP64 true relative residual, IC set-up seconds, CG seconds.
+int ref_model_cg_ic(void *h, const double *f, double *u, double tol, int maxit, int threads,
+                    int ordering, double *out) {
+    RefModel *m = (RefModel *)h;
+    assamble_stiffness &A = m->lin;
+    if (A.col_idx_.empty()) return -1;
+    int n = (int)A.col_idx_.size() - 1;
+    typedef Eigen::SparseMatrix<double, Eigen::RowMajor, int> SpR;
+    Eigen::Map<const SpR> K(n, n, (int)A.nz_val_.size(), A.col_idx_.data(), A.row_idx_.data(),
+                            A.nz_val_.data());
+    Eigen::Map<const Eigen::VectorXd> b(f, n);
+    Eigen::Map<Eigen::VectorXd> x(u, n);
+#ifdef _OPENMP
+    Eigen::setNbThreads(threads > 0 ? threads : 1);
+#else
+    (void)threads;
+#endif
+    double t0 = now_s(), t1, t2;
+    int its = 0;
+    double est = 0;
+    bool ok;
+    auto run = [&](auto &cg) {
+        cg.setTolerance(tol);
+        cg.setMaxIterations(maxit);
+        cg.compute(K);
+        t1 = now_s();
+        if (cg.info() != Eigen::Success) return false;
+        Eigen::VectorXd x0 = x;
+        x = cg.solveWithGuess(b, x0);
+        t2 = now_s();
+        its = (int)cg.iterations();
+        est = cg.error();
+        return true;
+    };
+    if (ordering == 1) {
+        Eigen::ConjugateGradient<SpR, Eigen::Lower | Eigen::Upper,
+                                 Eigen::IncompleteCholesky<double, Eigen::Lower, Eigen::AMDOrdering<int>>>
+            cg;
+        ok = run(cg);
+    } else {
+        Eigen::ConjugateGradient<SpR, Eigen::Lower | Eigen::Upper,
+                                 Eigen::IncompleteCholesky<double, Eigen::Lower, Eigen::NaturalOrdering<int>>>
+            cg;
+        ok = run(cg);
+    }
+    if (!ok) return -2;
+    Eigen::VectorXd r = b - K * x;
+    out[0] = its;
+    out[1] = est;
+    out[2] = r.norm() / b.norm();
+    out[3] = t1 - t0;
+    out[4] = t2 - t1;
+    return 0;
 }
 
 // Geometric-nonlinear tangent: assamble_nl_stiffness::build_CSR (once) +

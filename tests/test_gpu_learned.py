@@ -11,6 +11,9 @@ from oracle.gnn_oracle import TOTAL, GNNOracle, he_weights
 
 pytestmark = pytest.mark.gpu
 
+# relative residual of the LEARNED and MIXED solves in the benchmark
+LEARNED_RTOL = 1e-9
+
 
 def cantilever_ctx(factory, nx, ny, nz):
     m, ffull = mg.cantilever_large(nx, ny, nz)
@@ -49,6 +52,48 @@ def test_training_reduces_loss_and_stage_gains_iterations(gpu_ctx_factory):
     assert np.linalg.norm(ul - u64) / np.linalg.norm(u64) < 1e-6
     # what the trained stage gains over the same solver without it
     assert sl["iterations"] < sm["iterations"], (sl["iterations"], sm["iterations"])
+
+
+@pytest.mark.parametrize("case", ["cantilever", "tets", "simp"])
+def test_learned_displacement_against_reference_superlu(gpu_ctx_factory, reference, case):
+    """LEARNED (and MIXED beside it) at the benchmark's relative residual
+    against the reference's own solve of its own K, solution_api("SuperLU_func"):
+    within 1e-8 (relative L2).  Cases: the 40x10x10 cantilever (14,520 DOF),
+    the jittered tet block 24x8x8 with lognormal E, and a 40x12x12 SIMP block
+    whose stage was trained on another density sample."""
+    if case == "cantilever":
+        m, ffull = mg.cantilever_large(40, 10, 10)
+    elif case == "tets":
+        m, ffull = mg.tet_block(24, 8, 8)
+    else:
+        m, ffull = mg.cantilever_large(40, 12, 12)
+        m.E = 210e9 * mg.simp_density((40, 12, 12), 32, smooth=True) ** 3
+    ctx = gpu_ctx_factory()
+    fm = ctx.upload_mesh(m)
+    ctx.assemble_pattern()
+    ctx.assemble_linear()
+    f = mg.to_free(ffull, fm)
+    if case == "simp":
+        mt, _ = mg.cantilever_large(40, 12, 12)
+        mt.E = 210e9 * mg.simp_density((40, 12, 12), 31, smooth=True) ** 3
+        tr = gpu_ctx_factory()
+        tr.upload_mesh(mt)
+        tr.assemble_pattern()
+        tr.assemble_linear()
+        tr.learned_train(sample_iters=600, sample_every=2, steps=200, batch=16)
+        ctx.set_learned_weights(tr.learned_weights())
+    else:
+        ctx.learned_train(sample_iters=600, sample_every=2, steps=200, batch=16)
+    rm = reference.model(m)
+    rm.assemble()
+    rm.set_load(f)
+    u_ref = rm.solve()
+    for method in ("GPU_LEARNED", "GPU_MIXED"):
+        ctx.precond_reset()
+        u, st = ctx.solve(f, method=method, rtol=LEARNED_RTOL)
+        assert st["status"] == 0 and st["rejected_learned"] == 0, st
+        err = np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref)
+        assert err <= 1e-8, (method, err)
 
 
 def test_rejected_stage_falls_back_to_plain_pcg(gpu_ctx_factory, tmp_path):

@@ -41,9 +41,12 @@ def test_residual_norms_without_allocation(gpu_ctx_factory):
     for call in range(2):
         norms = torch.full((2 * nrhs,), float("nan"), dtype=torch.float64, device="cuda")
         torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         rc = fn(ctx.h, nrhs, dF.data_ptr(), dU.data_ptr(), norms.data_ptr())
         assert rc == 0, ob.lib().ofea_last_error()
         torch.cuda.synchronize()
+        # nothing was allocated on the device, on the first call either
+        assert torch.cuda.mem_get_info()[0] == free_before, call
         got = norms.cpu().numpy()
         rel = got[0::2] / got[1::2]
         # against the existing entry points: the solve's reported FP64 residual
