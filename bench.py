@@ -408,8 +408,8 @@ def run_reference(args):
     about a day at this size and MKL Pardiso, its default, is not installed).
     That full solve (IC set-up + CG) is `value`, measured once before the
     steps; each warm-up and timed step is then a bounded sample, 10 CG
-    iterations with the same preconditioner on the same K, and `ms_per_step`
-    is that sample's time."""
+    iterations with the same IC factor on the same K, and `ms_per_step` is
+    that sample's time."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -426,7 +426,7 @@ def run_reference(args):
     samples = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        _, st = rm.cg_ic(f, rtol=1e-30, max_iter=10, threads=threads)
+        _, st = rm.cg_ic_run(f, rtol=1e-30, max_iter=10)
         if i >= args.warmup:
             samples.append((time.perf_counter() - t0, st))
     step_s = statistics.mean(t for t, _ in samples)

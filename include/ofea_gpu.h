@@ -150,7 +150,12 @@ OFEA_API int ofea_spmv(ofea_ctx *ctx, const double *x, double *y);
 /* ---- solve -------------------------------------------------------------- */
 /* solution_api (src/linear_solution.cpp:17-64) / solution_nl_api (:66-137):
  * solve K u = f for nrhs right-hand sides (column-major n x nrhs, host).
- * opts NULL: defaults.  stats may be NULL (one entry per rhs otherwise). */
+ * opts NULL: defaults.  stats may be NULL (one entry per rhs otherwise).
+ * With 2..32 right-hand sides and PCG64 or MIXED, all of them are solved
+ * together by one persistent launch of the batched solver (ofea_batch_*,
+ * one variant), which reads K once per iteration for every load case; the
+ * first such call on a problem class tunes its tiles (OFEA_TUNE_FILE).
+ * LEARNED, and more than 32 right-hand sides, solve them one after another. */
 OFEA_API int ofea_solve(ofea_ctx *ctx, const double *f, double *u, int nrhs, const ofea_solve_opts *opts,
                ofea_solve_stats *stats);
 /* Drop the preconditioner built for the current K (coarse operator, smoother
@@ -239,6 +244,13 @@ OFEA_API int ofea_learned_level(ofea_ctx *ctx, int *na, int *nbr, float *Ehat, f
  * given stage inputs x (batch x na x 6, scaled level residuals). */
 OFEA_API int ofea_learned_gradient(ofea_ctx *ctx, const float *x, int batch, double *loss,
                                    float *grad);
+
+/* No counterpart in the reference.  The learned stage's dense layers run on
+ * the tensor cores (tcgen05.mma, BF16 operands in shared memory, FP32
+ * accumulation in tensor memory); this exposes that product on its own, for
+ * checking: D = A B^T with A (M x K) and B (N x K) row-major FP32 host arrays,
+ * each entry rounded to BF16 (nearest even), D (M x N) row-major FP32. */
+OFEA_API int ofea_tc_matmul(int device, int M, int N, int K, const float *A, const float *B, float *D);
 
 /* ---- batched reanalysis ---------------------------------------------------- */
 /* Replaces the per-variant factor + per-load-case dgstrs loop of the

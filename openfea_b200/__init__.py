@@ -100,6 +100,7 @@ def lib():
         "ofea_assemble_nl": (_I, [_P, _P, _P]),
         "ofea_get_csr": (_I, [_P, _P, _P, _P]),
         "ofea_matrix_upload_csc": (_I, [_P, _I, _P, _P, _I, _P, _P, _P]),
+        "ofea_tc_matmul": (_I, [_I, _I, _I, _I, _P, _P, _P]),
         "ofea_get_element_matrices": (_I, [_P, _I, _I, _P]),
         "ofea_spmv": (_I, [_P, _P, _P]),
         "ofea_solve": (_I, [_P, _P, _P, _I, _P, _P]),
@@ -257,6 +258,19 @@ def solve_batched(contexts, loads, method="GPU_MIXED", rtol=1e-8, **kw):
     stats = (SolveStats * len(contexts))()
     _check(lib().ofea_solve_batched(ctx, len(contexts), fp, up, nrhs, ctypes.byref(o), stats), "ofea_solve_batched")
     return U, [s_.as_dict() for s_ in stats]
+
+
+def tc_matmul(A, B, device=0):
+    """D = A B^T on the tensor cores (BF16 operands, FP32 accumulation), the
+    product the learned stage's dense layers use (ofea_tc_matmul)."""
+    A = np.ascontiguousarray(A, dtype=np.float32)
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    M, K = A.shape
+    N, K2 = B.shape
+    assert K == K2
+    D = np.zeros((M, N), dtype=np.float32)
+    _check(lib().ofea_tc_matmul(device, M, N, K, _ptr(A), _ptr(B), _ptr(D)), "ofea_tc_matmul")
+    return D
 
 
 def check_barrier_timeout(ctx, limit_ms=20):

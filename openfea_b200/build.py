@@ -21,7 +21,7 @@ OUT = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libofea_gpu.so")
 CLI = os.path.join(HERE, "ofea_cli")
 
-CU_SOURCES = ["api.cu", "pattern.cu", "integrate.cu", "sell.cu", "precond.cu", "solve.cu", "learned.cu", "batched.cu", "noalloc.cu", "devmem.cu", "ca.cu", "csc.cu"]
+CU_SOURCES = ["api.cu", "pattern.cu", "integrate.cu", "sell.cu", "precond.cu", "solve.cu", "learned.cu", "batched.cu", "noalloc.cu", "devmem.cu", "ca.cu", "csc.cu", "tc_gemm.cu"]
 HOST_SOURCES = ["host/model.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -5,12 +5,14 @@
 #include <cmath>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <mutex>
 #include <random>
 
 #include "host_pool.cuh"
 #include "ofea_internal.cuh"
 #include "precond.cuh"
+#include "tc_gemm.cuh"
 
 namespace ofea {
 
@@ -291,12 +293,13 @@ int ofea_mesh_upload(ofea_ctx *c, int nd, const double *xyz, int ne, const int *
         HVec<double> E8, E4;
         split_modulus(c, E_elem, E0, E8, E4);
         cudaStream_t s = c->stream;
-        c->xyz.upload(xyz, 3L * nd, s);
+        // from the library's host copies (page-locked blocks: direct DMA)
+        c->xyz.upload(c->xyz_h.data(), 3L * nd, s);
         c->topo8.upload(t8.data(), t8.size(), s);
         c->topo4.upload(t4.data(), t4.size(), s);
         c->E8.upload(E8.data(), E8.size(), s);
         c->E4.upload(E4.data(), E4.size(), s);
-        c->free_map.upload(free_map, nd, s);
+        c->free_map.upload(c->fm_h.data(), nd, s);
         OFEA_CUDA(cudaStreamSynchronize(s));
         c->mesh_ok = true;
     });
@@ -576,6 +579,27 @@ int ofea_solve(ofea_ctx *c, const double *f, double *u, int nrhs, const ofea_sol
         check_solve_ready(c, o);
         use_device(c);
         const int n = c->n;
+        if (nrhs > 1 && nrhs <= OFEA_BATCH_MAX_RHS && o.method != OFEA_SOLVER_LEARNED) {
+            // several load cases on one K: one persistent launch for all of
+            // them (the batched engine with one variant), K read once per
+            // iteration for every load case
+            std::unique_ptr<ofea_batch, void (*)(ofea_batch *)> b(batch_create(&c, 1, nrhs), batch_destroy);
+            const double *fp[1] = {f};
+            double *up[1] = {u};
+            std::vector<ofea_solve_stats> cs(nrhs);
+            batch_set_rhs(b.get(), fp);
+            batch_solve(b.get(), o, nullptr, cs.data());
+            batch_get_solution(b.get(), up);
+            for (int k = 0; k < nrhs; ++k) {
+                if (stats) stats[k] = cs[k];
+                if (cs[k].status != OFEA_OK && worst == OFEA_OK) {
+                    worst = cs[k].status;
+                    set_last_error(std::string("solve: ") + ofea_status_string(cs[k].status) +
+                                   ", relative residual " + fmt_e(cs[k].rel_residual));
+                }
+            }
+            return;
+        }
         c->w.f.ensure(std::max(n, 1));
         c->w.u.ensure(std::max(n, 1));
         for (int k = 0; k < nrhs; ++k) {
@@ -757,6 +781,41 @@ int ofea_residual_norms_noalloc(ofea_ctx *c, int nrhs, const double *d_f, const 
         need(c->K_ok && c->sell_ok, OFEA_ERR_STATE, "K not assembled (or its solver copy not built)");
         OFEA_CUDA(cudaSetDevice(c->device));
         residual_norms_noalloc(c, nrhs, d_f, d_u, d_norms);
+    });
+}
+
+int ofea_tc_matmul(int device, int M, int N, int K, const float *A, const float *B, float *D) {
+    return guarded([&] {
+        need(A && B && D && M > 0 && N > 0 && K > 0, OFEA_ERR_INVALID_ARG, "bad argument");
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+            cudaGetLastError();
+            fail(OFEA_ERR_NO_DEVICE, "no CUDA device visible");
+        }
+        need(device >= 0 && device < count, OFEA_ERR_INVALID_ARG, "device out of range");
+        OFEA_CUDA(cudaSetDevice(device));
+        cudaStream_t s = nullptr;
+        OFEA_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        try {
+            DevBuf<float> dA, dB, dD;
+            DevBuf<int> err;
+            dA.upload(A, (size_t)M * K, s);
+            dB.upload(B, (size_t)N * K, s);
+            dD.ensure((size_t)M * N);
+            err.ensure(1);
+            OFEA_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+            tc_gemm(s, M, N, K, 0, TcOperand{dA.p, K, 1}, TcOperand{dB.p, K, 1},
+                    TcEpilogue{kTcRowMajor, dD.p, nullptr, nullptr, 0}, err.p);
+            int herr = 0;
+            OFEA_CUDA(cudaMemcpyAsync(D, dD.p, sizeof(float) * M * N, cudaMemcpyDeviceToHost, s));
+            OFEA_CUDA(cudaMemcpyAsync(&herr, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+            OFEA_CUDA(cudaStreamSynchronize(s));
+            if (herr) fail(OFEA_ERR_TIMEOUT, "tensor-core product: a wait inside the kernel ran out");
+        } catch (...) {
+            cudaStreamDestroy(s);
+            throw;
+        }
+        cudaStreamDestroy(s);
     });
 }
 

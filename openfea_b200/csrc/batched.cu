@@ -1380,7 +1380,7 @@ void batch_tuning(ofea_batch *b, int method, int *rl, int *threads, int *ctas_pe
 // One graph launch per attempt; a pair whose true FP64 residual misses rtol
 // after the kernel (recurrence drift) is resumed from its u by the next
 // attempt.  stats: one per variant (worst load case).
-void batch_solve(ofea_batch *b, const ofea_solve_opts &o, ofea_solve_stats *stats) {
+void batch_solve(ofea_batch *b, const ofea_solve_opts &o, ofea_solve_stats *stats, ofea_solve_stats *case_stats) {
     if (o.method != OFEA_SOLVER_MIXED && o.method != OFEA_SOLVER_PCG64)
         fail(OFEA_ERR_UNKNOWN_SOLVER, "batch: method must be OFEA_SOLVER_PCG64 or OFEA_SOLVER_MIXED");
     if (!b->have_rhs) fail(OFEA_ERR_STATE, "batch: no load cases set");
@@ -1480,6 +1480,18 @@ void batch_solve(ofea_batch *b, const ofea_solve_opts &o, ofea_solve_stats *stat
             st.kernel_launches = launches;
         }
     }
+    if (case_stats)  // one entry per (variant, load case), load cases of a variant adjacent
+        for (int i = 0; i < VJ; ++i) {
+            ofea_solve_stats &st = case_stats[i];
+            st = ofea_solve_stats{};
+            st.status = hst[i];
+            if (st.status == OFEA_OK && !(hrel[i] <= o.rtol)) st.status = OFEA_ERR_NOT_CONVERGED;
+            st.iterations = iters_tot[i];
+            st.rel_residual = hrel[i];
+            st.refinements = attempts;
+            st.seconds = ms * 1e-3;
+            st.kernel_launches = launches;
+        }
 }
 
 // A cooperative launch whose barrier expects one CTA more than it has: every

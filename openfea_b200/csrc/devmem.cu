@@ -125,15 +125,25 @@ void dev_trim() {
 // ------------------------------------------------------ host block cache --
 // Large host blocks (host_pool.cuh): kept by rounded size, never returned to
 // the allocator until host_cache_trim(), so that the next context's vectors
-// land on pages that are already mapped.
+// land on pages that are already mapped.  Each block is also page-locked
+// (cudaHostRegister) when it is first allocated, so the device copies made
+// from it (mesh connectivity, coordinates, moduli) run as direct DMA at full
+// bus speed instead of through the driver's pageable staging; a block that
+// cannot be registered is used as it is.
 namespace ofea {
 namespace {
 
 constexpr std::size_t kHostSmall = 256u << 10, kHostGrain = 64u << 10, kHostCap = 1ull << 30;
 
+struct HostBlock {
+    void *p;
+    bool pinned;
+};
+
 struct HostCache {
     std::mutex mu;
-    std::multimap<std::size_t, void *> free;
+    std::multimap<std::size_t, HostBlock> free;
+    std::map<void *, bool> pinned;  // every large block handed out: registered or not
     std::size_t cached = 0;
 };
 
@@ -144,6 +154,11 @@ HostCache &host_cache() {
 
 std::size_t host_round(std::size_t bytes) { return (bytes + kHostGrain - 1) / kHostGrain * kHostGrain; }
 
+void release_block(void *p, bool pinned) {
+    if (pinned && cudaHostUnregister(p) != cudaSuccess) cudaGetLastError();
+    std::free(p);
+}
+
 }  // namespace
 
 void *host_cache_take(std::size_t bytes) {
@@ -153,19 +168,24 @@ void *host_cache_take(std::size_t bytes) {
         return p;
     }
     const std::size_t r = host_round(bytes);
+    HostCache &h = host_cache();
     {
-        HostCache &h = host_cache();
         std::lock_guard<std::mutex> lock(h.mu);
         auto it = h.free.find(r);
         if (it != h.free.end()) {
-            void *p = it->second;
+            HostBlock b = it->second;
             h.free.erase(it);
             h.cached -= r;
-            return p;
+            h.pinned[b.p] = b.pinned;
+            return b.p;
         }
     }
-    void *p = std::malloc(r);
+    void *p = std::aligned_alloc(4096, r);  // r is a multiple of 64 KB
     if (!p) throw std::bad_alloc();
+    bool pinned = cudaHostRegister(p, r, cudaHostRegisterDefault) == cudaSuccess;
+    if (!pinned) cudaGetLastError();
+    std::lock_guard<std::mutex> lock(h.mu);
+    h.pinned[p] = pinned;
     return p;
 }
 
@@ -178,18 +198,24 @@ void host_cache_give(void *p, std::size_t bytes) {
     const std::size_t r = host_round(bytes);
     HostCache &h = host_cache();
     std::lock_guard<std::mutex> lock(h.mu);
+    bool pinned = false;
+    auto it = h.pinned.find(p);
+    if (it != h.pinned.end()) {
+        pinned = it->second;
+        h.pinned.erase(it);
+    }
     if (h.cached + r > kHostCap) {
-        std::free(p);
+        release_block(p, pinned);
         return;
     }
-    h.free.emplace(r, p);
+    h.free.emplace(r, HostBlock{p, pinned});
     h.cached += r;
 }
 
 void host_cache_trim() {
     HostCache &h = host_cache();
     std::lock_guard<std::mutex> lock(h.mu);
-    for (auto &kv : h.free) std::free(kv.second);
+    for (auto &kv : h.free) release_block(kv.second.p, kv.second.pinned);
     h.free.clear();
     h.cached = 0;
 }

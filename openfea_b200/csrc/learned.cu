@@ -43,6 +43,7 @@
 #include <random>
 
 #include "precond.cuh"
+#include "tc_gemm.cuh"
 #include "sell.cuh"
 #include "solver_common.cuh"
 
@@ -167,113 +168,18 @@ __global__ void k_node_features(int na, const float *__restrict__ feat, const fl
 
 // ----------------------------------------------------------------- layers --
 
-// Z = X W^T + b (R x O, X is R x K, W is O x K), H = relu(Z) when H != null.
-// 64 x 64 tiles, K in chunks of 16, 256 threads with 4 x 4 outputs each.
-__global__ void __launch_bounds__(256) k_dense(long R, int O, int K, const float *__restrict__ X,
-                                               const float *__restrict__ W, const float *__restrict__ b,
-                                               float *__restrict__ Z, float *__restrict__ H) {
-    __shared__ float sX[64][17], sW[64][17];
-    const long r0 = (long)blockIdx.y * 64;
-    const int o0 = blockIdx.x * 64;
-    const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
-    float acc[4][4] = {};
-    for (int k0 = 0; k0 < K; k0 += 16) {
-        for (int v = threadIdx.x; v < 64 * 16; v += 256) {
-            const int i = v / 16, k = v % 16;
-            sX[i][k] = (r0 + i < R && k0 + k < K) ? X[(r0 + i) * K + k0 + k] : 0.f;
-            sW[i][k] = (o0 + i < O && k0 + k < K) ? W[(long)(o0 + i) * K + k0 + k] : 0.f;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            float xa[4], wb[4];
-#pragma unroll
-            for (int a = 0; a < 4; ++a) xa[a] = sX[tr * 4 + a][k];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) wb[q] = sW[tc * 4 + q][k];
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int q = 0; q < 4; ++q) acc[a][q] = fmaf(xa[a], wb[q], acc[a][q]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        const long r = r0 + tr * 4 + a;
-        if (r >= R) continue;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int o = o0 + tc * 4 + q;
-            if (o >= O) continue;
-            const float z = acc[a][q] + b[o];
-            Z[r * O + o] = z;
-            if (H) H[r * O + o] = z > 0.f ? z : 0.f;
-        }
-    }
-}
-
-// dX = dZ W  (R x K from R x O times O x K), same tiling.
-__global__ void __launch_bounds__(256) k_dense_bwd_data(long R, int O, int K, const float *__restrict__ dZ,
-                                                        const float *__restrict__ W, float *__restrict__ dX) {
-    __shared__ float sD[64][17], sW[16][65];
-    const long r0 = (long)blockIdx.y * 64;
-    const int k0 = blockIdx.x * 64;
-    const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
-    float acc[4][4] = {};
-    for (int o0 = 0; o0 < O; o0 += 16) {
-        for (int v = threadIdx.x; v < 64 * 16; v += 256) {
-            const int i = v / 16, o = v % 16;
-            sD[i][o] = (r0 + i < R && o0 + o < O) ? dZ[(r0 + i) * O + o0 + o] : 0.f;
-            const int oo = v / 64, kk = v % 64;
-            sW[oo][kk] = (o0 + oo < O && k0 + kk < K) ? W[(long)(o0 + oo) * K + k0 + kk] : 0.f;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int o = 0; o < 16; ++o) {
-            float da[4], wb[4];
-#pragma unroll
-            for (int a = 0; a < 4; ++a) da[a] = sD[tr * 4 + a][o];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) wb[q] = sW[o][tc * 4 + q];
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int q = 0; q < 4; ++q) acc[a][q] = fmaf(da[a], wb[q], acc[a][q]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        const long r = r0 + tr * 4 + a;
-        if (r >= R) continue;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int k = k0 + tc * 4 + q;
-            if (k < K) dX[r * K + k] = acc[a][q];
-        }
-    }
-}
-
-// Weight gradient partials: part[s][o*K + k] = sum over rows of chunk s of
-// dZ[r][o] X[r][k], part[s][O*K + o] = sum dZ[r][o] (bias).  One thread per
-// output, rows in order: summed afterwards in chunk order (deterministic).
-__global__ void __launch_bounds__(256) k_wgrad(long R, int O, int K, long chunk, const float *__restrict__ dZ,
-                                               const float *__restrict__ X, float *__restrict__ part) {
-    const int nout = O * K + O;
+// Bias-gradient partials: part[s][O*K + o] = sum over the rows of chunk s of
+// dZ[r][o], rows in order (the weight part of each partial comes from the
+// tensor-core product); summed afterwards in chunk order (deterministic).
+__global__ void k_bias_partials(long R, int O, int K, long chunk, const float *__restrict__ dZ,
+                                float *__restrict__ part) {
+    const int o = blockIdx.x * blockDim.x + threadIdx.x;
     const int s = blockIdx.y;
+    if (o >= O) return;
     const long rb = s * chunk, re = min(R, rb + chunk);
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nout; j += gridDim.x * blockDim.x) {
-        float acc = 0.f;
-        if (j < O * K) {
-            const int o = j / K, k = j % K;
-            for (long r = rb; r < re; ++r) acc = fmaf(dZ[r * O + o], X[r * K + k], acc);
-        } else {
-            const int o = j - O * K;
-            for (long r = rb; r < re; ++r) acc += dZ[r * O + o];
-        }
-        part[(long)s * nout + j] = acc;
-    }
+    float acc = 0.f;
+    for (long r = rb; r < re; ++r) acc += dZ[r * O + o];
+    part[(long)s * (O * K + O) + O * K + o] = acc;
 }
 
 // grad[j] = sum_s part[s][j] (fixed order), scattered to the W / b offsets.
@@ -849,6 +755,28 @@ static void upload_weights(ofea_ctx *c) {
     N.uploaded = true;
 }
 
+// The flag a tensor-core product sets when one of its waits ran out.
+static void tc_flag(ofea_ctx *c) {
+    Learned &N = c->learned;
+    if (!N.tc_err.p) {
+        N.tc_err.ensure(1);
+        OFEA_CUDA(cudaMemsetAsync(N.tc_err.p, 0, sizeof(int), c->stream));
+    }
+}
+
+// A tensor-core product whose wait ran out leaves the flag set: fail the call.
+static void check_tc(ofea_ctx *c) {
+    Learned &N = c->learned;
+    if (!N.tc_err.p) return;
+    int h = 0;
+    OFEA_CUDA(cudaMemcpyAsync(&h, N.tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    OFEA_CUDA(cudaStreamSynchronize(c->stream));
+    if (h) {
+        OFEA_CUDA(cudaMemsetAsync(N.tc_err.p, 0, sizeof(int), c->stream));
+        fail(OFEA_ERR_TIMEOUT, "learned stage: a tensor-core product's wait ran out");
+    }
+}
+
 // Network forward over the aggregates (input: the node features), scalings s.
 static void gnn_forward(ofea_ctx *c) {
     Learned &N = c->learned;
@@ -858,14 +786,18 @@ static void gnn_forward(ofea_ctx *c) {
     const int na = (int)R;
     const float *w = N.w.p;
     const int G = grid_for(c, R * kF, kBlock);
-    k_dense<<<dim3(tiles(kF, 64), tiles(R, 64)), 256, 0, s>>>(R, kF, kNFeat, N.X0.p, w + L.W0, w + L.b0, N.Z0.p,
-                                                              N.H[0].p);
+    tc_flag(c);
+    // Z = X W^T + b on the tensor cores (BF16 operands, FP32 accumulation)
+    auto dense = [&](int O, int K, const float *X, size_t offW, size_t offb, float *Z, float *H) {
+        tc_gemm(s, (int)R, O, K, 0, TcOperand{X, K, 1}, TcOperand{w + offW, K, 1},
+                TcEpilogue{kTcForward, Z, H, w + offb, 0}, N.tc_err.p);
+    };
+    dense(kF, kNFeat, N.X0.p, L.W0, L.b0, N.Z0.p, N.H[0].p);
     for (int l = 0; l < kLayers; ++l) {
         k_gnn_aggregate<<<G, kBlock, 0, s>>>(R, na, c->coarse2.nbr.p, N.invdeg.p, N.H[l].p, N.A[l].p);
-        k_dense<<<dim3(tiles(kF, 64), tiles(R, 64)), 256, 0, s>>>(R, kF, kA, N.A[l].p, w + L.W[l], w + L.b[l],
-                                                                 N.Zl[l].p, N.H[l + 1].p);
+        dense(kF, kA, N.A[l].p, L.W[l], L.b[l], N.Zl[l].p, N.H[l + 1].p);
     }
-    k_dense<<<dim3(1, tiles(R, 64)), 256, 0, s>>>(R, kOut, kF, N.H[kLayers].p, w + L.Wd, w + L.bd, N.Y.p, nullptr);
+    dense(kOut, kF, N.H[kLayers].p, L.Wd, L.bd, N.Y.p, nullptr);
     k_scales<<<grid_for(c, 6 * R, kBlock), kBlock, 0, s>>>((int)(6 * R), N.Y.p, N.scale.p);
     OFEA_CHECK_LAUNCH();
 }
@@ -879,21 +811,32 @@ static void gnn_backward(ofea_ctx *c) {
     const int na = (int)R;
     const float *w = N.w.p;
     float *g = N.g.p;
-    const long chunk = 2048;
+    const long chunk = 256;
     const int S = (int)((R + chunk - 1) / chunk);
     N.part.ensure((size_t)S * (kF * kA + kF));
+    tc_flag(c);
+    // weight gradient dZ^T X on the tensor cores, one partial per chunk of
+    // rows (output transposed: k_in is the tile's M), the bias sums beside it;
+    // partials summed in chunk order
     auto wgrad = [&](int O, int K, const float *dZ, const float *X, size_t offW, size_t offb) {
         const int nout = O * K + O;
-        k_wgrad<<<dim3(tiles(nout, 256), S), 256, 0, s>>>(R, O, K, chunk, dZ, X, N.part.p);
+        tc_gemm(s, K, O, R, chunk, TcOperand{X, 1, K}, TcOperand{dZ, 1, O},
+                TcEpilogue{kTcTransposedPartial, N.part.p, nullptr, nullptr, (long)nout}, N.tc_err.p);
+        k_bias_partials<<<dim3(tiles(O, 64), S), 64, 0, s>>>(R, O, K, chunk, dZ, N.part.p);
         k_wgrad_sum<<<tiles(nout, 256), 256, 0, s>>>(S, O, K, N.part.p, g + offW, g + offb);
     };
+    // dX = dZ W on the tensor cores
+    auto bwd_data = [&](int O, int K, const float *dZ, size_t offW, float *dX) {
+        tc_gemm(s, (int)R, K, O, 0, TcOperand{dZ, O, 1}, TcOperand{w + offW, 1, K},
+                TcEpilogue{kTcRowMajor, dX, nullptr, nullptr, 0}, N.tc_err.p);
+    };
     wgrad(kOut, kF, N.dY.p, N.H[kLayers].p, L.Wd, L.bd);
-    k_dense_bwd_data<<<dim3(tiles(kF, 64), tiles(R, 64)), 256, 0, s>>>(R, kOut, kF, N.dY.p, w + L.Wd, N.dH.p);
+    bwd_data(kOut, kF, N.dY.p, L.Wd, N.dH.p);
     const int Gf = grid_for(c, R * kF, kBlock);
     k_relu_bwd<<<Gf, kBlock, 0, s>>>(R * kF, N.dH.p, N.Zl[kLayers - 1].p, N.dZ.p);
     for (int l = kLayers - 1; l >= 0; --l) {
         wgrad(kF, kA, N.dZ.p, N.A[l].p, L.W[l], L.b[l]);
-        k_dense_bwd_data<<<dim3(tiles(kA, 64), tiles(R, 64)), 256, 0, s>>>(R, kF, kA, N.dZ.p, w + L.W[l], N.dA.p);
+        bwd_data(kF, kA, N.dZ.p, L.W[l], N.dA.p);
         const float *Zprev = l > 0 ? N.Zl[l - 1].p : N.Z0.p;
         k_gnn_aggregate_bwd<<<Gf, kBlock, 0, s>>>(R, na, c->coarse2.nbr.p, N.invdeg.p, N.dA.p, Zprev, N.dZ.p);
     }
@@ -1107,6 +1050,7 @@ void learned_train(ofea_ctx *c, int steps, int batch, float lr, unsigned seed, d
     OFEA_CUDA(cudaMemcpyAsync(N.host_w.data(), N.w.p, sizeof(float) * n, cudaMemcpyDeviceToHost, s));
     OFEA_CUDA(cudaStreamSynchronize(s));
     N.inference_ready = false;
+    check_tc(c);
     if (loss0) *loss0 = first;
     if (loss1) *loss1 = last;
 }
@@ -1124,6 +1068,7 @@ void learned_gradient(ofea_ctx *c, const float *h_x, int B, double *loss, float 
     const size_t n = Learned::layout().total;
     OFEA_CUDA(cudaMemcpyAsync(h_grad, N.g.p, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
     OFEA_CUDA(cudaStreamSynchronize(c->stream));
+    check_tc(c);
 }
 
 // Inference inside the V-cycle, after coarse_correct(t, x):

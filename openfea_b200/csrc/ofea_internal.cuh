@@ -160,6 +160,7 @@ struct Learned {
     DevBuf<float> Z0, H[5], A[4], Zl[4], Y, dY, dH, dZ, dA;  // network activations (one row per aggregate)
     DevBuf<float> pv[9];                                      // stage vectors (rows of a batch)
     DevBuf<float> batch_src, r32, data;
+    DevBuf<int> tc_err;  // set by a tensor-core product whose wait ran out
     long cap_rows = 0;
     int nlossp = 0, nsamples = 0, max_samples = 0;
 };
@@ -246,7 +247,8 @@ ofea_batch *batch_create(ofea_ctx *const *ctxs, int nv, int nrhs);
 void batch_destroy(ofea_batch *b);
 void batch_set_rhs(ofea_batch *b, const double *const *f);
 void batch_get_solution(ofea_batch *b, double *const *u);
-void batch_solve(ofea_batch *b, const ofea_solve_opts &o, ofea_solve_stats *stats);
+void batch_solve(ofea_batch *b, const ofea_solve_opts &o, ofea_solve_stats *stats,
+                 ofea_solve_stats *case_stats = nullptr);
 void batch_tuning(ofea_batch *b, int method, int *rl, int *threads, int *ctas_per_sm, double *ms_per_iter);
 void batch_set_trace(ofea_batch *b, int max_phases);
 void batch_phase_times(ofea_batch *b, double *ms, int cap, int *count);

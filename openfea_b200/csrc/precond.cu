@@ -476,44 +476,122 @@ __global__ void k_coarse_E_sum(int na, int nchunk_max, const int *__restrict__ a
 
 constexpr int kGJ = 64;
 
-// Inverse of the diagonal block A_JJ -> S (kGJ x kGJ), one CTA of 1024
-// threads, thread (ty, tx) owning rows ty, ty+16, ty+32, ty+48 of column tx.
-__global__ void __launch_bounds__(1024) k_gj_diag(int m, int j0, int bb, const double *__restrict__ A,
-                                                  double *__restrict__ S, const double *__restrict__ diag0) {
-    __shared__ double a[kGJ][kGJ + 1];
-    const int tx = threadIdx.x % kGJ, ty = threadIdx.x / kGJ;  // ty in 0..15
-    for (int rr = ty; rr < kGJ; rr += 16) a[rr][tx] = (rr < bb && tx < bb) ? A[(long)(j0 + rr) * m + j0 + tx] : 0.0;
-    __syncthreads();
-    for (int p = 0; p < bb; ++p) {
-        const double piv = a[p][p];
-        const bool drop = !(piv > 1e-12 * diag0[j0 + p]);
-        double rowp = a[p][tx];
-        double colp[4];
+// Gauss-Jordan inverse of a 32 x 32 block held by one warp, lane l owning
+// column l in registers (x[r] = entry (r, l)).  Pivot p: broadcast of the
+// pivot column by 32 shuffles, then the same update as a sequential
+// Gauss-Jordan step; the pivot row is each lane's own x[p].  A pivot that
+// vanishes against the original diagonal (a degenerate aggregate) drops its
+// direction: row and column p of the result are zero.  Pivots p >= bb are
+// padding (their rows and columns are zero and stay so).
+__device__ __forceinline__ void warp_gj32(double (&x)[32], int bb, const double *__restrict__ diag0) {
+    const int lane = threadIdx.x & 31;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) colp[q] = a[ty + 16 * q][p];
-        __syncthreads();
-        if (drop) {
-            // a vanishing pivot (degenerate aggregate) drops its direction
+    for (int p = 0; p < 32; ++p) {
+        if (p >= bb) break;
+        double colp[32];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int rr = ty + 16 * q;
-                if (rr == p || tx == p) a[rr][tx] = 0.0;
-            }
+        for (int r = 0; r < 32; ++r) colp[r] = __shfl_sync(0xffffffffu, x[r], p);
+        const double piv = colp[p];
+        const double rowp = x[p];
+        if (!(piv > 1e-12 * diag0[p])) {
+            x[p] = 0.0;
+            if (lane == p)
+#pragma unroll
+                for (int r = 0; r < 32; ++r) x[r] = 0.0;
         } else {
             const double inv = 1.0 / piv;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int rr = ty + 16 * q;
-                if (rr >= bb || tx >= bb) continue;
-                if (rr == p && tx == p) a[rr][tx] = inv;
-                else if (rr == p) a[rr][tx] = rowp * inv;
-                else if (tx == p) a[rr][tx] = -colp[q] * inv;
-                else a[rr][tx] -= colp[q] * rowp * inv;
+            for (int r = 0; r < 32; ++r) {
+                if (r == p) continue;
+                x[r] = (lane == p) ? -colp[r] * inv : x[r] - colp[r] * rowp * inv;
             }
+            x[p] = (lane == p) ? inv : rowp * inv;
+        }
+    }
+}
+
+// Inverse of the diagonal block A_JJ -> S (kGJ x kGJ, padded with zeros
+// beyond bb), one CTA of 4 warps.  With A_JJ = [A11 A12; A21 A22] in 32 x 32
+// blocks: X11 = A11^-1, T = X11 A12, U = A21 X11, X22 = (A22 - A21 T)^-1,
+// S = [X11 + T X22 U, -T X22; -X22 U, X22]: the block form of the same 64
+// Gauss-Jordan pivots (a dropped pivot zeroes its row and column here too),
+// with two warp-level 32-pivot eliminations in place of 64 CTA-wide steps.
+constexpr size_t kGjDiagSmem = sizeof(double) * (kGJ * (kGJ + 1) + 2 * 32 * 33);
+
+__global__ void __launch_bounds__(128) k_gj_diag(int m, int j0, int bb, const double *__restrict__ A,
+                                                 double *__restrict__ S, const double *__restrict__ diag0) {
+    extern __shared__ double gj_smem[];
+    double (*a)[kGJ + 1] = reinterpret_cast<double (*)[kGJ + 1]>(gj_smem);          // [64][65]
+    double (*t)[33] = reinterpret_cast<double (*)[33]>(gj_smem + kGJ * (kGJ + 1));  // [32][33]
+    double (*u)[33] = t + 32;                                                       // [32][33]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int v = tid; v < kGJ * kGJ; v += 128) {
+        const int r = v / kGJ, c = v % kGJ;
+        a[r][c] = (r < bb && c < bb) ? A[(long)(j0 + r) * m + j0 + c] : 0.0;
+    }
+    __syncthreads();
+    const int b1 = min(bb, 32), b2 = bb - b1;
+    if (warp == 0) {  // X11 in place of A11
+        double x[32];
+#pragma unroll
+        for (int r = 0; r < 32; ++r) x[r] = a[r][lane];
+        warp_gj32(x, b1, diag0 + j0);
+#pragma unroll
+        for (int r = 0; r < 32; ++r) a[r][lane] = x[r];
+    }
+    __syncthreads();
+    if (b2 > 0) {
+        // T = X11 A12 and U = A21 X11 (thread: column lane, rows warp + 4 q)
+        for (int q = 0; q < 8; ++q) {
+            const int r = warp + 4 * q;
+            double st = 0.0, su = 0.0;
+            for (int k = 0; k < 32; ++k) {
+                st = fma(a[r][k], a[k][32 + lane], st);
+                su = fma(a[32 + r][k], a[k][lane], su);
+            }
+            t[r][lane] = st;
+            u[r][lane] = su;
+        }
+        __syncthreads();
+        // Schur complement A22 - A21 T, in place of A22
+        for (int q = 0; q < 8; ++q) {
+            const int r = warp + 4 * q;
+            double s2 = 0.0;
+            for (int k = 0; k < 32; ++k) s2 = fma(a[32 + r][k], t[k][lane], s2);
+            a[32 + r][32 + lane] -= s2;
+        }
+        __syncthreads();
+        if (warp == 0) {  // X22 in place of the Schur complement
+            double x[32];
+#pragma unroll
+            for (int r = 0; r < 32; ++r) x[r] = a[32 + r][32 + lane];
+            warp_gj32(x, b2, diag0 + j0 + 32);
+#pragma unroll
+            for (int r = 0; r < 32; ++r) a[32 + r][32 + lane] = x[r];
+        }
+        __syncthreads();
+        // S12 = -T X22 in place of A12, S21 = -X22 U in place of A21
+        for (int q = 0; q < 8; ++q) {
+            const int r = warp + 4 * q;
+            double s12 = 0.0, s21 = 0.0;
+            for (int k = 0; k < 32; ++k) {
+                s12 = fma(t[r][k], a[32 + k][32 + lane], s12);
+                s21 = fma(a[32 + r][32 + k], u[k][lane], s21);
+            }
+            a[r][32 + lane] = -s12;
+            a[32 + r][lane] = -s21;
+        }
+        __syncthreads();
+        // S11 = X11 - T S21, in place of X11 (each thread reads only its own X11 entry)
+        for (int q = 0; q < 8; ++q) {
+            const int r = warp + 4 * q;
+            double s11 = 0.0;
+            for (int k = 0; k < 32; ++k) s11 = fma(t[r][k], a[32 + k][lane], s11);
+            a[r][lane] -= s11;
         }
         __syncthreads();
     }
-    for (int rr = ty; rr < kGJ; rr += 16) S[rr * kGJ + tx] = a[rr][tx];
+    for (int v = tid; v < kGJ * kGJ; v += 128) S[v] = a[v / kGJ][v % kGJ];
 }
 
 // Column panel, one warp per row i: P_i = A_{i,J} (saved for the update),
@@ -672,6 +750,7 @@ static void invert_spd(ofea_ctx *c, double *A, int m, int hb) {
     OFEA_CHECK_LAUNCH();
     const size_t upd_smem = sizeof(double) * (64 * (kGJ + 1) + kGJ * 65);
     OFEA_CUDA(cudaFuncSetAttribute(k_gj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem));
+    OFEA_CUDA(cudaFuncSetAttribute(k_gj_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGjDiagSmem));
     cudaEvent_t cross_done = nullptr, rest_done = nullptr;
     OFEA_CUDA(cudaEventCreateWithFlags(&cross_done, cudaEventDisableTiming));
     OFEA_CUDA(cudaEventCreateWithFlags(&rest_done, cudaEventDisableTiming));
@@ -681,7 +760,7 @@ static void invert_spd(ofea_ctx *c, double *A, int m, int hb) {
         const int lim = (int)std::min<long>(m, (long)j0 + bb + hb);
         dim3 tiles((lim + 63) / 64, (lim + 63) / 64);
         double *P = C.P.p + (size_t)(it & 1) * m * kGJ;
-        k_gj_diag<<<1, 1024, 0, s>>>(m, j0, bb, A, C.S.p, C.diag0.p);
+        k_gj_diag<<<1, 128, kGjDiagSmem, s>>>(m, j0, bb, A, C.S.p, C.diag0.p);
         k_gj_panel<<<grid_for(c, (long)lim * 32, 256), 256, 0, s>>>(m, lim, j0, bb, A, C.S.p, P);
         k_gj_rows<<<std::max(1, std::min((lim + 31) / 32, c->num_sms * 4)), 256, 0, s>>>(m, lim, j0, bb, A, C.S.p);
         if (rest_pending) OFEA_CUDA(cudaStreamWaitEvent(s, rest_done, 0));  // the previous panel's update is complete

@@ -19,6 +19,9 @@
 // Like the reference it writes the displacement into single_dis_vec_ (linear)
 // or x (Newton increment) and returns false on failure; it never exits.
 //
+// gpu_implicit_analysis() is the other binding point: it replaces the
+// CPU assembly and the solve of CAE_process::implict_analysis together.
+//
 // Settings (environment, read on first use): OFEA_DEVICE (GPU index, 0),
 // OFEA_RTOL (relative FP64 residual, 1e-10: a direct solve's accuracy),
 // OFEA_LEARNED_WEIGHTS (weight file for GPU_LEARNED; without it the stage is
@@ -99,6 +102,46 @@ bool gpu_solve(vector<int> &col_idx, vector<int> &row_idx, vector<double> &nz_va
 }
 
 }  // namespace
+
+// The whole linear analysis on the GPU, for CAE_process::implict_analysis
+// (src/cae.cpp:259-275): in place of build_CSR + fill_CSR_sparse_mat +
+// solution_api, the mesh goes to the device, which builds the pattern,
+// assembles K and solves; single_dis_vec_ receives u as before.
+bool gpu_implicit_analysis(data_management &d, elastic_mat &mat, string solver_type) {
+    const int method = gpu_method(solver_type);
+    ofea_ctx *ctx = method < 0 ? nullptr : thread_context();
+    if (!ctx) return false;
+    std::vector<double> xyz(3 * (size_t)d.nd_);
+    for (int i = 0; i < d.nd_; ++i)
+        for (int c = 0; c < 3; ++c) xyz[3 * (size_t)i + c] = d.coords_[i][c];
+    std::vector<int> topo(8 * (size_t)d.ne_), etype(d.ne_);
+    for (int e = 0; e < d.ne_; ++e) {
+        etype[e] = d.ele_list_idx_[e];  // ELE_TYPES: 0 C3D4, 1 C3D8
+        for (int a = 0; a < 8; ++a) topo[8 * (size_t)e + a] = d.node_topos_[e][a];  // 1-based, as read
+    }
+    int n = 0;
+    long long nnz = 0;
+    if (!report(ofea_mesh_upload(ctx, d.nd_, xyz.data(), d.ne_, topo.data(), etype.data(), nullptr,
+                                 mat.young_modulus, mat.poisson_ratio, d.resort_free_nodes_.data()),
+                "ofea_mesh_upload") ||
+        !report(ofea_assemble_pattern(ctx, &n, &nnz), "ofea_assemble_pattern") ||
+        !report(ofea_assemble_linear(ctx), "ofea_assemble_linear"))
+        return false;
+    if (method == OFEA_SOLVER_LEARNED) {
+        const char *path = std::getenv("OFEA_LEARNED_WEIGHTS");
+        int rc = path ? ofea_learned_load(ctx, path) : ofea_learned_train(ctx, nullptr, nullptr, nullptr);
+        if (!report(rc, path ? "ofea_learned_load" : "ofea_learned_train")) return false;
+    }
+    ofea_solve_opts opts;
+    ofea_solve_opts_default(&opts);
+    opts.method = method;
+    const char *rtol = std::getenv("OFEA_RTOL");
+    opts.rtol = rtol ? std::atof(rtol) : 1e-10;
+    ofea_solve_stats st;
+    d.single_dis_vec_.assign(n, 0.0);
+    return report(ofea_solve(ctx, d.single_load_vec_.data(), d.single_dis_vec_.data(), 1, &opts, &st),
+                  "ofea_solve");
+}
 
 bool solution_api(assamble_stiffness &item_ass, data_management &item_cae_data, string solver_type) {
     const int method = gpu_method(solver_type);

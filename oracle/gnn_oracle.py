@@ -20,6 +20,9 @@ Stage (linear and symmetric in the scaled coarse residual x):
 a polynomial in B Ehat with trainable global coefficients c (in the weight
 vector) between per-aggregate, per-mode scalings s set by the network.
 
+The dense products may be evaluated on bfloat16-rounded operands (bf16=True),
+as the GPU's tensor-core layers do.
+
 Loss over a batch of inputs x_b (the energy; its minimiser is Ehat^-1 x):
   L = sum_b (1/2 y_b . Ehat y_b - y_b . x_b) / (6 na)
 The backward pass here is checked against central finite differences
@@ -52,12 +55,25 @@ SLOTS = np.arange(27)
 DX, DY, DZ = SLOTS // 9 - 1, (SLOTS // 3) % 3 - 1, SLOTS % 3 - 1
 
 
+def bf16(x):
+    """Round to bfloat16 (nearest even) through float32, as the GPU's
+    tensor-core layers round their FP32 operands; returned as float64."""
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
 def unpack(w):
     return {k: w[o:o + int(np.prod(s))].reshape(s) for k, (o, s) in OFF.items()}
 
 
 class GNNOracle:
-    def __init__(self, nbr, Ehat, feat):
+    """bf16=True rounds both operands of every dense-layer product to
+    bfloat16 (the GPU runs those products on the tensor cores with BF16
+    operands and FP32 accumulation); everything else stays FP64."""
+
+    def __init__(self, nbr, Ehat, feat, bf16=False):
+        self.r = globals()["bf16"] if bf16 else (lambda v: v)
         self.nbr = np.asarray(nbr).reshape(-1, 27)
         self.na = self.nbr.shape[0]
         self.E = np.asarray(Ehat, dtype=np.float64).reshape(self.na, 27, 6, 6)
@@ -127,17 +143,18 @@ class GNNOracle:
     def forward(self, w):
         p = unpack(np.asarray(w, dtype=np.float64))
         cache = {}
-        Z = self.feat @ p["W0"].T + p["b0"]
+        r = self.r
+        Z = r(self.feat) @ r(p["W0"]).T + p["b0"]
         cache["Z0"] = Z
         H = np.maximum(Z, 0)
         for l in range(L):
             Aa = self.agg(H)
             cache[f"A{l}"] = Aa
-            Z = Aa @ p[f"W{l + 1}"].T + p[f"b{l + 1}"]
+            Z = r(Aa) @ r(p[f"W{l + 1}"]).T + p[f"b{l + 1}"]
             cache[f"Z{l + 1}"] = Z
             H = np.maximum(Z, 0)
         cache["H"] = H
-        Y = H @ p["Wd"].T + p["bd"]
+        Y = r(H) @ r(p["Wd"]).T + p["bd"]
         return Y, cache, p
 
     def scales(self, w):
@@ -165,20 +182,21 @@ class GNNOracle:
         # y = s * M (s * x):  dL/ds = d * M(s x) + x * M(s d)  (M symmetric)
         ds = np.sum(d * wv + x * self.apply_M(sc * d, p["c0"]), axis=0)
         g = {"c0": np.array([np.sum(sc * d * vk) for vk in V])}
+        r = self.r
         dY = 0.5 * ds * sc[0]
-        g["Wd"] = dY.T @ c["H"]
+        g["Wd"] = r(dY).T @ r(c["H"])
         g["bd"] = dY.sum(axis=0)
-        dH = dY @ p["Wd"]
+        dH = r(dY) @ r(p["Wd"])
         dZ = dH * (c[f"Z{L}"] > 0)
         for l in reversed(range(L)):
             Aa = c[f"A{l}"]
-            g[f"W{l + 1}"] = dZ.T @ Aa
+            g[f"W{l + 1}"] = r(dZ).T @ r(Aa)
             g[f"b{l + 1}"] = dZ.sum(axis=0)
-            dA = dZ @ p[f"W{l + 1}"]
+            dA = r(dZ) @ r(p[f"W{l + 1}"])
             dH = self.agg_bwd(dA)
             Zp = c[f"Z{l}"] if l > 0 else c["Z0"]
             dZ = dH * (Zp > 0)
-        g["W0"] = dZ.T @ self.feat
+        g["W0"] = r(dZ).T @ r(self.feat)
         g["b0"] = dZ.sum(axis=0)
         flat = np.zeros(TOTAL)
         for k, (o, s) in OFF.items():

@@ -162,8 +162,10 @@ class Reference:
         L.ref_model_nl_solve.argtypes = [_P, _P, _P]
         L.ref_model_solve_multi.restype = _I
         L.ref_model_solve_multi.argtypes = [_P, _I, _P, _P]
-        L.ref_model_cg_ic.restype = _I
-        L.ref_model_cg_ic.argtypes = [_P, _P, _P, _D, _I, _I, _I, _P]
+        L.ref_model_cg_ic_setup.restype = _D
+        L.ref_model_cg_ic_setup.argtypes = [_P, _I]
+        L.ref_model_cg_ic_run.restype = _I
+        L.ref_model_cg_ic_run.argtypes = [_P, _P, _P, _D, _I, _P]
         L.ref_element_ke.argtypes = [_I, _P, _D, _D, _P]
         L.ref_element_nl.argtypes = [_I, _P, _P, _D, _D, _P, _P]
         self.L = L
@@ -252,19 +254,30 @@ class RefModel:
             raise RuntimeError("reference SuperLU_class solve failed")
         return U
 
-    def cg_ic(self, f, rtol=1e-10, max_iter=100000, threads=1, ordering="natural", u0=None):
-        """Vendored Eigen ConjugateGradient + IncompleteCholesky (FP64) on the
-        reference-assembled K (call assemble() first).  Returns u and a dict of
-        iterations, true relative residual and set-up / CG seconds."""
+    def cg_ic_setup(self, threads=1):
+        """Vendored Eigen IncompleteCholesky of the reference-assembled K
+        (call assemble() first); returns the set-up seconds."""
+        t = self.r.L.ref_model_cg_ic_setup(self.h, threads)
+        if t < 0:
+            raise RuntimeError(f"Eigen IC set-up failed ({t})")
+        return t
+
+    def cg_ic_run(self, f, rtol=1e-10, max_iter=100000, u0=None):
+        """One Eigen ConjugateGradient solve (FP64) with the IC factor of
+        cg_ic_setup, started from u0 (zero)."""
         f = _f64(f)
         u = np.zeros(self.n) if u0 is None else _f64(u0).copy()
-        out = np.zeros(5)
-        st = self.r.L.ref_model_cg_ic(self.h, _ptr(f), _ptr(u), rtol, max_iter, threads,
-                                      1 if ordering == "amd" else 0, _ptr(out))
-        if st != 0:
-            raise RuntimeError(f"Eigen CG+IC failed ({st})")
-        return u, dict(iterations=int(out[0]), est_rel_residual=out[1], rel_residual=out[2],
-                       setup_s=out[3], cg_s=out[4], threads=threads, ordering=ordering)
+        out = np.zeros(4)
+        if self.r.L.ref_model_cg_ic_run(self.h, _ptr(f), _ptr(u), rtol, max_iter, _ptr(out)) != 0:
+            raise RuntimeError("Eigen CG: no IC set-up")
+        return u, dict(iterations=int(out[0]), est_rel_residual=out[1], rel_residual=out[2], cg_s=out[3])
+
+    def cg_ic(self, f, rtol=1e-10, max_iter=100000, threads=1, u0=None):
+        """IC set-up + one CG solve; the stats carry both times."""
+        t = self.cg_ic_setup(threads)
+        u, st = self.cg_ic_run(f, rtol, max_iter, u0)
+        st.update(setup_s=t, threads=threads, ordering="natural")
+        return u, st
 
     def full_displacement(self):
         uf = np.zeros(3 * self.nd)

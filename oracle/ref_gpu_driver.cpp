@@ -10,9 +10,11 @@
 // ("Pardiso_class", src/cae.cpp:232,274), which this driver takes from the
 // command line instead.
 //
-//   ref_gpu_driver -i model.inp -o out.vtk -solver GPU_PCG [-nl] [-E 2.1e5 -nu 0.3]
+//   ref_gpu_driver -i model.inp -o out.vtk -solver GPU_PCG [-nl] [-gpu-assembly] [-E 2.1e5 -nu 0.3]
 //
 // -E / -nu override the file's *Elastic (the shipped CA sample has none).
+// -gpu-assembly runs the linear analysis through gpu_implicit_analysis (the
+// binding that also moves build_CSR + fill_CSR_sparse_mat to the device).
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -29,11 +31,15 @@
 #include "include/post_process.h"
 #include "include/set_bcs.h"
 
+namespace CAE {
+bool gpu_implicit_analysis(data_management &d, elastic_mat &mat, string solver_type);
+}
+
 using namespace CAE;
 
 int main(int argc, char **argv) {
     std::string in, out, solver = "GPU_PCG";
-    bool nl = false, override_mat = false;
+    bool nl = false, override_mat = false, gpu_assembly = false;
     double E = 0, nu = 0;
     for (int i = 1; i < argc; ++i) {
         std::string a = argv[i];
@@ -41,6 +47,7 @@ int main(int argc, char **argv) {
         else if (a == "-o" && i + 1 < argc) out = argv[++i];
         else if (a == "-solver" && i + 1 < argc) solver = argv[++i];
         else if (a == "-nl") nl = true;
+        else if (a == "-gpu-assembly") gpu_assembly = true;
         else if (a == "-E" && i + 1 < argc) E = std::atof(argv[++i]), override_mat = true;
         else if (a == "-nu" && i + 1 < argc) nu = std::atof(argv[++i]), override_mat = true;
         else {
@@ -90,6 +97,8 @@ int main(int argc, char **argv) {
             std::printf("newton %d residual %.6e\n", loop, res_norm);
         }
         data.single_dis_vec_ = u;
+    } else if (gpu_assembly) {
+        if (!gpu_implicit_analysis(data, mat, solver)) return 1;
     } else {
         assamble_stiffness assam;
         assam.build_CSR(data);

@@ -35,6 +35,19 @@
 using namespace CAE;
 
 namespace {
+// Eigen CG + IC solver of the scale oracle on a model's K.  K is symmetric,
+// so the reference's CSC arrays are read as CSR, which lets Eigen's SpMV use
+// OpenMP threads (the IC triangular solves are serial).
+struct CgIc {
+    typedef Eigen::SparseMatrix<double, Eigen::RowMajor, int> SpR;
+    Eigen::Map<const SpR> K;
+    Eigen::ConjugateGradient<SpR, Eigen::Lower | Eigen::Upper,
+                             Eigen::IncompleteCholesky<double, Eigen::Lower, Eigen::NaturalOrdering<int>>>
+        cg;
+    CgIc(int n, assamble_stiffness &A)
+        : K(n, n, (int)A.nz_val_.size(), A.col_idx_.data(), A.row_idx_.data(), A.nz_val_.data()) {}
+};
+
 struct RefModel {
     data_management data;
     elastic_mat mat{};
@@ -42,6 +55,8 @@ struct RefModel {
     assamble_nl_stiffness nl;
     std::vector<double> E_elem;  // empty -> one material for all elements
     double t_csr = 0, t_fill = 0, t_solve = 0;
+    CgIc *cgic = nullptr;
+    ~RefModel() { delete cgic; }
 };
 
 double now_s() {
@@ -268,64 +283,53 @@ int ref_model_solve_multi(void *h, int nrhs, const double *F, double *U) {
 // The scale oracle where a direct factor does not fit in time: the vendored
 // Eigen 3.4.0 ConjugateGradient (FP64) with its IncompleteCholesky
 // preconditioner (Lin-More modified IC, externals/eigen-3.4.0/Eigen/src/
-// IterativeLinearSolvers/IncompleteCholesky.h) on the reference-assembled K.
-// K is symmetric, so the reference's CSC arrays are read as CSR, which lets
-// Eigen's SpMV use `threads` OpenMP threads (the IC triangular solves are
-// serial).  ordering: 0 natural (the reference's node-interleaved numbering),
-// 1 AMD.  u holds the start vector on entry.  Stops at ||f - K u|| <= tol ||f||
-// or after maxit iterations.  out[0..4] = iterations, Eigen's residual
-// estimate, the FP64 true relative residual, IC set-up seconds, CG seconds.
-int ref_model_cg_ic(void *h, const double *f, double *u, double tol, int maxit, int threads,
-                    int ordering, double *out) {
+// IterativeLinearSolvers/IncompleteCholesky.h) on the reference-assembled K,
+// in the reference's own node-interleaved numbering (natural ordering: fewer
+// iterations than AMD here, 101 against 165 on a 40x10x10 cantilever).
+// ref_model_cg_ic_setup factors once; each ref_model_cg_ic_run is one CG
+// solve with that factor.
+
+// IC set-up on the current K; returns its seconds, or a negative value.
+double ref_model_cg_ic_setup(void *h, int threads) {
     RefModel *m = (RefModel *)h;
     assamble_stiffness &A = m->lin;
-    if (A.col_idx_.empty()) return -1;
-    int n = (int)A.col_idx_.size() - 1;
-    typedef Eigen::SparseMatrix<double, Eigen::RowMajor, int> SpR;
-    Eigen::Map<const SpR> K(n, n, (int)A.nz_val_.size(), A.col_idx_.data(), A.row_idx_.data(),
-                            A.nz_val_.data());
-    Eigen::Map<const Eigen::VectorXd> b(f, n);
-    Eigen::Map<Eigen::VectorXd> x(u, n);
+    if (A.col_idx_.empty()) return -1.0;
 #ifdef _OPENMP
     Eigen::setNbThreads(threads > 0 ? threads : 1);
 #else
     (void)threads;
 #endif
-    double t0 = now_s(), t1, t2;
-    int its = 0;
-    double est = 0;
-    bool ok;
-    auto run = [&](auto &cg) {
-        cg.setTolerance(tol);
-        cg.setMaxIterations(maxit);
-        cg.compute(K);
-        t1 = now_s();
-        if (cg.info() != Eigen::Success) return false;
-        Eigen::VectorXd x0 = x;
-        x = cg.solveWithGuess(b, x0);
-        t2 = now_s();
-        its = (int)cg.iterations();
-        est = cg.error();
-        return true;
-    };
-    if (ordering == 1) {
-        Eigen::ConjugateGradient<SpR, Eigen::Lower | Eigen::Upper,
-                                 Eigen::IncompleteCholesky<double, Eigen::Lower, Eigen::AMDOrdering<int>>>
-            cg;
-        ok = run(cg);
-    } else {
-        Eigen::ConjugateGradient<SpR, Eigen::Lower | Eigen::Upper,
-                                 Eigen::IncompleteCholesky<double, Eigen::Lower, Eigen::NaturalOrdering<int>>>
-            cg;
-        ok = run(cg);
-    }
-    if (!ok) return -2;
-    Eigen::VectorXd r = b - K * x;
-    out[0] = its;
-    out[1] = est;
+    const int n = (int)A.col_idx_.size() - 1;
+    const double t0 = now_s();
+    delete m->cgic;
+    m->cgic = new CgIc(n, A);
+    m->cgic->cg.compute(m->cgic->K);
+    if (m->cgic->cg.info() != Eigen::Success) return -2.0;
+    return now_s() - t0;
+}
+
+// One CG solve with the factor of ref_model_cg_ic_setup, started from u:
+// stops at ||f - K u|| <= tol ||f|| (Eigen's recursive residual) or after
+// maxit iterations.  out[0..3] = iterations, Eigen's residual estimate, the
+// FP64 true relative residual, CG seconds.
+int ref_model_cg_ic_run(void *h, const double *f, double *u, double tol, int maxit, double *out) {
+    RefModel *m = (RefModel *)h;
+    CgIc *s = m->cgic;
+    if (!s) return -1;
+    const int n = (int)s->K.rows();
+    Eigen::Map<const Eigen::VectorXd> b(f, n);
+    Eigen::Map<Eigen::VectorXd> x(u, n);
+    s->cg.setTolerance(tol);
+    s->cg.setMaxIterations(maxit);
+    const double t0 = now_s();
+    Eigen::VectorXd x0 = x;
+    x = s->cg.solveWithGuess(b, x0);
+    const double t1 = now_s();
+    Eigen::VectorXd r = b - s->K * x;
+    out[0] = (double)s->cg.iterations();
+    out[1] = s->cg.error();
     out[2] = r.norm() / b.norm();
     out[3] = t1 - t0;
-    out[4] = t2 - t1;
     return 0;
 }
 

@@ -84,15 +84,19 @@ def run_driver(args, tmp_path, tag):
     return out, r.stdout
 
 
-@pytest.mark.parametrize("solver", ["GPU_PCG", "GPU_MIXED", "GPU_LEARNED"])
-def test_reference_flow_with_gpu_solution_api(golden, inp_file, tmp_path, solver):
+@pytest.mark.parametrize("solver, where", [("GPU_PCG", "solution_api"), ("GPU_MIXED", "solution_api"),
+                                           ("GPU_LEARNED", "solution_api"), ("GPU_MIXED", "implict_analysis")])
+def test_reference_flow_with_gpu_solution_api(golden, inp_file, tmp_path, solver, where):
     """The shipped sample (sample_model/CA/mesh_o.inp, E = 2.1e5, nu = 0.3):
-    the reference's own driver sequence with solution_api("GPU_*") writes the
-    golden cadcae_o.vtk displacement to its 6 printed digits."""
+    the reference's own driver sequence with solution_api("GPU_*") (K
+    assembled by the reference), or with gpu_implicit_analysis in place of
+    its assembly and solve, writes the golden cadcae_o.vtk displacement to its
+    6 printed digits."""
     if not os.path.exists(DRIVER):
         pytest.skip("oracle/_ref/ref_gpu_driver not built (needs the reference tree)")
     args = ["-i", inp_file("mesh_o.inp"), "-E", "2.1e5", "-nu", "0.3"]
-    out_gpu, _ = run_driver(args + ["-solver", solver], tmp_path, solver)
+    extra = ["-gpu-assembly"] if where == "implict_analysis" else []
+    out_gpu, _ = run_driver(args + ["-solver", solver] + extra, tmp_path, solver + where)
     out_cpu, _ = run_driver(args + ["-solver", "SuperLU_func"], tmp_path, "superlu")
     ug = golden("cadcae_o_u.npz")["u"].reshape(-1, 3)
     u_gpu, u_cpu = read_vtk_u(out_gpu, ug.shape[0]), read_vtk_u(out_cpu, ug.shape[0])

@@ -32,10 +32,12 @@ def test_gradient_matches_cpu_oracle(gpu_ctx_factory):
     ctx.set_learned_weights(w)
     x = np.random.default_rng(6).normal(0, 1, (2, nbr.shape[0], 6)).astype(np.float32)
     loss_g, g_gpu = ctx.learned_gradient(x)
-    net = GNNOracle(nbr, E.astype(np.float64), feat.astype(np.float64))
+    # the dense layers run on the tensor cores with BF16 operands: the oracle
+    # rounds the same operands to BF16 and computes in FP64
+    net = GNNOracle(nbr, E.astype(np.float64), feat.astype(np.float64), bf16=True)
     loss_c, g_cpu = net.grad(w.astype(np.float64), x.astype(np.float64))
     assert g_gpu.size == TOTAL
-    # FP32 kernels against the FP64 oracle
+    # FP32 accumulation against the FP64 oracle
     assert abs(loss_g - loss_c) <= 1e-4 * abs(loss_c)
     assert np.abs(g_gpu - g_cpu).max() <= 1e-4 * np.abs(g_cpu).max()
 

@@ -112,3 +112,30 @@ def test_vtk_writer_layout(tmp_path, golden, inp_file):
     t = m.topo[0]
     assert L2[k + 1] == "\t".join(map(str, [8] + [t[a] - 1 for a in (0, 1, 3, 2, 4, 5, 7, 6)]))
     assert L2[L2.index("CELL_TYPES\t\t1") + 1] == "11"
+
+
+def test_solution_api_binding_forwards_cpu_solvers(golden, inp_file, tmp_path):
+    """The reference-side binding (openfea_b200/integration/ofea_solution_api.cpp)
+    compiles against the reference's headers and, for the reference's own
+    solver strings, hands the call to the reference's dispatch unchanged: the
+    reference's flow through it with "SuperLU_func" writes the shipped
+    cadcae_o.vtk displacement (6 printed digits).  No GPU is involved."""
+    import subprocess
+    drv = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_driver")
+    if not os.path.exists(drv):
+        pytest.skip("oracle/_ref/ref_gpu_driver not built (needs the reference tree)")
+    out = tmp_path / "o.vtk"
+    r = subprocess.run([drv, "-i", inp_file("mesh_o.inp"), "-o", str(out), "-solver", "SuperLU_func",
+                        "-E", "2.1e5", "-nu", "0.3"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = out.read_text().split("\n")
+    ug = golden("cadcae_o_u.npz")["u"].reshape(-1, 3)
+    for c, name in enumerate("xyz"):
+        j = lines.index(f"SCALARS u_{name} double 1")
+        v = np.array([float(x) for x in lines[j + 2:j + 2 + ug.shape[0]]])
+        assert np.abs(v - ug[:, c]).max() <= 3e-6 * np.abs(ug).max()
+    if not has_gpu():
+        # a GPU solver string without a GPU fails with the library's status, no exit()
+        r = subprocess.run([drv, "-i", inp_file("mesh_o.inp"), "-o", str(tmp_path / "g.vtk"), "-solver",
+                            "GPU_PCG", "-E", "2.1e5", "-nu", "0.3"], capture_output=True, text=True, timeout=300)
+        assert r.returncode == 1 and "no CUDA device" in r.stderr
