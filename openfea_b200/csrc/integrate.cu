@@ -303,6 +303,99 @@ __global__ void __launch_bounds__(128) k_hex_integrate(
     }
 }
 
+// Linear C3D8 element blocks, kLinHex elements per CTA of 128 threads.
+// Phase 1, thread (element, q): J at Gauss point q, det J (the weight) and
+// the gradients of all 8 shape functions, once per point.  Phase 2, thread
+// per upper block (a <= b) of an element: T = sum_q w g_a g_b^T and
+// d = sum_q w g_a . g_b, then K_ab = lam T + mu T^T + mu d I and
+// K_ba = K_ab^T (the same sums, so Ke is exactly symmetric): the nodal-block
+// form of B^T D B with 36 of the 64 blocks computed.
+constexpr int kLinHex = 16;
+
+__global__ void __launch_bounds__(128) k_hex_integrate_lin(int ne8, const int *__restrict__ topo8,
+                                                           const double *__restrict__ xyz,
+                                                           const double *__restrict__ E8, double nu,
+                                                           double *__restrict__ Ke) {
+    __shared__ double sX[kLinHex][24];
+    __shared__ double sG[kLinHex][8][8][4];  // [element][q][a][d], d padded to 4
+    __shared__ double sW[kLinHex][8];
+    const int tid = threadIdx.x;
+    for (long base = (long)blockIdx.x * kLinHex; base < ne8; base += (long)gridDim.x * kLinHex) {
+        const int nel = (int)min((long)kLinHex, ne8 - base);
+        for (int v = tid; v < nel * 24; v += 128) {
+            const int le = v / 24, t = v % 24, a = t / 3, cc = t - 3 * a;
+            sX[le][t] = xyz[3L * topo8[8 * (base + le) + a] + cc];
+        }
+        __syncthreads();
+        {
+            const int le = tid >> 3, q = tid & 7;
+            if (le < nel) {
+                const double *dN = c_hex_dN + q * 24;
+                double J[9];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        double acc = 0;
+#pragma unroll
+                        for (int b = 0; b < 8; ++b) acc += dN[i * 8 + b] * sX[le][3 * b + j];
+                        J[3 * i + j] = acc;
+                    }
+                double Ji[9];
+                inv3(J, Ji);
+                sW[le][q] = det_sarrus(J);  // Gauss weight 1
+#pragma unroll
+                for (int a = 0; a < 8; ++a)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+                        sG[le][q][a][d] = Ji[3 * d] * dN[a] + Ji[3 * d + 1] * dN[8 + a] + Ji[3 * d + 2] * dN[16 + a];
+            }
+        }
+        __syncthreads();
+        for (int v = tid; v < nel * 36; v += 128) {
+            const int le = v / 36;
+            int pr = v % 36, a = 0;  // pr -> (a, b), a <= b, row by row
+            while (pr >= 8 - a) {
+                pr -= 8 - a;
+                ++a;
+            }
+            const int b = a + pr;
+            double T[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, d = 0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const double w = sW[le][q];
+                const double ga0 = w * sG[le][q][a][0], ga1 = w * sG[le][q][a][1], ga2 = w * sG[le][q][a][2];
+                const double gb0 = sG[le][q][b][0], gb1 = sG[le][q][b][1], gb2 = sG[le][q][b][2];
+                T[0] = fma(ga0, gb0, T[0]);
+                T[1] = fma(ga0, gb1, T[1]);
+                T[2] = fma(ga0, gb2, T[2]);
+                T[3] = fma(ga1, gb0, T[3]);
+                T[4] = fma(ga1, gb1, T[4]);
+                T[5] = fma(ga1, gb2, T[5]);
+                T[6] = fma(ga2, gb0, T[6]);
+                T[7] = fma(ga2, gb1, T[7]);
+                T[8] = fma(ga2, gb2, T[8]);
+            }
+            d = T[0] + T[4] + T[8];
+            const Lame L = lame(E8[base + le], nu);
+            double kab[9];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) kab[3 * i + j] = L.lam * T[3 * i + j] + L.mu * T[3 * j + i] + (i == j ? L.mu * d : 0.0);
+            double *ke = Ke + 576L * (base + le);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) ke[(a * 8 + b) * 9 + i] = kab[i];
+            if (b != a)
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) ke[(b * 8 + a) * 9 + 3 * i + j] = kab[3 * j + i];
+        }
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------ C3D4 --
 
 constexpr int kTetPerCta = 8;  // 16 threads per element: (a,b)
@@ -396,7 +489,8 @@ __global__ void __launch_bounds__(128) k_tet_integrate(
 
 // -------------------------------------------------------------- assembly --
 
-constexpr int kRowCap = 64;  // blocks accumulated in shared memory per warp
+constexpr int kRowCap = 64;    // blocks accumulated in shared memory per warp
+constexpr int kIncBatch = 8;   // incidences whose loads are in flight together
 
 // One warp per free node (block row).  Rows wider than kRowCap accumulate in
 // global memory instead (still owned by the warp).
@@ -418,21 +512,40 @@ __global__ void __launch_bounds__(kBlock) k_gather_assemble(
         __syncwarp();
         const int node = node_of_free[r];
         double fsum = 0.0;
-        for (int k = inc_ptr[node]; k < inc_ptr[node + 1]; ++k) {
-            const int ga = inc[k];
-            const int g = ga >> 3, a = ga & 7;
-            const bool hex = g < ne8;
-            const int npe = hex ? 8 : 4;
-            const double *row = hex ? Ke + 576L * g + 72 * a : Ke + ke8 + 144L * (g - ne8) + 36 * a;
-            const uint16_t *sl = slot + 8L * k;
-            for (int v = lane; v < 9 * npe; v += 32) {
-                int b = v / 9;
-                int s = sl[b];
-                if (s != kNoSlot) acc[9 * s + (v - 9 * b)] += row[v];
+        const int kb = inc_ptr[node], kend = inc_ptr[node + 1];
+        // incidences in batches of kIncBatch: every load of a batch is issued
+        // before the first sum, then the sums run in ascending incidence order
+        for (int k0 = kb; k0 < kend; k0 += kIncBatch) {
+            const int nk = min(kIncBatch, kend - k0);
+            const int my_inc = lane < nk ? inc[k0 + lane] : 0;
+            double val[kIncBatch][3];
+            int sl[kIncBatch][3];
+#pragma unroll
+            for (int j = 0; j < kIncBatch; ++j) {
+                const int ga = __shfl_sync(0xffffffffu, my_inc, j);
+                const int g = ga >> 3, a = ga & 7;
+                const bool hex = g < ne8;
+                const int nv = hex ? 72 : 36;
+                const double *row = hex ? Ke + 576L * g + 72 * a : Ke + ke8 + 144L * (g - ne8) + 36 * a;
+#pragma unroll
+                for (int t = 0; t < 3; ++t) {
+                    const int v = lane + 32 * t;
+                    const bool ok = j < nk && v < nv;
+                    sl[j][t] = ok ? (int)slot[8L * (k0 + j) + v / 9] : (int)kNoSlot;
+                    val[j][t] = ok ? row[v] : 0.0;
+                }
+                if (WITH_F && lane < 3 && j < nk)
+                    fsum += hex ? Fe[24L * g + 3 * a + lane] : Fe[24L * ne8 + 12L * (g - ne8) + 3 * a + lane];
             }
-            if (WITH_F && lane < 3)
-                fsum += hex ? Fe[24L * g + 3 * a + lane] : Fe[24L * ne8 + 12L * (g - ne8) + 3 * a + lane];
-            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < kIncBatch; ++j) {
+#pragma unroll
+                for (int t = 0; t < 3; ++t) {
+                    const int v = lane + 32 * t;
+                    if (sl[j][t] != kNoSlot) acc[9 * sl[j][t] + v % 9] += val[j][t];
+                }
+                __syncwarp();
+            }
         }
         if (in_smem) {
             double *out = Kb + 9L * rb;
@@ -491,8 +604,8 @@ static void integrate(ofea_ctx *c, bool nl, const double *d_u) {
             k_hex_integrate<true><<<g, 128, 0, s>>>(c->ne8, c->topo8.p, c->xyz.p, c->E8.p, c->nu,
                                                     c->free_map.p, d_u, c->Ke.p, Fe8);
         else
-            k_hex_integrate<false><<<g, 128, 0, s>>>(c->ne8, c->topo8.p, c->xyz.p, c->E8.p, c->nu,
-                                                     nullptr, nullptr, c->Ke.p, nullptr);
+            k_hex_integrate_lin<<<std::min(grid_for(c, (c->ne8 + kLinHex - 1) / kLinHex, 1), c->num_sms * 16),
+                                  128, 0, s>>>(c->ne8, c->topo8.p, c->xyz.p, c->E8.p, c->nu, c->Ke.p);
         OFEA_CHECK_LAUNCH();
     }
     if (c->ne4 > 0) {
