@@ -338,7 +338,7 @@ int ofea_assemble_pattern(ofea_ctx *c, int *n, long long *nnz) {
 
 static void after_assembly(ofea_ctx *c) {
     build_block_jacobi(c);
-    build_sell(c);
+    if (!c->sell_ok) build_sell(c);  // the assembly kernels write it themselves
     OFEA_CUDA(cudaMemcpyAsync(c->herr.p, c->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     OFEA_CUDA(cudaStreamSynchronize(c->stream));
     c->jacobi_ok = c->herr.p[0] == 0;
@@ -421,6 +421,7 @@ int ofea_matrix_upload_csc(ofea_ctx *c, int nd, const double *xyz, const int *fr
         c->mesh_ok = true;
         c->pattern_ok = true;
         c->K_ok = true;
+        c->sell_ok = c->sell_layout_ok = false;
         after_assembly(c);
         geometry_start(c);
     });

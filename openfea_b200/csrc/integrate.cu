@@ -25,6 +25,7 @@
 #include <mutex>
 
 #include "ofea_internal.cuh"
+#include "sell.cuh"
 
 namespace ofea {
 
@@ -494,12 +495,20 @@ constexpr int kIncBatch = 8;   // incidences whose loads are in flight together
 
 // One warp per free node (block row).  Rows wider than kRowCap accumulate in
 // global memory instead (still owned by the warp).
+// The solver copy of K (BSELL-32, sell.cuh) that the owning warp writes with
+// its row: slice layout of the current pattern and the three value arrays.
+struct SellOut {
+    const int *sl_ptr, *sl_g;
+    double *sv64;
+    __nv_bfloat16 *sv16, *svg;
+};
+
 template <bool WITH_F>
 __global__ void __launch_bounds__(kBlock) k_gather_assemble(
     int nfree, int ne8, const int *__restrict__ node_of_free, const int *__restrict__ inc_ptr,
     const int *__restrict__ inc, const uint16_t *__restrict__ slot, const int *__restrict__ rowptr,
     const double *__restrict__ Ke, double *__restrict__ Kb, const double *__restrict__ Fe,
-    double *__restrict__ fint) {
+    double *__restrict__ fint, SellOut so) {
     __shared__ double s_acc[kWarpsPerBlock][kRowCap * 9];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long ke8 = 576L * ne8;
@@ -552,6 +561,33 @@ __global__ void __launch_bounds__(kBlock) k_gather_assemble(
             for (int v = lane; v < 9 * deg; v += 32) out[v] = acc[v];
         }
         if (WITH_F && lane < 3) fint[3L * r + lane] = fsum;
+        // the same row in the solver's layout (as k_fill_sell writes it):
+        // slots up to the slice width, padding slots zero; FP64 and BF16
+        // planes, then the BF16 copy grouped by four slots
+        {
+            const int sl = r / kSlice, t = r % kSlice;
+            const long S = so.sl_ptr[sl];
+            const int W = so.sl_ptr[sl + 1] - (int)S;
+            for (int v = lane; v < 9 * W; v += 32) {
+                const int k = v / 9, e = v - 9 * k;
+                const double x = k < deg ? acc[v] : 0.0;
+                so.sv64[((S + k) * 9 + e) * kSlice + t] = x;
+                so.sv16[((S + k) * 9 + e) * kSlice + t] = __double2bfloat16(x);
+            }
+            const long G = so.sl_g[sl];
+            uint2 *svg2 = reinterpret_cast<uint2 *>(so.svg);
+            for (int p = lane; p < 9 * ((W + 3) / 4); p += 32) {
+                const int g = p / 9, e = p - 9 * g;
+                unsigned h[2] = {0u, 0u};
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int k = 4 * g + u;
+                    const double x = k < deg ? acc[9 * k + e] : 0.0;
+                    h[u >> 1] |= (unsigned)__bfloat16_as_ushort(__double2bfloat16(x)) << (16 * (u & 1));
+                }
+                svg2[((G + g) * 9 + e) * kSlice + t] = make_uint2(h[0], h[1]);
+            }
+        }
         __syncwarp();
     }
 }
@@ -624,18 +660,20 @@ static void integrate(ofea_ctx *c, bool nl, const double *d_u) {
 
 static void gather(ofea_ctx *c, bool with_f, double *d_fint) {
     c->Kb.ensure((size_t)std::max<long long>(9 * c->nnzb, 1));
+    if (!c->sell_layout_ok) build_sell_layout(c);
+    const SellOut so{c->sl_ptr.p, c->sl_g.p, c->sv64.p, c->sv16.p, c->sv16g.p};
     int gw = grid_for(c, c->nfree, kWarpsPerBlock);
     if (with_f)
         k_gather_assemble<true><<<gw, kBlock, 0, c->stream>>>(
             c->nfree, c->ne8, c->node_of_free.p, c->inc_ptr.p, c->inc.p, c->slot.p, c->rowptr.p,
-            c->Ke.p, c->Kb.p, c->Fe.p, d_fint);
+            c->Ke.p, c->Kb.p, c->Fe.p, d_fint, so);
     else
         k_gather_assemble<false><<<gw, kBlock, 0, c->stream>>>(
             c->nfree, c->ne8, c->node_of_free.p, c->inc_ptr.p, c->inc.p, c->slot.p, c->rowptr.p,
-            c->Ke.p, c->Kb.p, nullptr, nullptr);
+            c->Ke.p, c->Kb.p, nullptr, nullptr, so);
     OFEA_CHECK_LAUNCH();
     c->K_ok = true;
-    c->sell_ok = false;
+    c->sell_ok = true;  // written by the gather
     c->coarse.K_ok = false;
     c->coarse2.K_ok = false;
 }

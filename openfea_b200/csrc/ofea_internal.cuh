@@ -207,7 +207,8 @@ struct ofea_ctx {
     ofea::DevBuf<int> sl_g;            // slot-group offsets of the grouped BF16 copy (sell.cuh)
     ofea::DevBuf<__nv_bfloat16> sv16g; // grouped BF16 copy for the single-matrix V-cycle SpMVs
     long long sell_len = 0;
-    bool sell_ok = false;
+    bool sell_ok = false;         // values of the solver copy current
+    bool sell_layout_ok = false;  // slice pointers, columns and buffers for the current pattern
     ofea::Coarse coarse;      // exact coarse level
     ofea::Coarse coarse2;     // nested finer level of the learned stage
     ofea::Learned learned;
@@ -229,6 +230,7 @@ void assemble_nl(ofea_ctx *c, const double *d_u, double *d_fint);
 void build_block_jacobi(ofea_ctx *c);
 void stress_recovery(ofea_ctx *c, const double *d_u, int mode, double *d_elem, double *d_node);
 // sell.cu
+void build_sell_layout(ofea_ctx *c);
 void build_sell(ofea_ctx *c);
 // solve.cu
 void spmv64(ofea_ctx *c, const double *d_x, double *d_y);

@@ -332,6 +332,7 @@ void build_pattern(ofea_ctx *c) {
     c->pattern_ok = true;
     c->K_ok = false;
     c->sell_ok = false;
+    c->sell_layout_ok = false;
     c->coarse.geom_ok = false;
     c->coarse.K_ok = false;
     c->coarse2.geom_ok = false;

@@ -20,9 +20,26 @@ __global__ void k_slice_width(int nfree, const int *__restrict__ rowptr, int *__
     }
 }
 
-__global__ void k_fill_sell(int nfree, const int *__restrict__ rowptr, const int *__restrict__ cols,
-                            const double *__restrict__ Kb, const int *__restrict__ sl_ptr,
-                            int *__restrict__ scols, double *__restrict__ sv64,
+// Pattern part of the layout: the slots' block columns (padding: the row's
+// own column, row 0 past the last row).  Once per pattern.
+__global__ void k_fill_scols(int nfree, const int *__restrict__ rowptr, const int *__restrict__ cols,
+                             const int *__restrict__ sl_ptr, int *__restrict__ scols) {
+    const int nslice = (nfree + kSlice - 1) / kSlice;
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < (long)nslice * kSlice;
+         g += (long)gridDim.x * blockDim.x) {
+        const int s = (int)(g / kSlice), t = (int)(g % kSlice);
+        const int r = s * kSlice + t;
+        const long S = sl_ptr[s];
+        const int W = sl_ptr[s + 1] - (int)S;
+        const int rb = r < nfree ? rowptr[r] : 0;
+        const int deg = r < nfree ? rowptr[r + 1] - rb : 0;
+        for (int k = 0; k < W; ++k) scols[(S + k) * kSlice + t] = k < deg ? cols[rb + k] : (r < nfree ? r : 0);
+    }
+}
+
+// Values: FP64 and BF16 planes, and the grouped BF16 copy, from block-CSR K.
+__global__ void k_fill_sell(int nfree, const int *__restrict__ rowptr, const double *__restrict__ Kb,
+                            const int *__restrict__ sl_ptr, double *__restrict__ sv64,
                             __nv_bfloat16 *__restrict__ sv16, const int *__restrict__ sl_g,
                             __nv_bfloat16 *__restrict__ svg) {
     const int nslice = (nfree + kSlice - 1) / kSlice;
@@ -41,7 +58,6 @@ __global__ void k_fill_sell(int nfree, const int *__restrict__ rowptr, const int
             for (int u = 0; u < 4; ++u) {
                 const int k = 4 * g + u;
                 const bool real = k < deg;
-                if (k < W) scols[(S + k) * kSlice + t] = real ? cols[rb + k] : (r < nfree ? r : 0);
 #pragma unroll
                 for (int e = 0; e < 9; ++e) {
                     const double v = real ? Kb[9L * (rb + k) + e] : 0.0;
@@ -64,7 +80,7 @@ __global__ void k_group_width(int nslice, const int *__restrict__ sl_ptr, int *_
         gw[s] = (sl_ptr[s + 1] - sl_ptr[s] + 3) / 4;
 }
 
-void build_sell(ofea_ctx *c) {
+void build_sell_layout(ofea_ctx *c) {
     cudaStream_t s = c->stream;
     const int nslice = (c->nfree + kSlice - 1) / kSlice;
     c->sl_ptr.ensure((size_t)nslice + 1);
@@ -85,9 +101,18 @@ void build_sell(ofea_ctx *c) {
     OFEA_CHECK_LAUNCH();
     const long long groups = exclusive_scan(width, c->sl_g.p, nslice, s, width + nslice + 1, tmp_len);
     c->sv16g.ensure((size_t)std::max<long long>(groups, 1) * 9 * kSlice * 4);
+    k_fill_scols<<<grid_for(c, (long)nslice * kSlice, kBlock), kBlock, 0, s>>>(c->nfree, c->rowptr.p, c->cols.p,
+                                                                              c->sl_ptr.p, c->scols.p);
+    OFEA_CHECK_LAUNCH();
+    c->sell_layout_ok = true;
+}
+
+void build_sell(ofea_ctx *c) {
+    if (!c->sell_layout_ok) build_sell_layout(c);
+    cudaStream_t s = c->stream;
+    const int nslice = (c->nfree + kSlice - 1) / kSlice;
     k_fill_sell<<<grid_for(c, (long)nslice * kSlice, kBlock), kBlock, 0, s>>>(
-        c->nfree, c->rowptr.p, c->cols.p, c->Kb.p, c->sl_ptr.p, c->scols.p, c->sv64.p, c->sv16.p, c->sl_g.p,
-        c->sv16g.p);
+        c->nfree, c->rowptr.p, c->Kb.p, c->sl_ptr.p, c->sv64.p, c->sv16.p, c->sl_g.p, c->sv16g.p);
     OFEA_CHECK_LAUNCH();
     c->sell_ok = true;
 }
