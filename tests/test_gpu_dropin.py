@@ -41,7 +41,8 @@ def test_csc_upload_matches_reference_superlu(gpu_ctx_factory, reference, inp_fi
     ctx.upload_csc(arrays["xyz"], arrays["free_map"], cp, ri, val)
     rp, col, kv = ctx.get_csr()
     assert np.array_equal(rp, cp) and np.array_equal(col, ri) and np.array_equal(kv, val)
-    for method, rtol, bar in (("GPU_PCG", 1e-12, 1e-9), ("GPU_MIXED", 1e-10, 1e-8)):
+    # (the FP64 residual floor of these samples is near 1e-11: 7.8e-12 and 7.5e-11)
+    for method, rtol, bar in (("GPU_PCG", 1e-10, 1e-9), ("GPU_MIXED", 1e-10, 1e-8)):
         u, st = ctx.solve(f, method=method, rtol=rtol)
         assert st["status"] == 0
         assert rel2(u, u_ref) <= bar, (method, rel2(u, u_ref))
