@@ -3,7 +3,7 @@
 Run where the reference tree and oracle/_ref/libofea_ref.so (make -C oracle)
 exist:
 
-    python tests/golden/make_golden.py [/path/to/OpenFEA]
+    python tests/golden/make_golden.py <reference tree>   (or OFEA_REFERENCE_DIR)
 
 Writes:
   *.inp.gz              the reference's sample models used as test inputs
@@ -19,7 +19,7 @@ Writes:
                         sample_model/CA/cadcae_ca.vtk (525 nodes of the
                         modified model)
 
-    python tests/golden/make_golden.py --ca-only [/path/to/OpenFEA]
+    python tests/golden/make_golden.py --ca-only <reference tree>
 
 writes only the sample_model/CA fixtures (no oracle/_ref needed).
   ref_elements.npz      element matrices from the reference's element routines
@@ -164,7 +164,9 @@ def main(ref_root):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if a != "--ca-only"]
-    root = args[0] if args else "/root/reference"
+    root = args[0] if args else os.environ.get("OFEA_REFERENCE_DIR")
+    if not root:
+        sys.exit("usage: make_golden.py [--ca-only] <reference tree>  (or set OFEA_REFERENCE_DIR)")
     if "--ca-only" in sys.argv:
         ca_fixtures(root)
     else:
