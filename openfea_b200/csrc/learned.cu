@@ -593,6 +593,49 @@ __global__ void k_poly_out(int na, const float *__restrict__ s, const float *__r
 }
 
 
+// Level-1 restriction from the level-2 one: c1 = P^T c2, P the map of
+// level-1 modes into its children's modes (child_coeffs); Z1 = Z2 P, so this
+// is Z1^T t without a second pass over the fine vector.  Thread per (parent,
+// mode), children summed in table order.
+__global__ void k_restrict_parent(int na1, const int *__restrict__ children, const float *__restrict__ pdel,
+                                  const float *__restrict__ c2, float *__restrict__ c1) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 6 * na1; i += gridDim.x * blockDim.x) {
+        const int P = i / 6, k = i % 6;
+        float acc = 0.f;
+        for (int ch = 0; ch < 8; ++ch) {
+            const int J = children[8L * P + ch];
+            if (J < 0) continue;
+            const float *g = c2 + 6L * J;
+            const float dx = pdel[4L * J], dy = pdel[4L * J + 1], dz = pdel[4L * J + 2], ratio = pdel[4L * J + 3];
+            float v;
+            switch (k) {  // row k of (child_coeffs' matrix)^T applied to g
+                case 0: v = g[0]; break;
+                case 1: v = g[1]; break;
+                case 2: v = g[2]; break;
+                case 3: v = -dz * g[1] + dy * g[2] + ratio * g[3]; break;
+                case 4: v = dz * g[0] - dx * g[2] + ratio * g[4]; break;
+                default: v = -dy * g[0] + dx * g[1] + ratio * g[5]; break;
+            }
+            acc += v;
+        }
+        c1[i] = acc;
+    }
+}
+
+// Both coarse corrections in level-2 modes: g = D^-1/2 (s * wv) + P e1,
+// written over c2 (one prolongation then adds Z2 g = Z1 e1 + Z2 D^-1/2 y).
+__global__ void k_poly_out_e1(int na, const float *__restrict__ s, const float *__restrict__ wv,
+                              const float *__restrict__ dsq, const int *__restrict__ parent,
+                              const float *__restrict__ pdel, const float *__restrict__ e1, float *__restrict__ g) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 6 * na; i += gridDim.x * blockDim.x) {
+        const int J = i / 6, l = i % 6;
+        float pe[6];
+        child_coeffs(J, parent, pdel, e1, pe);
+        const float d = dsq[i];
+        g[i] = (d > 0.f ? s[i] * wv[i] / d : 0.f) + pe[l];
+    }
+}
+
 int tiles(long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
@@ -903,16 +946,14 @@ static double read_loss(ofea_ctx *c) {
 // level-1 correction e1 = E1^-1 Z1^T t, the level-2 restriction c2 = Z2^T t,
 // then S = D^-1/2 (c2 - E2 P e1).  With level1_done the
 // caller has already computed e1 (coarse_correct) into the coarse level's evec.
-static void learned_input(ofea_ctx *c, const float *t, bool level1_done) {
+static void learned_input(ofea_ctx *c, const float *t) {
     Coarse &C1 = c->coarse;
     Coarse &C2 = c->coarse2;
     Learned &N = c->learned;
     cudaStream_t s = c->stream;
     const int na = C2.na;
-    if (!level1_done) {
-        restrict_level(c, C1, t, C1.cvec.p);
-        coarse_gemv(c, C1.cvec.p, C1.evec.p);
-    }
+    restrict_level(c, C1, t, C1.cvec.p);
+    coarse_gemv(c, C1.cvec.p, C1.evec.p);
     restrict_level(c, C2, t, C2.cvec.p);
     k_lrn_shift<<<grid_for(c, 32L * na, kBlock), kBlock, 0, s>>>(na, C2.nbr.p, N.Ehat.p, N.dsq.p, N.parent.p,
                                                                   N.pdel.p, C1.evec.p, C2.cvec.p, N.shifted.p);
@@ -928,7 +969,7 @@ void learned_add_sample(ofea_ctx *c, const double *d_r) {
     const int na = C2.na;
     N.r32.ensure(c->n);
     k_f64_to_f32<<<grid_for(c, c->n, kBlock), kBlock, 0, s>>>(c->n, d_r, N.r32.p);
-    learned_input(c, N.r32.p, false);
+    learned_input(c, N.r32.p);
     k_gnn_sigma<<<1, kBlock, 0, s>>>(na, N.shifted.p, N.sigma.p);
     k_gnn_sample<<<grid_for(c, 6L * na, kBlock), kBlock, 0, s>>>(na, N.shifted.p, N.sigma.p,
                                                                  N.data.p + (size_t)N.nsamples * 6 * na);
@@ -1071,17 +1112,28 @@ void learned_gradient(ofea_ctx *c, const float *h_x, int B, double *loss, float 
     check_tc(c);
 }
 
-// Inference inside the V-cycle, after coarse_correct(t, x):
-// x += Z2 D^-1/2 s * M(s * D^-1/2 (c2 - E2 P e1)).
-void learned_apply(ofea_ctx *c, const float *t, float *x) {
+// The coarse part of the LEARNED V-cycle: x += Z1 e1 + Z2 D^-1/2 y with
+// e1 = E1^-1 Z1^T t (the exact level) and y = s * M(s * D^-1/2 (c2 - E2 P e1))
+// (the learned stage), c2 = Z2^T t.  One restriction and one prolongation
+// pass over the fine vector serve both levels (Z1 = Z2 P): c1 = P^T c2, and
+// the level-1 correction joins the stage's output in level-2 modes.
+void learned_coarse_correct(ofea_ctx *c, const float *t, float *x) {
+    Coarse &C1 = c->coarse;
     Coarse &C2 = c->coarse2;
     Learned &N = c->learned;
     const Learned::Layout L = Learned::layout();
+    cudaStream_t s = c->stream;
     const int na = C2.na;
-    learned_input(c, t, true);
+    restrict_level(c, C2, t, C2.cvec.p);
+    k_restrict_parent<<<grid_for(c, 6L * C1.na, kBlock), kBlock, 0, s>>>(C1.na, N.children.p, N.pdel.p, C2.cvec.p,
+                                                                       C1.cvec.p);
+    coarse_gemv(c, C1.cvec.p, C1.evec.p);
+    k_lrn_shift<<<grid_for(c, 32L * na, kBlock), kBlock, 0, s>>>(na, C2.nbr.p, N.Ehat.p, N.dsq.p, N.parent.p,
+                                                                  N.pdel.p, C1.evec.p, C2.cvec.p, N.shifted.p);
     float *wv = N.pv[3].p;
     apply_M(c, na, N.scale.p, N.shifted.p, N.w.p + L.c0, wv);
-    k_poly_out<<<grid_for(c, 6L * na, kBlock), kBlock, 0, c->stream>>>(na, N.scale.p, wv, N.dsq.p, C2.cvec.p);
+    k_poly_out_e1<<<grid_for(c, 6L * na, kBlock), kBlock, 0, s>>>(na, N.scale.p, wv, N.dsq.p, N.parent.p,
+                                                                   N.pdel.p, C1.evec.p, C2.cvec.p);
     prolong_level(c, C2, C2.cvec.p, x);
     OFEA_CHECK_LAUNCH();
 }

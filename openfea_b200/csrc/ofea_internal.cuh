@@ -243,7 +243,7 @@ void setup_learned_levels(ofea_ctx *c);
 void geometry_start(ofea_ctx *c);
 void geometry_join(ofea_ctx *c);
 void learned_prepare_inference(ofea_ctx *c);
-void learned_apply(ofea_ctx *c, const float *t, float *x);
+void learned_coarse_correct(ofea_ctx *c, const float *t, float *x);
 // Batched persistent solver (batched.cu).
 ofea_batch *batch_create(ofea_ctx *const *ctxs, int nv, int nrhs);
 void batch_destroy(ofea_batch *b);

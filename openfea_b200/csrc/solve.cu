@@ -565,12 +565,12 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
             // initial preconditioner application z_0 = M(r_0)
             k_set_itB<<<1, 1, 0, s>>>(ws.fl, -1);
             vc_resid(c, w.b32.p, w.x32.p, w.t32.p);
-            coarse_correct(c, w.t32.p, w.x32.p);
-            if (learned) learned_apply(c, w.t32.p, w.x32.p);
+            if (learned) learned_coarse_correct(c, w.t32.p, w.x32.p);
+            else coarse_correct(c, w.t32.p, w.x32.p);
             k_fcg_post<<<G, kBlock, 0, s>>>(nf, c->sl_ptr.p, c->scols.p, c->sl_g.p, c->sv16g.p, c->Dinv32.p, wsm, w.b32.p,
                                             w.x32.p, w.r.p, w.z32a.p, w.z32b.p, ws.P, ws.fl);
             OFEA_CHECK_LAUNCH();
-            launches += 6;
+            launches += learned ? 12 : 6;
             auto chunk = [&](int iters) {
                 for (int it = 0; it < iters; ++it) {
                     k_fcg_A<<<G, kBlock, 0, s>>>(nf, c->sl_ptr.p, c->scols.p, c->sv64.p, w.z32a.p, w.z32b.p,
@@ -578,14 +578,14 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
                     k_fcg_B<<<G, kBlock, 0, s>>>(nf, c->Dinv32.p, wsm, w.p0.p, w.p1.p, w.q.p, d_u, w.r.p,
                                                  w.b32.p, w.x32.p, ws.P, ws.fl);
                     vc_resid(c, w.b32.p, w.x32.p, w.t32.p);
-                    coarse_correct(c, w.t32.p, w.x32.p);
-                    if (learned) learned_apply(c, w.t32.p, w.x32.p);
+                    if (learned) learned_coarse_correct(c, w.t32.p, w.x32.p);
+                    else coarse_correct(c, w.t32.p, w.x32.p);
                     k_fcg_post<<<G, kBlock, 0, s>>>(nf, c->sl_ptr.p, c->scols.p, c->sl_g.p, c->sv16g.p, c->Dinv32.p, wsm,
                                                     w.b32.p, w.x32.p, w.r.p, w.z32a.p, w.z32b.p, ws.P, ws.fl);
                 }
                 OFEA_CHECK_LAUNCH();
             };
-            drive(c, oo, ws, per_chunk, chunk, hf, launches, learned ? 7 + 7 : 7, timed_out, t_start, {});
+            drive(c, oo, ws, per_chunk, chunk, hf, launches, learned ? 13 : 7, timed_out, t_start, {});
         } else {
             auto chunk = [&](int iters) {
                 for (int it = 0; it < iters; ++it) {
