@@ -944,8 +944,7 @@ static double read_loss(ofea_ctx *c) {
 
 // Network input of the learned level for a fine-level vector t (FP32): the
 // level-1 correction e1 = E1^-1 Z1^T t, the level-2 restriction c2 = Z2^T t,
-// then S = D^-1/2 (c2 - E2 P e1).  With level1_done the
-// caller has already computed e1 (coarse_correct) into the coarse level's evec.
+// then S = D^-1/2 (c2 - E2 P e1) (the training samples' inputs).
 static void learned_input(ofea_ctx *c, const float *t) {
     Coarse &C1 = c->coarse;
     Coarse &C2 = c->coarse2;
