@@ -485,6 +485,9 @@ constexpr int kGJ = 64;
 // padding (their rows and columns are zero and stay so).
 __device__ __forceinline__ void warp_gj32(double (&x)[32], int bb, const double *__restrict__ diag0) {
     const int lane = threadIdx.x & 31;
+    // the pivots' drop thresholds, one per lane, loaded once (a load per
+    // pivot would put a memory latency on every step of the chain)
+    const double thr = lane < bb ? 1e-12 * diag0[lane] : 0.0;
 #pragma unroll
     for (int p = 0; p < 32; ++p) {
         if (p >= bb) break;
@@ -493,7 +496,7 @@ __device__ __forceinline__ void warp_gj32(double (&x)[32], int bb, const double 
         for (int r = 0; r < 32; ++r) colp[r] = __shfl_sync(0xffffffffu, x[r], p);
         const double piv = colp[p];
         const double rowp = x[p];
-        if (!(piv > 1e-12 * diag0[p])) {
+        if (!(piv > __shfl_sync(0xffffffffu, thr, p))) {
             x[p] = 0.0;
             if (lane == p)
 #pragma unroll

@@ -9,8 +9,9 @@
 // swizzle (8 x 8 core matrices of 128 contiguous bytes; the two core
 // matrices of one 16-wide MMA step 128 bytes apart, row groups 1024 bytes
 // apart); one thread issues four tcgen05.mma (M = 128, N = 64, K = 16) into
-// the TMEM accumulator and commits them to an mbarrier that every thread
-// waits on before the slice is overwritten.  The epilogue reads the
+// the TMEM accumulator and commits them to the stage's mbarrier.  Two stages:
+// the threads fill one while the tensor core reads the other, and wait on a
+// stage's mbarrier before they refill it.  The epilogue reads the
 // accumulator with tcgen05.ld (warp w reads TMEM lanes 32w..32w+31, one
 // output row per thread) and writes Z (+ bias, ReLU), dX or the weight-
 // gradient partials.  Every output element is one accumulator's sum over the
@@ -28,6 +29,7 @@ namespace {
 
 constexpr int kTM = 128, kTN = 64, kTK = 64, kTcThreads = 128;
 constexpr uint32_t kTmemCols = 64;
+constexpr size_t kTcSmem = 2 * (kTM + kTN) * kTK * sizeof(__nv_bfloat16);  // 48 KB
 // kind::f16 instruction descriptor: D F32 (bits 4-5 = 1), A and B BF16 (bits
 // 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at bit 17,
 // M >> 4 at bit 24.
@@ -78,7 +80,30 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigne
 __device__ __forceinline__ void stage(__nv_bfloat16 *tile, int rows, const TcOperand &op, int r0, int R, long k0,
                                       long kend) {
     const int total = rows * kTK;
-    if (op.ks == 1) {  // contiguous along the reduction: consecutive threads take consecutive k
+    if (op.ks == 1 && (op.ms & 3) == 0 && (reinterpret_cast<uintptr_t>(op.p) & 15) == 0) {
+        // contiguous along the reduction, rows 16-byte aligned: four k per
+        // thread as one 16-byte load, stored as four adjacent BF16 of a core row
+        for (int idx = threadIdx.x; idx < total / 4; idx += kTcThreads) {
+            const int rr = idx / (kTK / 4), kk = 4 * (idx % (kTK / 4));
+            const long r = r0 + rr, k = k0 + kk;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (r < R) {
+                const float *src = op.p + r * op.ms + k;
+                if (k + 3 < kend) {
+                    v = *reinterpret_cast<const float4 *>(src);
+                } else {
+                    if (k < kend) v.x = src[0];
+                    if (k + 1 < kend) v.y = src[1];
+                    if (k + 2 < kend) v.z = src[2];
+                }
+            }
+            __nv_bfloat162 lo = __floats2bfloat162_rn(v.x, v.y), hi = __floats2bfloat162_rn(v.z, v.w);
+            uint2 packed;
+            packed.x = *reinterpret_cast<uint32_t *>(&lo);
+            packed.y = *reinterpret_cast<uint32_t *>(&hi);
+            *reinterpret_cast<uint2 *>(tile + kmaj(rr, kk)) = packed;
+        }
+    } else if (op.ks == 1) {  // contiguous along the reduction: consecutive threads take consecutive k
         for (int idx = threadIdx.x; idx < total; idx += kTcThreads) {
             const int rr = idx / kTK, kk = idx % kTK;
             const long r = r0 + rr, k = k0 + kk;
@@ -97,30 +122,46 @@ __device__ __forceinline__ void stage(__nv_bfloat16 *tile, int rows, const TcOpe
 
 __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(int M, int N, long Kred, long kchunk, TcOperand A,
                                                         TcOperand B, TcEpilogue epi, int *err) {
-    __shared__ __align__(1024) __nv_bfloat16 sA[kTM * kTK];
-    __shared__ __align__(1024) __nv_bfloat16 sB[kTN * kTK];
-    __shared__ __align__(8) unsigned long long mbar;
+    // two stages of A (128 x 64) and B (64 x 64) BF16 tiles, 1024-byte aligned
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    __nv_bfloat16 *const stages = reinterpret_cast<__nv_bfloat16 *>(tc_smem);
+    constexpr int kStage = (kTM + kTN) * kTK;  // elements per stage: A then B
+    __shared__ __align__(8) unsigned long long mbar[2];
     __shared__ uint32_t s_tmem;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * kTM, n0 = blockIdx.y * kTN;
     const long kb = (long)blockIdx.z * kchunk, ke = min(Kred, kb + kchunk);
-    const uint32_t bar = smem_u32(&mbar);
+    const uint32_t bar0 = smem_u32(&mbar[0]);  // stage b's mbarrier at bar0 + 8 b
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
                      "r"(kTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0 + 8u), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
-    uint32_t parity = 0;
+    unsigned parity = 0u, pending = 0u;  // bit b: stage b's next phase, stage b has MMAs in flight
     bool ok = true, any = false;
-    for (long k0 = kb; k0 < ke; k0 += kTK) {
+    // slice i goes to stage i % 2: its staging overlaps the MMAs of slice
+    // i - 1; before a stage is refilled, the MMAs that read it (slice i - 2)
+    // must be complete
+    int i = 0;
+    for (long k0 = kb; k0 < ke; k0 += kTK, ++i) {
+        const int b = i & 1;
+        if (pending >> b & 1u) {
+            const bool mine = mbar_wait(bar0 + 8u * b, parity >> b & 1u, 2000000000ull);
+            parity ^= 1u << b;
+            pending &= ~(1u << b);
+            ok = __syncthreads_and(mine) != 0;
+            if (!ok) break;
+        }
+        __nv_bfloat16 *sA = stages + b * kStage, *sB = sA + kTM * kTK;
         stage(sA, kTM, A, m0, M, k0, ke);
         stage(sB, kTN, B, n0, N, k0, ke);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the tiles, to the tensor core's proxy
@@ -139,15 +180,18 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(int M, int N, long Kred,
                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
                     ::"r"(tmem), "l"(da), "l"(db), "r"(kIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-                         : "memory");
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(bar0 + 8u * b) : "memory");
         }
+        pending |= 1u << b;
         any = true;
-        const bool mine = mbar_wait(bar, parity, 2000000000ull);
-        parity ^= 1u;
-        ok = __syncthreads_and(mine) != 0;  // also: nobody overwrites the tiles before every wait is over
-        if (!ok) break;
     }
+    // the MMAs still in flight
+    for (int b = 0; b < 2 && ok; ++b)
+        if (pending >> b & 1u) {
+            const bool mine = mbar_wait(bar0 + 8u * b, parity >> b & 1u, 2000000000ull);
+            ok = __syncthreads_and(mine) != 0;
+        }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (!ok) {
         if (tid == 0) atomicExch(err, 1);
@@ -202,10 +246,11 @@ void tc_gemm(cudaStream_t s, int M, int N, long Kred, long kchunk, const TcOpera
     if (kchunk <= 0) kchunk = Kred;
     const long nz = Kred > 0 ? (Kred + kchunk - 1) / kchunk : 1;
     dim3 grid((M + kTM - 1) / kTM, (N + kTN - 1) / kTN, (unsigned)nz);
-    // 8 KB of dynamic shared memory the kernel does not use keep the CTAs per
-    // SM at 6 or fewer, so their TMEM (64 columns each) always fits the SM's
-    // 512 columns and no allocation has to wait for another CTA to finish
-    k_tc_gemm<<<grid, kTcThreads, 8192, s>>>(M, N, Kred, kchunk, A, B, epi, err);
+    // two 24 KB stages: at most 4 CTAs per SM, so their TMEM (64 columns
+    // each) always fits the SM's 512 columns and no allocation has to wait
+    // for another CTA to finish
+    OFEA_CUDA(cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    k_tc_gemm<<<grid, kTcThreads, kTcSmem, s>>>(M, N, Kred, kchunk, A, B, epi, err);
     OFEA_CHECK_LAUNCH();
 }
 
