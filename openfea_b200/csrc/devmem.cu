@@ -10,6 +10,7 @@
 // rounded (256 B, or 2 MB from 1 MB up) so that contexts of the same problem
 // reuse each other's blocks exactly.  ofea_trim_device_memory returns the
 // cached blocks to the driver.
+#include <algorithm>
 #include <cstdlib>
 #include <map>
 #include <mutex>
@@ -212,7 +213,53 @@ void host_cache_give(void *p, std::size_t bytes) {
     h.cached += r;
 }
 
+namespace {
+struct PinnedCache {
+    std::mutex mu;
+    std::multimap<std::size_t, void *> free;
+};
+PinnedCache &pinned_cache() {
+    static PinnedCache *c = new PinnedCache();  // never destroyed: blocks may be freed during exit
+    return *c;
+}
+constexpr std::size_t kPinnedGrain = 4096;
+}  // namespace
+
+// Small page-locked blocks (flag and scalar buffers of contexts) kept by
+// rounded size and handed out again; host_cache_trim() frees them.
+void *pinned_take(std::size_t bytes) {
+    const std::size_t r = (std::max<std::size_t>(bytes, 1) + kPinnedGrain - 1) / kPinnedGrain * kPinnedGrain;
+    PinnedCache &c = pinned_cache();
+    {
+        std::lock_guard<std::mutex> lock(c.mu);
+        auto it = c.free.find(r);
+        if (it != c.free.end()) {
+            void *p = it->second;
+            c.free.erase(it);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    OFEA_CUDA(cudaMallocHost(&p, r));
+    return p;
+}
+
+void pinned_give(void *p, std::size_t bytes) {
+    if (!p) return;
+    const std::size_t r = (std::max<std::size_t>(bytes, 1) + kPinnedGrain - 1) / kPinnedGrain * kPinnedGrain;
+    PinnedCache &c = pinned_cache();
+    std::lock_guard<std::mutex> lock(c.mu);
+    c.free.emplace(r, p);
+}
+
 void host_cache_trim() {
+    {
+        PinnedCache &c = pinned_cache();
+        std::lock_guard<std::mutex> lock(c.mu);
+        for (auto &kv : c.free)
+            if (cudaFreeHost(kv.second) != cudaSuccess) cudaGetLastError();
+        c.free.clear();
+    }
     HostCache &h = host_cache();
     std::lock_guard<std::mutex> lock(h.mu);
     for (auto &kv : h.free) release_block(kv.second.p, kv.second.pinned);

@@ -490,116 +490,107 @@ __global__ void __launch_bounds__(128) k_tet_integrate(
 
 // -------------------------------------------------------------- assembly --
 
-constexpr int kSliceCap = 32;  // slots of a slice accumulated in shared memory
+constexpr int kRowCap = 64;    // blocks accumulated in shared memory per warp
 constexpr int kIncBatch = 8;   // incidences whose loads are in flight together
-constexpr size_t kGatherSmem = sizeof(double) * kSlice * kSliceCap * 9;  // 72 KB
 
-// The solver copy of K (BSELL-32, sell.cuh) written with the rows: slice
-// layout of the current pattern and the three value arrays.
+// The solver copy of K (BSELL-32, sell.cuh) that the owning warp writes with
+// its row: slice layout of the current pattern and the three value arrays.
 struct SellOut {
     const int *sl_ptr, *sl_g;
     double *sv64;
     __nv_bfloat16 *sv16, *svg;
 };
 
-// One CTA per slice (the 32 block rows the solver's BSELL layout groups), a
-// warp per 4 rows: each row sums its incident elements' block rows in
-// ascending element order through the slot map (every load of a batch of
-// incidences issued before the first sum), writes the block-CSR row, and the
-// CTA then writes the slice's FP64 and BF16 planes and the grouped BF16 copy
-// with 32 rows side by side (coalesced).  A slice wider than kSliceCap slots
-// accumulates its rows in the block-CSR output instead of shared memory.
+// One warp per free node (block row).  Rows wider than kRowCap accumulate in
+// global memory instead (still owned by the warp).  The warp also writes its
+// row into the solver's BSELL copies (the separate fill pass is gone).
+
 template <bool WITH_F>
 __global__ void __launch_bounds__(kBlock) k_gather_assemble(
     int nfree, int ne8, const int *__restrict__ node_of_free, const int *__restrict__ inc_ptr,
     const int *__restrict__ inc, const uint16_t *__restrict__ slot, const int *__restrict__ rowptr,
     const double *__restrict__ Ke, double *__restrict__ Kb, const double *__restrict__ Fe,
     double *__restrict__ fint, SellOut so) {
-    extern __shared__ double s_acc[];  // [row t][slot k][entry e]
-    __shared__ int s_deg[kSlice], s_rb[kSlice];
+    __shared__ double s_acc[kWarpsPerBlock][kRowCap * 9];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long ke8 = 576L * ne8;
-    const int nslice = (nfree + kSlice - 1) / kSlice;
-    for (int sl = blockIdx.x; sl < nslice; sl += gridDim.x) {
-        const long S = so.sl_ptr[sl];
-        const int W = so.sl_ptr[sl + 1] - (int)S;
-        const bool fits = W <= kSliceCap;
-        for (int t = warp * (kSlice / kWarpsPerBlock); t < (warp + 1) * (kSlice / kWarpsPerBlock); ++t) {
-            const int r = sl * kSlice + t;
-            const int rb = r < nfree ? rowptr[r] : 0, deg = r < nfree ? rowptr[r + 1] - rb : 0;
-            if (lane == 0) {
-                s_deg[t] = deg;
-                s_rb[t] = rb;
-            }
-            double *acc = fits ? s_acc + (long)t * kSliceCap * 9 : Kb + 9L * rb;
-            for (int v = lane; v < 9 * deg; v += 32) acc[v] = 0.0;
-            __syncwarp();
-            if (r >= nfree) continue;
-            const int node = node_of_free[r];
-            double fsum = 0.0;
-            const int kb = inc_ptr[node], kend = inc_ptr[node + 1];
-            for (int k0 = kb; k0 < kend; k0 += kIncBatch) {
-                const int nk = min(kIncBatch, kend - k0);
-                const int my_inc = lane < nk ? inc[k0 + lane] : 0;
-                double val[kIncBatch][3];
-                int sl_[kIncBatch][3];
+    const int nwarps = gridDim.x * kWarpsPerBlock;
+    for (int r = blockIdx.x * kWarpsPerBlock + warp; r < nfree; r += nwarps) {
+        const int rb = rowptr[r], deg = rowptr[r + 1] - rb;
+        const bool in_smem = deg <= kRowCap;
+        double *acc = in_smem ? s_acc[warp] : Kb + 9L * rb;
+        for (int v = lane; v < 9 * deg; v += 32) acc[v] = 0.0;
+        __syncwarp();
+        const int node = node_of_free[r];
+        double fsum = 0.0;
+        const int kb = inc_ptr[node], kend = inc_ptr[node + 1];
+        // incidences in batches of kIncBatch: every load of a batch is issued
+        // before the first sum, then the sums run in ascending incidence order
+        for (int k0 = kb; k0 < kend; k0 += kIncBatch) {
+            const int nk = min(kIncBatch, kend - k0);
+            const int my_inc = lane < nk ? inc[k0 + lane] : 0;
+            double val[kIncBatch][3];
+            int sl[kIncBatch][3];
 #pragma unroll
-                for (int j = 0; j < kIncBatch; ++j) {
-                    const int ga = __shfl_sync(0xffffffffu, my_inc, j);
-                    const int g = ga >> 3, a = ga & 7;
-                    const bool hex = g < ne8;
-                    const int nv = hex ? 72 : 36;
-                    const double *row = hex ? Ke + 576L * g + 72 * a : Ke + ke8 + 144L * (g - ne8) + 36 * a;
+            for (int j = 0; j < kIncBatch; ++j) {
+                const int ga = __shfl_sync(0xffffffffu, my_inc, j);
+                const int g = ga >> 3, a = ga & 7;
+                const bool hex = g < ne8;
+                const int nv = hex ? 72 : 36;
+                const double *row = hex ? Ke + 576L * g + 72 * a : Ke + ke8 + 144L * (g - ne8) + 36 * a;
 #pragma unroll
-                    for (int q = 0; q < 3; ++q) {
-                        const int v = lane + 32 * q;
-                        const bool ok = j < nk && v < nv;
-                        sl_[j][q] = ok ? (int)slot[8L * (k0 + j) + v / 9] : (int)kNoSlot;
-                        val[j][q] = ok ? row[v] : 0.0;
-                    }
-                    if (WITH_F && lane < 3 && j < nk)
-                        fsum += hex ? Fe[24L * g + 3 * a + lane] : Fe[24L * ne8 + 12L * (g - ne8) + 3 * a + lane];
+                for (int t = 0; t < 3; ++t) {
+                    const int v = lane + 32 * t;
+                    const bool ok = j < nk && v < nv;
+                    sl[j][t] = ok ? (int)slot[8L * (k0 + j) + v / 9] : (int)kNoSlot;
+                    val[j][t] = ok ? row[v] : 0.0;
                 }
+                if (WITH_F && lane < 3 && j < nk)
+                    fsum += hex ? Fe[24L * g + 3 * a + lane] : Fe[24L * ne8 + 12L * (g - ne8) + 3 * a + lane];
+            }
 #pragma unroll
-                for (int j = 0; j < kIncBatch; ++j) {
+            for (int j = 0; j < kIncBatch; ++j) {
 #pragma unroll
-                    for (int q = 0; q < 3; ++q) {
-                        const int v = lane + 32 * q;
-                        if (sl_[j][q] != kNoSlot) acc[9 * sl_[j][q] + v % 9] += val[j][q];
-                    }
-                    __syncwarp();
+                for (int t = 0; t < 3; ++t) {
+                    const int v = lane + 32 * t;
+                    if (sl[j][t] != kNoSlot) acc[9 * sl[j][t] + v % 9] += val[j][t];
                 }
+                __syncwarp();
             }
-            if (fits) {
-                double *out = Kb + 9L * rb;
-                for (int v = lane; v < 9 * deg; v += 32) out[v] = acc[v];
+        }
+        if (in_smem) {
+            double *out = Kb + 9L * rb;
+            for (int v = lane; v < 9 * deg; v += 32) out[v] = acc[v];
+        }
+        if (WITH_F && lane < 3) fint[3L * r + lane] = fsum;
+        // the same row in the solver's layout (as k_fill_sell writes it):
+        // slots up to the slice width, padding slots zero; FP64 and BF16
+        // planes, then the BF16 copy grouped by four slots
+        {
+            const int sl = r / kSlice, t = r % kSlice;
+            const long S = so.sl_ptr[sl];
+            const int W = so.sl_ptr[sl + 1] - (int)S;
+            for (int v = lane; v < 9 * W; v += 32) {
+                const int k = v / 9, e = v - 9 * k;
+                const double x = k < deg ? acc[v] : 0.0;
+                so.sv64[((S + k) * 9 + e) * kSlice + t] = x;
+                so.sv16[((S + k) * 9 + e) * kSlice + t] = __double2bfloat16(x);
             }
-            if (WITH_F && lane < 3) fint[3L * r + lane] = fsum;
-        }
-        __syncthreads();
-        // the slice in the solver's layout, 32 rows side by side: slots up to
-        // the slice width, padding slots zero (as k_fill_sell writes it)
-        auto value = [&](int t, int k, int e) -> double {
-            if (k >= s_deg[t]) return 0.0;
-            return fits ? s_acc[((long)t * kSliceCap + k) * 9 + e] : Kb[9L * (s_rb[t] + k) + e];
-        };
-        for (int idx = threadIdx.x; idx < W * 9 * kSlice; idx += blockDim.x) {
-            const int t = idx % kSlice, ke = idx / kSlice, k = ke / 9, e = ke - 9 * k;
-            const double x = value(t, k, e);
-            so.sv64[(S * 9 + ke) * kSlice + t] = x;
-            so.sv16[(S * 9 + ke) * kSlice + t] = __double2bfloat16(x);
-        }
-        const long G = so.sl_g[sl];
-        uint2 *svg2 = reinterpret_cast<uint2 *>(so.svg);
-        for (int idx = threadIdx.x; idx < ((W + 3) / 4) * 9 * kSlice; idx += blockDim.x) {
-            const int t = idx % kSlice, ge = idx / kSlice, g = ge / 9, e = ge - 9 * g;
-            unsigned h[2] = {0u, 0u};
+            const long G = so.sl_g[sl];
+            uint2 *svg2 = reinterpret_cast<uint2 *>(so.svg);
+            for (int p = lane; p < 9 * ((W + 3) / 4); p += 32) {
+                const int g = p / 9, e = p - 9 * g;
+                unsigned h[2] = {0u, 0u};
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
-                h[u >> 1] |= (unsigned)__bfloat16_as_ushort(__double2bfloat16(value(t, 4 * g + u, e))) << (16 * (u & 1));
-            svg2[((G + g) * 9 + e) * kSlice + t] = make_uint2(h[0], h[1]);
+                for (int u = 0; u < 4; ++u) {
+                    const int k = 4 * g + u;
+                    const double x = k < deg ? acc[9 * k + e] : 0.0;
+                    h[u >> 1] |= (unsigned)__bfloat16_as_ushort(__double2bfloat16(x)) << (16 * (u & 1));
+                }
+                svg2[((G + g) * 9 + e) * kSlice + t] = make_uint2(h[0], h[1]);
+            }
         }
-        __syncthreads();
+        __syncwarp();
     }
 }
 
@@ -673,18 +664,13 @@ static void gather(ofea_ctx *c, bool with_f, double *d_fint) {
     c->Kb.ensure((size_t)std::max<long long>(9 * c->nnzb, 1));
     if (!c->sell_layout_ok) build_sell_layout(c);
     const SellOut so{c->sl_ptr.p, c->sl_g.p, c->sv64.p, c->sv16.p, c->sv16g.p};
-    const int nslice = (c->nfree + kSlice - 1) / kSlice;
-    const int gw = std::max(1, std::min(nslice, c->num_sms * 2));
-    OFEA_CUDA(cudaFuncSetAttribute(k_gather_assemble<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)kGatherSmem));
-    OFEA_CUDA(cudaFuncSetAttribute(k_gather_assemble<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)kGatherSmem));
+    int gw = grid_for(c, c->nfree, kWarpsPerBlock);
     if (with_f)
-        k_gather_assemble<true><<<gw, kBlock, kGatherSmem, c->stream>>>(
+        k_gather_assemble<true><<<gw, kBlock, 0, c->stream>>>(
             c->nfree, c->ne8, c->node_of_free.p, c->inc_ptr.p, c->inc.p, c->slot.p, c->rowptr.p,
             c->Ke.p, c->Kb.p, c->Fe.p, d_fint, so);
     else
-        k_gather_assemble<false><<<gw, kBlock, kGatherSmem, c->stream>>>(
+        k_gather_assemble<false><<<gw, kBlock, 0, c->stream>>>(
             c->nfree, c->ne8, c->node_of_free.p, c->inc_ptr.p, c->inc.p, c->slot.p, c->rowptr.p,
             c->Ke.p, c->Kb.p, nullptr, nullptr, so);
     OFEA_CHECK_LAUNCH();

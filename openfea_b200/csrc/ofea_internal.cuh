@@ -94,19 +94,28 @@ struct DevBuf {
     }
 };
 
-// Pinned host scratch.
+// Pinned host scratch.  Blocks come from a per-process cache (devmem.cu):
+// cudaMallocHost takes milliseconds, and a fresh context would otherwise pay
+// it for every small flag buffer.
+void *pinned_take(size_t bytes);
+void pinned_give(void *p, size_t bytes);
+
 template <class T>
 struct HostBuf {
     T *p = nullptr;
     size_t n = 0;
+    HostBuf() = default;
+    HostBuf(const HostBuf &) = delete;
+    HostBuf &operator=(const HostBuf &) = delete;
     ~HostBuf() {
-        if (p) cudaFreeHost(p);
+        if (p) pinned_give(p, n * sizeof(T));
     }
     void ensure(size_t count) {
         if (count <= n && p) return;
-        if (p) cudaFreeHost(p);
+        if (p) pinned_give(p, n * sizeof(T));
         p = nullptr;
-        OFEA_CUDA(cudaMallocHost((void **)&p, count * sizeof(T)));
+        n = 0;
+        p = static_cast<T *>(pinned_take(count * sizeof(T)));
         n = count;
     }
 };

@@ -476,40 +476,44 @@ __global__ void k_coarse_E_sum(int na, int nchunk_max, const int *__restrict__ a
 
 constexpr int kGJ = 64;
 
-// Gauss-Jordan inverse of a 32 x 32 block held by one warp, lane l owning
-// column l in registers (x[r] = entry (r, l)).  Pivot p: broadcast of the
-// pivot column by 32 shuffles, then the same update as a sequential
-// Gauss-Jordan step; the pivot row is each lane's own x[p].  A pivot that
-// vanishes against the original diagonal (a degenerate aggregate) drops its
-// direction: row and column p of the result are zero.  Pivots p >= bb are
-// padding (their rows and columns are zero and stay so).
-__device__ __forceinline__ void warp_gj32(double (&x)[32], int bb, const double *__restrict__ diag0) {
-    const int lane = threadIdx.x & 31;
-    // the pivots' drop thresholds, one per lane, loaded once (a load per
-    // pivot would put a memory latency on every step of the chain)
+// Gauss-Jordan inverse, in place, of a 32 x 32 block of the shared-memory
+// tile a (rows and columns off .. off+31) by one warp, lane l owning column
+// off+l.  Pivot p: every lane copies the pivot column to registers, then
+// updates its own column as a sequential Gauss-Jordan step (the pivot row is
+// each lane's own entry).  A pivot that vanishes against the original
+// diagonal (a degenerate aggregate) drops its direction: row and column p of
+// the result are zero.  Pivots p >= bb are padding (their rows and columns
+// are zero and stay so).  The pivot loop is not unrolled: the warp's code
+// stays small (a fully unrolled form stalled on instruction fetch).
+__device__ __forceinline__ void warp_gj32(double (*a)[kGJ + 1], int off, int bb,
+                                          const double *__restrict__ diag0) {
+    const int lane = threadIdx.x & 31, col = off + lane;
+    // the pivots' drop thresholds, one per lane, loaded once
     const double thr = lane < bb ? 1e-12 * diag0[lane] : 0.0;
-#pragma unroll
-    for (int p = 0; p < 32; ++p) {
-        if (p >= bb) break;
+#pragma unroll 1
+    for (int p = 0; p < bb; ++p) {
         double colp[32];
 #pragma unroll
-        for (int r = 0; r < 32; ++r) colp[r] = __shfl_sync(0xffffffffu, x[r], p);
-        const double piv = colp[p];
-        const double rowp = x[p];
-        if (!(piv > __shfl_sync(0xffffffffu, thr, p))) {
-            x[p] = 0.0;
+        for (int r = 0; r < 32; ++r) colp[r] = a[off + r][off + p];
+        const double piv = a[off + p][off + p];
+        const double rowp = a[off + p][col];
+        const bool drop = !(piv > __shfl_sync(0xffffffffu, thr, p));
+        __syncwarp();
+        if (drop) {
+            a[off + p][col] = 0.0;
             if (lane == p)
 #pragma unroll
-                for (int r = 0; r < 32; ++r) x[r] = 0.0;
+                for (int r = 0; r < 32; ++r) a[off + r][col] = 0.0;
         } else {
             const double inv = 1.0 / piv;
 #pragma unroll
             for (int r = 0; r < 32; ++r) {
                 if (r == p) continue;
-                x[r] = (lane == p) ? -colp[r] * inv : x[r] - colp[r] * rowp * inv;
+                a[off + r][col] = (lane == p) ? -colp[r] * inv : a[off + r][col] - colp[r] * rowp * inv;
             }
-            x[p] = (lane == p) ? inv : rowp * inv;
+            a[off + p][col] = (lane == p) ? inv : rowp * inv;
         }
+        __syncwarp();
     }
 }
 
@@ -534,14 +538,7 @@ __global__ void __launch_bounds__(128) k_gj_diag(int m, int j0, int bb, const do
     }
     __syncthreads();
     const int b1 = min(bb, 32), b2 = bb - b1;
-    if (warp == 0) {  // X11 in place of A11
-        double x[32];
-#pragma unroll
-        for (int r = 0; r < 32; ++r) x[r] = a[r][lane];
-        warp_gj32(x, b1, diag0 + j0);
-#pragma unroll
-        for (int r = 0; r < 32; ++r) a[r][lane] = x[r];
-    }
+    if (warp == 0) warp_gj32(a, 0, b1, diag0 + j0);  // X11 in place of A11
     __syncthreads();
     if (b2 > 0) {
         // T = X11 A12 and U = A21 X11 (thread: column lane, rows warp + 4 q)
@@ -564,14 +561,7 @@ __global__ void __launch_bounds__(128) k_gj_diag(int m, int j0, int bb, const do
             a[32 + r][32 + lane] -= s2;
         }
         __syncthreads();
-        if (warp == 0) {  // X22 in place of the Schur complement
-            double x[32];
-#pragma unroll
-            for (int r = 0; r < 32; ++r) x[r] = a[32 + r][32 + lane];
-            warp_gj32(x, b2, diag0 + j0 + 32);
-#pragma unroll
-            for (int r = 0; r < 32; ++r) a[32 + r][32 + lane] = x[r];
-        }
+        if (warp == 0) warp_gj32(a, 32, b2, diag0 + j0 + 32);  // X22 in place of the Schur complement
         __syncthreads();
         // S12 = -T X22 in place of A12, S21 = -X22 U in place of A21
         for (int q = 0; q < 8; ++q) {

@@ -75,47 +75,67 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigne
     }
 }
 
-// Stage rows [r0, r0 + rows) x reduction [k0, k0 + kTK) of an operand as
+// Stage rows [r0, r0 + ROWS) x reduction [k0, k0 + kTK) of an operand as
 // BF16 into the K-major tile.  Entries outside [0, R) x [k0, kend) are zero.
-__device__ __forceinline__ void stage(__nv_bfloat16 *tile, int rows, const TcOperand &op, int r0, int R, long k0,
+// Every load of the slice is issued before the first conversion (the
+// thread's values are in registers), so the loads' latencies overlap.
+template <int ROWS>
+__device__ __forceinline__ void stage(__nv_bfloat16 *tile, const TcOperand &op, int r0, int R, long k0,
                                       long kend) {
-    const int total = rows * kTK;
+    constexpr int kV = ROWS * kTK / 4 / kTcThreads;  // float4 groups per thread
+    constexpr int kS = ROWS * kTK / kTcThreads;      // scalars per thread
     if (op.ks == 1 && (op.ms & 3) == 0 && (reinterpret_cast<uintptr_t>(op.p) & 15) == 0) {
         // contiguous along the reduction, rows 16-byte aligned: four k per
         // thread as one 16-byte load, stored as four adjacent BF16 of a core row
-        for (int idx = threadIdx.x; idx < total / 4; idx += kTcThreads) {
+        float4 v[kV];
+#pragma unroll
+        for (int q = 0; q < kV; ++q) {
+            const int idx = threadIdx.x + q * kTcThreads;
             const int rr = idx / (kTK / 4), kk = 4 * (idx % (kTK / 4));
             const long r = r0 + rr, k = k0 + kk;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            v[q] = make_float4(0.f, 0.f, 0.f, 0.f);
             if (r < R) {
                 const float *src = op.p + r * op.ms + k;
                 if (k + 3 < kend) {
-                    v = *reinterpret_cast<const float4 *>(src);
+                    v[q] = *reinterpret_cast<const float4 *>(src);
                 } else {
-                    if (k < kend) v.x = src[0];
-                    if (k + 1 < kend) v.y = src[1];
-                    if (k + 2 < kend) v.z = src[2];
+                    if (k < kend) v[q].x = src[0];
+                    if (k + 1 < kend) v[q].y = src[1];
+                    if (k + 2 < kend) v[q].z = src[2];
                 }
             }
-            __nv_bfloat162 lo = __floats2bfloat162_rn(v.x, v.y), hi = __floats2bfloat162_rn(v.z, v.w);
+        }
+#pragma unroll
+        for (int q = 0; q < kV; ++q) {
+            const int idx = threadIdx.x + q * kTcThreads;
+            const int rr = idx / (kTK / 4), kk = 4 * (idx % (kTK / 4));
+            __nv_bfloat162 lo = __floats2bfloat162_rn(v[q].x, v[q].y), hi = __floats2bfloat162_rn(v[q].z, v[q].w);
             uint2 packed;
             packed.x = *reinterpret_cast<uint32_t *>(&lo);
             packed.y = *reinterpret_cast<uint32_t *>(&hi);
             *reinterpret_cast<uint2 *>(tile + kmaj(rr, kk)) = packed;
         }
-    } else if (op.ks == 1) {  // contiguous along the reduction: consecutive threads take consecutive k
-        for (int idx = threadIdx.x; idx < total; idx += kTcThreads) {
-            const int rr = idx / kTK, kk = idx % kTK;
-            const long r = r0 + rr, k = k0 + kk;
-            const float v = (r < R && k < kend) ? op.p[r * op.ms + k] : 0.f;
-            tile[kmaj(rr, kk)] = __float2bfloat16_rn(v);
-        }
-    } else {  // contiguous along the rows
-        for (int idx = threadIdx.x; idx < total; idx += kTcThreads) {
-            const int kk = idx / rows, rr = idx % rows;
-            const long r = r0 + rr, k = k0 + kk;
-            const float v = (r < R && k < kend) ? op.p[r * op.ms + k * op.ks] : 0.f;
-            tile[kmaj(rr, kk)] = __float2bfloat16_rn(v);
+    } else {
+        // scalar loads, 32 per thread in flight; consecutive threads take
+        // consecutive addresses
+        const bool along_k = op.ks == 1;
+        constexpr int kH = kS < 32 ? kS : 32;
+#pragma unroll
+        for (int h = 0; h < kS; h += kH) {
+            float v[kH];
+#pragma unroll
+            for (int q = 0; q < kH; ++q) {
+                const int idx = threadIdx.x + (h + q) * kTcThreads;
+                const int rr = along_k ? idx / kTK : idx % ROWS, kk = along_k ? idx % kTK : idx / ROWS;
+                const long r = r0 + rr, k = k0 + kk;
+                v[q] = (r < R && k < kend) ? op.p[r * op.ms + k * op.ks] : 0.f;
+            }
+#pragma unroll
+            for (int q = 0; q < kH; ++q) {
+                const int idx = threadIdx.x + (h + q) * kTcThreads;
+                const int rr = along_k ? idx / kTK : idx % ROWS, kk = along_k ? idx % kTK : idx / ROWS;
+                tile[kmaj(rr, kk)] = __float2bfloat16_rn(v[q]);
+            }
         }
     }
 }
@@ -162,8 +182,8 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_gemm(int M, int N, long Kred,
             if (!ok) break;
         }
         __nv_bfloat16 *sA = stages + b * kStage, *sB = sA + kTM * kTK;
-        stage(sA, kTM, A, m0, M, k0, ke);
-        stage(sB, kTN, B, n0, N, k0, ke);
+        stage<kTM>(sA, A, m0, M, k0, ke);
+        stage<kTN>(sB, B, n0, N, k0, ke);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the tiles, to the tensor core's proxy
         __syncthreads();
         if (tid == 0) {
