@@ -191,6 +191,20 @@ OFEA_API int ofea_residual_norms_noalloc(ofea_ctx *ctx, int nrhs, const double *
  * the iterations more numerous.  Invalidates the coarse levels. */
 OFEA_API int ofea_set_coarse_nodes(ofea_ctx *ctx, int nodes);
 
+/* No counterpart in the reference: how ofea_assemble_linear runs.  0
+ * (default): C3D8 meshes whose nodes lie in at most 8 elements are integrated
+ * and assembled in one pass that writes only the solver's copy of K (block
+ * CSR values and element matrices are derived from it when ofea_get_csr or
+ * ofea_get_element_matrices asks); other meshes take the two-pass assembly
+ * (element matrices, then a gather).  1: always the two-pass assembly.  Both
+ * give the same bits. */
+OFEA_API int ofea_set_assembly_path(ofea_ctx *ctx, int path);
+
+/* Which assembly produced the current K: 0 the one-pass C3D8 assembly, 1 the
+ * two-pass assembly or K uploaded as CSC.  OFEA_ERR_STATE before an
+ * assembly. */
+OFEA_API int ofea_get_assembly_path(ofea_ctx *ctx, int *path);
+
 /* ---- learned coarse-correction stage -------------------------------------- */
 /* No counterpart in the reference.  OFEA_SOLVER_LEARNED adds a second coarse
  * stage to the mixed V-cycle, on nested aggregates (cells half as wide as the

@@ -122,6 +122,8 @@ def lib():
         "ofea_profile_solver_kernels": (_I, [_P, _I, _I, _P, _P]),
         "ofea_precond_reset": (_I, [_P]),
         "ofea_set_coarse_nodes": (_I, [_P, _I]),
+        "ofea_set_assembly_path": (_I, [_P, _I]),
+        "ofea_get_assembly_path": (_I, [_P, ctypes.POINTER(ctypes.c_int)]),
         "ofea_trim_device_memory": (_I, []),
         "ofea_learn_opts_default": (None, [_P]),
         "ofea_batch_create": (_I, [ctypes.POINTER(_P), _P, _I, _I]),
@@ -406,6 +408,16 @@ class Context:
     def set_coarse_nodes(self, nodes):
         """Target free nodes per coarse aggregate (default 1000)."""
         _check(lib().ofea_set_coarse_nodes(self.h, int(nodes)), "ofea_set_coarse_nodes")
+
+    def set_assembly_path(self, path):
+        """0: one-pass C3D8 assembly where the mesh allows it (default); 1: two-pass."""
+        _check(lib().ofea_set_assembly_path(self.h, int(path)), "ofea_set_assembly_path")
+
+    def assembly_path(self):
+        """0 if K came from the one-pass C3D8 assembly, 1 if from the two-pass one (or a CSC upload)."""
+        v = ctypes.c_int(-1)
+        _check(lib().ofea_get_assembly_path(self.h, ctypes.byref(v)), "ofea_get_assembly_path")
+        return v.value
 
     def precond_reset(self):
         """Rebuild the preconditioner at the next solve (as after a new assembly)."""

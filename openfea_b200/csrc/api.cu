@@ -337,7 +337,8 @@ int ofea_assemble_pattern(ofea_ctx *c, int *n, long long *nnz) {
 }
 
 static void after_assembly(ofea_ctx *c) {
-    build_block_jacobi(c);
+    if (!c->jacobi_fresh) build_block_jacobi(c);  // the fused assembly inverts the diagonal itself
+    c->jacobi_fresh = false;
     if (!c->sell_ok) build_sell(c);  // the assembly kernels write it themselves
     OFEA_CUDA(cudaMemcpyAsync(c->herr.p, c->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     OFEA_CUDA(cudaStreamSynchronize(c->stream));
@@ -421,6 +422,9 @@ int ofea_matrix_upload_csc(ofea_ctx *c, int nd, const double *xyz, const int *fr
         c->mesh_ok = true;
         c->pattern_ok = true;
         c->K_ok = true;
+        c->kb_ok = true;
+        c->asm_path = 1;
+        c->jacobi_fresh = false;
         c->sell_ok = c->sell_layout_ok = false;
         after_assembly(c);
         geometry_start(c);
@@ -436,6 +440,7 @@ int ofea_get_csr(ofea_ctx *c, int *rowptr, int *col, double *val) {
         const int nf = c->nfree;
         std::vector<int> brp(nf + 1), bcol(c->nnzb);
         std::vector<double> bval(val ? 9 * c->nnzb : 0);
+        if (val) ensure_kb(c);
         OFEA_CUDA(cudaMemcpyAsync(brp.data(), c->rowptr.p, sizeof(int) * (nf + 1), cudaMemcpyDeviceToHost, c->stream));
         OFEA_CUDA(cudaMemcpyAsync(bcol.data(), c->cols.p, sizeof(int) * c->nnzb, cudaMemcpyDeviceToHost, c->stream));
         if (val)
@@ -463,9 +468,10 @@ int ofea_get_csr(ofea_ctx *c, int *rowptr, int *col, double *val) {
 int ofea_get_element_matrices(ofea_ctx *c, int first, int count, double *Ke) {
     return guarded([&] {
         need(c != nullptr && Ke != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
-        need(c->K_ok && c->Ke.p && !c->matrix_only, OFEA_ERR_STATE, "no assembly yet");
+        need(c->K_ok && !c->matrix_only, OFEA_ERR_STATE, "no assembly yet");
         need(first >= 0 && count >= 0 && first + count <= c->ne, OFEA_ERR_INVALID_ARG, "range");
         use_device(c);
+        ensure_element_matrices(c);
         std::vector<double> blk(576);
         double *out = Ke;
         for (int e = first; e < first + count; ++e) {
@@ -512,6 +518,22 @@ static void check_solve_ready(ofea_ctx *c, const ofea_solve_opts &o) {
     if (o.method != OFEA_SOLVER_PCG64 && o.method != OFEA_SOLVER_MIXED && o.method != OFEA_SOLVER_LEARNED)
         fail(OFEA_ERR_UNKNOWN_SOLVER, "unknown solver method");
     if (!c->jacobi_ok) fail(OFEA_ERR_BREAKDOWN, "a diagonal block of K is not positive definite");
+}
+
+int ofea_set_assembly_path(ofea_ctx *c, int path) {
+    return guarded([&] {
+        need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
+        need(path == 0 || path == 1, OFEA_ERR_INVALID_ARG, "assembly path must be 0 (automatic) or 1 (two-pass)");
+        c->fused_off = path == 1;
+    });
+}
+
+int ofea_get_assembly_path(ofea_ctx *c, int *path) {
+    return guarded([&] {
+        need(c != nullptr && path != nullptr, OFEA_ERR_INVALID_ARG, "NULL argument");
+        need(c->K_ok, OFEA_ERR_STATE, "K not assembled");
+        *path = c->asm_path;
+    });
 }
 
 int ofea_set_coarse_nodes(ofea_ctx *c, int nodes) {

@@ -1298,6 +1298,9 @@ ofea_batch *batch_create(ofea_ctx *const *ctxs, int nv, int nrhs) {
         ofea_ctx *c = ctxs[v];
         if (!c) fail(OFEA_ERR_INVALID_ARG, "batch: NULL context");
         if (!c->K_ok || !c->sell_ok) fail(OFEA_ERR_STATE, "batch: variant " + std::to_string(v) + " not assembled");
+        OFEA_CUDA(cudaSetDevice(c->device));
+        ensure_sv16(c);  // BF16 planes of the V-cycle SpMMs (a fused assembly leaves them to be derived)
+        OFEA_CUDA(cudaStreamSynchronize(c->stream));
         if (c->device != ctxs[0]->device) fail(OFEA_ERR_INVALID_ARG, "batch: variants on different GPUs");
         b->ctx.push_back(c);
     }

@@ -92,6 +92,74 @@ __device__ __forceinline__ void inv3(const double *J, double *Ji) {
     Ji[8] = (J[0] * J[4] - J[1] * J[3]) * id;
 }
 
+// Jacobian of the 8-node brick at Gauss point q from its node coordinates
+// X[8][3], the physical gradients g_a[d] = sum_i Jinv[d][i] dN_i(a), stored
+// to out[a * sa + d * sd] as they are formed, and the point's weight det J
+// (Gauss weight 1), returned.  Every linear C3D8 path evaluates the point
+// through this function, so they give the same bits.
+__device__ __forceinline__ double hex_point(const double *X, int q, double *out, int sa, int sd) {
+    const double *dN = c_hex_dN + q * 24;
+    double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 2
+    for (int b = 0; b < 8; ++b) {  // J_ij = sum_b dN_i(b) X_bj, b ascending
+        const double x0 = X[3 * b], x1 = X[3 * b + 1], x2 = X[3 * b + 2];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double dn = dN[i * 8 + b];
+            J[3 * i] = fma(dn, x0, J[3 * i]);
+            J[3 * i + 1] = fma(dn, x1, J[3 * i + 1]);
+            J[3 * i + 2] = fma(dn, x2, J[3 * i + 2]);
+        }
+    }
+    double Ji[9];
+    inv3(J, Ji);
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            out[a * sa + d * sd] = fma(Ji[3 * d + 2], dN[16 + a], fma(Ji[3 * d + 1], dN[8 + a], Ji[3 * d] * dN[a]));
+    return det_sarrus(J);
+}
+
+// One Gauss point of T = sum_q w g_u g_v^T (w on the u side).
+__device__ __forceinline__ void lin_T_step(double *T, double w, const double *gu, const double *gv) {
+    const double a0 = w * gu[0], a1 = w * gu[1], a2 = w * gu[2];
+    T[0] = fma(a0, gv[0], T[0]);
+    T[1] = fma(a0, gv[1], T[1]);
+    T[2] = fma(a0, gv[2], T[2]);
+    T[3] = fma(a1, gv[0], T[3]);
+    T[4] = fma(a1, gv[1], T[4]);
+    T[5] = fma(a1, gv[2], T[5]);
+    T[6] = fma(a2, gv[0], T[6]);
+    T[7] = fma(a2, gv[1], T[7]);
+    T[8] = fma(a2, gv[2], T[8]);
+}
+
+// Linear elastic block from T: K_uv = lam T + mu T^T + mu tr(T) I, operation
+// order fixed (explicit FMAs) so every assembly path gives the same bits.
+__device__ __forceinline__ void lin_block(const double *T, double lam, double mu, double *k) {
+    const double md = mu * (T[0] + T[4] + T[8]);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            k[3 * i + j] = fma(lam, T[3 * i + j], i == j ? fma(mu, T[3 * j + i], md) : mu * T[3 * j + i]);
+}
+
+// Block-Jacobi inverse of one diagonal block; false (and the identity) for a
+// block without a positive determinant.
+__device__ __forceinline__ bool jacobi_inverse(const double *A, double *Ai) {
+    const double det = A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) +
+                       A[2] * (A[3] * A[7] - A[4] * A[6]);
+    if (!(det > 0.0) || !isfinite(det)) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) Ai[i] = (i % 4 == 0) ? 1.0 : 0.0;
+        return false;
+    }
+    inv3(A, Ai);
+    return true;
+}
+
 // Linear nodal block accumulation: k += w (lam ga gb^T + mu gb ga^T + mu (ga.gb) I).
 __device__ __forceinline__ void add_block_lin(double *k, const double *ga, const double *gb,
                                               double wl, double wm) {
@@ -317,7 +385,7 @@ __global__ void __launch_bounds__(128) k_hex_integrate_lin(int ne8, const int *_
                                                            const double *__restrict__ xyz,
                                                            const double *__restrict__ E8, double nu,
                                                            double *__restrict__ Ke) {
-    __shared__ double sX[kLinHex][24];
+    __shared__ double sX[kLinHex][25];  // odd stride: the 16 elements of a warp hit distinct banks
     __shared__ double sG[kLinHex][8][8][4];  // [element][q][a][d], d padded to 4
     __shared__ double sW[kLinHex][8];
     const int tid = threadIdx.x;
@@ -329,27 +397,9 @@ __global__ void __launch_bounds__(128) k_hex_integrate_lin(int ne8, const int *_
         }
         __syncthreads();
         {
-            const int le = tid >> 3, q = tid & 7;
+            const int q = tid >> 4, le = tid & 15;  // a warp shares two Gauss points (constant-cache broadcasts)
             if (le < nel) {
-                const double *dN = c_hex_dN + q * 24;
-                double J[9];
-#pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        double acc = 0;
-#pragma unroll
-                        for (int b = 0; b < 8; ++b) acc += dN[i * 8 + b] * sX[le][3 * b + j];
-                        J[3 * i + j] = acc;
-                    }
-                double Ji[9];
-                inv3(J, Ji);
-                sW[le][q] = det_sarrus(J);  // Gauss weight 1
-#pragma unroll
-                for (int a = 0; a < 8; ++a)
-#pragma unroll
-                    for (int d = 0; d < 3; ++d)
-                        sG[le][q][a][d] = Ji[3 * d] * dN[a] + Ji[3 * d + 1] * dN[8 + a] + Ji[3 * d + 2] * dN[16 + a];
+                sW[le][q] = hex_point(sX[le], q, &sG[le][q][0][0], 4, 1);
             }
         }
         __syncthreads();
@@ -361,29 +411,12 @@ __global__ void __launch_bounds__(128) k_hex_integrate_lin(int ne8, const int *_
                 ++a;
             }
             const int b = a + pr;
-            double T[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, d = 0;
+            double T[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const double w = sW[le][q];
-                const double ga0 = w * sG[le][q][a][0], ga1 = w * sG[le][q][a][1], ga2 = w * sG[le][q][a][2];
-                const double gb0 = sG[le][q][b][0], gb1 = sG[le][q][b][1], gb2 = sG[le][q][b][2];
-                T[0] = fma(ga0, gb0, T[0]);
-                T[1] = fma(ga0, gb1, T[1]);
-                T[2] = fma(ga0, gb2, T[2]);
-                T[3] = fma(ga1, gb0, T[3]);
-                T[4] = fma(ga1, gb1, T[4]);
-                T[5] = fma(ga1, gb2, T[5]);
-                T[6] = fma(ga2, gb0, T[6]);
-                T[7] = fma(ga2, gb1, T[7]);
-                T[8] = fma(ga2, gb2, T[8]);
-            }
-            d = T[0] + T[4] + T[8];
+            for (int q = 0; q < 8; ++q) lin_T_step(T, sW[le][q], sG[le][q][a], sG[le][q][b]);
             const Lame L = lame(E8[base + le], nu);
             double kab[9];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
-#pragma unroll
-                for (int j = 0; j < 3; ++j) kab[3 * i + j] = L.lam * T[3 * i + j] + L.mu * T[3 * j + i] + (i == j ? L.mu * d : 0.0);
+            lin_block(T, L.lam, L.mu, kab);
             double *ke = Ke + 576L * (base + le);
 #pragma unroll
             for (int i = 0; i < 9; ++i) ke[(a * 8 + b) * 9 + i] = kab[i];
@@ -397,7 +430,296 @@ __global__ void __launch_bounds__(128) k_hex_integrate_lin(int ne8, const int *_
     }
 }
 
-// ------------------------------------------------------------------ C3D4 --
+// ------------------------------------------------- fused linear assembly --
+// Linear C3D8 meshes: integration and assembly in one pass, no element
+// matrices in HBM.  One CTA per BSELL slice (32 block rows, sell.cuh) at a
+// time, one CTA per SM:
+//   * the slice's incident elements (sorted and de-duplicated once per
+//     pattern: se_ptr/se_list, and inc_loc = an incidence's position in that
+//     list) have their node coordinates and Lame constants staged in shared
+//     memory, and each row's incidences (position, local node, the slots of
+//     the element's 8 nodes) form a small table there;
+//   * chunk by chunk (ascending element order) thread (element, q) writes the
+//     8 shape-function gradients and det J of its Gauss point to shared memory;
+//   * thread (warp k, lane t) owns slot k of row t: it walks the row's
+//     incidences in ascending element order and adds the element block that
+//     lands in slot k to 9 registers.  The block is formed from the gradients
+//     exactly as k_hex_integrate_lin forms it (upper block, transposed for
+//     b < a) and the sums run in the gather's order, so K carries the same
+//     bits as the two-pass assembly;
+//   * the slice is written once: FP64 planes (coalesced), the grouped BF16
+//     copy through shared memory, and the diagonal block's inverse.
+// The block sums read 56 gradient doubles from shared memory per block: the
+// kernel is bound by shared-memory bandwidth, so slot loads that differ
+// between warps (1 to 8 blocks per row) do not idle the SM.  Meshes it does
+// not cover (tetrahedra, nodes in more than 8 elements, rows wider than 27
+// blocks, slices touching more than kFuMaxElem elements) take the two-pass
+// path.
+constexpr int kFuMaxW = 27;               // widest slice: 27 blocks
+constexpr int kFuNW = kFuMaxW;            // warps per CTA: warp k owns slot k
+constexpr int kFuThreads = 32 * kFuNW;
+constexpr int kFuRowInc = 8;              // incident elements per node
+constexpr int kFuMaxElem = 192;           // distinct elements per slice
+constexpr int kFuChunk = 96;              // elements whose gradients are in shared memory at once
+constexpr int kFuGS = 8 * 3 * 8 + 8 + 1;  // per element: g[a][d][q], det J [q]; odd stride
+constexpr int kFuXS = 25;                 // coordinate doubles per element (odd stride)
+constexpr size_t kFuSmem = sizeof(double) * (kFuMaxElem * kFuXS + kFuMaxElem * 2 + kFuChunk * kFuGS);
+
+// Block K_ab of an element from its gradients in shared memory (layout of
+// k_hex_assemble_fused): the upper block (a <= b) as k_hex_integrate_lin
+// computes it, transposed for b < a.
+__device__ __forceinline__ void fused_block(const double *G, int a, int b, double lam, double mu, double *kab) {
+    const bool sw = a > b;
+    const int u = sw ? b : a, v = sw ? a : b;
+    double T[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+    for (int q = 0; q < 8; ++q) {
+        const double gu[3] = {G[(3 * u) * 8 + q], G[(3 * u + 1) * 8 + q], G[(3 * u + 2) * 8 + q]};
+        const double gv[3] = {G[(3 * v) * 8 + q], G[(3 * v + 1) * 8 + q], G[(3 * v + 2) * 8 + q]};
+        lin_T_step(T, G[192 + q], gu, gv);
+    }
+    double k[9];
+    lin_block(T, lam, mu, k);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) kab[3 * i + j] = sw ? k[3 * j + i] : k[3 * i + j];
+}
+
+__global__ void __launch_bounds__(kFuThreads, 1) k_hex_assemble_fused(
+    int nfree, const int *__restrict__ node_of_free, const int *__restrict__ inc_ptr,
+    const int *__restrict__ inc, const uint16_t *__restrict__ slot, const uint16_t *__restrict__ inc_loc,
+    const int *__restrict__ se_ptr, const int *__restrict__ se_list, const int *__restrict__ topo8,
+    const double *__restrict__ xyz, const double *__restrict__ E8, double nu, const int *__restrict__ diag_pos,
+    const int *__restrict__ sl_ptr, const int *__restrict__ sl_g, double *__restrict__ sv64,
+    __nv_bfloat16 *__restrict__ svg, double *__restrict__ Dinv, float *__restrict__ Dinv32, int *__restrict__ err) {
+    extern __shared__ double fsm[];
+    double *sX = fsm;                      // [kFuMaxElem][kFuXS] node coordinates
+    double *sL = sX + kFuMaxElem * kFuXS;  // [kFuMaxElem][2]  lam, mu
+    double *sG = sL + kFuMaxElem * 2;      // [kFuChunk][kFuGS] gradients, then the BF16 staging
+    // row t's incidences: position in the slice's list, local node, and the
+    // slots of the element's 8 nodes as bytes (0xFF: fixed node)
+    __shared__ unsigned long long s_sl[kSlice][kFuRowInc];
+    __shared__ uint16_t s_loc[kSlice][kFuRowInc];
+    __shared__ unsigned char s_a[kSlice][kFuRowInc];
+    __shared__ int s_ninc[kSlice];
+    const int tid = threadIdx.x, lane = tid & 31, k = tid >> 5;
+    const int nslice = (nfree + kSlice - 1) / kSlice;
+    for (int s = blockIdx.x; s < nslice; s += gridDim.x) {
+        const int e0 = se_ptr[s], nes = se_ptr[s + 1] - e0;
+        const long S = sl_ptr[s];
+        const int W = sl_ptr[s + 1] - (int)S;
+        __syncthreads();  // the previous slice is written out
+        for (int v = tid; v < nes * 24; v += kFuThreads) {
+            const int le = v / 24, t = v - 24 * le, a = t / 3, d = t - 3 * a;
+            sX[le * kFuXS + t] = xyz[3L * topo8[8L * se_list[e0 + le] + a] + d];
+        }
+        for (int le = tid; le < nes; le += kFuThreads) {
+            const Lame L = lame(E8[se_list[e0 + le]], nu);
+            sL[2 * le] = L.lam;
+            sL[2 * le + 1] = L.mu;
+        }
+        if (tid < kSlice * kFuRowInc) {
+            const int t = tid / kFuRowInc, i = tid % kFuRowInc, r = s * kSlice + t;
+            int n = 0;
+            if (r < nfree) {
+                const int node = node_of_free[r], p0 = inc_ptr[node];
+                n = inc_ptr[node + 1] - p0;
+                if (i < n) {
+                    const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(slot) + (p0 + i));
+                    const unsigned w4[4] = {raw.x, raw.y, raw.z, raw.w};
+                    unsigned long long by = 0;
+#pragma unroll
+                    for (int b = 0; b < 8; ++b) {
+                        const unsigned kk = (w4[b >> 1] >> (16 * (b & 1))) & 0xFFFFu;
+                        by |= (unsigned long long)(kk < (unsigned)kFuMaxW ? kk : 0xFFu) << (8 * b);
+                    }
+                    s_sl[t][i] = by;
+                    s_loc[t][i] = inc_loc[p0 + i];
+                    s_a[t][i] = (unsigned char)(inc[p0 + i] & 7);
+                }
+            }
+            if (i == 0) s_ninc[t] = n;
+        }
+        const int r = s * kSlice + lane;
+        int cur = 0;  // next incidence of row `lane`
+        double acc[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) acc[e] = 0.0;
+        for (int c0 = 0; c0 < nes; c0 += kFuChunk) {
+            const int nel = min(kFuChunk, nes - c0);
+            __syncthreads();  // staging done; the previous chunk's gradients consumed
+            if (tid < kFuChunk * 8) {  // q-major: a warp shares its Gauss point (constant-cache broadcasts)
+                const int q = tid / kFuChunk, le = tid - q * kFuChunk;
+                if (le < nel) {
+                    double *G = sG + le * kFuGS;
+                    G[192 + q] = hex_point(sX + kFuXS * (c0 + le), q, G + q, 24, 8);
+                }
+            }
+            __syncthreads();
+            if (k < W) {
+                const int ninc = s_ninc[lane], chunk_hi = c0 + nel;
+                const unsigned kk4 = (unsigned)k * 0x01010101u;
+                for (; cur < ninc; ++cur) {
+                    const int loc = s_loc[lane][cur];
+                    if (loc >= chunk_hi) break;
+                    if (loc < c0) continue;  // ascending by construction; never read outside the chunk
+                    const unsigned long long by = s_sl[lane][cur];
+                    const unsigned m0 = __vcmpeq4((unsigned)by, kk4), m1 = __vcmpeq4((unsigned)(by >> 32), kk4);
+                    if ((m0 | m1) == 0u) continue;
+                    const int b = m0 ? (__ffs(m0) - 1) >> 3 : 4 + ((__ffs(m1) - 1) >> 3);
+                    double kab[9];
+                    fused_block(sG + (loc - c0) * kFuGS, s_a[lane][cur], b, sL[2 * loc], sL[2 * loc + 1], kab);
+#pragma unroll
+                    for (int e = 0; e < 9; ++e) acc[e] += kab[e];
+                }
+            }
+        }
+        __syncthreads();  // every chunk consumed: sG becomes the BF16 staging area
+        __nv_bfloat16 *sB = reinterpret_cast<__nv_bfloat16 *>(sG);  // [W][9][32]
+        const int dp = r < nfree ? diag_pos[r] : -1;
+        if (k < W) {
+#pragma unroll
+            for (int e = 0; e < 9; ++e) {
+                sv64[((S + k) * 9 + e) * kSlice + lane] = acc[e];
+                sB[(k * 9 + e) * kSlice + lane] = __double2bfloat16(acc[e]);
+            }
+        }
+        // block-Jacobi: the owner of the diagonal slot inverts it; a free node
+        // outside every element (empty row) gets the identity and the flag
+        if (k == dp || (r < nfree && dp < 0 && k == 0)) {
+            if (k != dp)
+#pragma unroll
+                for (int e = 0; e < 9; ++e) acc[e] = 0.0;
+            double Ai[9];
+            if (!jacobi_inverse(acc, Ai)) atomicExch(err, 1);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                Dinv[9L * r + i] = Ai[i];
+                Dinv32[9L * r + i] = (float)Ai[i];
+            }
+        }
+        __syncthreads();
+        const long G = sl_g[s];
+        const int ng = (W + 3) / 4;
+        uint2 *svg2 = reinterpret_cast<uint2 *>(svg);
+        for (int v = tid; v < ng * 9 * kSlice; v += kFuThreads) {
+            const int g = v / (9 * kSlice), rem = v - g * 9 * kSlice, e = rem / kSlice, t = rem - e * kSlice;
+            unsigned h[2] = {0u, 0u};
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int kk = 4 * g + u;
+                if (kk < W) h[u >> 1] |= (unsigned)__bfloat16_as_ushort(sB[(kk * 9 + e) * kSlice + t]) << (16 * (u & 1));
+            }
+            svg2[((G + g) * 9 + e) * kSlice + t] = make_uint2(h[0], h[1]);
+        }
+    }
+}
+
+// Per pattern: the sorted distinct elements of every slice's rows (pass 0
+// counts them, pass 1 writes them and every incidence's position in its
+// slice's list).  One CTA per slice, a bitonic sort of the slice's <= 256
+// incidences.  stats[0]: a node in more than kFuRowInc elements, stats[1]:
+// the widest slice, stats[2]: the most elements of a slice.
+constexpr int kSeThreads = kSlice * kFuRowInc;  // one thread per incidence of a slice
+
+template <bool FILL>
+__global__ void __launch_bounds__(kSeThreads) k_slice_elements(
+    int nfree, const int *__restrict__ node_of_free, const int *__restrict__ inc_ptr, const int *__restrict__ inc,
+    const int *__restrict__ sl_ptr, const int *__restrict__ se_ptr, int *__restrict__ se_cnt,
+    int *__restrict__ se_list, uint16_t *__restrict__ inc_loc, int *__restrict__ stats) {
+    __shared__ int key[kSeThreads];
+    __shared__ int rowbeg[kSlice + 1];
+    __shared__ int rownode[kSlice];
+    __shared__ int wsum[kSeThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nslice = (nfree + kSlice - 1) / kSlice;
+    for (int s = blockIdx.x; s < nslice; s += gridDim.x) {
+        if (warp == 0) {
+            const int r = s * kSlice + lane;
+            const int node = r < nfree ? node_of_free[r] : -1;
+            int cnt = node >= 0 ? inc_ptr[node + 1] - inc_ptr[node] : 0;
+            if (cnt > kFuRowInc) {
+                atomicExch(stats, 1);
+                cnt = kFuRowInc;
+            }
+            int v = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += t;
+            }
+            rownode[lane] = node;
+            rowbeg[lane + 1] = v;
+            if (lane == 0) rowbeg[0] = 0;
+            if (!FILL && lane == 0) atomicMax(stats + 1, sl_ptr[s + 1] - sl_ptr[s]);
+        }
+        __syncthreads();
+        const int total = rowbeg[kSlice];
+        int p = -1;
+        if (tid < total) {
+            int row = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1)
+                if (row + step < kSlice && rowbeg[row + step] <= tid) row += step;
+            p = inc_ptr[rownode[row]] + (tid - rowbeg[row]);
+            key[tid] = inc[p] >> 3;
+        } else {
+            key[tid] = 0x7FFFFFFF;
+        }
+        __syncthreads();
+        for (int k = 2; k <= kSeThreads; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                const int ixj = tid ^ j;
+                if (ixj > tid) {
+                    const int x = key[tid], y = key[ixj];
+                    if ((x > y) == ((tid & k) == 0)) {
+                        key[tid] = y;
+                        key[ixj] = x;
+                    }
+                }
+                __syncthreads();
+            }
+        const int kv = key[tid];
+        const int flag = tid < total && (tid == 0 || key[tid - 1] != kv);
+        // block scan of the flags: rank of each distinct element
+        const unsigned bal = __ballot_sync(0xffffffffu, flag);
+        if (lane == 0) wsum[warp] = __popc(bal);
+        __syncthreads();
+        int before = 0, count = 0;
+        for (int w = 0; w < kSeThreads / 32; ++w) {
+            if (w < warp) before += wsum[w];
+            count += wsum[w];
+        }
+        const int rank = before + __popc(bal & ((1u << lane) - 1u));
+        if (!FILL) {
+            if (tid == 0) {
+                se_cnt[s] = count;
+                atomicMax(stats + 2, count);
+            }
+        } else {
+            __syncthreads();  // every thread has read key[] for its flag
+            if (flag) {
+                se_list[se_ptr[s] + rank] = kv;
+                key[rank] = kv;  // compacted in place: rank <= tid, and every key is read
+            }
+            __syncthreads();
+            if (p >= 0) {
+                const int g = inc[p] >> 3;
+                int lo = 0, hi = count - 1;  // g is in key[0..count)
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (key[mid] < g) lo = mid + 1;
+                    else hi = mid;
+                }
+                inc_loc[p] = (uint16_t)lo;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ C3D4 --// ------------------------------------------------------------------ C3D4 --
 
 constexpr int kTetPerCta = 8;  // 16 threads per element: (a,b)
 
@@ -595,36 +917,44 @@ __global__ void __launch_bounds__(kBlock) k_gather_assemble(
 }
 
 // Block-Jacobi: invert each diagonal 3x3 block (FP64, and an FP32 copy).
-__global__ void k_block_jacobi(int nfree, const int *__restrict__ rowptr,
-                               const int *__restrict__ diag_pos, const double *__restrict__ Kb,
+__global__ void k_block_jacobi(int nfree, const int *__restrict__ diag_pos, KBlocks K,
                                double *__restrict__ Dinv, float *__restrict__ Dinv32,
                                int *__restrict__ err) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nfree; r += gridDim.x * blockDim.x) {
         const int dp = diag_pos[r];
         double A[9], Ai[9];
         if (dp >= 0) {
-            const double *D = Kb + 9L * (rowptr[r] + dp);
 #pragma unroll
-            for (int i = 0; i < 9; ++i) A[i] = D[i];
+            for (int i = 0; i < 9; ++i) A[i] = K.at(r, dp, i);
         } else {  // free node outside every element: K has an empty row
 #pragma unroll
             for (int i = 0; i < 9; ++i) A[i] = 0.0;
         }
-        double det = A[0] * (A[4] * A[8] - A[5] * A[7]) - A[1] * (A[3] * A[8] - A[5] * A[6]) +
-                     A[2] * (A[3] * A[7] - A[4] * A[6]);
-        if (!(det > 0.0) || !isfinite(det)) {
-            atomicExch(err, 1);
-#pragma unroll
-            for (int i = 0; i < 9; ++i) Ai[i] = (i % 4 == 0) ? 1.0 : 0.0;
-        } else {
-            inv3(A, Ai);
-        }
+        if (!jacobi_inverse(A, Ai)) atomicExch(err, 1);
 #pragma unroll
         for (int i = 0; i < 9; ++i) {
             Dinv[9L * r + i] = Ai[i];
             Dinv32[9L * r + i] = (float)Ai[i];
         }
     }
+}
+
+// Block-CSR values from the FP64 BSELL copy (for callers that read K in CSR
+// after a fused assembly, which writes only the solver's copy).
+__global__ void k_sell_to_kb(int nfree, const int *__restrict__ rowptr, const int *__restrict__ sl_ptr,
+                             const double *__restrict__ sv64, double *__restrict__ Kb) {
+    for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < 9L * nfree; v += (long)gridDim.x * blockDim.x) {
+        const int r = (int)(v / 9), e = (int)(v - 9L * r);
+        const long S = sl_ptr[r / kSlice];
+        const int rb = rowptr[r], deg = rowptr[r + 1] - rb, t = r % kSlice;
+        for (int k = 0; k < deg; ++k) Kb[9L * (rb + k) + e] = sv64[((S + k) * 9 + e) * kSlice + t];
+    }
+}
+
+// BF16 plane copy from the FP64 planes (the batched engine's operand).
+__global__ void k_sv64_to_sv16(long len, const double *__restrict__ sv64, __nv_bfloat16 *__restrict__ sv16) {
+    for (long v = blockIdx.x * (long)blockDim.x + threadIdx.x; v < len; v += (long)gridDim.x * blockDim.x)
+        sv16[v] = __double2bfloat16(sv64[v]);
 }
 
 static void integrate(ofea_ctx *c, bool nl, const double *d_u) {
@@ -658,6 +988,7 @@ static void integrate(ofea_ctx *c, bool nl, const double *d_u) {
                                                      nullptr, nullptr, Ke4, nullptr);
         OFEA_CHECK_LAUNCH();
     }
+    c->ke_ok = true;
 }
 
 static void gather(ofea_ctx *c, bool with_f, double *d_fint) {
@@ -675,12 +1006,77 @@ static void gather(ofea_ctx *c, bool with_f, double *d_fint) {
             c->Ke.p, c->Kb.p, nullptr, nullptr, so);
     OFEA_CHECK_LAUNCH();
     c->K_ok = true;
-    c->sell_ok = true;  // written by the gather
+    c->kb_ok = true;
+    c->asm_path = 1;
+    c->sell_ok = true;  // written by the gather, BF16 planes included
+    c->sv16_ok = true;
+    c->jacobi_fresh = false;
     c->coarse.K_ok = false;
     c->coarse2.K_ok = false;
 }
 
+// Slice element lists of the current pattern (one host sync, once per
+// pattern); se_state 1 when the fused assembly covers the mesh, -1 if not.
+static void build_slice_elements(ofea_ctx *c) {
+    c->se_state = -1;
+    if (c->ne4 != 0 || c->ne8 == 0 || c->nfree == 0 || c->fused_off) return;
+    if (!c->sell_layout_ok) build_sell_layout(c);
+    cudaStream_t s = c->stream;
+    const int nslice = (c->nfree + kSlice - 1) / kSlice;
+    const int tmp_len = nslice / 1024 + 4;
+    c->scratch_i.ensure((size_t)nslice + 1 + tmp_len + 4);
+    int *cnt = c->scratch_i.p, *tmp = cnt + nslice + 1, *stats = tmp + tmp_len;
+    c->se_ptr.ensure((size_t)nslice + 1);
+    OFEA_CUDA(cudaMemsetAsync(stats, 0, 4 * sizeof(int), s));
+    const int g = std::min(nslice, c->num_sms * 8);
+    k_slice_elements<false><<<g, kSeThreads, 0, s>>>(c->nfree, c->node_of_free.p, c->inc_ptr.p, c->inc.p,
+                                                     c->sl_ptr.p, nullptr, cnt, nullptr, nullptr, stats);
+    OFEA_CHECK_LAUNCH();
+    const long long total = exclusive_scan(cnt, c->se_ptr.p, nslice, s, tmp, tmp_len);
+    c->herr.ensure(4);
+    OFEA_CUDA(cudaMemcpyAsync(c->herr.p, stats, 3 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    OFEA_CUDA(cudaStreamSynchronize(s));
+    if (c->herr.p[0] != 0 || c->herr.p[1] > kFuMaxW || c->herr.p[2] > kFuMaxElem) return;
+    c->se_list.ensure((size_t)std::max<long long>(total, 1));
+    c->inc_loc.ensure((size_t)std::max<long>(8L * c->ne8, 1));
+    k_slice_elements<true><<<g, kSeThreads, 0, s>>>(c->nfree, c->node_of_free.p, c->inc_ptr.p, c->inc.p,
+                                                    c->sl_ptr.p, c->se_ptr.p, nullptr, c->se_list.p,
+                                                    c->inc_loc.p, stats);
+    OFEA_CHECK_LAUNCH();
+    c->se_state = 1;
+}
+
+// Fused linear assembly when the mesh allows it; false leaves K untouched.
+static bool assemble_linear_fused(ofea_ctx *c) {
+    if (c->se_state == 0) build_slice_elements(c);
+    if (c->se_state != 1 || c->fused_off) return false;
+    upload_hex_table();
+    cudaStream_t s = c->stream;
+    c->Dinv.ensure((size_t)9 * std::max(c->nfree, 1));
+    c->Dinv32.ensure((size_t)9 * std::max(c->nfree, 1));
+    OFEA_CUDA(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), s));
+    OFEA_CUDA(cudaFuncSetAttribute(k_hex_assemble_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFuSmem));
+    const int nslice = (c->nfree + kSlice - 1) / kSlice;
+    const int g = std::min(nslice, c->num_sms);
+    k_hex_assemble_fused<<<g, kFuThreads, kFuSmem, s>>>(
+        c->nfree, c->node_of_free.p, c->inc_ptr.p, c->inc.p, c->slot.p, c->inc_loc.p, c->se_ptr.p, c->se_list.p,
+        c->topo8.p, c->xyz.p, c->E8.p, c->nu, c->diag_pos.p, c->sl_ptr.p, c->sl_g.p, c->sv64.p, c->sv16g.p,
+        c->Dinv.p, c->Dinv32.p, c->err_flag.p);
+    OFEA_CHECK_LAUNCH();
+    c->K_ok = true;
+    c->asm_path = 0;
+    c->sell_ok = true;
+    c->kb_ok = false;        // block CSR on demand (ensure_kb)
+    c->sv16_ok = false;      // BF16 planes on demand (ensure_sv16)
+    c->ke_ok = false;        // element matrices on demand (ensure_element_matrices)
+    c->jacobi_fresh = true;  // Dinv written by the kernel
+    c->coarse.K_ok = false;
+    c->coarse2.K_ok = false;
+    return true;
+}
+
 void assemble_linear(ofea_ctx *c) {
+    if (assemble_linear_fused(c)) return;
     integrate(c, false, nullptr);
     gather(c, false, nullptr);
 }
@@ -695,10 +1091,31 @@ void build_block_jacobi(ofea_ctx *c) {
     c->Dinv32.ensure((size_t)9 * std::max(c->nfree, 1));
     OFEA_CUDA(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), c->stream));
     k_block_jacobi<<<grid_for(c, c->nfree, kBlock), kBlock, 0, c->stream>>>(
-        c->nfree, c->rowptr.p, c->diag_pos.p, c->Kb.p, c->Dinv.p, c->Dinv32.p, c->err_flag.p);
+        c->nfree, c->diag_pos.p, kblocks(c), c->Dinv.p, c->Dinv32.p, c->err_flag.p);
     OFEA_CHECK_LAUNCH();
 }
 
+void ensure_kb(ofea_ctx *c) {
+    if (c->kb_ok) return;
+    c->Kb.ensure((size_t)std::max<long long>(9 * c->nnzb, 1));
+    k_sell_to_kb<<<grid_for(c, 9L * c->nfree, kBlock), kBlock, 0, c->stream>>>(c->nfree, c->rowptr.p, c->sl_ptr.p,
+                                                                              c->sv64.p, c->Kb.p);
+    OFEA_CHECK_LAUNCH();
+    c->kb_ok = true;
+}
+
+void ensure_sv16(ofea_ctx *c) {
+    if (c->sv16_ok) return;
+    const long len = 9L * std::max<long long>(c->sell_len, 1) * kSlice;
+    k_sv64_to_sv16<<<grid_for(c, len, kBlock), kBlock, 0, c->stream>>>(len, c->sv64.p, c->sv16.p);
+    OFEA_CHECK_LAUNCH();
+    c->sv16_ok = true;
+}
+
+void ensure_element_matrices(ofea_ctx *c) {
+    if (c->ke_ok) return;
+    integrate(c, false, nullptr);  // the fused assembly left none: the linear ones it summed
+}
 
 // --------------------------------------------------------- stress recovery --
 // simulation_post::get_cauchy_stress_3d (src/post_process.cpp:79-167): seven

@@ -13,9 +13,12 @@
 //   slot       uint16[8*len(inc)]      for incidence k and local node b: block
 //                                      position within the row, 0xFFFF if b is fixed
 //   Kb         double[9*nnzb]          K values, block-row-major, 3x3 blocks row-major
+//                                      (derived from sv64 on demand after a fused assembly)
 //   sl_ptr, scols, sv64, sv16          the solver's copy of K in BSELL-32 (sell.cuh),
 //                                      FP64 values and a BF16 rounding
-//   Ke         double[576*ne8 + 144*ne4]  element matrices (scratch of the assembly):
+//   se_ptr, se_list, inc_loc           per BSELL slice the sorted elements of its rows, and
+//                                      each incidence's position in them (fused assembly)
+//   Ke         double[576*ne8 + 144*ne4]  element matrices (scratch of the two-pass assembly):
 //                                      element g, block (a,b), entries 3x3 row-major
 //   Dinv       double[9*nfree]         inverted diagonal blocks (block-Jacobi), + FP32 copy
 //   coarse                             aggregates, E = Z^T K Z and its FP32 inverse (precond.cu)
@@ -209,6 +212,17 @@ struct ofea_ctx {
     ofea::DevBuf<double> Kb, Ke, Fe, Dinv, u_nl, f_int;
     ofea::DevBuf<float> Dinv32;
     bool K_ok = false, jacobi_ok = false;
+    // what the last assembly left current besides the solver copy: the fused
+    // linear assembly writes only sv64, sv16g and Dinv; Kb, sv16 and Ke are
+    // derived on demand (ensure_kb, ensure_sv16, ensure_element_matrices)
+    bool kb_ok = false, sv16_ok = false, ke_ok = false, jacobi_fresh = false;
+    int asm_path = 1;  // 0: the fused assembly made K, 1: the two-pass assembly or a CSC upload
+    // per-slice element lists of the fused assembly (integrate.cu), per pattern:
+    // se_state 0 not built, 1 built, -1 the mesh takes the two-pass assembly
+    ofea::DevBuf<int> se_ptr, se_list;
+    ofea::DevBuf<uint16_t> inc_loc;
+    int se_state = 0;
+    bool fused_off = false;  // ofea_set_assembly_path(ctx, 1): always the two-pass assembly
     // solver layout of K (sell.cuh): BSELL-32, FP64 and BF16 values
     ofea::DevBuf<int> sl_ptr, scols;
     ofea::DevBuf<double> sv64;
@@ -237,6 +251,9 @@ void upload_csc(ofea_ctx *c, int n, const int *col_ptr, const int *row_idx, cons
 void assemble_linear(ofea_ctx *c);
 void assemble_nl(ofea_ctx *c, const double *d_u, double *d_fint);
 void build_block_jacobi(ofea_ctx *c);
+void ensure_kb(ofea_ctx *c);
+void ensure_sv16(ofea_ctx *c);
+void ensure_element_matrices(ofea_ctx *c);
 void stress_recovery(ofea_ctx *c, const double *d_u, int mode, double *d_elem, double *d_node);
 // sell.cu
 void build_sell_layout(ofea_ctx *c);

@@ -333,6 +333,7 @@ void build_pattern(ofea_ctx *c) {
     c->K_ok = false;
     c->sell_ok = false;
     c->sell_layout_ok = false;
+    c->se_state = 0;
     c->coarse.geom_ok = false;
     c->coarse.K_ok = false;
     c->coarse2.geom_ok = false;

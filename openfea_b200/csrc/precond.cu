@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(kGW * 32) k_galerkin_blocks(
     int na, const int *__restrict__ agg_ptr, const int *__restrict__ agg_nodes, const int *__restrict__ agg_of,
     const int *__restrict__ agg_cell, const int *__restrict__ node_of_free, const double *__restrict__ xyz,
     const double *__restrict__ centroid, double inv_scale, const int *__restrict__ rowptr,
-    const int *__restrict__ cols, const double *__restrict__ Kb, double *__restrict__ Eb, int *__restrict__ err) {
+    const int *__restrict__ cols, KBlocks KB, double *__restrict__ Eb, int *__restrict__ err) {
     extern __shared__ double gsm[];
     double (*acc)[27 * 36] = reinterpret_cast<double (*)[27 * 36]>(gsm);                  // [kGW][27 * 36]
     double (*stage)[32][18] = reinterpret_cast<double (*)[32][18]>(gsm + kGW * 27 * 36);  // [kGW][32][18]
@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(kGW * 32) k_galerkin_blocks(
                     for (int d = 0; d < 3; ++d) dj[d] = (xyz[3L * nj + d] - centroid[3L * J + d]) * inv_scale;
                     double K[9];
 #pragma unroll
-                    for (int e = 0; e < 9; ++e) K[e] = Kb[9L * (rb + k) + e];
+                    for (int e = 0; e < 9; ++e) K[e] = KB.at(i, k, e);
                     // W[:, l] = K e_l (l < 3), K (e_(l-3) x dj) (l >= 3); v[r * 6 + l]
 #pragma unroll
                     for (int r = 0; r < 3; ++r)
@@ -476,115 +476,64 @@ __global__ void k_coarse_E_sum(int na, int nchunk_max, const int *__restrict__ a
 
 constexpr int kGJ = 64;
 
-// Gauss-Jordan inverse, in place, of a 32 x 32 block of the shared-memory
-// tile a (rows and columns off .. off+31) by one warp, lane l owning column
-// off+l.  Pivot p: every lane copies the pivot column to registers, then
-// updates its own column as a sequential Gauss-Jordan step (the pivot row is
-// each lane's own entry).  A pivot that vanishes against the original
-// diagonal (a degenerate aggregate) drops its direction: row and column p of
-// the result are zero.  Pivots p >= bb are padding (their rows and columns
-// are zero and stay so).  The pivot loop is not unrolled: the warp's code
-// stays small (a fully unrolled form stalled on instruction fetch).
-__device__ __forceinline__ void warp_gj32(double (*a)[kGJ + 1], int off, int bb,
-                                          const double *__restrict__ diag0) {
-    const int lane = threadIdx.x & 31, col = off + lane;
-    // the pivots' drop thresholds, one per lane, loaded once
-    const double thr = lane < bb ? 1e-12 * diag0[lane] : 0.0;
+// Inverse of the diagonal block A_JJ -> S (kGJ x kGJ, padded with zeros
+// beyond bb) by one CTA of 256 threads: thread (ti, tj) keeps the entries
+// (ti + 16 u, tj + 16 v), u, v = 0..3, in registers.  Pivot p: the holders of
+// row p and column p publish them to shared memory (two buffers, so one
+// barrier per pivot), then every thread applies the Gauss-Jordan step to its
+// 16 entries: a_rc -= a_rp a_pc / a_pp, row p scaled by 1 / a_pp, column p by
+// -1 / a_pp, a_pp <- 1 / a_pp.  A pivot that vanishes against the original
+// diagonal (a degenerate aggregate) drops its direction: the step runs with
+// 1 / a_pp replaced by 0, which zeroes row and column p and leaves the rest.
+constexpr int kGjT = 16;  // threads per row / column of the thread grid
+
+__global__ void __launch_bounds__(kGjT * kGjT) k_gj_diag(int m, int j0, int bb, const double *__restrict__ A,
+                                                         double *__restrict__ S, const double *__restrict__ diag0) {
+    __shared__ double srow[2][kGJ], scol[2][kGJ], sthr[kGJ];
+    const int tid = threadIdx.x, ti = tid / kGjT, tj = tid % kGjT;
+    double a[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int r = ti + kGjT * u, c = tj + kGjT * v;
+            a[u][v] = (r < bb && c < bb) ? A[(long)(j0 + r) * m + j0 + c] : 0.0;
+        }
+    if (tid < kGJ) sthr[tid] = tid < bb ? 1e-12 * diag0[j0 + tid] : 0.0;
 #pragma unroll 1
     for (int p = 0; p < bb; ++p) {
-        double colp[32];
+        const int buf = p & 1, pq = p / kGjT, pr = p % kGjT;
 #pragma unroll
-        for (int r = 0; r < 32; ++r) colp[r] = a[off + r][off + p];
-        const double piv = a[off + p][off + p];
-        const double rowp = a[off + p][col];
-        const bool drop = !(piv > __shfl_sync(0xffffffffu, thr, p));
-        __syncwarp();
-        if (drop) {
-            a[off + p][col] = 0.0;
-            if (lane == p)
+        for (int w = 0; w < 4; ++w) {
+            if (w != pq) continue;
+            if (ti == pr)
 #pragma unroll
-                for (int r = 0; r < 32; ++r) a[off + r][col] = 0.0;
-        } else {
-            const double inv = 1.0 / piv;
+                for (int v = 0; v < 4; ++v) srow[buf][tj + kGjT * v] = a[w][v];
+            if (tj == pr)
 #pragma unroll
-            for (int r = 0; r < 32; ++r) {
-                if (r == p) continue;
-                a[off + r][col] = (lane == p) ? -colp[r] * inv : a[off + r][col] - colp[r] * rowp * inv;
+                for (int u = 0; u < 4; ++u) scol[buf][ti + kGjT * u] = a[u][w];
+        }
+        __syncthreads();
+        const double piv = srow[buf][p];
+        const double d = piv > sthr[p] ? 1.0 / piv : 0.0;
+        double cr[4], rc[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) cr[u] = scol[buf][ti + kGjT * u] * d;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) rc[v] = srow[buf][tj + kGjT * v];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const bool rp = ti + kGjT * u == p, cp = tj + kGjT * v == p;
+                const double upd = fma(-cr[u], rc[v], a[u][v]);
+                a[u][v] = rp ? (cp ? d : rc[v] * d) : (cp ? -cr[u] : upd);
             }
-            a[off + p][col] = (lane == p) ? inv : rowp * inv;
-        }
-        __syncwarp();
     }
-}
-
-// Inverse of the diagonal block A_JJ -> S (kGJ x kGJ, padded with zeros
-// beyond bb), one CTA of 4 warps.  With A_JJ = [A11 A12; A21 A22] in 32 x 32
-// blocks: X11 = A11^-1, T = X11 A12, U = A21 X11, X22 = (A22 - A21 T)^-1,
-// S = [X11 + T X22 U, -T X22; -X22 U, X22]: the block form of the same 64
-// Gauss-Jordan pivots (a dropped pivot zeroes its row and column here too),
-// with two warp-level 32-pivot eliminations in place of 64 CTA-wide steps.
-constexpr size_t kGjDiagSmem = sizeof(double) * (kGJ * (kGJ + 1) + 2 * 32 * 33);
-
-__global__ void __launch_bounds__(128) k_gj_diag(int m, int j0, int bb, const double *__restrict__ A,
-                                                 double *__restrict__ S, const double *__restrict__ diag0) {
-    extern __shared__ double gj_smem[];
-    double (*a)[kGJ + 1] = reinterpret_cast<double (*)[kGJ + 1]>(gj_smem);          // [64][65]
-    double (*t)[33] = reinterpret_cast<double (*)[33]>(gj_smem + kGJ * (kGJ + 1));  // [32][33]
-    double (*u)[33] = t + 32;                                                       // [32][33]
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int v = tid; v < kGJ * kGJ; v += 128) {
-        const int r = v / kGJ, c = v % kGJ;
-        a[r][c] = (r < bb && c < bb) ? A[(long)(j0 + r) * m + j0 + c] : 0.0;
-    }
-    __syncthreads();
-    const int b1 = min(bb, 32), b2 = bb - b1;
-    if (warp == 0) warp_gj32(a, 0, b1, diag0 + j0);  // X11 in place of A11
-    __syncthreads();
-    if (b2 > 0) {
-        // T = X11 A12 and U = A21 X11 (thread: column lane, rows warp + 4 q)
-        for (int q = 0; q < 8; ++q) {
-            const int r = warp + 4 * q;
-            double st = 0.0, su = 0.0;
-            for (int k = 0; k < 32; ++k) {
-                st = fma(a[r][k], a[k][32 + lane], st);
-                su = fma(a[32 + r][k], a[k][lane], su);
-            }
-            t[r][lane] = st;
-            u[r][lane] = su;
-        }
-        __syncthreads();
-        // Schur complement A22 - A21 T, in place of A22
-        for (int q = 0; q < 8; ++q) {
-            const int r = warp + 4 * q;
-            double s2 = 0.0;
-            for (int k = 0; k < 32; ++k) s2 = fma(a[32 + r][k], t[k][lane], s2);
-            a[32 + r][32 + lane] -= s2;
-        }
-        __syncthreads();
-        if (warp == 0) warp_gj32(a, 32, b2, diag0 + j0 + 32);  // X22 in place of the Schur complement
-        __syncthreads();
-        // S12 = -T X22 in place of A12, S21 = -X22 U in place of A21
-        for (int q = 0; q < 8; ++q) {
-            const int r = warp + 4 * q;
-            double s12 = 0.0, s21 = 0.0;
-            for (int k = 0; k < 32; ++k) {
-                s12 = fma(t[r][k], a[32 + k][32 + lane], s12);
-                s21 = fma(a[32 + r][32 + k], u[k][lane], s21);
-            }
-            a[r][32 + lane] = -s12;
-            a[32 + r][lane] = -s21;
-        }
-        __syncthreads();
-        // S11 = X11 - T S21, in place of X11 (each thread reads only its own X11 entry)
-        for (int q = 0; q < 8; ++q) {
-            const int r = warp + 4 * q;
-            double s11 = 0.0;
-            for (int k = 0; k < 32; ++k) s11 = fma(t[r][k], a[32 + k][lane], s11);
-            a[r][lane] -= s11;
-        }
-        __syncthreads();
-    }
-    for (int v = tid; v < kGJ * kGJ; v += 128) S[v] = a[v / kGJ][v % kGJ];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) S[(ti + kGjT * u) * kGJ + tj + kGjT * v] = a[u][v];
 }
 
 // Column panel, one warp per row i: P_i = A_{i,J} (saved for the update),
@@ -743,7 +692,6 @@ static void invert_spd(ofea_ctx *c, double *A, int m, int hb) {
     OFEA_CHECK_LAUNCH();
     const size_t upd_smem = sizeof(double) * (64 * (kGJ + 1) + kGJ * 65);
     OFEA_CUDA(cudaFuncSetAttribute(k_gj_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)upd_smem));
-    OFEA_CUDA(cudaFuncSetAttribute(k_gj_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGjDiagSmem));
     cudaEvent_t cross_done = nullptr, rest_done = nullptr;
     OFEA_CUDA(cudaEventCreateWithFlags(&cross_done, cudaEventDisableTiming));
     OFEA_CUDA(cudaEventCreateWithFlags(&rest_done, cudaEventDisableTiming));
@@ -753,7 +701,7 @@ static void invert_spd(ofea_ctx *c, double *A, int m, int hb) {
         const int lim = (int)std::min<long>(m, (long)j0 + bb + hb);
         dim3 tiles((lim + 63) / 64, (lim + 63) / 64);
         double *P = C.P.p + (size_t)(it & 1) * m * kGJ;
-        k_gj_diag<<<1, 128, kGjDiagSmem, s>>>(m, j0, bb, A, C.S.p, C.diag0.p);
+        k_gj_diag<<<1, kGjT * kGjT, 0, s>>>(m, j0, bb, A, C.S.p, C.diag0.p);
         k_gj_panel<<<grid_for(c, (long)lim * 32, 256), 256, 0, s>>>(m, lim, j0, bb, A, C.S.p, P);
         k_gj_rows<<<std::max(1, std::min((lim + 31) / 32, c->num_sms * 4)), 256, 0, s>>>(m, lim, j0, bb, A, C.S.p);
         if (rest_pending) OFEA_CUDA(cudaStreamWaitEvent(s, rest_done, 0));  // the previous panel's update is complete
@@ -853,7 +801,7 @@ void coarse_E_partials(ofea_ctx *c, Coarse &C, int nchunk) {
     OFEA_CUDA(cudaFuncSetAttribute(k_galerkin_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm_bytes));
     k_galerkin_blocks<<<std::max(1, C.na), kGW * 32, gsm_bytes, c->stream>>>(
         C.na, C.agg_ptr.p, C.agg_nodes.p, C.agg_of.p, C.agg_cell.p, c->node_of_free.p, c->xyz.p, C.centroid.p,
-        C.inv_scale, c->rowptr.p, c->cols.p, c->Kb.p, C.part.p, c->err_flag.p);
+        C.inv_scale, c->rowptr.p, c->cols.p, kblocks(c), C.part.p, c->err_flag.p);
     OFEA_CHECK_LAUNCH();
 }
 

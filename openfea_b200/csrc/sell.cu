@@ -115,6 +115,7 @@ void build_sell(ofea_ctx *c) {
         c->nfree, c->rowptr.p, c->Kb.p, c->sl_ptr.p, c->sv64.p, c->sv16.p, c->sl_g.p, c->sv16g.p);
     OFEA_CHECK_LAUNCH();
     c->sell_ok = true;
+    c->sv16_ok = true;
 }
 
 }  // namespace ofea

@@ -119,6 +119,22 @@ __device__ __forceinline__ void for_each_sell_row(int nfree, const int *__restri
     }
 }
 
+// Read access to block (r, k) of K: block CSR when it is current, else the
+// FP64 BSELL copy (all a fused assembly writes).
+struct KBlocks {
+    const double *Kb;  // null: read sv64
+    const int *rowptr, *sl_ptr;
+    const double *sv64;
+    __device__ __forceinline__ double at(int r, int k, int e) const {
+        if (Kb) return Kb[9L * (rowptr[r] + k) + e];
+        return sv64[((long)(sl_ptr[r / kSlice] + k) * 9 + e) * kSlice + (r % kSlice)];
+    }
+};
+
+inline KBlocks kblocks(const ofea_ctx *c) {
+    return KBlocks{c->kb_ok ? c->Kb.p : nullptr, c->rowptr.p, c->sl_ptr.p, c->sv64.p};
+}
+
 void build_sell(ofea_ctx *c);
 
 }  // namespace ofea
