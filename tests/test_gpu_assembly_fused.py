@@ -15,10 +15,12 @@ pytestmark = pytest.mark.gpu
 
 
 def jittered(nx, ny, nz, seed=3):
-    m = mg.structured_hex(nx, ny, nz, 1.0, 0.6, 0.9, 210e9, 0.3)
+    ext = np.array([1.0, 0.6, 0.9])
+    m = mg.structured_hex(nx, ny, nz, *ext, 210e9, 0.3)
     rng = np.random.default_rng(seed)
-    interior = np.all((m.xyz > 1e-9) & (m.xyz < np.array([1.0, 0.6, 0.9]) - 1e-9), axis=1)
-    m.xyz[interior] += rng.uniform(-0.02, 0.02, (int(interior.sum()), 3))
+    interior = np.all((m.xyz > 1e-9) & (m.xyz < ext - 1e-9), axis=1)
+    h = 0.15 * min(ext / np.array([nx, ny, nz]))  # distorted, never inverted
+    m.xyz[interior] += rng.uniform(-h, h, (int(interior.sum()), 3))
     m.E = rng.uniform(20e9, 300e9, m.ne)
     return m
 
