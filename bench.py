@@ -583,13 +583,18 @@ def run_ours(args):
         # a short launch list for profilers: a brief training (20 steps), then
         # one LEARNED, one MIXED and one plain solve
         ctx.learned_train(None, sample_iters=200, sample_every=4, steps=20, batch=16)
+        ctx.set_setup_trace(True)
         st_l = solve("GPU_LEARNED")
+        ph_l = ctx.setup_phase_times()
         st_m = solve("GPU_MIXED")
+        ph_m = ctx.setup_phase_times()
+        ctx.set_setup_trace(False)
         st_p = solve("GPU_PCG")
         torch.cuda.synchronize()
         if rank == 0:
             print(json.dumps({"mode": "solve-only", "shape": args.shape, "n": n, "nnz": nnz,
-                              "learned": st_l, "mixed": st_m, "plain": st_p}), flush=True)
+                              "learned": st_l, "mixed": st_m, "plain": st_p,
+                              "setup_phases_ms": {"GPU_LEARNED": ph_l, "GPU_MIXED": ph_m}}), flush=True)
         ctx.close()
         if dist:
             dist.destroy_process_group()
@@ -643,6 +648,15 @@ def run_ours(args):
     plain_s = max_over_ranks(min(st64["seconds"], st64b["seconds"]))
     oracle_err["GPU_PCG"] = oracle_error(u_dev, "cantilever", args.shape)
     err_vs_plain = float(torch.linalg.norm(u_learned - u_dev) / torch.linalg.norm(u_dev))
+
+    # the set-up's phases (CUDA events on the context stream), one traced
+    # solve of each preconditioned method after the timed region
+    ctx.set_setup_trace(True)
+    solve("GPU_LEARNED")
+    setup_phases = {"GPU_LEARNED": ctx.setup_phase_times()}
+    solve("GPU_MIXED")
+    setup_phases["GPU_MIXED"] = ctx.setup_phase_times()
+    ctx.set_setup_trace(False)
 
     # roofline of the dominant kernels (CUDA events on the launching stream)
     solve("GPU_MIXED")
@@ -727,6 +741,7 @@ def run_ours(args):
                    "learned_gain_vs_mixed": mixed_s / sec,
                    "learned_training": train,
                    "precond_setup_s": stats[-1]["setup_seconds"],
+                   "setup_phases_ms": setup_phases,
                    "mesh_pattern_assembly_s": setup_s},
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "phases": phases[-1] if phases else None},

@@ -191,6 +191,21 @@ OFEA_API int ofea_residual_norms_noalloc(ofea_ctx *ctx, int nrhs, const double *
  * the iterations more numerous.  Invalidates the coarse levels. */
 OFEA_API int ofea_set_coarse_nodes(ofea_ctx *ctx, int nodes);
 
+/* No counterpart in the reference: how the MIXED / LEARNED coarse level
+ * solves with E = Z^T K Z.  0 (default): E is banded in aggregate order, and
+ * where its block half-bandwidth is at most 8 blocks of 64 it is factored as
+ * a block LDL^T by one thread-block cluster and applied as two FP32
+ * triangular GEMVs; wider bands take the dense inverse.  1: always the dense
+ * inverse (blocked Gauss-Jordan, one FP32 GEMV).  A direction whose pivot
+ * vanishes (a degenerate aggregate) is dropped by both.  Invalidates the
+ * preconditioner of the current K. */
+OFEA_API int ofea_set_coarse_solver(ofea_ctx *ctx, int method);
+/* The current coarse solve applied to a host vector: y = E^-1 c (m values
+ * each, FP32 arithmetic as in the V-cycle); *m_out (if not NULL) = m and
+ * *factored (if not NULL) = 1 for the block LDL^T form.  The coarse level
+ * must exist (after a MIXED or LEARNED solve); c and y may be NULL to query. */
+OFEA_API int ofea_coarse_apply(ofea_ctx *ctx, const double *c, double *y, int *m_out, int *factored);
+
 /* No counterpart in the reference: how ofea_assemble_linear runs.  0
  * (default): C3D8 meshes whose nodes lie in at most 8 elements are integrated
  * and assembled in one pass that writes only the solver's copy of K (block
@@ -374,6 +389,17 @@ OFEA_API int ofea_ca_reanalysis(ofea_ctx *base, ofea_ctx *modified, const double
  * (every array the kernel must touch, counted once). */
 OFEA_API int ofea_profile_solver_kernels(ofea_ctx *ctx, int method, int reps, double *ms,
                                          double *bytes);
+/* Set-up trace (no counterpart in the reference): with on != 0 every later
+ * MIXED or LEARNED solve records CUDA events on the context's stream at the
+ * phase boundaries of its preconditioner set-up (the coarse levels' Galerkin
+ * blocks, the coarse inverse, the smoother interval, the network).
+ * ofea_setup_phase_times returns the last set-up's phases: ms[i] = device
+ * milliseconds of phase i, names = the phase names separated by ',' (NUL
+ * terminated, cut at names_len); *count = how many exist, up to cap are
+ * written (ms and names may be NULL to query). */
+OFEA_API int ofea_set_setup_trace(ofea_ctx *ctx, int on);
+OFEA_API int ofea_setup_phase_times(ofea_ctx *ctx, double *ms, int cap, int *count, char *names,
+                                    int names_len);
 
 #ifdef __cplusplus
 }

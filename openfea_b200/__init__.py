@@ -120,8 +120,12 @@ def lib():
         "ofea_write_vtk_stress": (_I, [ctypes.c_char_p, _I, _P, _I, _P, _P, _P, _D, _P]),
         "ofea_stress": (_I, [_P, _P, _I, _P, _P]),
         "ofea_profile_solver_kernels": (_I, [_P, _I, _I, _P, _P]),
+        "ofea_set_setup_trace": (_I, [_P, _I]),
+        "ofea_setup_phase_times": (_I, [_P, _P, _I, ctypes.POINTER(_I), ctypes.c_char_p, _I]),
         "ofea_precond_reset": (_I, [_P]),
         "ofea_set_coarse_nodes": (_I, [_P, _I]),
+        "ofea_set_coarse_solver": (_I, [_P, _I]),
+        "ofea_coarse_apply": (_I, [_P, _P, _P, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
         "ofea_set_assembly_path": (_I, [_P, _I]),
         "ofea_get_assembly_path": (_I, [_P, ctypes.POINTER(ctypes.c_int)]),
         "ofea_trim_device_memory": (_I, []),
@@ -409,6 +413,25 @@ class Context:
         """Target free nodes per coarse aggregate (default 1000)."""
         _check(lib().ofea_set_coarse_nodes(self.h, int(nodes)), "ofea_set_coarse_nodes")
 
+    def set_coarse_solver(self, method):
+        """0: block LDL^T factor of the banded coarse matrix where its band
+        allows (default); 1: dense Gauss-Jordan inverse."""
+        _check(lib().ofea_set_coarse_solver(self.h, int(method)), "ofea_set_coarse_solver")
+
+    def coarse_apply(self, c=None):
+        """y = E^-1 c by the current coarse solve (FP32 arithmetic); with c
+        None, (m, factored) only."""
+        m, fac = ctypes.c_int(0), ctypes.c_int(0)
+        _check(lib().ofea_coarse_apply(self.h, None, None, ctypes.byref(m), ctypes.byref(fac)), "ofea_coarse_apply")
+        if c is None:
+            return m.value, bool(fac.value)
+        c = np.ascontiguousarray(c, dtype=np.float64)
+        if c.shape != (m.value,):
+            raise ValueError(f"coarse vector must have {m.value} values")
+        y = np.zeros(m.value)
+        _check(lib().ofea_coarse_apply(self.h, _ptr(c), _ptr(y), None, None), "ofea_coarse_apply")
+        return y
+
     def set_assembly_path(self, path):
         """0: one-pass C3D8 assembly where the mesh allows it (default); 1: two-pass."""
         _check(lib().ofea_set_assembly_path(self.h, int(path)), "ofea_set_assembly_path")
@@ -432,6 +455,22 @@ class Context:
         _check(lib().ofea_profile_solver_kernels(self.h, m, reps, _ptr(ms), _ptr(by)),
                "ofea_profile_solver_kernels")
         return ms, by
+
+    def set_setup_trace(self, on=True):
+        """Record the preconditioner set-up's phase boundaries (CUDA events)
+        on the next MIXED / LEARNED solves."""
+        _check(lib().ofea_set_setup_trace(self.h, int(bool(on))), "ofea_set_setup_trace")
+
+    def setup_phase_times(self):
+        """{phase: device ms} of the last traced set-up, in order."""
+        n = ctypes.c_int(0)
+        _check(lib().ofea_setup_phase_times(self.h, None, 0, ctypes.byref(n), None, 0), "ofea_setup_phase_times")
+        ms = np.zeros(max(n.value, 1))
+        buf = ctypes.create_string_buffer(64 * max(n.value, 1) + 1)
+        _check(lib().ofea_setup_phase_times(self.h, _ptr(ms), n.value, ctypes.byref(n), buf, len(buf)),
+               "ofea_setup_phase_times")
+        names = buf.value.decode().split(",") if n.value else []
+        return dict(zip(names, ms[:n.value].tolist()))
 
     # ---- learned coarse-correction stage
     def learned_train(self, f=None, sample_iters=600, sample_every=4, steps=400, batch=16, lr=1e-3,

@@ -150,6 +150,7 @@ int ofea_ctx_destroy(ofea_ctx *c) {
                 cudaStreamSynchronize(x);
                 cudaStreamDestroy(x);
             }
+        setup_marks_clear(c);
         if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
         delete c;
     });
@@ -547,6 +548,41 @@ int ofea_set_coarse_nodes(ofea_ctx *c, int nodes) {
             c->coarse2.geom_ok = c->coarse2.K_ok = false;
         c->learned.links_ok = false;
         }
+    });
+}
+
+int ofea_set_coarse_solver(ofea_ctx *c, int method) {
+    return guarded([&] {
+        need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
+        need(method == 0 || method == 1, OFEA_ERR_INVALID_ARG, "coarse solver must be 0 (factor) or 1 (dense)");
+        geometry_join(c);
+        if (method != c->coarse_solver) {
+            c->coarse_solver = method;
+            c->coarse.K_ok = false;
+            c->coarse2.K_ok = false;
+        }
+    });
+}
+
+int ofea_coarse_apply(ofea_ctx *c, const double *cv, double *y, int *m_out, int *factored) {
+    return guarded([&] {
+        need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
+        use_device(c);
+        Coarse &C = c->coarse;
+        need(C.K_ok, OFEA_ERR_STATE, "no coarse level: run a MIXED or LEARNED solve first");
+        const int m = C.m;
+        if (m_out) *m_out = m;
+        if (factored) *factored = C.factored ? 1 : 0;
+        if (!cv || !y) return;
+        std::vector<float> h(m);
+        for (int i = 0; i < m; ++i) h[i] = (float)cv[i];
+        DevBuf<float> dc, de;
+        dc.upload(h.data(), m, c->stream);
+        de.ensure(m);
+        coarse_gemv(c, dc.p, de.p);
+        OFEA_CUDA(cudaMemcpyAsync(h.data(), de.p, sizeof(float) * m, cudaMemcpyDeviceToHost, c->stream));
+        OFEA_CUDA(cudaStreamSynchronize(c->stream));
+        for (int i = 0; i < m; ++i) y[i] = h[i];
     });
 }
 
@@ -990,6 +1026,42 @@ int ofea_profile_solver_kernels(ofea_ctx *c, int method, int reps, double *ms, d
         use_device(c);
         c->w.t.ensure(std::max(c->n, 1));
         profile_kernels(c, method, reps, ms, bytes);
+    });
+}
+
+int ofea_set_setup_trace(ofea_ctx *c, int on) {
+    return guarded([&] {
+        need(c != nullptr, OFEA_ERR_INVALID_ARG, "ctx is NULL");
+        use_device(c);
+        c->setup_trace = on != 0;
+        if (!on) setup_marks_clear(c);
+    });
+}
+
+int ofea_setup_phase_times(ofea_ctx *c, double *ms, int cap, int *count, char *names, int names_len) {
+    return guarded([&] {
+        need(c != nullptr && count != nullptr && cap >= 0 && names_len >= 0, OFEA_ERR_INVALID_ARG,
+             "bad argument");
+        use_device(c);
+        const auto &mk = c->setup_marks;
+        const int n = mk.empty() ? 0 : (int)mk.size() - 1;
+        *count = n;
+        std::string joined;
+        for (int i = 0; i < n; ++i) {
+            if (ms && i < cap) {
+                OFEA_CUDA(cudaEventSynchronize(mk[i + 1].second));
+                float t = 0.f;
+                OFEA_CUDA(cudaEventElapsedTime(&t, mk[i].second, mk[i + 1].second));
+                ms[i] = t;
+            }
+            if (i) joined += ',';
+            joined += mk[i + 1].first;
+        }
+        if (names && names_len > 0) {
+            const size_t k = std::min(joined.size(), (size_t)names_len - 1);
+            std::copy(joined.begin(), joined.begin() + k, names);
+            names[k] = '\0';
+        }
     });
 }
 

@@ -1090,6 +1090,7 @@ void prepare(ofea_batch *b, bool mixed) {
     if (mixed && !b->mixed_ready) {
         for (ofea_ctx *c : b->ctx) {
             setup_coarse(c, c->coarse_nodes);
+            coarse_dense_inverse(c);
             OFEA_CUDA(cudaStreamSynchronize(c->stream));
         }
         build_desc(b, true);

@@ -709,7 +709,9 @@ void setup_learned_level(ofea_ctx *c) {
     const int na = C2.na;
     const int nchunk = 1;
     OFEA_CUDA(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), s));
+    setup_mark(c, "geometry");
     coarse_E_partials(c, C2, nchunk);
+    setup_mark(c, "galerkin_level2");
     N.Eb.ensure((size_t)na * 27 * 36);
     N.Ehat.ensure((size_t)na * 27 * 36);
     N.dsq.ensure((size_t)6 * na);
@@ -724,6 +726,7 @@ void setup_learned_level(ofea_ctx *c) {
     OFEA_CUDA(cudaMemcpyAsync(c->herr.p, c->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     OFEA_CUDA(cudaStreamSynchronize(s));
     if (c->herr.p[0]) fail(OFEA_ERR_CAPACITY, "learned level: cells smaller than the element couplings");
+    setup_mark(c, "level2_blocks");
     double mean = 0;
     for (float v : f) mean += v;
     mean /= std::max(na, 1);
@@ -738,6 +741,7 @@ void setup_learned_level(ofea_ctx *c) {
     N.shifted.ensure(6L * na);
     N.sigma.ensure(4);
     N.scale.ensure(6L * na);
+    setup_mark(c, "level2_inverse_features");
     C2.K_ok = true;
 }
 
@@ -756,6 +760,7 @@ void setup_learned_levels(ofea_ctx *c) {
             C1.na, C1.m, C1.nbr.p, c->learned.children.p, c->coarse2.agg_cell.p, c->learned.pdel.p,
             c->learned.Eb.p, E);
         OFEA_CHECK_LAUNCH();
+        setup_mark(c, "e1_from_e2");
         coarse_finish(c);
     }
 }

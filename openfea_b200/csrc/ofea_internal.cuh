@@ -149,6 +149,13 @@ struct Coarse {
     DevBuf<int> agg_of, agg_ptr, agg_nodes, agg_cell, cell_agg, nbr;
     DevBuf<double> centroid, E, S, P, diag0, pp, part;
     DevBuf<float> Einv32, cvec, evec, pw;
+    // the coarse solve as a block LDL^T factor (precond.cu): S_k, L_ik and the
+    // FP32 array F (U = diag(S) V below, V^T above); dense_ok: Einv32 holds the
+    // dense inverse (the Gauss-Jordan path, or formed from F on demand)
+    bool factored = false, dense_ok = false;
+    int nbw = 0, ldf = 0;  // block half-bandwidth; row stride of F (m rounded up to 4)
+    DevBuf<double> Sb, Lb;
+    DevBuf<float> F32, zvec;
     std::vector<int> agg_cell_h, cell_agg_h;  // host copies (nesting of the learned level)
     std::vector<double> centroid_h;
 };
@@ -236,10 +243,15 @@ struct ofea_ctx {
     ofea::Coarse coarse2;     // nested finer level of the learned stage
     ofea::Learned learned;
     int coarse_nodes = 1000;  // target free nodes per aggregate
+    int coarse_solver = 0;    // 0: block LDL^T factor where the band allows, 1: dense inverse
     ofea::SolverWork w;
     ofea::DevBuf<int> scratch_i;
     ofea::DevBuf<int> err_flag;
     ofea::HostBuf<int> herr;
+    // set-up trace (ofea_set_setup_trace): events recorded on the context
+    // stream at the phase boundaries of the last preconditioner set-up
+    bool setup_trace = false;
+    std::vector<std::pair<const char *, cudaEvent_t>> setup_marks;
 };
 
 namespace ofea {
@@ -263,6 +275,10 @@ void spmv64(ofea_ctx *c, const double *d_x, double *d_y);
 void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_opts &o,
                   ofea_solve_stats &st, const std::function<void(const double *)> &on_chunk = {});
 void profile_kernels(ofea_ctx *c, int method, int reps, double *ms, double *bytes);
+// set-up trace: setup_mark records an event named `phase` (the phase that
+// ends there) when tracing is on; setup_marks_clear drops the last set-up's
+void setup_mark(ofea_ctx *c, const char *phase);
+void setup_marks_clear(ofea_ctx *c);
 // learned.cu
 void setup_learned_level(ofea_ctx *c);
 void setup_learned_levels(ofea_ctx *c);

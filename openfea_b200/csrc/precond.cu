@@ -10,7 +10,10 @@
 // `coarse_nodes` nodes; each non-empty cell I is an aggregate with six modes
 // (three translations, three rotations about its centroid, scaled by the
 // cell size).  E = Z^T K Z (FP64, 6 x 6 blocks between neighbouring cells) is
-// inverted on the device by blocked Gauss-Jordan and applied as an FP32 GEMV.
+// banded in cell order; it is factored on the device as a block LDL^T (one
+// thread-block cluster) and applied as two FP32 triangular GEMVs, or, where
+// the band is too wide, inverted by blocked Gauss-Jordan and applied as one
+// FP32 GEMV.
 //
 // The smoother's SpMV reads a BF16 rounding of K into FP32 arithmetic; that
 // is accurate for the high-frequency error the smoother damps, and the smooth
@@ -487,9 +490,19 @@ constexpr int kGJ = 64;
 // 1 / a_pp replaced by 0, which zeroes row and column p and leaves the rest.
 constexpr int kGjT = 16;  // threads per row / column of the thread grid
 
-__global__ void __launch_bounds__(kGjT * kGjT) k_gj_diag(int m, int j0, int bb, const double *__restrict__ A,
-                                                         double *__restrict__ S, const double *__restrict__ diag0) {
-    __shared__ double srow[2][kGJ], scol[2][kGJ], sthr[kGJ];
+// The diagonal-block step of both coarse inversions: A_JJ (rows and columns
+// j0..j0+bb of the m x m row-major A) -> its inverse S (kGJ x kGJ row-major,
+// zero beyond bb), by the CTA's kGjT x kGjT threads.  Pivot p: the holders of
+// row p and column p publish them to shared memory and zero them in their
+// registers, the holder of a_pp publishes d = 1 / a_pp (0 for a vanishing
+// pivot), one barrier, then every entry takes the same update
+// a_rc <- a_rc - cr_r rc_c with cr_r = a_rp d (r != p), cr_p = -d,
+// rc_c = a_pc (c != p), rc_p = 1, which gives a_rc - a_rp a_pc d off row and
+// column p, a_pc d on row p, -a_rp d on column p and d at (p, p).
+__device__ __forceinline__ void gj_block_inverse(int m, int j0, int bb, const double *__restrict__ A,
+                                                 double *__restrict__ S, const double *__restrict__ diag0,
+                                                 double (*srow)[kGJ], double (*scol)[kGJ], double *sthr,
+                                                 double *sd) {
     const int tid = threadIdx.x, ti = tid / kGjT, tj = tid % kGjT;
     double a[4][4];
 #pragma unroll
@@ -497,43 +510,57 @@ __global__ void __launch_bounds__(kGjT * kGjT) k_gj_diag(int m, int j0, int bb, 
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
             const int r = ti + kGjT * u, c = tj + kGjT * v;
-            a[u][v] = (r < bb && c < bb) ? A[(long)(j0 + r) * m + j0 + c] : 0.0;
+            a[u][v] = (r < bb && c < bb) ? __ldcg(A + (long)(j0 + r) * m + j0 + c) : 0.0;
         }
-    if (tid < kGJ) sthr[tid] = tid < bb ? 1e-12 * diag0[j0 + tid] : 0.0;
+    if (tid < kGJ) sthr[tid] = tid < bb ? 1e-12 * __ldcg(diag0 + j0 + tid) : 0.0;
+    __syncthreads();
 #pragma unroll 1
     for (int p = 0; p < bb; ++p) {
         const int buf = p & 1, pq = p / kGjT, pr = p % kGjT;
 #pragma unroll
         for (int w = 0; w < 4; ++w) {
-            if (w != pq) continue;
+            if (w != pq || (ti != pr && tj != pr)) continue;
+            double rowv[4], colv[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) rowv[v] = a[w][v];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) colv[u] = a[u][w];
+            if (ti == pr && tj == pr) sd[buf] = a[w][w] > sthr[p] ? 1.0 / a[w][w] : 0.0;
             if (ti == pr)
 #pragma unroll
-                for (int v = 0; v < 4; ++v) srow[buf][tj + kGjT * v] = a[w][v];
+                for (int v = 0; v < 4; ++v) {
+                    srow[buf][tj + kGjT * v] = rowv[v];
+                    a[w][v] = 0.0;
+                }
             if (tj == pr)
 #pragma unroll
-                for (int u = 0; u < 4; ++u) scol[buf][ti + kGjT * u] = a[u][w];
+                for (int u = 0; u < 4; ++u) {
+                    scol[buf][ti + kGjT * u] = colv[u];
+                    a[u][w] = 0.0;
+                }
         }
         __syncthreads();
-        const double piv = srow[buf][p];
-        const double d = piv > sthr[p] ? 1.0 / piv : 0.0;
+        const double d = sd[buf];
         double cr[4], rc[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) cr[u] = scol[buf][ti + kGjT * u] * d;
+        for (int u = 0; u < 4; ++u) cr[u] = ti + kGjT * u == p ? -d : scol[buf][ti + kGjT * u] * d;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) rc[v] = srow[buf][tj + kGjT * v];
+        for (int v = 0; v < 4; ++v) rc[v] = tj + kGjT * v == p ? 1.0 : srow[buf][tj + kGjT * v];
 #pragma unroll
         for (int u = 0; u < 4; ++u)
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const bool rp = ti + kGjT * u == p, cp = tj + kGjT * v == p;
-                const double upd = fma(-cr[u], rc[v], a[u][v]);
-                a[u][v] = rp ? (cp ? d : rc[v] * d) : (cp ? -cr[u] : upd);
-            }
+            for (int v = 0; v < 4; ++v) a[u][v] = fma(-cr[u], rc[v], a[u][v]);
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
         for (int v = 0; v < 4; ++v) S[(ti + kGjT * u) * kGJ + tj + kGjT * v] = a[u][v];
+}
+
+__global__ void __launch_bounds__(kGjT * kGjT) k_gj_diag(int m, int j0, int bb, const double *__restrict__ A,
+                                                         double *__restrict__ S, const double *__restrict__ diag0) {
+    __shared__ double srow[2][kGJ], scol[2][kGJ], sthr[kGJ], sd[2];
+    gj_block_inverse(m, j0, bb, A, S, diag0, srow, scol, sthr, sd);
 }
 
 // Column panel, one warp per row i: P_i = A_{i,J} (saved for the update),
@@ -667,6 +694,330 @@ __global__ void k_round_f32(long n, const double *__restrict__ a, float *__restr
         b[i] = (float)a[i];
 }
 
+// ------------------------------------------------ banded block LDL^T factor --
+// The coarse solve of a banded E (half-bandwidth hb, so block half-bandwidth
+// bw = floor((hb + 63) / 64) in 64 x 64 blocks) as a block LDL^T factor
+// instead of the dense inverse:
+//   for k = 0 .. nb-1:  S_k = (A_kk)^-1                  (gj_block_inverse)
+//                       L_ik = A_ik S_k                  (k < i <= k + bw)
+//                       A_ij -= L_ik A_jk^T              (k < j <= i <= k + bw)
+// so A = L D L^T with L unit block-lower and D^-1 = diag(S_k); then, with
+// V = L^-1 (unit block-lower, dense below the diagonal),
+//   A^-1 = V^T diag(S) V,   V_ij = -sum_{l = max(j, i - bw)}^{i-1} L_il V_lj.
+// The FP32 array F (m x m) keeps U = diag(S) V in its block-lower triangle
+// (diagonal blocks: S_k) and V^T in its strict block-upper triangle, and
+// A^-1 c = V^T (U c): two triangular GEMVs reading F once.  A vanishing pivot
+// of a diagonal block drops its direction (zero row and column of S_k, hence
+// of L's column and of the result), as in the dense Gauss-Jordan inverse.
+// Flops: nb steps of (bw + 1)(bw + 2)/2 tile products for the factor and
+// about nb^2 bw / 2 for V (about a tenth of the dense inverse at m = 3000,
+// hb = 191), and the factor's serial chain is nb short steps of one cluster
+// instead of nb multi-kernel panels.
+constexpr int kLdlCluster = 8;   // CTAs of the factor's one thread-block cluster
+constexpr int kLdlMaxBw = 8;     // widest block band factored (wider: dense inverse)
+constexpr int kLdlLd = kGJ + 1;  // shared-memory tile row stride (odd: no bank conflicts)
+constexpr int kVuCols = 16;      // columns of V per CTA of k_ldl_vu
+static_assert(kLdlMaxBw <= kLdlCluster, "one L tile per CTA of the factor's cluster");
+
+__device__ __forceinline__ void cluster_arrive() {
+    __threadfence();  // this CTA's global writes are visible to the cluster's other CTAs
+    asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory"); }
+
+__device__ __forceinline__ void cluster_sync_all() {
+    cluster_arrive();
+    cluster_wait();
+}
+
+__device__ __forceinline__ unsigned cluster_rank() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+    return r;
+}
+
+// sT[r][c] = G[(r0 + r) * ld + c0 + c] (zero outside rows < rmax, cols < cmax);
+// transposed: sT[c][r].  By the CTA's 256 threads, all sixteen loads of a
+// thread issued before the first store.  Loads bypass L1: other CTAs of the
+// cluster wrote these tiles during the kernel.
+template <bool TRANS>
+__device__ __forceinline__ void ldl_load_tile(double (*sT)[kLdlLd], const double *__restrict__ G, long ld, int r0,
+                                              int c0, int rmax, int cmax) {
+    constexpr int kPer = kGJ * kGJ / 256;
+    double x[kPer];
+#pragma unroll
+    for (int t = 0; t < kPer; ++t) {
+        const int v = threadIdx.x + 256 * t, r = v / kGJ, c = v % kGJ;
+        x[t] = (r0 + r < rmax && c0 + c < cmax) ? __ldcg(G + (long)(r0 + r) * ld + c0 + c) : 0.0;
+    }
+#pragma unroll
+    for (int t = 0; t < kPer; ++t) {
+        const int v = threadIdx.x + 256 * t, r = v / kGJ, c = v % kGJ;
+        if (TRANS) sT[c][r] = x[t];
+        else sT[r][c] = x[t];
+    }
+}
+
+// acc[u][v] = sum_q sX[ti + 16u][q] sY[q][tj + 16v]  (thread (ti, tj) of 16 x 16)
+__device__ __forceinline__ void ldl_tile_product(const double (*sX)[kLdlLd], const double (*sY)[kLdlLd],
+                                                 double (&acc)[4][4]) {
+    const int ti = threadIdx.x / kGjT, tj = threadIdx.x % kGjT;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
+#pragma unroll 4
+    for (int q = 0; q < kGJ; ++q) {
+        double x[4], y[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = sX[ti + kGjT * u][q];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) y[v] = sY[q][tj + kGjT * v];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) acc[u][v] = fma(x[u], y[v], acc[u][v]);
+    }
+}
+
+// Update tile A_ij -= L_ik A_jk^T of step k (L_ik is tile a of step k's L
+// tiles), by the CTA's 256 threads; the tile's old values are loaded before
+// the product so their latency overlaps it.
+__device__ __forceinline__ void ldl_update_tile(int m, int k, int bw, int a, int i, int j, double *__restrict__ A,
+                                                const double *__restrict__ Lb, double (*sX)[kLdlLd],
+                                                double (*sY)[kLdlLd]) {
+    const int ti = threadIdx.x / kGjT, tj = threadIdx.x % kGjT;
+    ldl_load_tile<false>(sX, Lb + ((long)k * bw + a) * kGJ * kGJ, kGJ, 0, 0, kGJ, kGJ);
+    ldl_load_tile<true>(sY, A, m, kGJ * j, kGJ * k, m, m);
+    double old[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int r = kGJ * i + ti + kGjT * u, c = kGJ * j + tj + kGjT * v;
+            old[u][v] = (r < m && c < m) ? __ldcg(A + (long)r * m + c) : 0.0;
+        }
+    __syncthreads();
+    double acc[4][4];
+    ldl_tile_product(sX, sY, acc);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int r = kGJ * i + ti + kGjT * u, c = kGJ * j + tj + kGjT * v;
+            if (r < m && c < m) A[(long)r * m + c] = old[u][v] - acc[u][v];
+        }
+    __syncthreads();
+}
+
+// The factor: one cluster of kLdlCluster CTAs of kGjT^2 threads.  A (m x m,
+// symmetric, band hb) is updated in place in its block-lower band; S_k go to
+// Sb [nb][64][64], L_ik to Lb [nb][bw][64][64] (tile k + 1 + t at t).
+// Step k: CTA t computes L tile t (one each: bw <= kLdlMaxBw = kLdlCluster);
+// CTA 0 then goes on, without waiting for the others, to the next diagonal
+// tile A_{k+1,k+1} -= L_{k+1,k} A_{k+1,k}^T (its own L tile) and that tile's
+// inverse S_{k+1}, while CTAs 1.. wait for every L tile and update the rest
+// of the trailing band; one cluster barrier ends the step.  The serial chain
+// per step is one L tile, one update tile and one diagonal-block inverse.
+__global__ void __cluster_dims__(kLdlCluster, 1, 1) __launch_bounds__(kGjT * kGjT)
+    k_ldl_band(int m, int nb, int bw, double *__restrict__ A, double *__restrict__ Sb, double *__restrict__ Lb,
+               const double *__restrict__ diag0) {
+    extern __shared__ double ldl_sm[];
+    double (*sX)[kLdlLd] = reinterpret_cast<double (*)[kLdlLd]>(ldl_sm);
+    double (*sY)[kLdlLd] = reinterpret_cast<double (*)[kLdlLd]>(ldl_sm + kGJ * kLdlLd);
+    __shared__ double srow[2][kGJ], scol[2][kGJ], sthr[kGJ], sd[2];
+    const int rank = (int)cluster_rank();
+    const int ti = threadIdx.x / kGjT, tj = threadIdx.x % kGjT;
+    if (rank == 0) gj_block_inverse(m, 0, min(kGJ, m), A, Sb, diag0, srow, scol, sthr, sd);
+    cluster_sync_all();
+    for (int k = 0; k < nb; ++k) {
+        const int j0 = kGJ * k;
+        const double *Sk = Sb + (long)k * kGJ * kGJ;
+        const int nl = min(bw, nb - 1 - k);
+        if (nl == 0) break;  // the last step: nothing below the diagonal
+        if (rank < nl) {  // L_ik = A_ik S_k, i = k + 1 + rank
+            ldl_load_tile<false>(sX, A, m, kGJ * (k + 1 + rank), j0, m, m);
+            ldl_load_tile<false>(sY, Sk, kGJ, 0, 0, kGJ, kGJ);
+            __syncthreads();
+            double acc[4][4];
+            ldl_tile_product(sX, sY, acc);
+            double *L = Lb + ((long)k * bw + rank) * kGJ * kGJ;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) L[(ti + kGjT * u) * kGJ + tj + kGjT * v] = acc[u][v];
+            __syncthreads();
+        }
+        cluster_arrive();  // the L tiles are written
+        if (rank == 0) {
+            // tile p = 0 (the next diagonal block) needs only CTA 0's own L tile
+            ldl_update_tile(m, k, bw, 0, k + 1, k + 1, A, Lb, sX, sY);
+            const int j1 = kGJ * (k + 1);
+            gj_block_inverse(m, j1, min(kGJ, m - j1), A, Sb + (long)(k + 1) * kGJ * kGJ, diag0, srow, scol, sthr,
+                             sd);
+            cluster_wait();
+        } else {
+            cluster_wait();
+            // update tiles p = a (a + 1) / 2 + b (b <= a < nl), p >= 1
+            for (int p = rank; p < nl * (nl + 1) / 2; p += kLdlCluster - 1) {
+                int a = 0;
+                while ((a + 1) * (a + 2) / 2 <= p) ++a;
+                const int b = p - a * (a + 1) / 2;
+                ldl_update_tile(m, k, bw, a, k + 1 + a, k + 1 + b, A, Lb, sX, sY);
+            }
+        }
+        cluster_sync_all();
+    }
+}
+
+// V and U of the factor into F: CTA (block column j, strip s) walks block rows
+// i = j .. nb-1 with the last bw + 1 blocks of its kVuCols columns of V in
+// shared memory (FP64).  The tiles it multiplies form one sequence (for each
+// i: L_il for l = max(j, i - bw) .. i - 1, then S_i); the next tile's loads
+// are in flight while the current one is multiplied (two shared buffers).
+__global__ void __launch_bounds__(256) k_ldl_vu(int m, int ldf, int nb, int bw, const double *__restrict__ Sb,
+                                                const double *__restrict__ Lb, float *__restrict__ F) {
+    extern __shared__ double vu_sm[];
+    constexpr int SW = kGJ / kVuCols;  // strips per block column
+    constexpr int kPer = kGJ * kGJ / 256;
+    double (*ring)[kGJ][kVuCols + 1] = reinterpret_cast<double (*)[kGJ][kVuCols + 1]>(vu_sm + 2 * kGJ * kLdlLd);
+    const int j = blockIdx.x / SW, s = blockIdx.x % SW, c0 = kGJ * j + kVuCols * s;
+    if (j >= nb || c0 >= m) return;  // the whole CTA leaves together
+    const int tr = threadIdx.x / kVuCols, tc = threadIdx.x % kVuCols;  // rows tr + 16 u, column tc
+    const int R = bw + 1;
+    for (int v = threadIdx.x; v < kGJ * kVuCols; v += blockDim.x) {  // V_jj = I
+        const int r = v / kVuCols, c = v % kVuCols;
+        ring[j % R][r][c] = r == kVuCols * s + c ? 1.0 : 0.0;
+    }
+    // tile (i, l): L_il for l < i, S_i for l == i
+    auto tile = [&](int i, int l) -> const double * {
+        return l < i ? Lb + ((long)l * bw + (i - l - 1)) * kGJ * kGJ : Sb + (long)i * kGJ * kGJ;
+    };
+    double x[kPer];
+    auto fetch = [&](const double *G) {
+#pragma unroll
+        for (int t = 0; t < kPer; ++t) x[t] = G[threadIdx.x + 256 * t];
+    };
+    int i = j, l = j, buf = 0;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    fetch(tile(i, l));
+    for (;;) {
+#pragma unroll
+        for (int t = 0; t < kPer; ++t) {
+            const int v = threadIdx.x + 256 * t;
+            vu_sm[buf * kGJ * kLdlLd + (v / kGJ) * kLdlLd + v % kGJ] = x[t];
+        }
+        __syncthreads();
+        int ni = i, nl = l + 1;
+        if (l == i) {
+            ni = i + 1;
+            nl = max(j, ni - bw);
+        }
+        const bool more = ni < nb;
+        if (more) fetch(tile(ni, nl));  // in flight during this tile's product
+        const double(*X)[kLdlLd] = reinterpret_cast<const double(*)[kLdlLd]>(vu_sm + buf * kGJ * kLdlLd);
+        if (l < i) {  // acc += L_il V_lj
+            const double(*Vl)[kVuCols + 1] = ring[l % R];
+#pragma unroll 8
+            for (int q = 0; q < kGJ; ++q) {
+                const double y = Vl[q][tc];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) acc[u] = fma(X[tr + 16 * u][q], y, acc[u]);
+            }
+        } else {
+            if (i > j) {  // V_ij = -acc; the slot's last reader (V_{i-bw-1,j}) is done
+#pragma unroll
+                for (int u = 0; u < 4; ++u) ring[i % R][tr + 16 * u][tc] = -acc[u];
+                __syncthreads();
+            }
+            const double(*Vi)[kVuCols + 1] = ring[i % R];
+            double u4[4] = {0.0, 0.0, 0.0, 0.0};  // U_ij = S_i V_ij
+#pragma unroll 8
+            for (int q = 0; q < kGJ; ++q) {
+                const double y = Vi[q][tc];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) u4[u] = fma(X[tr + 16 * u][q], y, u4[u]);
+            }
+            const int col = c0 + tc;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int row = kGJ * i + tr + 16 * u;
+                if (row < m && col < m) F[(long)row * ldf + col] = (float)u4[u];
+                acc[u] = 0.0;
+            }
+            if (i > j)  // V_ij^T into the block-upper triangle, 64 consecutive floats per column of V
+                for (int v = threadIdx.x; v < kGJ * kVuCols; v += blockDim.x) {
+                    const int r = v % kGJ, cc = v / kGJ, row = kGJ * i + r;
+                    if (row < m && c0 + cc < m) F[(long)(c0 + cc) * ldf + row] = (float)Vi[r][cc];
+                }
+        }
+        if (!more) break;
+        i = ni;
+        l = nl;
+        buf ^= 1;
+    }
+}
+
+// Dot product of a row of F (16-byte aligned, ldf a multiple of 4) with v over
+// columns [lo, hi), lo a multiple of 4: float4 loads, two in flight per lane,
+// per-lane partial sums combined in a fixed order.
+__device__ __forceinline__ float coarse_row_dot(const float *__restrict__ row, const float *__restrict__ v, int lo,
+                                                int hi, int lane) {
+    const float4 *r4 = reinterpret_cast<const float4 *>(row);
+    const float4 *v4 = reinterpret_cast<const float4 *>(v);
+    const int n4 = hi / 4;
+    float s0 = 0.0f, s1 = 0.0f;
+    int j = lo / 4 + lane;
+    for (; j + 32 < n4; j += 64) {
+        const float4 a = r4[j], b = r4[j + 32], x = v4[j], y = v4[j + 32];
+        s0 = fmaf(a.x, x.x, fmaf(a.y, x.y, fmaf(a.z, x.z, fmaf(a.w, x.w, s0))));
+        s1 = fmaf(b.x, y.x, fmaf(b.y, y.y, fmaf(b.z, y.z, fmaf(b.w, y.w, s1))));
+    }
+    if (j < n4) {
+        const float4 a = r4[j], x = v4[j];
+        s0 = fmaf(a.x, x.x, fmaf(a.y, x.y, fmaf(a.z, x.z, fmaf(a.w, x.w, s0))));
+    }
+    for (int t = 4 * n4 + lane; t < hi; t += 32) s1 = fmaf(row[t], v[t], s1);  // tail: hi = m, m % 4 != 0
+    return warp_sum(s0 + s1);
+}
+
+// z = U c: row r over the columns of its own and earlier blocks.
+__global__ void __launch_bounds__(kBlock) k_coarse_apply_lower(int m, int ldf, const float *__restrict__ F,
+                                                               const float *__restrict__ cvec,
+                                                               float *__restrict__ z) {
+    const int lane = threadIdx.x & 31;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32; i < m; i += gridDim.x * blockDim.x / 32) {
+        const float s = coarse_row_dot(F + (long)i * ldf, cvec, 0, min(m, kGJ * (i / kGJ + 1)), lane);
+        if (lane == 0) z[i] = s;
+    }
+}
+
+// e = V^T z: z_r plus row r over the columns of later blocks.
+__global__ void __launch_bounds__(kBlock) k_coarse_apply_upper(int m, int ldf, const float *__restrict__ F,
+                                                               const float *__restrict__ z,
+                                                               float *__restrict__ evec) {
+    const int lane = threadIdx.x & 31;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32; i < m; i += gridDim.x * blockDim.x / 32) {
+        const int lo = min(m, kGJ * (i / kGJ + 1));
+        const float s = lo < m ? coarse_row_dot(F + (long)i * ldf, z, lo, m, lane) : 0.0f;
+        if (lane == 0) evec[i] = z[i] + s;
+    }
+}
+
+// The dense inverse V^T U from the factor (for the batched solver, which
+// applies a dense inverse): entry (r, c) = [blk(r) >= blk(c)] F[r][c] +
+// sum over q >= max(64 (blk(r) + 1), 64 blk(c)) of F[r][q] F[q][c].
+__global__ void __launch_bounds__(kBlock) k_dense_from_factor(int m, int ldf, const float *__restrict__ F,
+                                                              float *__restrict__ Einv) {
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < (long)m * m; e += (long)gridDim.x * blockDim.x) {
+        const int r = (int)(e / m), c = (int)(e % m), br = r / kGJ, bc = c / kGJ;
+        float s = br >= bc ? F[(long)r * ldf + c] : 0.0f;
+        for (int q = kGJ * max(br + 1, bc); q < m; ++q) s = fmaf(F[(long)r * ldf + q], F[(long)q * ldf + c], s);
+        Einv[e] = s;
+    }
+}
+
 // hb: half-bandwidth of A (A_ik = 0 for |i - k| > hb).  Before panel J is
 // processed, rows and columns beyond j0 + bb + hb are still untouched band
 // (their entries in the panel's rows and columns are zero), so every step
@@ -721,6 +1072,44 @@ static void invert_spd(ofea_ctx *c, double *A, int m, int hb) {
     OFEA_CHECK_LAUNCH();
     cudaEventDestroy(cross_done);
     cudaEventDestroy(rest_done);
+}
+
+// The block LDL^T factor of the banded A (block half-bandwidth bw <= kLdlMaxBw)
+// and its FP32 apply array C.F32 (k_ldl_band, k_ldl_vu).
+static void factor_band(ofea_ctx *c, double *A, int m, int bw) {
+    Coarse &C = c->coarse;
+    cudaStream_t s = c->stream;
+    const int nb = (m + kGJ - 1) / kGJ;
+    C.nbw = bw;
+    C.Sb.ensure((size_t)nb * kGJ * kGJ);
+    C.Lb.ensure(std::max<size_t>(1, (size_t)nb * bw * kGJ * kGJ));
+    C.ldf = (m + 3) & ~3;  // rows 16-byte aligned for the apply's float4 loads
+    C.F32.ensure((size_t)m * C.ldf);
+    C.zvec.ensure(std::max(m, 1));
+    C.diag0.ensure(m);
+    k_diag_of<<<grid_for(c, m, kBlock), kBlock, 0, s>>>(m, A, C.diag0.p);
+    OFEA_CHECK_LAUNCH();
+    const int band_smem = (int)(sizeof(double) * 2 * kGJ * kLdlLd);
+    OFEA_CUDA(cudaFuncSetAttribute(k_ldl_band, cudaFuncAttributeMaxDynamicSharedMemorySize, band_smem));
+    k_ldl_band<<<kLdlCluster, kGjT * kGjT, band_smem, s>>>(m, nb, bw, A, C.Sb.p, C.Lb.p, C.diag0.p);
+    OFEA_CHECK_LAUNCH();
+    setup_mark(c, "coarse_ldl_band");
+    const int vu_smem = (int)(sizeof(double) * (2 * kGJ * kLdlLd + (size_t)(bw + 1) * kGJ * (kVuCols + 1)));
+    OFEA_CUDA(cudaFuncSetAttribute(k_ldl_vu, cudaFuncAttributeMaxDynamicSharedMemorySize, vu_smem));
+    k_ldl_vu<<<nb * (kGJ / kVuCols), 256, vu_smem, s>>>(m, C.ldf, nb, bw, C.Sb.p, C.Lb.p, C.F32.p);
+    OFEA_CHECK_LAUNCH();
+    setup_mark(c, "coarse_ldl_vu");
+}
+
+void coarse_dense_inverse(ofea_ctx *c) {
+    Coarse &C = c->coarse;
+    if (!C.K_ok) fail(OFEA_ERR_STATE, "coarse level missing");
+    if (C.dense_ok) return;
+    const int m = C.m;
+    C.Einv32.ensure((size_t)m * m);
+    k_dense_from_factor<<<grid_for(c, (long)m * m, kBlock), kBlock, 0, c->stream>>>(m, C.ldf, C.F32.p, C.Einv32.p);
+    OFEA_CHECK_LAUNCH();
+    C.dense_ok = true;
 }
 
 // ----------------------------------------------------- lambda_max(D^-1 K) --
@@ -836,7 +1225,6 @@ double *coarse_begin_E(ofea_ctx *c) {
     Coarse &C = c->coarse;
     const int m = C.m;
     C.E.ensure((size_t)m * m);
-    C.Einv32.ensure((size_t)m * m);
     C.cvec.ensure(std::max(m, 1));
     C.evec.ensure(std::max(m, 1));
     OFEA_CUDA(cudaMemsetAsync(C.E.p, 0, sizeof(double) * m * m, c->stream));
@@ -859,11 +1247,23 @@ void coarse_finish(ofea_ctx *c) {
     OFEA_CUDA(cudaStreamWaitEvent(c->aux_stream, fork, 0));
     lambda_max_launch(c, kPowerSteps, c->aux_stream);
     OFEA_CUDA(cudaEventRecord(join, c->aux_stream));
-    invert_spd(c, C.E.p, m, 6 * C.band + 5);
-    k_round_f32<<<grid_for(c, (long)m * m, kBlock), kBlock, 0, s>>>((long)m * m, C.E.p, C.Einv32.p);
-    OFEA_CHECK_LAUNCH();
+    const int hb = 6 * C.band + 5, nb = (m + kGJ - 1) / kGJ;
+    const int bw = std::min(nb - 1, (hb + kGJ - 1) / kGJ);
+    C.factored = c->coarse_solver == 0 && bw <= kLdlMaxBw;
+    C.dense_ok = !C.factored;
+    if (C.factored) {
+        factor_band(c, C.E.p, m, bw);
+    } else {
+        invert_spd(c, C.E.p, m, hb);
+        setup_mark(c, "coarse_inverse");
+        C.Einv32.ensure((size_t)m * m);
+        k_round_f32<<<grid_for(c, (long)m * m, kBlock), kBlock, 0, s>>>((long)m * m, C.E.p, C.Einv32.p);
+        OFEA_CHECK_LAUNCH();
+        setup_mark(c, "coarse_round_f32");
+    }
     OFEA_CUDA(cudaStreamWaitEvent(s, join, 0));
     C.lmax = lambda_max_read(c, kPowerSteps);
+    setup_mark(c, "lambda_max_join");
     cudaEventDestroy(fork);
     cudaEventDestroy(join);
     C.K_ok = true;
@@ -878,13 +1278,16 @@ void setup_coarse(ofea_ctx *c, int target_nodes) {
     coarse_begin_E(c);
     OFEA_CUDA(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), s));
     const int nchunk = 1;
+    setup_mark(c, "geometry");
     coarse_E_partials(c, C, nchunk);
+    setup_mark(c, "galerkin_level1");
     k_coarse_E_sum<<<grid_for(c, (long)C.na * 27 * 36, kBlock), kBlock, 0, s>>>(
         C.na, nchunk, C.agg_cell.p, C.cell_agg.p, C.nc[0], C.nc[1], C.nc[2], m, C.part.p, C.E.p);
     OFEA_CHECK_LAUNCH();
     OFEA_CUDA(cudaMemcpyAsync(c->herr.p, c->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     OFEA_CUDA(cudaStreamSynchronize(s));
     if (c->herr.p[0]) fail(OFEA_ERR_CAPACITY, "coarse cells smaller than the element couplings");
+    setup_mark(c, "coarse_E_sum");
     coarse_finish(c);
 }
 
@@ -981,7 +1384,13 @@ void prolong_level(ofea_ctx *c, const Coarse &C, const float *g, float *x) {
 
 void coarse_gemv(ofea_ctx *c, const float *cvec, float *evec) {
     Coarse &C = c->coarse;
-    k_coarse_gemv<<<grid_for(c, (long)C.m * 32, kBlock), kBlock, 0, c->stream>>>(C.m, C.Einv32.p, cvec, evec);
+    const int g = grid_for(c, (long)C.m * 32, kBlock);
+    if (C.factored) {
+        k_coarse_apply_lower<<<g, kBlock, 0, c->stream>>>(C.m, C.ldf, C.F32.p, cvec, C.zvec.p);
+        k_coarse_apply_upper<<<g, kBlock, 0, c->stream>>>(C.m, C.ldf, C.F32.p, C.zvec.p, evec);
+    } else {
+        k_coarse_gemv<<<g, kBlock, 0, c->stream>>>(C.m, C.Einv32.p, cvec, evec);
+    }
     OFEA_CHECK_LAUNCH();
 }
 

@@ -19,6 +19,9 @@ float smoother_weight(const ofea_ctx *c);
 // x += Z E^-1 Z^T t  (FP32 vectors of n entries)
 // evec = E^-1 cvec (FP32 GEMV with the coarse level's inverse)
 void coarse_gemv(ofea_ctx *c, const float *cvec, float *evec);
+// Einv32 = the dense FP32 inverse of E (formed from the factor when the
+// coarse solve is factored); for the batched solver, which applies it densely.
+void coarse_dense_inverse(ofea_ctx *c);
 void coarse_correct(ofea_ctx *c, const float *t, float *x);
 // t = b - K32 x
 void vc_resid(ofea_ctx *c, const float *b, const float *x, float *t);

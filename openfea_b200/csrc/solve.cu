@@ -375,6 +375,19 @@ __global__ void k_set_itB(Flags *fl, int v) { fl->itB = v; }
 
 // ------------------------------------------------------------------- host --
 
+void setup_marks_clear(ofea_ctx *c) {
+    for (auto &m : c->setup_marks) cudaEventDestroy(m.second);
+    c->setup_marks.clear();
+}
+
+void setup_mark(ofea_ctx *c, const char *phase) {
+    if (!c->setup_trace) return;
+    cudaEvent_t e = nullptr;
+    OFEA_CUDA(cudaEventCreate(&e));
+    c->setup_marks.emplace_back(phase, e);
+    OFEA_CUDA(cudaEventRecord(e, c->stream));
+}
+
 namespace {
 
 struct Workspace {
@@ -504,10 +517,13 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
         const bool had = c->coarse.K_ok;
         cudaEvent_t es;
         OFEA_CUDA(cudaEventCreate(&es));
+        setup_marks_clear(c);
+        setup_mark(c, "start");
         if (learned) {
             if (!c->learned.have_weights) fail(OFEA_ERR_STATE, "train or load the learned stage first");
             setup_learned_levels(c);
             learned_prepare_inference(c);
+            setup_mark(c, "network");
         } else {
             setup_coarse(c, c->coarse_nodes);
         }
