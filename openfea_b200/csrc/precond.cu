@@ -492,10 +492,12 @@ constexpr int kGjT = 16;  // threads per row / column of the thread grid
 
 // The diagonal-block step of both coarse inversions: A_JJ (rows and columns
 // j0..j0+bb of the m x m row-major A) -> its inverse S (kGJ x kGJ row-major,
-// zero beyond bb), by the CTA's kGjT x kGjT threads.  Pivot p: the holders of
-// row p and column p publish them to shared memory and zero them in their
-// registers, the holder of a_pp publishes d = 1 / a_pp (0 for a vanishing
-// pivot), one barrier, then every entry takes the same update
+// zero beyond bb), by the CTA's kGjT x kGjT threads; thread (ti, tj) holds
+// the 4 x 4 block of rows 4 ti .. 4 ti + 3 and columns 4 tj .. 4 tj + 3.
+// Pivot p = 4 pb + pp (pp unrolled, so every register index is fixed): the
+// holders of row p and column p publish them to shared memory and zero them
+// in their registers, the holder of a_pp publishes d = 1 / a_pp (0 for a
+// vanishing pivot), one barrier, then every entry takes the same update
 // a_rc <- a_rc - cr_r rc_c with cr_r = a_rp d (r != p), cr_p = -d,
 // rc_c = a_pc (c != p), rc_p = 1, which gives a_rc - a_rp a_pc d off row and
 // column p, a_pc d on row p, -a_rp d on column p and d at (p, p).
@@ -509,52 +511,50 @@ __device__ __forceinline__ void gj_block_inverse(int m, int j0, int bb, const do
     for (int u = 0; u < 4; ++u)
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            const int r = ti + kGjT * u, c = tj + kGjT * v;
+            const int r = 4 * ti + u, c = 4 * tj + v;
             a[u][v] = (r < bb && c < bb) ? __ldcg(A + (long)(j0 + r) * m + j0 + c) : 0.0;
         }
     if (tid < kGJ) sthr[tid] = tid < bb ? 1e-12 * __ldcg(diag0 + j0 + tid) : 0.0;
     __syncthreads();
+    const int npb = (bb + 3) / 4;  // pivots beyond bb (zero rows) only drop their direction
 #pragma unroll 1
-    for (int p = 0; p < bb; ++p) {
-        const int buf = p & 1, pq = p / kGjT, pr = p % kGjT;
+    for (int pb = 0; pb < npb; ++pb) {
 #pragma unroll
-        for (int w = 0; w < 4; ++w) {
-            if (w != pq || (ti != pr && tj != pr)) continue;
-            double rowv[4], colv[4];
+        for (int pp = 0; pp < 4; ++pp) {
+            const int p = 4 * pb + pp, buf = pp & 1;
+            const bool rowp = ti == pb, colp = tj == pb;
+            if (rowp && colp) sd[buf] = a[pp][pp] > sthr[p] ? 1.0 / a[pp][pp] : 0.0;
+            if (colp)
 #pragma unroll
-            for (int v = 0; v < 4; ++v) rowv[v] = a[w][v];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) colv[u] = a[u][w];
-            if (ti == pr && tj == pr) sd[buf] = a[w][w] > sthr[p] ? 1.0 / a[w][w] : 0.0;
-            if (ti == pr)
+                for (int u = 0; u < 4; ++u) scol[buf][4 * ti + u] = a[u][pp];
+            if (rowp)
 #pragma unroll
                 for (int v = 0; v < 4; ++v) {
-                    srow[buf][tj + kGjT * v] = rowv[v];
-                    a[w][v] = 0.0;
+                    srow[buf][kGjT * v + tj] = a[pp][v];  // column 4 tj + v, stored lane-contiguous
+                    a[pp][v] = 0.0;
                 }
-            if (tj == pr)
+            if (colp)
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    scol[buf][ti + kGjT * u] = colv[u];
-                    a[u][w] = 0.0;
-                }
+                for (int u = 0; u < 4; ++u) a[u][pp] = 0.0;
+            __syncthreads();
+            const double d = sd[buf];
+            double cr[4], rc[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) cr[u] = scol[buf][4 * ti + u] * d;
+            if (rowp) cr[pp] = -d;
+#pragma unroll
+            for (int v = 0; v < 4; ++v) rc[v] = srow[buf][kGjT * v + tj];
+            if (colp) rc[pp] = 1.0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) a[u][v] = fma(-cr[u], rc[v], a[u][v]);
         }
-        __syncthreads();
-        const double d = sd[buf];
-        double cr[4], rc[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) cr[u] = ti + kGjT * u == p ? -d : scol[buf][ti + kGjT * u] * d;
-#pragma unroll
-        for (int v = 0; v < 4; ++v) rc[v] = tj + kGjT * v == p ? 1.0 : srow[buf][tj + kGjT * v];
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-            for (int v = 0; v < 4; ++v) a[u][v] = fma(-cr[u], rc[v], a[u][v]);
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int v = 0; v < 4; ++v) S[(ti + kGjT * u) * kGJ + tj + kGjT * v] = a[u][v];
+        for (int v = 0; v < 4; ++v) S[(4 * ti + u) * kGJ + 4 * tj + v] = a[u][v];
 }
 
 __global__ void __launch_bounds__(kGjT * kGjT) k_gj_diag(int m, int j0, int bb, const double *__restrict__ A,
