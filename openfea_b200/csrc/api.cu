@@ -201,18 +201,18 @@ static void check_nodes(ofea_ctx *c, int nd, const double *xyz, const int *free_
     for (int i = 0; i < nfree; ++i)
         need(seen[i], OFEA_ERR_INVALID_ARG, "free_map must number free nodes 0..nfree-1");
     std::vector<char> finite(kHostChunks, 1);
-    host_for_chunks([&](int k) {
-        for (long i = chunk_begin(3L * nd, k); i < chunk_begin(3L * nd, k + 1); ++i)
-            if (!std::isfinite(xyz[i])) {
-                finite[k] = 0;
-                return;
-            }
+    c->xyz_h.resize(3L * nd);
+    c->fm_h.resize(nd);
+    host_for_chunks([&](int k) {  // checks and the host copies, chunk by chunk
+        const long i0 = chunk_begin(3L * nd, k), i1 = chunk_begin(3L * nd, k + 1);
+        for (long i = i0; i < i1; ++i)
+            if (!std::isfinite(xyz[i])) finite[k] = 0;
+        std::copy(xyz + i0, xyz + i1, c->xyz_h.data() + i0);
+        std::copy(free_map + chunk_begin(nd, k), free_map + chunk_begin(nd, k + 1), c->fm_h.data() + chunk_begin(nd, k));
     });
     for (int k = 0; k < kHostChunks; ++k) need(finite[k] != 0, OFEA_ERR_INVALID_ARG, "non-finite coordinate");
     c->nfree = nfree;
     c->n = 3 * nfree;
-    c->xyz_h.assign(xyz, xyz + 3L * nd);
-    c->fm_h.assign(free_map, free_map + nd);
 }
 
 int ofea_mesh_upload(ofea_ctx *c, int nd, const double *xyz, int ne, const int *topo,
@@ -236,19 +236,26 @@ int ofea_mesh_upload(ofea_ctx *c, int nd, const double *xyz, int ne, const int *
         c->ne = ne;
         c->E0 = E0;
         c->nu = nu;
-        c->elem_type.assign(etype, etype + ne);
-        c->elem_local.resize(ne);
-        // pass 1 (chunks of elements): checks and per-chunk counts by type; the
-        // error reported is the first one in element order
+        // the nodes first: their host copies are then copied to the device
+        // while the element passes run (page-locked blocks: asynchronous DMA)
+        check_nodes(c, nd, xyz, free_map);
+        cudaStream_t s = c->stream;
+        c->xyz.upload(c->xyz_h.data(), 3L * nd, s);
+        c->free_map.upload(c->fm_h.data(), nd, s);
+        // pass 1 (chunks of elements): checks, per-chunk counts by type and
+        // the host copy of the types; the error reported is the first one in
+        // element order
         struct Scan {
             long n8 = 0, n4 = 0;
             const char *why = nullptr;
         };
         std::vector<Scan> sc(kHostChunks);
+        c->elem_type.resize(ne);
         host_for_chunks([&](int k) {
             Scan &r = sc[k];
             for (long e = chunk_begin(ne, k); e < chunk_begin(ne, k + 1); ++e) {
                 const int t = etype[e];
+                c->elem_type[e] = t;
                 if (t != 0 && t != 1) {
                     r.why = "element type must be 0 (C3D4) or 1 (C3D8)";
                     return;
@@ -266,41 +273,45 @@ int ofea_mesh_upload(ofea_ctx *c, int nd, const double *xyz, int ne, const int *
                             return;
                         }
                 }
+                if (E_elem && !std::isfinite(E_elem[e])) {
+                    r.why = "non-finite Young's modulus";
+                    return;
+                }
                 (t == 1 ? r.n8 : r.n4)++;
             }
         });
         std::vector<long> o8(kHostChunks + 1, 0), o4(kHostChunks + 1, 0);
+        for (int k = 0; k < kHostChunks; ++k)
+            if (sc[k].why) OFEA_CUDA(cudaStreamSynchronize(s));  // the node copies have left the host blocks
         for (int k = 0; k < kHostChunks; ++k) {
             need(sc[k].why == nullptr, OFEA_ERR_INVALID_ARG, sc[k].why);
             o8[k + 1] = o8[k] + sc[k].n8;
             o4[k + 1] = o4[k] + sc[k].n4;
         }
-        // pass 2: 0-based device connectivity per type, element -> position, host copy
+        // pass 2: 0-based device connectivity and modulus per type, element ->
+        // position, host copy of the connectivity
         HVec<int> t8(8L * o8[kHostChunks]), t4(4L * o4[kHostChunks]);
+        HVec<double> E8(o8[kHostChunks]), E4(o4[kHostChunks]);
+        c->elem_local.resize(ne);
         c->topo_h.resize(8L * ne);
         host_for_chunks([&](int k) {
             long p8 = o8[k], p4 = o4[k];
             for (long e = chunk_begin(ne, k); e < chunk_begin(ne, k + 1); ++e) {
                 const bool hex = etype[e] == 1;
-                int *dst = hex ? &t8[8 * p8] : &t4[4 * p4];
-                c->elem_local[e] = (int)(hex ? p8++ : p4++);
+                const long p = hex ? p8++ : p4++;
+                int *dst = hex ? &t8[8 * p] : &t4[4 * p];
+                (hex ? E8 : E4)[p] = E_elem ? E_elem[e] : E0;
+                c->elem_local[e] = (int)p;
                 for (int a = 0; a < (hex ? 8 : 4); ++a) dst[a] = topo[8L * e + a] - 1;
                 for (int a = 0; a < 8; ++a) c->topo_h[8L * e + a] = topo[8L * e + a] > 0 ? topo[8L * e + a] - 1 : 0;
             }
         });
         c->ne8 = (int)o8[kHostChunks];
         c->ne4 = (int)o4[kHostChunks];
-        check_nodes(c, nd, xyz, free_map);
-        HVec<double> E8, E4;
-        split_modulus(c, E_elem, E0, E8, E4);
-        cudaStream_t s = c->stream;
-        // from the library's host copies (page-locked blocks: direct DMA)
-        c->xyz.upload(c->xyz_h.data(), 3L * nd, s);
         c->topo8.upload(t8.data(), t8.size(), s);
         c->topo4.upload(t4.data(), t4.size(), s);
         c->E8.upload(E8.data(), E8.size(), s);
         c->E4.upload(E4.data(), E4.size(), s);
-        c->free_map.upload(c->fm_h.data(), nd, s);
         OFEA_CUDA(cudaStreamSynchronize(s));
         c->mesh_ok = true;
     });
@@ -661,15 +672,29 @@ int ofea_solve(ofea_ctx *c, const double *f, double *u, int nrhs, const ofea_sol
         }
         c->w.f.ensure(std::max(n, 1));
         c->w.u.ensure(std::max(n, 1));
+        // the caller's vectors pass through a page-locked block of the host
+        // cache (copied on the host pool's threads, then one DMA each way)
+        HVec<double> stage(std::max(n, 1));
         for (int k = 0; k < nrhs; ++k) {
             ofea_solve_stats st{};
-            OFEA_CUDA(cudaMemcpyAsync(c->w.f.p, f + (long)k * n, sizeof(double) * n,
-                                      cudaMemcpyHostToDevice, c->stream));
+            host_for_chunks([&](int q) {
+                std::copy(f + (long)k * n + chunk_begin(n, q), f + (long)k * n + chunk_begin(n, q + 1),
+                          stage.data() + chunk_begin(n, q));
+            });
+            OFEA_CUDA(cudaMemcpyAsync(c->w.f.p, stage.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
             OFEA_CUDA(cudaMemsetAsync(c->w.u.p, 0, sizeof(double) * n, c->stream));
-            solve_device(c, c->w.f.p, c->w.u.p, o, st);
-            OFEA_CUDA(cudaMemcpyAsync(u + (long)k * n, c->w.u.p, sizeof(double) * n,
-                                      cudaMemcpyDeviceToHost, c->stream));
+            try {
+                solve_device(c, c->w.f.p, c->w.u.p, o, st);
+            } catch (...) {
+                cudaStreamSynchronize(c->stream);  // no copy reads the staging block after it is released
+                throw;
+            }
+            OFEA_CUDA(cudaMemcpyAsync(stage.data(), c->w.u.p, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
             OFEA_CUDA(cudaStreamSynchronize(c->stream));
+            host_for_chunks([&](int q) {
+                std::copy(stage.data() + chunk_begin(n, q), stage.data() + chunk_begin(n, q + 1),
+                          u + (long)k * n + chunk_begin(n, q));
+            });
             if (stats) stats[k] = st;
             if (st.status != OFEA_OK && worst == OFEA_OK) {
                 worst = st.status;

@@ -20,6 +20,7 @@ inline long chunk_begin(long n, int k) { return n * k / kHostChunks; }
 }  // namespace ofea
 
 #include <cstddef>
+#include <new>
 #include <vector>
 
 namespace ofea {
@@ -32,6 +33,8 @@ void *host_cache_take(std::size_t bytes);
 void host_cache_give(void *p, std::size_t bytes);
 void host_cache_trim();
 
+// HVec<T>(n) and resize(n) default-initialize the new elements (no zero
+// fill of tens of MB on the caller's thread): every user writes them all.
 template <class T>
 struct CachedAlloc {
     using value_type = T;
@@ -40,6 +43,14 @@ struct CachedAlloc {
     CachedAlloc(const CachedAlloc<U> &) {}
     T *allocate(std::size_t n) { return static_cast<T *>(host_cache_take(n * sizeof(T))); }
     void deallocate(T *p, std::size_t n) { host_cache_give(p, n * sizeof(T)); }
+    template <class U>
+    void construct(U *p) {
+        ::new (static_cast<void *>(p)) U;
+    }
+    template <class U, class... Args>
+    void construct(U *p, Args &&...args) {
+        ::new (static_cast<void *>(p)) U(static_cast<Args &&>(args)...);
+    }
     template <class U>
     bool operator==(const CachedAlloc<U> &) const { return true; }
     template <class U>
