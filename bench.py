@@ -248,7 +248,8 @@ def run_learned_simp(ob, mg, local, shape, rtol=1e-8, steps=2):
     t0 = time.perf_counter()
     train = ctr.learned_train(None, sample_iters=2000, sample_every=1, steps=400, batch=16, lr=1e-3, seed=1234)
     train["wall_s"] = time.perf_counter() - t0
-    cte.set_learned_weights(ctr.learned_weights())
+    weights = ctr.learned_weights()
+    cte.set_learned_weights(weights)
 
     errs = {}
     shape_s = f"{nx}x{ny}x{nz}"
@@ -280,7 +281,7 @@ def run_learned_simp(ob, mg, local, shape, rtol=1e-8, steps=2):
         "gain_learned_vs_mixed": mixed["seconds"] / learned["seconds"],
         "error_vs_oracle": errs,
         "training": train,
-    }
+    }, weights
 
 
 def run_ca(ob, mg, local, shape, n_basis=4, rtol=1e-6):
@@ -703,9 +704,20 @@ def run_ours(args):
     batched = None
     if not args.no_batched:
         batched = run_batched(ob, mg, local, hbm, dist=dist)
-    learned_simp = None
+    learned_simp = transfer = None
     if not args.no_simp:
-        learned_simp = run_learned_simp(ob, mg, local, (nx, ny, nz), rtol=args.rtol)
+        learned_simp, simp_weights = run_learned_simp(ob, mg, local, (nx, ny, nz), rtol=args.rtol)
+        # the headline workload with a stage trained on another matrix (the
+        # SIMP density sample's), not on the benchmark's own K
+        ctx.set_learned_weights(simp_weights)
+        stt = [solve("GPU_LEARNED") for _ in range(3)]
+        bt = min(stt, key=lambda s_: s_["seconds"])
+        assert bt["status"] == 0 and bt["rel_residual"] <= args.rtol, bt
+        transfer = {"weights": "trained on the SIMP density sample (seed 11) of the same mesh, not on this K",
+                    "seconds": bt["seconds"], "iterations": bt["iterations"],
+                    "rejected_learned": bt["rejected_learned"], "gain_vs_mixed": mixed_s / bt["seconds"],
+                    "error_vs_oracle": oracle_error(u_dev, "cantilever", args.shape)}
+        ctx.set_learned_weights(weights)
     ca = None
     if not args.no_ca:
         ca = run_ca(ob, mg, local, (nx, ny, nz))
@@ -740,6 +752,7 @@ def run_ours(args):
                    "mixed_without_learned_s": mixed_s, "mixed_without_learned_iterations": stm[-1]["iterations"],
                    "learned_gain_vs_mixed": mixed_s / sec,
                    "learned_training": train,
+                   "learned_with_transferred_weights": transfer,
                    "precond_setup_s": stats[-1]["setup_seconds"],
                    "setup_phases_ms": setup_phases,
                    "mesh_pattern_assembly_s": setup_s},
