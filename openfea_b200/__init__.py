@@ -287,7 +287,7 @@ def check_barrier_timeout(ctx, limit_ms=20):
     return r.value
 
 
-def solve_opts(method="GPU_PCG", rtol=1e-8, max_iter=100000, time_budget_s=0.0, check_every=16,
+def solve_opts(method="GPU_PCG", rtol=1e-8, max_iter=100000, time_budget_s=0.0, check_every=0,
                ru_delta=0.1, use_graph=True) -> SolveOpts:
     o = SolveOpts()
     lib().ofea_solve_opts_default(ctypes.byref(o))

@@ -93,7 +93,7 @@ void ofea_solve_opts_default(ofea_solve_opts *o) {
     o->rtol = 1e-8;
     o->max_iter = 100000;
     o->time_budget_s = 0;
-    o->check_every = 16;
+    o->check_every = 0;  // by method
     o->ru_delta = 0.1;
     o->use_graph = 1;
 }

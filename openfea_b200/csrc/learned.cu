@@ -294,6 +294,26 @@ __device__ __forceinline__ void child_coeffs(int J, const int *__restrict__ pare
     g[5] = ratio * e[5];
 }
 
+// t[a] += sum_b e[6a + b] v[b] for one 6 x 6 FP32 block e (16-byte aligned:
+// blocks are 144 bytes apart), loaded as nine 16-byte words before the
+// first product; the sums run in the order a, then b = 0..5.
+__device__ __forceinline__ void block6_apply(const float *__restrict__ e, const float (&v)[6], float (&t)[6]) {
+    float w[36];
+    const float4 *e4 = reinterpret_cast<const float4 *>(e);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        const float4 x = __ldg(e4 + q);
+        w[4 * q] = x.x;
+        w[4 * q + 1] = x.y;
+        w[4 * q + 2] = x.z;
+        w[4 * q + 3] = x.w;
+    }
+#pragma unroll
+    for (int a = 0; a < 6; ++a)
+#pragma unroll
+        for (int b = 0; b < 6; ++b) t[a] = fmaf(w[6 * a + b], v[b], t[a]);
+}
+
 // Scaled level-2 residual with the exact level-1 correction taken out:
 //   S_I = D_I^-1/2 (c2 - E2 P e1)_I = c2_I / dsq_I - sum_s Ehat[I,s] (dsq o P e1)_J(s).
 // Warp per aggregate, lane s < 27 handles neighbour slot s.
@@ -310,9 +330,7 @@ __global__ void __launch_bounds__(kBlock) k_lrn_shift(int na, const int *__restr
             float g[6];
             child_coeffs(J, parent, pdel, e1, g);
             for (int l = 0; l < 6; ++l) g[l] *= dsq[6L * J + l];
-            const float *e = Ehat + (27L * I + lane) * 36;
-            for (int k = 0; k < 6; ++k)
-                for (int l = 0; l < 6; ++l) v[k] = fmaf(e[6 * k + l], g[l], v[k]);
+            block6_apply(Ehat + (27L * I + lane) * 36, g, v);
         }
         for (int k = 0; k < 6; ++k) v[k] = warp_sum(v[k]);
         if (lane < 6) {
@@ -437,10 +455,10 @@ __global__ void __launch_bounds__(kBlock) k_poly_next(long R, int na, const int 
         float t[6] = {0, 0, 0, 0, 0, 0};
         const int J = lane < 27 ? nbr[27L * I + lane] : -1;
         if (J >= 0) {
-            const float *e = Ehat + (27L * I + lane) * 36;
-            const float *v = vin + 6 * (base + J);
-            for (int a = 0; a < 6; ++a)
-                for (int b = 0; b < 6; ++b) t[a] = fmaf(e[6 * a + b], v[b], t[a]);
+            const float2 *v2 = reinterpret_cast<const float2 *>(vin + 6 * (base + J));
+            const float2 x0 = v2[0], x1 = v2[1], x2 = v2[2];
+            const float v[6] = {x0.x, x0.y, x1.x, x1.y, x2.x, x2.y};
+            block6_apply(Ehat + (27L * I + lane) * 36, v, t);
         }
         for (int a = 0; a < 6; ++a) t[a] = warp_sum(t[a]);
         if (lane < 6) {
@@ -470,11 +488,9 @@ __global__ void __launch_bounds__(kBlock) k_poly_energy(long R, int na, const in
         float t[6] = {0, 0, 0, 0, 0, 0};
         const int J = lane < 27 ? nbr[27L * I + lane] : -1;
         if (J >= 0) {
-            const float *e = Ehat + (27L * I + lane) * 36;
             float y[6];
             for (int b = 0; b < 6; ++b) y[b] = s[6L * J + b] * wv[6 * (base + J) + b];
-            for (int a = 0; a < 6; ++a)
-                for (int b = 0; b < 6; ++b) t[a] = fmaf(e[6 * a + b], y[b], t[a]);
+            block6_apply(Ehat + (27L * I + lane) * 36, y, t);
         }
         for (int a = 0; a < 6; ++a) t[a] = warp_sum(t[a]);
         if (lane < 6) {

@@ -499,7 +499,11 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
     OFEA_CUDA(cudaEventCreate(&e0));
     OFEA_CUDA(cudaEventCreate(&e1));
     OFEA_CUDA(cudaEventRecord(e0, s));
-    int per_chunk = o.check_every > 0 ? o.check_every : 16;
+    // default poll interval: a preconditioned iteration is long and its solves
+    // short (a poll every 4 iterations wastes fewer iterations after
+    // convergence than it costs in host round trips); plain PCG polls every 16
+    const bool precond = o.method == OFEA_SOLVER_MIXED || o.method == OFEA_SOLVER_LEARNED;
+    int per_chunk = o.check_every > 0 ? o.check_every : (precond ? 4 : 16);
     per_chunk = std::max(1, std::min(per_chunk, o.max_iter));
     long long launches = 0;
     Flags hf{};
