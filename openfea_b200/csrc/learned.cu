@@ -317,11 +317,17 @@ __device__ __forceinline__ void block6_apply(const float *__restrict__ e, const 
 // Scaled level-2 residual with the exact level-1 correction taken out:
 //   S_I = D_I^-1/2 (c2 - E2 P e1)_I = c2_I / dsq_I - sum_s Ehat[I,s] (dsq o P e1)_J(s).
 // Warp per aggregate, lane s < 27 handles neighbour slot s.
+// FIRST: also the stage's first term on S (as k_poly_first with x = S):
+// v1 = B (sc * S) into v1, c_1 v1 into out.
+template <bool FIRST>
 __global__ void __launch_bounds__(kBlock) k_lrn_shift(int na, const int *__restrict__ nbr,
                                                       const float *__restrict__ Ehat, const float *__restrict__ dsq,
                                                       const int *__restrict__ parent, const float *__restrict__ pdel,
                                                       const float *__restrict__ e1, const float *__restrict__ c2,
-                                                      float *__restrict__ S) {
+                                                      float *__restrict__ S, const float *__restrict__ Binv = nullptr,
+                                                      const float *__restrict__ sc = nullptr,
+                                                      const float *__restrict__ coef = nullptr,
+                                                      float *__restrict__ v1 = nullptr, float *__restrict__ out = nullptr) {
     const int lane = threadIdx.x & 31;
     for (int I = (blockIdx.x * blockDim.x + threadIdx.x) / 32; I < na; I += gridDim.x * blockDim.x / 32) {
         float v[6] = {0, 0, 0, 0, 0, 0};
@@ -333,12 +339,27 @@ __global__ void __launch_bounds__(kBlock) k_lrn_shift(int na, const int *__restr
             block6_apply(Ehat + (27L * I + lane) * 36, g, v);
         }
         for (int k = 0; k < 6; ++k) v[k] = warp_sum(v[k]);
+        float Sv = 0.f;
         if (lane < 6) {
             float vk = v[0];
             for (int k = 1; k < 6; ++k)
                 if (lane == k) vk = v[k];
             const float d = dsq[6L * I + lane];
-            S[6L * I + lane] = d > 0.f ? c2[6L * I + lane] / d - vk : 0.f;
+            Sv = d > 0.f ? c2[6L * I + lane] / d - vk : 0.f;
+            S[6L * I + lane] = Sv;
+        }
+        if (FIRST) {
+            const float uu = lane < 6 ? (sc ? sc[6L * I + lane] * Sv : Sv) : 0.f;
+            float u[6];
+#pragma unroll
+            for (int l = 0; l < 6; ++l) u[l] = __shfl_sync(0xffffffffu, uu, l);
+            if (lane < 6) {
+                const float *B = Binv + 36L * I;
+                float w = 0.f;
+                for (int l = 0; l < 6; ++l) w = fmaf(B[6 * lane + l], u[l], w);
+                v1[6L * I + lane] = w;
+                out[6L * I + lane] = coef[0] * w;
+            }
         }
     }
 }
@@ -613,42 +634,30 @@ __global__ void k_poly_out(int na, const float *__restrict__ s, const float *__r
 // level-1 modes into its children's modes (child_coeffs); Z1 = Z2 P, so this
 // is Z1^T t without a second pass over the fine vector.  Thread per (parent,
 // mode), children summed in table order.
-__global__ void k_restrict_parent(int na1, const int *__restrict__ children, const float *__restrict__ pdel,
-                                  const float *__restrict__ c2, float *__restrict__ c1) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 6 * na1; i += gridDim.x * blockDim.x) {
-        const int P = i / 6, k = i % 6;
-        float acc = 0.f;
-        for (int ch = 0; ch < 8; ++ch) {
-            const int J = children[8L * P + ch];
-            if (J < 0) continue;
-            const float *g = c2 + 6L * J;
-            const float dx = pdel[4L * J], dy = pdel[4L * J + 1], dz = pdel[4L * J + 2], ratio = pdel[4L * J + 3];
-            float v;
-            switch (k) {  // row k of (child_coeffs' matrix)^T applied to g
-                case 0: v = g[0]; break;
-                case 1: v = g[1]; break;
-                case 2: v = g[2]; break;
-                case 3: v = -dz * g[1] + dy * g[2] + ratio * g[3]; break;
-                case 4: v = dz * g[0] - dx * g[2] + ratio * g[4]; break;
-                default: v = -dy * g[0] + dx * g[1] + ratio * g[5]; break;
-            }
-            acc += v;
+// Both coarse corrections in level-2 modes, g_J = D^-1/2 (s * wv)_J + (P e1)_J,
+// added to the fine vector in the same pass: x_r += Z2_r g_J(r) (one
+// prolongation serves Z1 e1 + Z2 D^-1/2 y; each row forms its aggregate's g).
+__global__ void k_prolong_learned(int nfree, const int *__restrict__ agg_of, const int *__restrict__ node_of_free,
+                                  const double *__restrict__ xyz, const double *__restrict__ centroid,
+                                  double inv_scale, const float *__restrict__ s, const float *__restrict__ wv,
+                                  const float *__restrict__ dsq, const int *__restrict__ parent,
+                                  const float *__restrict__ pdel, const float *__restrict__ e1,
+                                  float *__restrict__ x) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nfree; r += gridDim.x * blockDim.x) {
+        const int J = agg_of[r], node = node_of_free[r];
+        float e[6];
+        child_coeffs(J, parent, pdel, e1, e);
+#pragma unroll
+        for (int l = 0; l < 6; ++l) {
+            const float d = dsq[6L * J + l];
+            e[l] = (d > 0.f ? s[6L * J + l] * wv[6L * J + l] / d : 0.f) + e[l];
         }
-        c1[i] = acc;
-    }
-}
-
-// Both coarse corrections in level-2 modes: g = D^-1/2 (s * wv) + P e1,
-// written over c2 (one prolongation then adds Z2 g = Z1 e1 + Z2 D^-1/2 y).
-__global__ void k_poly_out_e1(int na, const float *__restrict__ s, const float *__restrict__ wv,
-                              const float *__restrict__ dsq, const int *__restrict__ parent,
-                              const float *__restrict__ pdel, const float *__restrict__ e1, float *__restrict__ g) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 6 * na; i += gridDim.x * blockDim.x) {
-        const int J = i / 6, l = i % 6;
-        float pe[6];
-        child_coeffs(J, parent, pdel, e1, pe);
-        const float d = dsq[i];
-        g[i] = (d > 0.f ? s[i] * wv[i] / d : 0.f) + pe[l];
+        const float dx = (float)((xyz[3L * node] - centroid[3L * J]) * inv_scale);
+        const float dy = (float)((xyz[3L * node + 1] - centroid[3L * J + 1]) * inv_scale);
+        const float dz = (float)((xyz[3L * node + 2] - centroid[3L * J + 2]) * inv_scale);
+        x[3L * r] += e[0] + dz * e[4] - dy * e[5];
+        x[3L * r + 1] += e[1] - dz * e[3] + dx * e[5];
+        x[3L * r + 2] += e[2] + dy * e[3] - dx * e[4];
     }
 }
 
@@ -715,6 +724,8 @@ void setup_learned_level(ofea_ctx *c) {
         N.children.upload(ch.data(), ch.size(), c->stream);
         N.pdel.upload(pd.data(), pd.size(), c->stream);
         N.invdeg.ensure(na2);
+        N.rp_cnt.ensure(std::max(C1.na, 1));
+        OFEA_CUDA(cudaMemsetAsync(N.rp_cnt.p, 0, sizeof(unsigned) * std::max(C1.na, 1), c->stream));
         k_invdeg<<<grid_for(c, na2, kBlock), kBlock, 0, c->stream>>>(na2, C2.nbr.p, N.invdeg.p);
         OFEA_CHECK_LAUNCH();
         OFEA_CUDA(cudaStreamSynchronize(c->stream));
@@ -908,18 +919,24 @@ static void gnn_backward(ofea_ctx *c) {
     OFEA_CHECK_LAUNCH();
 }
 
+// The stage's terms after the first (pv[0] and its share of out present).
+static void apply_M_rest(ofea_ctx *c, long Rp, const float *coef, float *out) {
+    Learned &N = c->learned;
+    const Coarse &C2 = c->coarse2;
+    const int na = C2.na;
+    const int Gw = grid_for(c, 32 * Rp, kBlock);
+    for (int k = 1; k < kTerms; ++k)
+        k_poly_next<<<Gw, kBlock, 0, c->stream>>>(Rp, na, C2.nbr.p, N.Ehat.p, N.Binv.p, coef, k, N.pv[k - 1].p,
+                                                  N.pv[k].p, out);
+    OFEA_CHECK_LAUNCH();
+}
+
 // out = M(s * x) over Rp rows; the basis v_k lands in pv[0..2].  s and c may be null.
 static void apply_M(ofea_ctx *c, long Rp, const float *s_, const float *x, const float *coef, float *out) {
     Learned &N = c->learned;
-    const Coarse &C2 = c->coarse2;
-    cudaStream_t s = c->stream;
-    const int na = C2.na;
-    k_poly_first<<<grid_for(c, Rp, kBlock), kBlock, 0, s>>>(Rp, na, N.Binv.p, s_, x, coef, N.pv[0].p, out);
-    const int Gw = grid_for(c, 32 * Rp, kBlock);
-    for (int k = 1; k < kTerms; ++k)
-        k_poly_next<<<Gw, kBlock, 0, s>>>(Rp, na, C2.nbr.p, N.Ehat.p, N.Binv.p, coef, k, N.pv[k - 1].p, N.pv[k].p,
-                                          out);
-    OFEA_CHECK_LAUNCH();
+    const int na = c->coarse2.na;
+    k_poly_first<<<grid_for(c, Rp, kBlock), kBlock, 0, c->stream>>>(Rp, na, N.Binv.p, s_, x, coef, N.pv[0].p, out);
+    apply_M_rest(c, Rp, coef, out);
 }
 
 // Loss and full gradient (N.g) of a batch of Bsz samples already in N.batch_src.
@@ -975,7 +992,7 @@ static void learned_input(ofea_ctx *c, const float *t) {
     restrict_level(c, C1, t, C1.cvec.p);
     coarse_gemv(c, C1.cvec.p, C1.evec.p);
     restrict_level(c, C2, t, C2.cvec.p);
-    k_lrn_shift<<<grid_for(c, 32L * na, kBlock), kBlock, 0, s>>>(na, C2.nbr.p, N.Ehat.p, N.dsq.p, N.parent.p,
+    k_lrn_shift<false><<<grid_for(c, 32L * na, kBlock), kBlock, 0, s>>>(na, C2.nbr.p, N.Ehat.p, N.dsq.p, N.parent.p,
                                                                   N.pdel.p, C1.evec.p, C2.cvec.p, N.shifted.p);
     OFEA_CHECK_LAUNCH();
 }
@@ -1144,17 +1161,20 @@ void learned_coarse_correct(ofea_ctx *c, const float *t, float *x) {
     const Learned::Layout L = Learned::layout();
     cudaStream_t s = c->stream;
     const int na = C2.na;
-    restrict_level(c, C2, t, C2.cvec.p);
-    k_restrict_parent<<<grid_for(c, 6L * C1.na, kBlock), kBlock, 0, s>>>(C1.na, N.children.p, N.pdel.p, C2.cvec.p,
-                                                                       C1.cvec.p);
+    const RestrictFold fold{N.parent.p, N.children.p, N.pdel.p, N.rp_cnt.p, C1.cvec.p};
+    restrict_level(c, C2, t, C2.cvec.p, &fold);  // c2 = Z2^T t and c1 = P^T c2
     coarse_gemv(c, C1.cvec.p, C1.evec.p);
-    k_lrn_shift<<<grid_for(c, 32L * na, kBlock), kBlock, 0, s>>>(na, C2.nbr.p, N.Ehat.p, N.dsq.p, N.parent.p,
-                                                                  N.pdel.p, C1.evec.p, C2.cvec.p, N.shifted.p);
+    // the shifted residual and the stage's first term in one launch, then the
+    // stage's other terms
     float *wv = N.pv[3].p;
-    apply_M(c, na, N.scale.p, N.shifted.p, N.w.p + L.c0, wv);
-    k_poly_out_e1<<<grid_for(c, 6L * na, kBlock), kBlock, 0, s>>>(na, N.scale.p, wv, N.dsq.p, N.parent.p,
-                                                                   N.pdel.p, C1.evec.p, C2.cvec.p);
-    prolong_level(c, C2, C2.cvec.p, x);
+    const float *coef = N.w.p + L.c0;
+    k_lrn_shift<true><<<grid_for(c, 32L * na, kBlock), kBlock, 0, s>>>(
+        na, C2.nbr.p, N.Ehat.p, N.dsq.p, N.parent.p, N.pdel.p, C1.evec.p, C2.cvec.p, N.shifted.p, N.Binv.p,
+        N.scale.p, coef, N.pv[0].p, wv);
+    apply_M_rest(c, na, coef, wv);
+    k_prolong_learned<<<grid_for(c, c->nfree, kBlock), kBlock, 0, s>>>(
+        c->nfree, C2.agg_of.p, c->node_of_free.p, c->xyz.p, C2.centroid.p, C2.inv_scale, N.scale.p, wv, N.dsq.p,
+        N.parent.p, N.pdel.p, C1.evec.p, x);
     OFEA_CHECK_LAUNCH();
 }
 

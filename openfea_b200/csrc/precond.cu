@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstring>
 #include <condition_variable>
 #include <functional>
 #include <future>
@@ -204,6 +205,19 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
             if (J >= 0) band = std::max(band, std::abs(J - a));
         }
     C.band = band;
+    // per free row in aggregate order: its offset from the aggregate's
+    // centroid in cell units (FP64, rounded to FP32) and the row, for the
+    // restriction's coalesced reads
+    HVec<float> off(4L * nf);
+    const double isc = C.inv_scale;
+    host_for_chunks([&](int k) {
+        for (long idx = chunk_begin(nf, k); idx < chunk_begin(nf, k + 1); ++idx) {
+            const int r = nodes[idx], a = agg_of[r], node = nof[r];
+            for (int d = 0; d < 3; ++d) off[4 * idx + d] = (float)((X[3L * node + d] - cen[3L * a + d]) * isc);
+            int rr = r;
+            std::memcpy(&off[4 * idx + 3], &rr, sizeof(int));
+        }
+    });
     if (!c->geo_stream) OFEA_CUDA(cudaStreamCreateWithFlags(&c->geo_stream, cudaStreamNonBlocking));
     cudaStream_t st = c->geo_stream;  // its own stream: may run beside the assembly (geometry_start)
     C.agg_of.upload(agg_of.data(), nf, st);
@@ -213,6 +227,7 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
     C.cell_agg.upload(cell_agg.data(), ncell, st);
     C.centroid.upload(cen.data(), cen.size(), st);
     C.nbr.upload(nbr.data(), nbr.size(), st);
+    C.agg_off.upload(off.data(), off.size(), st);
     OFEA_CUDA(cudaStreamSynchronize(st));
     C.agg_cell_h = std::move(agg_cell3);
     C.cell_agg_h = std::move(cell_agg);
@@ -960,26 +975,32 @@ __global__ void __launch_bounds__(256) k_ldl_vu(int m, int ldf, int nb, int bw, 
 }
 
 // Dot product of a row of F (16-byte aligned, ldf a multiple of 4) with v over
-// columns [lo, hi), lo a multiple of 4: float4 loads, two in flight per lane,
+// columns [lo, hi), lo a multiple of 4: float4 loads, four in flight per lane,
 // per-lane partial sums combined in a fixed order.
 __device__ __forceinline__ float coarse_row_dot(const float *__restrict__ row, const float *__restrict__ v, int lo,
                                                 int hi, int lane) {
     const float4 *r4 = reinterpret_cast<const float4 *>(row);
     const float4 *v4 = reinterpret_cast<const float4 *>(v);
     const int n4 = hi / 4;
-    float s0 = 0.0f, s1 = 0.0f;
+    float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     int j = lo / 4 + lane;
-    for (; j + 32 < n4; j += 64) {
-        const float4 a = r4[j], b = r4[j + 32], x = v4[j], y = v4[j + 32];
-        s0 = fmaf(a.x, x.x, fmaf(a.y, x.y, fmaf(a.z, x.z, fmaf(a.w, x.w, s0))));
-        s1 = fmaf(b.x, y.x, fmaf(b.y, y.y, fmaf(b.z, y.z, fmaf(b.w, y.w, s1))));
+    for (; j + 96 < n4; j += 128) {
+        float4 a[4], x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            a[u] = r4[j + 32 * u];
+            x[u] = v4[j + 32 * u];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            s[u] = fmaf(a[u].x, x[u].x, fmaf(a[u].y, x[u].y, fmaf(a[u].z, x[u].z, fmaf(a[u].w, x[u].w, s[u]))));
     }
-    if (j < n4) {
+    for (; j < n4; j += 32) {
         const float4 a = r4[j], x = v4[j];
-        s0 = fmaf(a.x, x.x, fmaf(a.y, x.y, fmaf(a.z, x.z, fmaf(a.w, x.w, s0))));
+        s[0] = fmaf(a.x, x.x, fmaf(a.y, x.y, fmaf(a.z, x.z, fmaf(a.w, x.w, s[0]))));
     }
-    for (int t = 4 * n4 + lane; t < hi; t += 32) s1 = fmaf(row[t], v[t], s1);  // tail: hi = m, m % 4 != 0
-    return warp_sum(s0 + s1);
+    for (int t = 4 * n4 + lane; t < hi; t += 32) s[0] = fmaf(row[t], v[t], s[0]);  // tail: hi = m, m % 4 != 0
+    return warp_sum((s[0] + s[1]) + (s[2] + s[3]));
 }
 
 // z = U c: row r over the columns of its own and earlier blocks.
@@ -1307,23 +1328,30 @@ __global__ void __launch_bounds__(kBlock, 2048 / kBlock) k_vc_resid(int nfree, c
 }
 
 // c_I = Z_I^T t: one CTA per aggregate, fixed-order reduction.
-__global__ void __launch_bounds__(kBlock) k_restrict(int na, const int *__restrict__ agg_ptr,
-                                                     const int *__restrict__ agg_nodes,
-                                                     const int *__restrict__ node_of_free,
-                                                     const double *__restrict__ xyz,
-                                                     const double *__restrict__ centroid,
-                                                     double inv_scale, const float *__restrict__ t,
-                                                     float *__restrict__ cvec) {
-    __shared__ float sh[kWarpsPerBlock];
+// cvec_I = Z_I^T t (6 values per aggregate): one CTA of NT threads per
+// aggregate, the rows' offsets and indices read in aggregate order (agg_off),
+// sums in a fixed order (per thread, then warps).  With a parent table
+// (`children` non-null: the learned level nested in the coarse level) the
+// last CTA to finish among a parent's children also forms the parent's
+// coarse residual c1_P = P^T (children's c2), in child order, so the
+// restriction serves both levels in one launch; `cnt` (one counter per
+// parent) is zero between launches.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_restrict(int na, const int *__restrict__ agg_ptr,
+                                                 const float4 *__restrict__ off, const float *__restrict__ t,
+                                                 float *__restrict__ cvec, const int *__restrict__ parent,
+                                                 const int *__restrict__ children, const float *__restrict__ pdel,
+                                                 unsigned *__restrict__ cnt, float *__restrict__ c1) {
+    constexpr int NW = NT / 32;
+    __shared__ float sh[6][NW];
+    __shared__ int s_last;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int I = blockIdx.x; I < na; I += gridDim.x) {
         float a[6] = {0, 0, 0, 0, 0, 0};
-        const float cx = (float)centroid[3L * I], cy = (float)centroid[3L * I + 1],
-                    cz = (float)centroid[3L * I + 2];
-        for (int idx = agg_ptr[I] + threadIdx.x; idx < agg_ptr[I + 1]; idx += blockDim.x) {
-            const int r = agg_nodes[idx], node = node_of_free[r];
-            const float dx = ((float)xyz[3L * node] - cx) * (float)inv_scale;
-            const float dy = ((float)xyz[3L * node + 1] - cy) * (float)inv_scale;
-            const float dz = ((float)xyz[3L * node + 2] - cz) * (float)inv_scale;
+        for (int idx = agg_ptr[I] + threadIdx.x; idx < agg_ptr[I + 1]; idx += NT) {
+            const float4 o = off[idx];
+            const int r = __float_as_int(o.w);
+            const float dx = o.x, dy = o.y, dz = o.z;
             const float tx = t[3L * r], ty = t[3L * r + 1], tz = t[3L * r + 2];
             a[0] += tx;
             a[1] += ty;
@@ -1332,9 +1360,54 @@ __global__ void __launch_bounds__(kBlock) k_restrict(int na, const int *__restri
             a[4] += dz * tx - dx * tz;   // (e_y x d) . t
             a[5] += -dy * tx + dx * ty;  // (e_z x d) . t
         }
+#pragma unroll
         for (int k = 0; k < 6; ++k) {
-            float s = block_sum(a[k], sh);
-            if (threadIdx.x == 0) cvec[6 * I + k] = s;
+            a[k] = warp_sum(a[k]);
+            if (lane == 0) sh[k][w] = a[k];
+        }
+        __syncthreads();
+        if (threadIdx.x < 6) {
+            float v = 0.f;
+#pragma unroll
+            for (int q = 0; q < NW; ++q) v += sh[threadIdx.x][q];
+            cvec[6 * I + threadIdx.x] = v;
+        }
+        if (children) {
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();  // this aggregate's values are visible before the count
+                const int P = parent[I];
+                int nch = 0;
+                for (int ch = 0; ch < 8; ++ch) nch += children[8L * P + ch] >= 0;
+                s_last = atomicAdd(cnt + P, 1u) == (unsigned)(nch - 1) ? P : -1;
+            }
+            __syncthreads();
+            const int P = s_last;
+            if (P >= 0 && threadIdx.x < 6) {
+                __threadfence();
+                const int k = threadIdx.x;
+                float acc = 0.f;
+                for (int ch = 0; ch < 8; ++ch) {  // row k of (the child's mode map)^T applied to c2_J
+                    const int J = children[8L * P + ch];
+                    if (J < 0) continue;
+                    const float *g = cvec + 6L * J;
+                    const float dx = pdel[4L * J], dy = pdel[4L * J + 1], dz = pdel[4L * J + 2],
+                                ratio = pdel[4L * J + 3];
+                    const float g0 = __ldcg(g), g1 = __ldcg(g + 1), g2 = __ldcg(g + 2);
+                    float v;
+                    switch (k) {
+                        case 0: v = g0; break;
+                        case 1: v = g1; break;
+                        case 2: v = g2; break;
+                        case 3: v = -dz * g1 + dy * g2 + ratio * __ldcg(g + 3); break;
+                        case 4: v = dz * g0 - dx * g2 + ratio * __ldcg(g + 4); break;
+                        default: v = -dy * g0 + dx * g1 + ratio * __ldcg(g + 5); break;
+                    }
+                    acc += v;
+                }
+                c1[6 * P + k] = acc;
+                if (k == 0) cnt[P] = 0u;
+            }
         }
         __syncthreads();
     }
@@ -1370,9 +1443,18 @@ __global__ void k_prolong(int nfree, const int *__restrict__ agg_of, const int *
     }
 }
 
-void restrict_level(ofea_ctx *c, const Coarse &C, const float *t, float *cvec) {
-    k_restrict<<<std::min(C.na, c->num_sms * 8), kBlock, 0, c->stream>>>(
-        C.na, C.agg_ptr.p, C.agg_nodes.p, c->node_of_free.p, c->xyz.p, C.centroid.p, C.inv_scale, t, cvec);
+void restrict_level(ofea_ctx *c, const Coarse &C, const float *t, float *cvec, const RestrictFold *fold) {
+    const int g = std::min(C.na, c->num_sms * 16);
+    const float4 *off = reinterpret_cast<const float4 *>(C.agg_off.p);
+    const int *par = fold ? fold->parent : nullptr, *ch = fold ? fold->children : nullptr;
+    const float *pd = fold ? fold->pdel : nullptr;
+    unsigned *cnt = fold ? fold->cnt : nullptr;
+    float *c1 = fold ? fold->c1 : nullptr;
+    // 128 threads for aggregates of a few hundred rows (the nested level), 256 beyond
+    if (C.max_agg <= 512)
+        k_restrict<128><<<g, 128, 0, c->stream>>>(C.na, C.agg_ptr.p, off, t, cvec, par, ch, pd, cnt, c1);
+    else
+        k_restrict<256><<<g, 256, 0, c->stream>>>(C.na, C.agg_ptr.p, off, t, cvec, par, ch, pd, cnt, c1);
     OFEA_CHECK_LAUNCH();
 }
 

