@@ -634,30 +634,59 @@ __global__ void k_poly_out(int na, const float *__restrict__ s, const float *__r
 // level-1 modes into its children's modes (child_coeffs); Z1 = Z2 P, so this
 // is Z1^T t without a second pass over the fine vector.  Thread per (parent,
 // mode), children summed in table order.
-// Both coarse corrections in level-2 modes, g_J = D^-1/2 (s * wv)_J + (P e1)_J,
-// added to the fine vector in the same pass: x_r += Z2_r g_J(r) (one
-// prolongation serves Z1 e1 + Z2 D^-1/2 y; each row forms its aggregate's g).
-__global__ void k_prolong_learned(int nfree, const int *__restrict__ agg_of, const int *__restrict__ node_of_free,
-                                  const double *__restrict__ xyz, const double *__restrict__ centroid,
-                                  double inv_scale, const float *__restrict__ s, const float *__restrict__ wv,
-                                  const float *__restrict__ dsq, const int *__restrict__ parent,
-                                  const float *__restrict__ pdel, const float *__restrict__ e1,
-                                  float *__restrict__ x) {
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nfree; r += gridDim.x * blockDim.x) {
-        const int J = agg_of[r], node = node_of_free[r];
-        float e[6];
-        child_coeffs(J, parent, pdel, e1, e);
+// Both coarse corrections in level-2 modes: g = D^-1/2 (s * wv) + P e1,
+// written over c2 (one prolongation then adds Z2 g = Z1 e1 + Z2 D^-1/2 y).
+__global__ void k_poly_out_e1(int na, const float *__restrict__ s, const float *__restrict__ wv,
+                              const float *__restrict__ dsq, const int *__restrict__ parent,
+                              const float *__restrict__ pdel, const float *__restrict__ e1, float *__restrict__ g) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 6 * na; i += gridDim.x * blockDim.x) {
+        const int J = i / 6, l = i % 6;
+        float pe[6];
+        child_coeffs(J, parent, pdel, e1, pe);
+        const float d = dsq[i];
+        g[i] = (d > 0.f ? s[i] * wv[i] / d : 0.f) + pe[l];
+    }
+}
+
+// c1 = P^T c2: the coarse level's residual from its children's (row k of
+// each child's mode map transposed), children summed in table order; every
+// load of the eight children is issued before the first sum.
+__global__ void k_restrict_parent(int na1, const int *__restrict__ children, const float *__restrict__ pdel,
+                                  const float *__restrict__ c2, float *__restrict__ c1) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 6 * na1; i += gridDim.x * blockDim.x) {
+        const int P = i / 6, k = i % 6;
+        int J[8];
+        float g[8][3], dl[8][4];
 #pragma unroll
-        for (int l = 0; l < 6; ++l) {
-            const float d = dsq[6L * J + l];
-            e[l] = (d > 0.f ? s[6L * J + l] * wv[6L * J + l] / d : 0.f) + e[l];
+        for (int ch = 0; ch < 8; ++ch) J[ch] = children[8L * P + ch];
+#pragma unroll
+        for (int ch = 0; ch < 8; ++ch) {
+            const int j = J[ch] < 0 ? 0 : J[ch];
+            // the three values row k combines, and the offsets they are weighted by
+            const int a0 = k < 3 ? k : (k == 3 ? 1 : 0), a1 = k < 3 ? k : (k == 5 ? 1 : 2);
+            g[ch][0] = c2[6L * j + a0];
+            g[ch][1] = c2[6L * j + a1];
+            g[ch][2] = c2[6L * j + k];
+            dl[ch][0] = pdel[4L * j];
+            dl[ch][1] = pdel[4L * j + 1];
+            dl[ch][2] = pdel[4L * j + 2];
+            dl[ch][3] = pdel[4L * j + 3];
         }
-        const float dx = (float)((xyz[3L * node] - centroid[3L * J]) * inv_scale);
-        const float dy = (float)((xyz[3L * node + 1] - centroid[3L * J + 1]) * inv_scale);
-        const float dz = (float)((xyz[3L * node + 2] - centroid[3L * J + 2]) * inv_scale);
-        x[3L * r] += e[0] + dz * e[4] - dy * e[5];
-        x[3L * r + 1] += e[1] - dz * e[3] + dx * e[5];
-        x[3L * r + 2] += e[2] + dy * e[3] - dx * e[4];
+        float acc = 0.f;
+#pragma unroll
+        for (int ch = 0; ch < 8; ++ch) {
+            if (J[ch] < 0) continue;
+            const float dx = dl[ch][0], dy = dl[ch][1], dz = dl[ch][2], ratio = dl[ch][3];
+            float v;
+            switch (k) {
+                case 0: case 1: case 2: v = g[ch][2]; break;
+                case 3: v = -dz * g[ch][0] + dy * g[ch][1] + ratio * g[ch][2]; break;   // g1, g2, g3
+                case 4: v = dz * g[ch][0] - dx * g[ch][1] + ratio * g[ch][2]; break;    // g0, g2, g4
+                default: v = -dy * g[ch][0] + dx * g[ch][1] + ratio * g[ch][2]; break;  // g0, g1, g5
+            }
+            acc += v;
+        }
+        c1[i] = acc;
     }
 }
 
@@ -724,8 +753,6 @@ void setup_learned_level(ofea_ctx *c) {
         N.children.upload(ch.data(), ch.size(), c->stream);
         N.pdel.upload(pd.data(), pd.size(), c->stream);
         N.invdeg.ensure(na2);
-        N.rp_cnt.ensure(std::max(C1.na, 1));
-        OFEA_CUDA(cudaMemsetAsync(N.rp_cnt.p, 0, sizeof(unsigned) * std::max(C1.na, 1), c->stream));
         k_invdeg<<<grid_for(c, na2, kBlock), kBlock, 0, c->stream>>>(na2, C2.nbr.p, N.invdeg.p);
         OFEA_CHECK_LAUNCH();
         OFEA_CUDA(cudaStreamSynchronize(c->stream));
@@ -1161,8 +1188,9 @@ void learned_coarse_correct(ofea_ctx *c, const float *t, float *x) {
     const Learned::Layout L = Learned::layout();
     cudaStream_t s = c->stream;
     const int na = C2.na;
-    const RestrictFold fold{N.parent.p, N.children.p, N.pdel.p, N.rp_cnt.p, C1.cvec.p};
-    restrict_level(c, C2, t, C2.cvec.p, &fold);  // c2 = Z2^T t and c1 = P^T c2
+    restrict_level(c, C2, t, C2.cvec.p);
+    k_restrict_parent<<<grid_for(c, 6L * C1.na, 128), 128, 0, s>>>(C1.na, N.children.p, N.pdel.p, C2.cvec.p,
+                                                                 C1.cvec.p);
     coarse_gemv(c, C1.cvec.p, C1.evec.p);
     // the shifted residual and the stage's first term in one launch, then the
     // stage's other terms
@@ -1172,9 +1200,9 @@ void learned_coarse_correct(ofea_ctx *c, const float *t, float *x) {
         na, C2.nbr.p, N.Ehat.p, N.dsq.p, N.parent.p, N.pdel.p, C1.evec.p, C2.cvec.p, N.shifted.p, N.Binv.p,
         N.scale.p, coef, N.pv[0].p, wv);
     apply_M_rest(c, na, coef, wv);
-    k_prolong_learned<<<grid_for(c, c->nfree, kBlock), kBlock, 0, s>>>(
-        c->nfree, C2.agg_of.p, c->node_of_free.p, c->xyz.p, C2.centroid.p, C2.inv_scale, N.scale.p, wv, N.dsq.p,
-        N.parent.p, N.pdel.p, C1.evec.p, x);
+    k_poly_out_e1<<<grid_for(c, 6L * na, kBlock), kBlock, 0, s>>>(na, N.scale.p, wv, N.dsq.p, N.parent.p,
+                                                                   N.pdel.p, C1.evec.p, C2.cvec.p);
+    prolong_level(c, C2, C2.cvec.p, x);
     OFEA_CHECK_LAUNCH();
 }
 

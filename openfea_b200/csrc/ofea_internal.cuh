@@ -150,6 +150,7 @@ struct Coarse {
     DevBuf<double> centroid, E, S, P, diag0, pp, part;
     DevBuf<float> Einv32, cvec, evec, pw;
     DevBuf<float> agg_off;  // [nfree][4] in aggregate order: offset from the centroid (cell units), row
+    DevBuf<float> row_off;  // [nfree][4] in row order: the same offset, aggregate
     // the coarse solve as a block LDL^T factor (precond.cu): S_k, L_ik and the
     // FP32 array F (U = diag(S) V below, V^T above); dense_ok: Einv32 holds the
     // dense inverse (the Gauss-Jordan path, or formed from F on demand)
@@ -177,7 +178,6 @@ struct Learned {
     DevBuf<double> Eb, sigma, lossp, cpart;      // E2 blocks, sample RMS, loss / coefficient partials
     DevBuf<float> Ehat, dsq, feat, pdel, shifted, invdeg, Binv, X0, scale;
     DevBuf<int> parent, children;
-    DevBuf<unsigned> rp_cnt;  // per coarse aggregate: children restricted so far (zero between V-cycles)
     DevBuf<float> Z0, H[5], A[4], Zl[4], Y, dY, dH, dZ, dA;  // network activations (one row per aggregate)
     DevBuf<float> pv[9];                                      // stage vectors (rows of a batch)
     DevBuf<float> batch_src, r32, data;

@@ -208,14 +208,21 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
     // per free row in aggregate order: its offset from the aggregate's
     // centroid in cell units (FP64, rounded to FP32) and the row, for the
     // restriction's coalesced reads
-    HVec<float> off(4L * nf);
+    // (agg_off), and the same offsets in row order with the aggregate
+    // (row_off) for the prolongation
+    HVec<float> off(4L * nf), roff(4L * nf);
     const double isc = C.inv_scale;
     host_for_chunks([&](int k) {
         for (long idx = chunk_begin(nf, k); idx < chunk_begin(nf, k + 1); ++idx) {
             const int r = nodes[idx], a = agg_of[r], node = nof[r];
-            for (int d = 0; d < 3; ++d) off[4 * idx + d] = (float)((X[3L * node + d] - cen[3L * a + d]) * isc);
+            for (int d = 0; d < 3; ++d) {
+                const float v = (float)((X[3L * node + d] - cen[3L * a + d]) * isc);
+                off[4 * idx + d] = v;
+                roff[4L * r + d] = v;
+            }
             int rr = r;
             std::memcpy(&off[4 * idx + 3], &rr, sizeof(int));
+            std::memcpy(&roff[4L * r + 3], &a, sizeof(int));
         }
     });
     if (!c->geo_stream) OFEA_CUDA(cudaStreamCreateWithFlags(&c->geo_stream, cudaStreamNonBlocking));
@@ -228,6 +235,7 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
     C.centroid.upload(cen.data(), cen.size(), st);
     C.nbr.upload(nbr.data(), nbr.size(), st);
     C.agg_off.upload(off.data(), off.size(), st);
+    C.row_off.upload(roff.data(), roff.size(), st);
     OFEA_CUDA(cudaStreamSynchronize(st));
     C.agg_cell_h = std::move(agg_cell3);
     C.cell_agg_h = std::move(cell_agg);
@@ -1330,21 +1338,13 @@ __global__ void __launch_bounds__(kBlock, 2048 / kBlock) k_vc_resid(int nfree, c
 // c_I = Z_I^T t: one CTA per aggregate, fixed-order reduction.
 // cvec_I = Z_I^T t (6 values per aggregate): one CTA of NT threads per
 // aggregate, the rows' offsets and indices read in aggregate order (agg_off),
-// sums in a fixed order (per thread, then warps).  With a parent table
-// (`children` non-null: the learned level nested in the coarse level) the
-// last CTA to finish among a parent's children also forms the parent's
-// coarse residual c1_P = P^T (children's c2), in child order, so the
-// restriction serves both levels in one launch; `cnt` (one counter per
-// parent) is zero between launches.
+// sums in a fixed order (per thread, then warps).
 template <int NT>
 __global__ void __launch_bounds__(NT) k_restrict(int na, const int *__restrict__ agg_ptr,
                                                  const float4 *__restrict__ off, const float *__restrict__ t,
-                                                 float *__restrict__ cvec, const int *__restrict__ parent,
-                                                 const int *__restrict__ children, const float *__restrict__ pdel,
-                                                 unsigned *__restrict__ cnt, float *__restrict__ c1) {
+                                                 float *__restrict__ cvec) {
     constexpr int NW = NT / 32;
     __shared__ float sh[6][NW];
-    __shared__ int s_last;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int I = blockIdx.x; I < na; I += gridDim.x) {
         float a[6] = {0, 0, 0, 0, 0, 0};
@@ -1372,43 +1372,6 @@ __global__ void __launch_bounds__(NT) k_restrict(int na, const int *__restrict__
             for (int q = 0; q < NW; ++q) v += sh[threadIdx.x][q];
             cvec[6 * I + threadIdx.x] = v;
         }
-        if (children) {
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                __threadfence();  // this aggregate's values are visible before the count
-                const int P = parent[I];
-                int nch = 0;
-                for (int ch = 0; ch < 8; ++ch) nch += children[8L * P + ch] >= 0;
-                s_last = atomicAdd(cnt + P, 1u) == (unsigned)(nch - 1) ? P : -1;
-            }
-            __syncthreads();
-            const int P = s_last;
-            if (P >= 0 && threadIdx.x < 6) {
-                __threadfence();
-                const int k = threadIdx.x;
-                float acc = 0.f;
-                for (int ch = 0; ch < 8; ++ch) {  // row k of (the child's mode map)^T applied to c2_J
-                    const int J = children[8L * P + ch];
-                    if (J < 0) continue;
-                    const float *g = cvec + 6L * J;
-                    const float dx = pdel[4L * J], dy = pdel[4L * J + 1], dz = pdel[4L * J + 2],
-                                ratio = pdel[4L * J + 3];
-                    const float g0 = __ldcg(g), g1 = __ldcg(g + 1), g2 = __ldcg(g + 2);
-                    float v;
-                    switch (k) {
-                        case 0: v = g0; break;
-                        case 1: v = g1; break;
-                        case 2: v = g2; break;
-                        case 3: v = -dz * g1 + dy * g2 + ratio * __ldcg(g + 3); break;
-                        case 4: v = dz * g0 - dx * g2 + ratio * __ldcg(g + 4); break;
-                        default: v = -dy * g0 + dx * g1 + ratio * __ldcg(g + 5); break;
-                    }
-                    acc += v;
-                }
-                c1[6 * P + k] = acc;
-                if (k == 0) cnt[P] = 0u;
-            }
-        }
         __syncthreads();
     }
 }
@@ -1427,15 +1390,14 @@ __global__ void __launch_bounds__(kBlock) k_coarse_gemv(int m, const float *__re
     }
 }
 
-// x_a += Z_a e_I(a), per free node.
-__global__ void k_prolong(int nfree, const int *__restrict__ agg_of, const int *__restrict__ node_of_free,
-                          const double *__restrict__ xyz, const double *__restrict__ centroid,
-                          double inv_scale, const float *__restrict__ evec, float *__restrict__ x) {
+// x_r += Z_r e_I(r), per free row: the row's offset from its aggregate's
+// centroid and the aggregate from row_off (one 16-byte load).
+__global__ void k_prolong(int nfree, const float4 *__restrict__ roff, const float *__restrict__ evec,
+                          float *__restrict__ x) {
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nfree; r += gridDim.x * blockDim.x) {
-        const int I = agg_of[r], node = node_of_free[r];
-        const float dx = (float)((xyz[3L * node] - centroid[3L * I]) * inv_scale);
-        const float dy = (float)((xyz[3L * node + 1] - centroid[3L * I + 1]) * inv_scale);
-        const float dz = (float)((xyz[3L * node + 2] - centroid[3L * I + 2]) * inv_scale);
+        const float4 o = roff[r];
+        const int I = __float_as_int(o.w);
+        const float dx = o.x, dy = o.y, dz = o.z;
         const float *e = evec + 6L * I;
         x[3L * r] += e[0] + dz * e[4] - dy * e[5];
         x[3L * r + 1] += e[1] - dz * e[3] + dx * e[5];
@@ -1443,24 +1405,20 @@ __global__ void k_prolong(int nfree, const int *__restrict__ agg_of, const int *
     }
 }
 
-void restrict_level(ofea_ctx *c, const Coarse &C, const float *t, float *cvec, const RestrictFold *fold) {
+void restrict_level(ofea_ctx *c, const Coarse &C, const float *t, float *cvec) {
     const int g = std::min(C.na, c->num_sms * 16);
     const float4 *off = reinterpret_cast<const float4 *>(C.agg_off.p);
-    const int *par = fold ? fold->parent : nullptr, *ch = fold ? fold->children : nullptr;
-    const float *pd = fold ? fold->pdel : nullptr;
-    unsigned *cnt = fold ? fold->cnt : nullptr;
-    float *c1 = fold ? fold->c1 : nullptr;
     // 128 threads for aggregates of a few hundred rows (the nested level), 256 beyond
     if (C.max_agg <= 512)
-        k_restrict<128><<<g, 128, 0, c->stream>>>(C.na, C.agg_ptr.p, off, t, cvec, par, ch, pd, cnt, c1);
+        k_restrict<128><<<g, 128, 0, c->stream>>>(C.na, C.agg_ptr.p, off, t, cvec);
     else
-        k_restrict<256><<<g, 256, 0, c->stream>>>(C.na, C.agg_ptr.p, off, t, cvec, par, ch, pd, cnt, c1);
+        k_restrict<256><<<g, 256, 0, c->stream>>>(C.na, C.agg_ptr.p, off, t, cvec);
     OFEA_CHECK_LAUNCH();
 }
 
 void prolong_level(ofea_ctx *c, const Coarse &C, const float *g, float *x) {
     k_prolong<<<grid_for(c, c->nfree, kBlock), kBlock, 0, c->stream>>>(
-        c->nfree, C.agg_of.p, c->node_of_free.p, c->xyz.p, C.centroid.p, C.inv_scale, g, x);
+        c->nfree, reinterpret_cast<const float4 *>(C.row_off.p), g, x);
     OFEA_CHECK_LAUNCH();
 }
 

@@ -28,15 +28,7 @@ void vc_resid(ofea_ctx *c, const float *b, const float *x, float *t);
 // Level-generic pieces (also used by the learned level):
 // cvec = Z^T t, x += Z g, and the Galerkin blocks of Z^T K Z into C.part
 // ([aggregate][27 neighbour slots][6 x 6]; nchunk must be 1).
-// With `fold`, the same launch also forms the parent level's c1 = P^T cvec
-// (the learned level nested in the coarse level).
-struct RestrictFold {
-    const int *parent, *children;
-    const float *pdel;
-    unsigned *cnt;  // one per parent, zero between launches
-    float *c1;
-};
-void restrict_level(ofea_ctx *c, const Coarse &C, const float *t, float *cvec, const RestrictFold *fold = nullptr);
+void restrict_level(ofea_ctx *c, const Coarse &C, const float *t, float *cvec);
 void prolong_level(ofea_ctx *c, const Coarse &C, const float *g, float *x);
 void coarse_E_partials(ofea_ctx *c, Coarse &C, int nchunk);
 
