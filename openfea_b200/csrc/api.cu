@@ -314,6 +314,10 @@ int ofea_mesh_upload(ofea_ctx *c, int nd, const double *xyz, int ne, const int *
         c->E4.upload(E4.data(), E4.size(), s);
         OFEA_CUDA(cudaStreamSynchronize(s));
         c->mesh_ok = true;
+        // the coarse levels' geometry depends on the mesh alone: it is built on
+        // a host thread while the caller builds the pattern and assembles K
+        // (every user of it joins the job first)
+        geometry_start(c);
     });
 }
 
@@ -340,9 +344,7 @@ int ofea_assemble_pattern(ofea_ctx *c, int *n, long long *nnz) {
         need(c->mesh_ok, OFEA_ERR_STATE, "no mesh uploaded");
         need(!c->matrix_only, OFEA_ERR_STATE, kNoElements);
         use_device(c);
-        geometry_join(c);
-        build_pattern(c);
-        geometry_start(c);  // coarse geometry on a host thread while the caller assembles
+        build_pattern(c);  // the coarse geometry, started by the mesh upload, may still be in flight
         if (n) *n = c->n;
         if (nnz) *nnz = 9 * c->nnzb;
     });

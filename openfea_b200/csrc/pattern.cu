@@ -334,9 +334,7 @@ void build_pattern(ofea_ctx *c) {
     c->sell_ok = false;
     c->sell_layout_ok = false;
     c->se_state = 0;
-    c->coarse.geom_ok = false;
-    c->coarse.K_ok = false;
-    c->coarse2.geom_ok = false;
+    c->coarse.K_ok = false;  // the coarse geometry depends on the mesh alone: it stays
     c->coarse2.K_ok = false;
     c->learned.links_ok = false;
 }

@@ -23,7 +23,6 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
-#include <cstring>
 #include <condition_variable>
 #include <functional>
 #include <future>
@@ -108,6 +107,23 @@ void host_for_chunks(const std::function<void(int)> &f) {
         for (int k; (k = next.fetch_add(1)) < kHostChunks;) f(k);
     };
     host_pool().run(work);
+}
+
+// Offsets of the free rows from their aggregates' centroids (cell units,
+// FP64 rounded to FP32): agg_off in aggregate order with the row index,
+// row_off in row order with the aggregate index.
+__global__ void k_transfer_offsets(int nf, const int *__restrict__ agg_nodes, const int *__restrict__ agg_of,
+                                   const int *__restrict__ nof, const double *__restrict__ xyz,
+                                   const double *__restrict__ centroid, double isc, float4 *__restrict__ agg_off,
+                                   float4 *__restrict__ row_off) {
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nf; idx += gridDim.x * blockDim.x) {
+        const int r = agg_nodes[idx], a = agg_of[r], node = nof[r];
+        const float dx = (float)((xyz[3L * node] - centroid[3L * a]) * isc);
+        const float dy = (float)((xyz[3L * node + 1] - centroid[3L * a + 1]) * isc);
+        const float dz = (float)((xyz[3L * node + 2] - centroid[3L * a + 2]) * isc);
+        agg_off[idx] = make_float4(dx, dy, dz, __int_as_float(r));
+        row_off[r] = make_float4(dx, dy, dz, __int_as_float(a));
+    }
 }
 
 // Bins the free nodes into the nc[0] x nc[1] x nc[2] cell grid over [lo, lo+ext]
@@ -205,26 +221,6 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
             if (J >= 0) band = std::max(band, std::abs(J - a));
         }
     C.band = band;
-    // per free row in aggregate order: its offset from the aggregate's
-    // centroid in cell units (FP64, rounded to FP32) and the row, for the
-    // restriction's coalesced reads
-    // (agg_off), and the same offsets in row order with the aggregate
-    // (row_off) for the prolongation
-    HVec<float> off(4L * nf), roff(4L * nf);
-    const double isc = C.inv_scale;
-    host_for_chunks([&](int k) {
-        for (long idx = chunk_begin(nf, k); idx < chunk_begin(nf, k + 1); ++idx) {
-            const int r = nodes[idx], a = agg_of[r], node = nof[r];
-            for (int d = 0; d < 3; ++d) {
-                const float v = (float)((X[3L * node + d] - cen[3L * a + d]) * isc);
-                off[4 * idx + d] = v;
-                roff[4L * r + d] = v;
-            }
-            int rr = r;
-            std::memcpy(&off[4 * idx + 3], &rr, sizeof(int));
-            std::memcpy(&roff[4L * r + 3], &a, sizeof(int));
-        }
-    });
     if (!c->geo_stream) OFEA_CUDA(cudaStreamCreateWithFlags(&c->geo_stream, cudaStreamNonBlocking));
     cudaStream_t st = c->geo_stream;  // its own stream: may run beside the assembly (geometry_start)
     C.agg_of.upload(agg_of.data(), nf, st);
@@ -234,14 +230,24 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
     C.cell_agg.upload(cell_agg.data(), ncell, st);
     C.centroid.upload(cen.data(), cen.size(), st);
     C.nbr.upload(nbr.data(), nbr.size(), st);
-    C.agg_off.upload(off.data(), off.size(), st);
-    C.row_off.upload(roff.data(), roff.size(), st);
+    // per free row its offset from the aggregate's centroid in cell units
+    // (FP64, rounded to FP32), in aggregate order with the row (agg_off, the
+    // restriction's coalesced reads) and in row order with the aggregate
+    // (row_off, the prolongation's); formed on the device from the node
+    // coordinates already there
+    DevBuf<int> nof_d;
+    nof_d.upload(nof.data(), nf, st);
+    C.agg_off.ensure(4L * std::max(nf, 1));
+    C.row_off.ensure(4L * std::max(nf, 1));
+    k_transfer_offsets<<<std::max(1, std::min((nf + 255) / 256, c->num_sms * 16)), 256, 0, st>>>(
+        nf, C.agg_nodes.p, C.agg_of.p, nof_d.p, c->xyz.p, C.centroid.p, C.inv_scale,
+        reinterpret_cast<float4 *>(C.agg_off.p), reinterpret_cast<float4 *>(C.row_off.p));
+    OFEA_CHECK_LAUNCH();
     OFEA_CUDA(cudaStreamSynchronize(st));
     C.agg_cell_h = std::move(agg_cell3);
     C.cell_agg_h = std::move(cell_agg);
     C.centroid_h = std::move(cen);
-    C.geom_ok = true;
-    C.K_ok = false;
+    C.geom_ok = true;  // K_ok is false already: every change of the geometry resets it first
 }
 
 void build_aggregation(ofea_ctx *c, int target_nodes) {
