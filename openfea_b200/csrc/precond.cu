@@ -336,9 +336,12 @@ void build_aggregation_fine(ofea_ctx *c) {
 // Stage 2: E entries from the chunk partials, fixed chunk order.
 // Galerkin blocks E[I][s] = sum over nodes i of I and row blocks K_ij with
 // aggregate(j) in neighbour slot s of Z_i^T K_ij Z_j (6 x 6, row-major), for
-// every aggregate I of a level.  One CTA per aggregate; warp w takes the
-// aggregate's nodes w, w + kGW, ... in order; lane t takes block t of the
-// node's row (32 at a time) and forms W = K_ij Z_j (3 x 6).  Lanes whose
+// every aggregate I of a level, with the rows' offsets of the V-cycle's
+// transfers (agg_off, row_off: FP64 offsets rounded to FP32, so E is the
+// exact Galerkin operator of the Z the V-cycle applies).  One CTA per
+// aggregate; warp w takes the aggregate's nodes w, w + kGW, ... in order;
+// lane t takes block t of the node's row (32 at a time) and forms
+// W = K_ij Z_j (3 x 6).  Lanes whose
 // blocks land in the same slot are summed in lane order (match_any, then 32
 // broadcast shuffles, or a shuffle tree when the whole warp shares one slot),
 // the group's first lane adds Z_i^T W to its warp's accumulator, and the
@@ -353,10 +356,9 @@ __device__ __forceinline__ void cross_e(int t, const double d[3], double z[3]) {
 }
 
 __global__ void __launch_bounds__(kGW * 32) k_galerkin_blocks(
-    int na, const int *__restrict__ agg_ptr, const int *__restrict__ agg_nodes, const int *__restrict__ agg_of,
-    const int *__restrict__ agg_cell, const int *__restrict__ node_of_free, const double *__restrict__ xyz,
-    const double *__restrict__ centroid, double inv_scale, const int *__restrict__ rowptr,
-    const int *__restrict__ cols, KBlocks KB, double *__restrict__ Eb, int *__restrict__ err) {
+    int na, const int *__restrict__ agg_ptr, const float4 *__restrict__ agg_off, const float4 *__restrict__ row_off,
+    const int *__restrict__ agg_cell, const int *__restrict__ rowptr, const int *__restrict__ cols, KBlocks KB,
+    double *__restrict__ Eb, int *__restrict__ err) {
     extern __shared__ double gsm[];
     double (*acc)[27 * 36] = reinterpret_cast<double (*)[27 * 36]>(gsm);                  // [kGW][27 * 36]
     double (*stage)[32][18] = reinterpret_cast<double (*)[32][18]>(gsm + kGW * 27 * 36);  // [kGW][32][18]
@@ -366,11 +368,10 @@ __global__ void __launch_bounds__(kGW * 32) k_galerkin_blocks(
         for (int v = threadIdx.x; v < kGW * 27 * 36; v += blockDim.x) (&acc[0][0])[v] = 0.0;
         __syncthreads();
         const int cx = agg_cell[3 * I], cy = agg_cell[3 * I + 1], cz = agg_cell[3 * I + 2];
-        const double cI[3] = {centroid[3L * I], centroid[3L * I + 1], centroid[3L * I + 2]};
         for (int idx = agg_ptr[I] + w; idx < agg_ptr[I + 1]; idx += kGW) {
-            const int i = agg_nodes[idx], ni = node_of_free[i];
-            double di[3];
-            for (int d = 0; d < 3; ++d) di[d] = (xyz[3L * ni + d] - cI[d]) * inv_scale;
+            const float4 oi = agg_off[idx];  // the row and its offset from the centroid (the V-cycle's Z)
+            const int i = __float_as_int(oi.w);
+            const double di[3] = {oi.x, oi.y, oi.z};
             const int rb = rowptr[i], deg = rowptr[i + 1] - rb;
             for (int c0 = 0; c0 < deg; c0 += 32) {
                 const int k = c0 + lane;
@@ -379,7 +380,9 @@ __global__ void __launch_bounds__(kGW * 32) k_galerkin_blocks(
                 for (int e = 0; e < 18; ++e) v[e] = 0.0;
                 int slot = -2;  // lanes past the row form their own group
                 if (k < deg) {
-                    const int j = cols[rb + k], J = agg_of[j];
+                    const int j = cols[rb + k];
+                    const float4 oj = row_off[j];
+                    const int J = __float_as_int(oj.w);
                     const int dx = agg_cell[3 * J] - cx, dy = agg_cell[3 * J + 1] - cy, dz = agg_cell[3 * J + 2] - cz;
                     if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1) {
                         slot = (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
@@ -387,9 +390,7 @@ __global__ void __launch_bounds__(kGW * 32) k_galerkin_blocks(
                         atomicExch(err, 1);
                         slot = -1;
                     }
-                    const int nj = node_of_free[j];
-                    double dj[3];
-                    for (int d = 0; d < 3; ++d) dj[d] = (xyz[3L * nj + d] - centroid[3L * J + d]) * inv_scale;
+                    const double dj[3] = {oj.x, oj.y, oj.z};
                     double K[9];
 #pragma unroll
                     for (int e = 0; e < 9; ++e) K[e] = KB.at(i, k, e);
@@ -1224,8 +1225,9 @@ void coarse_E_partials(ofea_ctx *c, Coarse &C, int nchunk) {
     const int gsm_bytes = (int)(sizeof(double) * kGW * (27 * 36 + 32 * 18));
     OFEA_CUDA(cudaFuncSetAttribute(k_galerkin_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm_bytes));
     k_galerkin_blocks<<<std::max(1, C.na), kGW * 32, gsm_bytes, c->stream>>>(
-        C.na, C.agg_ptr.p, C.agg_nodes.p, C.agg_of.p, C.agg_cell.p, c->node_of_free.p, c->xyz.p, C.centroid.p,
-        C.inv_scale, c->rowptr.p, c->cols.p, kblocks(c), C.part.p, c->err_flag.p);
+        C.na, C.agg_ptr.p, reinterpret_cast<const float4 *>(C.agg_off.p),
+        reinterpret_cast<const float4 *>(C.row_off.p), C.agg_cell.p, c->rowptr.p, c->cols.p, kblocks(c), C.part.p,
+        c->err_flag.p);
     OFEA_CHECK_LAUNCH();
 }
 
