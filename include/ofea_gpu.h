@@ -89,7 +89,9 @@ OFEA_API void ofea_solve_opts_default(ofea_solve_opts *opts);
 OFEA_API int ofea_ctx_create(ofea_ctx **out, int device);
 OFEA_API int ofea_ctx_destroy(ofea_ctx *ctx);
 /* No counterpart in the reference.  Device memory the library frees is kept
- * per GPU (up to 8 GB) and reused by later allocations of a fitting size, so
+ * per GPU (up to a quarter of its memory, at most 32 GB) and reused by later
+ * allocations of a fitting size (a failed cudaMalloc returns the cached
+ * blocks and retries), so
  * that a fresh context does not pay cudaMalloc for every buffer again; large
  * host blocks (the mesh's host copies, set-up scratch; up to 1 GB) are kept
  * the same way so that a new context does not fault in fresh pages.  This

@@ -211,6 +211,17 @@ struct __align__(128) Stage {
 };
 static_assert(sizeof(Stage::v) >= 6 * 32 * 32 * sizeof(float), "the restriction's per-warp sums fit in the stage");
 
+// Bulk prefetch of [p, p + bytes) from HBM into L2 (no data returned, no
+// completion to wait for).  p and bytes are multiples of 16 (the BSELL slot
+// blocks and the slices' vector runs are); issued in pieces of at most 32 KB.
+__device__ __forceinline__ void l2_prefetch(const void *p, long bytes) {
+    const size_t g = __cvta_generic_to_global(p);
+    for (long o = 0; o < bytes; o += 32768) {
+        const unsigned nb = (unsigned)min(32768L, bytes - o);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(g + o), "r"(nb) : "memory");
+    }
+}
+
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
@@ -373,9 +384,17 @@ __global__ void __launch_bounds__(32 * (NP / RL), batch_min_ctas(32 * (NP / RL),
         return ok;
     };
     auto X = [&](const BVar &B, int row, int c) { return vidx<NP>(B, row, c, j0); };
-    // CTA-level loop over slices: f(B, v, gsl, ls, row, live[RL], any)
-    auto for_slices = [&](auto f) {
+    // CTA-level loop over slices: f(B, v, gsl, ls, row, live[RL], any).
+    // pf(Bn, lsn), run by thread 0 as each slice starts, prefetches into L2
+    // what f will read of the CTA's next slice (its HBM latency then overlaps
+    // this slice's work).
+    auto for_slices_pf = [&](auto pf, auto f) {
         for (int gsl = blockIdx.x; gsl < a.nslices; gsl += gridDim.x) {
+            if (threadIdx.x == 0 && gsl + (int)gridDim.x < a.nslices) {
+                const int gn = gsl + (int)gridDim.x;
+                const BVar &Bn = a.var[a.slice_var[gn]];
+                pf(Bn, gn - Bn.slice0);
+            }
             const int v = a.slice_var[gsl];
             const BVar B = a.var[v];
             const int ls = gsl - B.slice0;
@@ -388,6 +407,27 @@ __global__ void __launch_bounds__(32 * (NP / RL), batch_min_ctas(32 * (NP / RL),
                 any |= live[q];
             }
             f(B, v, gsl, ls, row, live, any);
+        }
+    };
+    auto for_slices = [&](auto f) { for_slices_pf([](const BVar &, int) {}, f); };
+    // Prefetch pieces for a slice lsn of variant Bn: the rows' runs of a batch
+    // vector (esize bytes per entry), the rows' inverse diagonal blocks (FP32
+    // or FP64; a partial last slice is rounded down to 16 bytes).  Used by
+    // the vector phases only: in the matrix phases the prefetch measured
+    // slower (thread 0's descriptor loads delay the CTA's staging barrier,
+    // and K prefetched ahead competes with the gathered columns in L2).
+    auto pf_rows = [&](const BVar &Bn, int lsn, const void *base, int esize) {
+        const int row0 = lsn * kSlice, rows = min(kSlice, Bn.nfree - row0);
+        if (rows > 0)
+            l2_prefetch(static_cast<const char *>(base) + (Bn.dof0 + 3L * row0) * NP * esize,
+                        3L * rows * NP * esize);
+    };
+    auto pf_dinv = [&](const BVar &Bn, int lsn) {
+        const int row0 = lsn * kSlice, rows = min(kSlice, Bn.nfree - row0);
+        if (MIXED) {
+            if (rows > 0) l2_prefetch(Bn.Dinv32 + 9L * row0, (36L * rows) & ~15L);
+        } else {
+            if (rows > 0) l2_prefetch(Bn.Dinv + 9L * row0, (72L * rows) & ~15L);
         }
     };
 
@@ -566,7 +606,11 @@ __global__ void __launch_bounds__(32 * (NP / RL), batch_min_ctas(32 * (NP / RL),
         }
         if (!sync()) return false;
         // x += Z e
-        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, const bool (&live)[RL], bool any) {
+        for_slices_pf(
+            [&](const BVar &Bn, int lsn) {
+                pf_rows(Bn, lsn, a.x32, 4);
+            },
+            [&](const BVar &B, int v, int gsl, int ls, int row, const bool (&live)[RL], bool any) {
             if (!any || row >= B.nfree) return;
             const int I = B.agg_of[row], node = B.node_of_free[row];
             const float dx = (float)((B.xyz[3L * node] - B.centroid[3L * I]) * B.inv_scale);
@@ -704,7 +748,15 @@ __global__ void __launch_bounds__(32 * (NP / RL), batch_min_ctas(32 * (NP / RL),
         });
         if (!sync()) return;
         // B: u += alpha p, r -= alpha q, partial ||r||^2; start of M(r)
-        for_slices([&](const BVar &B, int v, int gsl, int ls, int row, const bool (&live)[RL], bool any) {
+        for_slices_pf(
+            [&](const BVar &Bn, int lsn) {
+                pf_rows(Bn, lsn, a.u, 8);
+                pf_rows(Bn, lsn, pnew, 8);
+                pf_rows(Bn, lsn, a.q, 8);
+                pf_rows(Bn, lsn, a.r, 8);
+                pf_dinv(Bn, lsn);
+            },
+            [&](const BVar &B, int v, int gsl, int ls, int row, const bool (&live)[RL], bool any) {
             double prr[RL] = {}, prz[RL] = {};
             if (any && row < B.nfree) {
                 double al[RL];

@@ -4,7 +4,8 @@
 // matrices, the learned level, batch vectors) the first time it needs them;
 // cudaMalloc / cudaFree of each cost up to milliseconds, which dominated the
 // first solve of a fresh context.  Freed blocks are therefore kept per device
-// (up to kCacheCap bytes) and handed to later requests of a fitting size;
+// (up to a quarter of the device's memory, at most 32 GB) and handed to
+// later requests of a fitting size;
 // a block is cached only after the device has finished every queued use of it
 // (cudaDeviceSynchronize, the wait cudaFree itself implies).  Sizes are
 // rounded (256 B, or 2 MB from 1 MB up) so that contexts of the same problem
@@ -22,11 +23,25 @@
 namespace ofea {
 namespace {
 
-constexpr size_t kCacheCap = size_t(8) << 30;  // bytes cached per device
+// Bytes cached per device: a quarter of the device's memory, at most 32 GB
+// (two contexts of a 1.6M-DOF problem and the blocks of earlier ones fit;
+// with 8 GB a fresh context of that size found part of its blocks freed).
+size_t cache_cap(int dev) {
+    size_t fr = 0, total = 0;
+    int cur = 0;
+    if (cudaGetDevice(&cur) != cudaSuccess || (cur != dev && cudaSetDevice(dev) != cudaSuccess) ||
+        cudaMemGetInfo(&fr, &total) != cudaSuccess) {
+        cudaGetLastError();
+        total = size_t(32) << 30;
+    }
+    if (cur != dev) cudaSetDevice(cur);
+    return std::min(size_t(32) << 30, total / 4);
+}
 
 struct DeviceCache {
     std::multimap<size_t, void *> free;  // size -> block
     size_t cached = 0;
+    size_t cap = 0;  // 0: not yet queried
 };
 
 // never destroyed: contexts may be freed during process teardown
@@ -94,7 +109,8 @@ void dev_free(void *p, size_t bytes, int dev) {
     if (have_cur) cudaSetDevice(cur);
     std::lock_guard<std::mutex> lock(state().mu);
     DeviceCache &c = state().cache[dev];
-    if (c.cached + bytes > kCacheCap) {
+    if (c.cap == 0) c.cap = cache_cap(dev);
+    if (c.cached + bytes > c.cap) {
         cudaSetDevice(dev);
         cudaFree(p);
         if (have_cur) cudaSetDevice(cur);

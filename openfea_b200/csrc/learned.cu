@@ -620,20 +620,6 @@ __global__ void k_scales(int n, const float *__restrict__ Y, float *__restrict__
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s[i] = expf(0.5f * Y[i]);
 }
 
-// Coarse correction in level-2 modes: g = D^-1/2 (s * wv), written over c2.
-__global__ void k_poly_out(int na, const float *__restrict__ s, const float *__restrict__ wv,
-                           const float *__restrict__ dsq, float *__restrict__ g) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 6 * na; i += gridDim.x * blockDim.x) {
-        const float d = dsq[i];
-        g[i] = d > 0.f ? s[i] * wv[i] / d : 0.f;
-    }
-}
-
-
-// Level-1 restriction from the level-2 one: c1 = P^T c2, P the map of
-// level-1 modes into its children's modes (child_coeffs); Z1 = Z2 P, so this
-// is Z1^T t without a second pass over the fine vector.  Thread per (parent,
-// mode), children summed in table order.
 // Both coarse corrections in level-2 modes: g = D^-1/2 (s * wv) + P e1,
 // written over c2 (one prolongation then adds Z2 g = Z1 e1 + Z2 D^-1/2 y).
 __global__ void k_poly_out_e1(int na, const float *__restrict__ s, const float *__restrict__ wv,
@@ -880,10 +866,9 @@ static void check_tc(ofea_ctx *c) {
 }
 
 // Network forward over the aggregates (input: the node features), scalings s.
-static void gnn_forward(ofea_ctx *c) {
+static void gnn_forward(ofea_ctx *c, cudaStream_t s) {
     Learned &N = c->learned;
     const Learned::Layout L = Learned::layout();
-    cudaStream_t s = c->stream;
     const long R = c->coarse2.na;
     const int na = (int)R;
     const float *w = N.w.p;
@@ -975,7 +960,7 @@ static void loss_and_grad(ofea_ctx *c, int Bsz) {
     const int na = C2.na;
     const long Rp = (long)Bsz * na;
     const float *coef = N.w.p + L.c0;
-    gnn_forward(c);
+    gnn_forward(c, c->stream);
     float *wv = N.pv[3].p, *d = N.pv[4].p, *md = N.pv[5].p;
     // y = s * M(s x): basis v_k of the first chain kept in pv[6..8]
     apply_M(c, Rp, N.scale.p, N.batch_src.p, coef, wv);
@@ -1207,11 +1192,51 @@ void learned_coarse_correct(ofea_ctx *c, const float *t, float *x) {
 }
 
 // Weights on the device and the network evaluated (the scalings s) for the current K.
-void learned_prepare_inference(ofea_ctx *c) {
+// The LEARNED solver's per-K set-up: both coarse levels as in
+// setup_learned_levels, with the network's scalings evaluated on the side
+// stream beside the coarse level's E1 = P^T E2 P and its factor (the network
+// reads the nested level's features alone); the context stream waits for it.
+void setup_learned_solver(ofea_ctx *c) {
     Learned &N = c->learned;
+    setup_coarse_geometry(c, c->coarse_nodes);
+    const bool need_e1 = !c->coarse.K_ok;
+    setup_learned_level(c);
     upload_weights(c);
     ensure_rows(c, c->coarse2.na);
-    gnn_forward(c);
+    tc_flag(c);
+    if (!c->side_stream) OFEA_CUDA(cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking));
+    cudaEvent_t fork = nullptr, join = nullptr;
+    OFEA_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    OFEA_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    bool forked = false;
+    try {
+        OFEA_CUDA(cudaEventRecord(fork, c->stream));
+        OFEA_CUDA(cudaStreamWaitEvent(c->side_stream, fork, 0));
+        forked = true;
+        gnn_forward(c, c->side_stream);
+        OFEA_CUDA(cudaEventRecord(join, c->side_stream));
+        if (need_e1) {
+            Coarse &C1 = c->coarse;
+            double *E = coarse_begin_E(c);
+            k_e1_from_e2<<<std::min(C1.na * 27, c->num_sms * 16), 64, 0, c->stream>>>(
+                C1.na, C1.m, C1.nbr.p, N.children.p, c->coarse2.agg_cell.p, N.pdel.p, N.Eb.p, E);
+            OFEA_CHECK_LAUNCH();
+            setup_mark(c, "e1_from_e2");
+            coarse_finish(c);
+        }
+        OFEA_CUDA(cudaStreamWaitEvent(c->stream, join, 0));
+    } catch (...) {
+        if (forked) {  // nothing on the context stream may overtake the side stream's work
+            cudaEventRecord(join, c->side_stream);
+            cudaStreamWaitEvent(c->stream, join, 0);
+        }
+        cudaEventDestroy(fork);
+        cudaEventDestroy(join);
+        throw;
+    }
+    cudaEventDestroy(fork);
+    cudaEventDestroy(join);
+    setup_mark(c, "network_join");
     N.inference_ready = true;
 }
 

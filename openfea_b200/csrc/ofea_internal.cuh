@@ -151,6 +151,7 @@ struct Coarse {
     DevBuf<float> Einv32, cvec, evec, pw;
     DevBuf<float> agg_off;  // [nfree][4] in aggregate order: offset from the centroid (cell units), row
     DevBuf<float> row_off;  // [nfree][4] in row order: the same offset, aggregate
+    DevBuf<unsigned long long> row_cell;  // [nfree] in row order: the aggregate's cell, 21 bits per axis
     // the coarse solve as a block LDL^T factor (precond.cu): S_k, L_ik and the
     // FP32 array F (U = diag(S) V below, V^T above); dense_ok: Einv32 holds the
     // dense inverse (the Gauss-Jordan path, or formed from F on demand)
@@ -193,7 +194,7 @@ struct ofea_ctx {
     int num_sms = 148;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    cudaStream_t side_stream = nullptr;  // second stream of the coarse inversion's lookahead (owned)
+    cudaStream_t side_stream = nullptr;  // the coarse inversion's lookahead; the network beside the coarse factor (owned)
     cudaStream_t aux_stream = nullptr;   // power iteration beside the coarse inversion (owned)
     cudaStream_t geo_stream = nullptr;   // uploads of the coarse geometry (owned)
     std::future<void> geom_job;          // coarse geometry built in the background after the pattern
@@ -286,7 +287,7 @@ void setup_learned_level(ofea_ctx *c);
 void setup_learned_levels(ofea_ctx *c);
 void geometry_start(ofea_ctx *c);
 void geometry_join(ofea_ctx *c);
-void learned_prepare_inference(ofea_ctx *c);
+void setup_learned_solver(ofea_ctx *c);
 void learned_coarse_correct(ofea_ctx *c, const float *t, float *x);
 // Batched persistent solver (batched.cu).
 ofea_batch *batch_create(ofea_ctx *const *ctxs, int nv, int nrhs);

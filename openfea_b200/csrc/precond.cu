@@ -111,11 +111,15 @@ void host_for_chunks(const std::function<void(int)> &f) {
 
 // Offsets of the free rows from their aggregates' centroids (cell units,
 // FP64 rounded to FP32): agg_off in aggregate order with the row index,
-// row_off in row order with the aggregate index.
+// row_off in row order with the aggregate index; row_cell in row order: the
+// aggregate's cell (x | y << 21 | z << 42).
+constexpr int kCellBits = 21;
+constexpr unsigned long long kCellMask = (1ull << kCellBits) - 1;
 __global__ void k_transfer_offsets(int nf, const int *__restrict__ agg_nodes, const int *__restrict__ agg_of,
                                    const int *__restrict__ nof, const double *__restrict__ xyz,
-                                   const double *__restrict__ centroid, double isc, float4 *__restrict__ agg_off,
-                                   float4 *__restrict__ row_off) {
+                                   const double *__restrict__ centroid, const int *__restrict__ agg_cell, double isc,
+                                   float4 *__restrict__ agg_off, float4 *__restrict__ row_off,
+                                   unsigned long long *__restrict__ row_cell) {
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nf; idx += gridDim.x * blockDim.x) {
         const int r = agg_nodes[idx], a = agg_of[r], node = nof[r];
         const float dx = (float)((xyz[3L * node] - centroid[3L * a]) * isc);
@@ -123,6 +127,8 @@ __global__ void k_transfer_offsets(int nf, const int *__restrict__ agg_nodes, co
         const float dz = (float)((xyz[3L * node + 2] - centroid[3L * a + 2]) * isc);
         agg_off[idx] = make_float4(dx, dy, dz, __int_as_float(r));
         row_off[r] = make_float4(dx, dy, dz, __int_as_float(a));
+        row_cell[r] = (unsigned long long)agg_cell[3L * a] | ((unsigned long long)agg_cell[3L * a + 1] << kCellBits) |
+                      ((unsigned long long)agg_cell[3L * a + 2] << (2 * kCellBits));
     }
 }
 
@@ -239,9 +245,12 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
     nof_d.upload(nof.data(), nf, st);
     C.agg_off.ensure(4L * std::max(nf, 1));
     C.row_off.ensure(4L * std::max(nf, 1));
+    C.row_cell.ensure(std::max(nf, 1));
+    for (int d = 0; d < 3; ++d)
+        if (nc[d] > (int)kCellMask) fail(OFEA_ERR_CAPACITY, "coarse level: more than 2^21 cells along an axis");
     k_transfer_offsets<<<std::max(1, std::min((nf + 255) / 256, c->num_sms * 16)), 256, 0, st>>>(
-        nf, C.agg_nodes.p, C.agg_of.p, nof_d.p, c->xyz.p, C.centroid.p, C.inv_scale,
-        reinterpret_cast<float4 *>(C.agg_off.p), reinterpret_cast<float4 *>(C.row_off.p));
+        nf, C.agg_nodes.p, C.agg_of.p, nof_d.p, c->xyz.p, C.centroid.p, C.agg_cell.p, C.inv_scale,
+        reinterpret_cast<float4 *>(C.agg_off.p), reinterpret_cast<float4 *>(C.row_off.p), C.row_cell.p);
     OFEA_CHECK_LAUNCH();
     OFEA_CUDA(cudaStreamSynchronize(st));
     C.agg_cell_h = std::move(agg_cell3);
@@ -340,7 +349,8 @@ void build_aggregation_fine(ofea_ctx *c) {
 // transfers (agg_off, row_off: FP64 offsets rounded to FP32, so E is the
 // exact Galerkin operator of the Z the V-cycle applies).  One CTA per
 // aggregate; warp w takes the aggregate's nodes w, w + kGW, ... in order;
-// lane t takes block t of the node's row (32 at a time) and forms
+// lane t takes block t of the node's row (32 at a time), finds the slot of
+// j's aggregate from j's packed cell (row_cell) and forms
 // W = K_ij Z_j (3 x 6).  Lanes whose
 // blocks land in the same slot are summed in lane order (match_any, then 32
 // broadcast shuffles, or a shuffle tree when the whole warp shares one slot),
@@ -357,8 +367,8 @@ __device__ __forceinline__ void cross_e(int t, const double d[3], double z[3]) {
 
 __global__ void __launch_bounds__(kGW * 32) k_galerkin_blocks(
     int na, const int *__restrict__ agg_ptr, const float4 *__restrict__ agg_off, const float4 *__restrict__ row_off,
-    const int *__restrict__ agg_cell, const int *__restrict__ rowptr, const int *__restrict__ cols, KBlocks KB,
-    double *__restrict__ Eb, int *__restrict__ err) {
+    const unsigned long long *__restrict__ row_cell, const int *__restrict__ agg_cell, const int *__restrict__ rowptr,
+    const int *__restrict__ cols, KBlocks KB, double *__restrict__ Eb, int *__restrict__ err) {
     extern __shared__ double gsm[];
     double (*acc)[27 * 36] = reinterpret_cast<double (*)[27 * 36]>(gsm);                  // [kGW][27 * 36]
     double (*stage)[32][18] = reinterpret_cast<double (*)[32][18]>(gsm + kGW * 27 * 36);  // [kGW][32][18]
@@ -368,11 +378,30 @@ __global__ void __launch_bounds__(kGW * 32) k_galerkin_blocks(
         for (int v = threadIdx.x; v < kGW * 27 * 36; v += blockDim.x) (&acc[0][0])[v] = 0.0;
         __syncthreads();
         const int cx = agg_cell[3 * I], cy = agg_cell[3 * I + 1], cz = agg_cell[3 * I + 2];
-        for (int idx = agg_ptr[I] + w; idx < agg_ptr[I + 1]; idx += kGW) {
-            const float4 oi = agg_off[idx];  // the row and its offset from the centroid (the V-cycle's Z)
+        const int idx_end = agg_ptr[I + 1];
+        int idx = agg_ptr[I] + w;
+        // The warp's rows are walked with the next row's offset and pattern
+        // range already in flight (loaded one row ahead): per row only the
+        // lanes' column loads and their dependent loads remain on the chain.
+        float4 oi = make_float4(0.f, 0.f, 0.f, 0.f), on = oi;  // current and next row: offset from the centroid, row
+        int rb = 0, re = 0;
+        if (idx < idx_end) {
+            oi = agg_off[idx];
+            rb = rowptr[__float_as_int(oi.w)];
+            re = rowptr[__float_as_int(oi.w) + 1];
+            if (idx + kGW < idx_end) on = agg_off[idx + kGW];
+        }
+        for (; idx < idx_end; idx += kGW) {
             const int i = __float_as_int(oi.w);
             const double di[3] = {oi.x, oi.y, oi.z};
-            const int rb = rowptr[i], deg = rowptr[i + 1] - rb;
+            const int deg = re - rb;
+            int rbn = 0, ren = 0;
+            float4 onn = on;
+            if (idx + kGW < idx_end) {
+                rbn = rowptr[__float_as_int(on.w)];
+                ren = rowptr[__float_as_int(on.w) + 1];
+                if (idx + 2 * kGW < idx_end) onn = agg_off[idx + 2 * kGW];
+            }
             for (int c0 = 0; c0 < deg; c0 += 32) {
                 const int k = c0 + lane;
                 double v[18];
@@ -382,8 +411,9 @@ __global__ void __launch_bounds__(kGW * 32) k_galerkin_blocks(
                 if (k < deg) {
                     const int j = cols[rb + k];
                     const float4 oj = row_off[j];
-                    const int J = __float_as_int(oj.w);
-                    const int dx = agg_cell[3 * J] - cx, dy = agg_cell[3 * J + 1] - cy, dz = agg_cell[3 * J + 2] - cz;
+                    const unsigned long long pc = row_cell[j];
+                    const int dx = (int)(pc & kCellMask) - cx, dy = (int)((pc >> kCellBits) & kCellMask) - cy,
+                              dz = (int)(pc >> (2 * kCellBits)) - cz;
                     if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1) {
                         slot = (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
                     } else {
@@ -465,6 +495,10 @@ __global__ void __launch_bounds__(kGW * 32) k_galerkin_blocks(
                 }
                 __syncwarp();
             }
+            oi = on;
+            on = onn;
+            rb = rbn;
+            re = ren;
         }
         __syncthreads();
         for (int v = threadIdx.x; v < 27 * 36; v += blockDim.x) {
@@ -1226,8 +1260,8 @@ void coarse_E_partials(ofea_ctx *c, Coarse &C, int nchunk) {
     OFEA_CUDA(cudaFuncSetAttribute(k_galerkin_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm_bytes));
     k_galerkin_blocks<<<std::max(1, C.na), kGW * 32, gsm_bytes, c->stream>>>(
         C.na, C.agg_ptr.p, reinterpret_cast<const float4 *>(C.agg_off.p),
-        reinterpret_cast<const float4 *>(C.row_off.p), C.agg_cell.p, c->rowptr.p, c->cols.p, kblocks(c), C.part.p,
-        c->err_flag.p);
+        reinterpret_cast<const float4 *>(C.row_off.p), C.row_cell.p, C.agg_cell.p, c->rowptr.p, c->cols.p, kblocks(c),
+        C.part.p, c->err_flag.p);
     OFEA_CHECK_LAUNCH();
 }
 

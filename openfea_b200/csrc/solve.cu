@@ -525,9 +525,7 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
         setup_mark(c, "start");
         if (learned) {
             if (!c->learned.have_weights) fail(OFEA_ERR_STATE, "train or load the learned stage first");
-            setup_learned_levels(c);
-            learned_prepare_inference(c);
-            setup_mark(c, "network");
+            setup_learned_solver(c);
         } else {
             setup_coarse(c, c->coarse_nodes);
         }
