@@ -1053,6 +1053,7 @@ struct ofea_batch {
     ofea::DevBuf<int> live, iters, status, live_cnt;
     ofea::DevBuf<ofea::GridSync> gs;
     ofea::DevBuf<unsigned long long> trace;  // per-phase timestamps when tracing (trace_cap > 0)
+    ofea::HostBuf<double> bounce[2];          // page-locked blocks between the callers' arrays and the device
     int trace_cap = 0;
     std::map<int, ofea::TuneCfg> tuned;  // by method
     // the captured graph of one launch and what it was captured for
@@ -1388,16 +1389,60 @@ void batch_destroy(ofea_batch *b) {
     delete b;
 }
 
+namespace {
+
+// dst <- src (host memory, bytes), split over the host pool's chunks when large.
+void host_copy(void *dst, const void *src, size_t bytes) {
+    if (bytes < (size_t(4) << 20)) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    const long units = (long)(bytes / 64);
+    host_for_chunks([&](int k) {
+        const size_t a = (size_t)chunk_begin(units, k) * 64;
+        const size_t e = k + 1 == kHostChunks ? bytes : (size_t)chunk_begin(units, k + 1) * 64;
+        std::memcpy(static_cast<char *>(dst) + a, static_cast<const char *>(src) + a, e - a);
+    });
+}
+
+// Two events for the bounce blocks, destroyed on every exit.
+struct EventPair {
+    cudaEvent_t e[2] = {nullptr, nullptr};
+    EventPair() {
+        for (auto &x : e) OFEA_CUDA(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    }
+    ~EventPair() {
+        for (auto &x : e)
+            if (x) cudaEventDestroy(x);
+    }
+};
+
+}  // namespace
+
+// The callers' arrays are pageable: each variant goes through one of two
+// page-locked bounce blocks, the host copy of one variant (over the host
+// pool's chunks) overlapping the DMA of the other.
 void batch_set_rhs(ofea_batch *b, const double *const *f) {
     OFEA_CUDA(cudaSetDevice(b->device));
     cudaStream_t s = b->stream;
+    size_t maxn = 1;
+    for (int v = 0; v < b->V; ++v) {
+        if (!f[v]) fail(OFEA_ERR_INVALID_ARG, "batch: NULL load array");
+        maxn = std::max(maxn, (size_t)b->ctx[v]->n * b->NR);
+    }
+    b->stage.ensure((size_t)b->ndof * b->NR);
+    for (auto &h : b->bounce) h.ensure(maxn);
+    EventPair ev;
     for (int v = 0; v < b->V; ++v) {
         const long n = b->ctx[v]->n;
-        if (!f[v]) fail(OFEA_ERR_INVALID_ARG, "batch: NULL load array");
-        b->stage.ensure((size_t)n * b->NR);
-        OFEA_CUDA(cudaMemcpyAsync(b->stage.p, f[v], sizeof(double) * n * b->NR, cudaMemcpyHostToDevice, s));
+        const int k = v & 1;
+        double *dst = b->stage.p + b->dof0[v] * b->NR;
+        if (v >= 2) OFEA_CUDA(cudaEventSynchronize(ev.e[k]));  // the DMA out of this block (variant v - 2) is done
+        host_copy(b->bounce[k].p, f[v], sizeof(double) * n * b->NR);
+        OFEA_CUDA(cudaMemcpyAsync(dst, b->bounce[k].p, sizeof(double) * n * b->NR, cudaMemcpyHostToDevice, s));
+        OFEA_CUDA(cudaEventRecord(ev.e[k], s));
         k_interleave<<<std::max(1, std::min(kMaxGrid, (int)((n * b->NR + 255) / 256))), 256, 0, s>>>(
-            n, b->NR, b->NP, b->stage.p, b->f.p + b->dof0[v] * b->NP);
+            n, b->NR, b->NP, dst, b->f.p + b->dof0[v] * b->NP);
         OFEA_CHECK_LAUNCH();
     }
     OFEA_CUDA(cudaStreamSynchronize(s));
@@ -1407,15 +1452,32 @@ void batch_set_rhs(ofea_batch *b, const double *const *f) {
 void batch_get_solution(ofea_batch *b, double *const *u) {
     OFEA_CUDA(cudaSetDevice(b->device));
     cudaStream_t s = b->stream;
+    size_t maxn = 1;
+    for (int v = 0; v < b->V; ++v) {
+        if (!u[v]) fail(OFEA_ERR_INVALID_ARG, "batch: NULL solution array");
+        maxn = std::max(maxn, (size_t)b->ctx[v]->n * b->NR);
+    }
+    b->stage.ensure((size_t)b->ndof * b->NR);
+    for (auto &h : b->bounce) h.ensure(maxn);
     for (int v = 0; v < b->V; ++v) {
         const long n = b->ctx[v]->n;
-        if (!u[v]) fail(OFEA_ERR_INVALID_ARG, "batch: NULL solution array");
-        b->stage.ensure((size_t)n * b->NR);
         k_deinterleave<<<std::max(1, std::min(kMaxGrid, (int)((n * b->NR + 255) / 256))), 256, 0, s>>>(
-            n, b->NR, b->NP, b->u.p + b->dof0[v] * b->NP, b->stage.p);
+            n, b->NR, b->NP, b->u.p + b->dof0[v] * b->NP, b->stage.p + b->dof0[v] * b->NR);
         OFEA_CHECK_LAUNCH();
-        OFEA_CUDA(cudaMemcpyAsync(u[v], b->stage.p, sizeof(double) * n * b->NR, cudaMemcpyDeviceToHost, s));
-        OFEA_CUDA(cudaStreamSynchronize(s));
+    }
+    EventPair ev;
+    for (int v = 0; v <= b->V; ++v) {
+        if (v < b->V) {  // block v & 1 was last read by the host copy of variant v - 2, already done
+            const long n = b->ctx[v]->n;
+            OFEA_CUDA(cudaMemcpyAsync(b->bounce[v & 1].p, b->stage.p + b->dof0[v] * b->NR, sizeof(double) * n * b->NR,
+                                      cudaMemcpyDeviceToHost, s));
+            OFEA_CUDA(cudaEventRecord(ev.e[v & 1], s));
+        }
+        if (v > 0) {
+            const int w = v - 1;
+            OFEA_CUDA(cudaEventSynchronize(ev.e[w & 1]));
+            host_copy(u[w], b->bounce[w & 1].p, sizeof(double) * b->ctx[w]->n * b->NR);
+        }
     }
 }
 
