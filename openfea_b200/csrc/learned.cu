@@ -327,7 +327,9 @@ __global__ void __launch_bounds__(kBlock) k_lrn_shift(int na, const int *__restr
                                                       float *__restrict__ S, const float *__restrict__ Binv = nullptr,
                                                       const float *__restrict__ sc = nullptr,
                                                       const float *__restrict__ coef = nullptr,
-                                                      float *__restrict__ v1 = nullptr, float *__restrict__ out = nullptr) {
+                                                      float *__restrict__ v1 = nullptr, float *__restrict__ out = nullptr,
+                                                      const int *__restrict__ stop = nullptr) {
+    if (vc_stopped(stop)) return;
     const int lane = threadIdx.x & 31;
     for (int I = (blockIdx.x * blockDim.x + threadIdx.x) / 32; I < na; I += gridDim.x * blockDim.x / 32) {
         float v[6] = {0, 0, 0, 0, 0, 0};
@@ -467,7 +469,9 @@ __global__ void k_poly_first(long R, int na, const float *__restrict__ Binv, con
 __global__ void __launch_bounds__(kBlock) k_poly_next(long R, int na, const int *__restrict__ nbr,
                                                       const float *__restrict__ Ehat, const float *__restrict__ Binv,
                                                       const float *__restrict__ c, int k, const float *__restrict__ vin,
-                                                      float *__restrict__ vout, float *__restrict__ out) {
+                                                      float *__restrict__ vout, float *__restrict__ out,
+                                                      const int *__restrict__ stop) {
+    if (vc_stopped(stop)) return;
     const int lane = threadIdx.x & 31;
     for (long r = (blockIdx.x * (long)blockDim.x + threadIdx.x) / 32; r < R;
          r += (long)gridDim.x * blockDim.x / 32) {
@@ -624,7 +628,9 @@ __global__ void k_scales(int n, const float *__restrict__ Y, float *__restrict__
 // written over c2 (one prolongation then adds Z2 g = Z1 e1 + Z2 D^-1/2 y).
 __global__ void k_poly_out_e1(int na, const float *__restrict__ s, const float *__restrict__ wv,
                               const float *__restrict__ dsq, const int *__restrict__ parent,
-                              const float *__restrict__ pdel, const float *__restrict__ e1, float *__restrict__ g) {
+                              const float *__restrict__ pdel, const float *__restrict__ e1, float *__restrict__ g,
+                              const int *__restrict__ stop) {
+    if (vc_stopped(stop)) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 6 * na; i += gridDim.x * blockDim.x) {
         const int J = i / 6, l = i % 6;
         float pe[6];
@@ -638,7 +644,8 @@ __global__ void k_poly_out_e1(int na, const float *__restrict__ s, const float *
 // each child's mode map transposed), children summed in table order; every
 // load of the eight children is issued before the first sum.
 __global__ void k_restrict_parent(int na1, const int *__restrict__ children, const float *__restrict__ pdel,
-                                  const float *__restrict__ c2, float *__restrict__ c1) {
+                                  const float *__restrict__ c2, float *__restrict__ c1, const int *__restrict__ stop) {
+    if (vc_stopped(stop)) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 6 * na1; i += gridDim.x * blockDim.x) {
         const int P = i / 6, k = i % 6;
         int J[8];
@@ -939,7 +946,7 @@ static void apply_M_rest(ofea_ctx *c, long Rp, const float *coef, float *out) {
     const int Gw = grid_for(c, 32 * Rp, kBlock);
     for (int k = 1; k < kTerms; ++k)
         k_poly_next<<<Gw, kBlock, 0, c->stream>>>(Rp, na, C2.nbr.p, N.Ehat.p, N.Binv.p, coef, k, N.pv[k - 1].p,
-                                                  N.pv[k].p, out);
+                                                  N.pv[k].p, out, c->vc_stop);
     OFEA_CHECK_LAUNCH();
 }
 
@@ -1175,7 +1182,7 @@ void learned_coarse_correct(ofea_ctx *c, const float *t, float *x) {
     const int na = C2.na;
     restrict_level(c, C2, t, C2.cvec.p);
     k_restrict_parent<<<grid_for(c, 6L * C1.na, 128), 128, 0, s>>>(C1.na, N.children.p, N.pdel.p, C2.cvec.p,
-                                                                 C1.cvec.p);
+                                                                 C1.cvec.p, c->vc_stop);
     coarse_gemv(c, C1.cvec.p, C1.evec.p);
     // the shifted residual and the stage's first term in one launch, then the
     // stage's other terms
@@ -1183,15 +1190,14 @@ void learned_coarse_correct(ofea_ctx *c, const float *t, float *x) {
     const float *coef = N.w.p + L.c0;
     k_lrn_shift<true><<<grid_for(c, 32L * na, kBlock), kBlock, 0, s>>>(
         na, C2.nbr.p, N.Ehat.p, N.dsq.p, N.parent.p, N.pdel.p, C1.evec.p, C2.cvec.p, N.shifted.p, N.Binv.p,
-        N.scale.p, coef, N.pv[0].p, wv);
+        N.scale.p, coef, N.pv[0].p, wv, c->vc_stop);
     apply_M_rest(c, na, coef, wv);
     k_poly_out_e1<<<grid_for(c, 6L * na, kBlock), kBlock, 0, s>>>(na, N.scale.p, wv, N.dsq.p, N.parent.p,
-                                                                   N.pdel.p, C1.evec.p, C2.cvec.p);
+                                                                   N.pdel.p, C1.evec.p, C2.cvec.p, c->vc_stop);
     prolong_level(c, C2, C2.cvec.p, x);
     OFEA_CHECK_LAUNCH();
 }
 
-// Weights on the device and the network evaluated (the scalings s) for the current K.
 // The LEARNED solver's per-K set-up: both coarse levels as in
 // setup_learned_levels, with the network's scalings evaluated on the side
 // stream beside the coarse level's E1 = P^T E2 P and its factor (the network

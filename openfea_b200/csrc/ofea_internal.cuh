@@ -152,6 +152,7 @@ struct Coarse {
     DevBuf<float> agg_off;  // [nfree][4] in aggregate order: offset from the centroid (cell units), row
     DevBuf<float> row_off;  // [nfree][4] in row order: the same offset, aggregate
     DevBuf<unsigned long long> row_cell;  // [nfree] in row order: the aggregate's cell, 21 bits per axis
+    DevBuf<int> nof;                      // [nfree] node of each free row (input of the transfer offsets)
     // the coarse solve as a block LDL^T factor (precond.cu): S_k, L_ik and the
     // FP32 array F (U = diag(S) V below, V^T above); dense_ok: Einv32 holds the
     // dense inverse (the Gauss-Jordan path, or formed from F on demand)
@@ -197,6 +198,9 @@ struct ofea_ctx {
     cudaStream_t side_stream = nullptr;  // the coarse inversion's lookahead; the network beside the coarse factor (owned)
     cudaStream_t aux_stream = nullptr;   // power iteration beside the coarse inversion (owned)
     cudaStream_t geo_stream = nullptr;   // uploads of the coarse geometry (owned)
+    // During a preconditioned solve's iterations: the solve's stop flag on the
+    // device (its V-cycle kernels return at once once it is set); else null.
+    const int *vc_stop = nullptr;
     std::future<void> geom_job;          // coarse geometry built in the background after the pattern
     // mesh
     int nd = 0, ne = 0, ne8 = 0, ne4 = 0, nfree = 0, n = 0;

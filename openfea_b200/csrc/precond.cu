@@ -241,15 +241,14 @@ static void bin_nodes(ofea_ctx *c, Coarse &C, const int nc[3], const double lo[3
     // restriction's coalesced reads) and in row order with the aggregate
     // (row_off, the prolongation's); formed on the device from the node
     // coordinates already there
-    DevBuf<int> nof_d;
-    nof_d.upload(nof.data(), nf, st);
+    C.nof.upload(nof.data(), nf, st);
     C.agg_off.ensure(4L * std::max(nf, 1));
     C.row_off.ensure(4L * std::max(nf, 1));
     C.row_cell.ensure(std::max(nf, 1));
     for (int d = 0; d < 3; ++d)
         if (nc[d] > (int)kCellMask) fail(OFEA_ERR_CAPACITY, "coarse level: more than 2^21 cells along an axis");
     k_transfer_offsets<<<std::max(1, std::min((nf + 255) / 256, c->num_sms * 16)), 256, 0, st>>>(
-        nf, C.agg_nodes.p, C.agg_of.p, nof_d.p, c->xyz.p, C.centroid.p, C.agg_cell.p, C.inv_scale,
+        nf, C.agg_nodes.p, C.agg_of.p, C.nof.p, c->xyz.p, C.centroid.p, C.agg_cell.p, C.inv_scale,
         reinterpret_cast<float4 *>(C.agg_off.p), reinterpret_cast<float4 *>(C.row_off.p), C.row_cell.p);
     OFEA_CHECK_LAUNCH();
     OFEA_CUDA(cudaStreamSynchronize(st));
@@ -1055,7 +1054,8 @@ __device__ __forceinline__ float coarse_row_dot(const float *__restrict__ row, c
 // z = U c: row r over the columns of its own and earlier blocks.
 __global__ void __launch_bounds__(kBlock) k_coarse_apply_lower(int m, int ldf, const float *__restrict__ F,
                                                                const float *__restrict__ cvec,
-                                                               float *__restrict__ z) {
+                                                               float *__restrict__ z, const int *__restrict__ stop) {
+    if (vc_stopped(stop)) return;
     const int lane = threadIdx.x & 31;
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32; i < m; i += gridDim.x * blockDim.x / 32) {
         const float s = coarse_row_dot(F + (long)i * ldf, cvec, 0, min(m, kGJ * (i / kGJ + 1)), lane);
@@ -1066,7 +1066,8 @@ __global__ void __launch_bounds__(kBlock) k_coarse_apply_lower(int m, int ldf, c
 // e = V^T z: z_r plus row r over the columns of later blocks.
 __global__ void __launch_bounds__(kBlock) k_coarse_apply_upper(int m, int ldf, const float *__restrict__ F,
                                                                const float *__restrict__ z,
-                                                               float *__restrict__ evec) {
+                                                               float *__restrict__ evec, const int *__restrict__ stop) {
+    if (vc_stopped(stop)) return;
     const int lane = threadIdx.x & 31;
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32; i < m; i += gridDim.x * blockDim.x / 32) {
         const int lo = min(m, kGJ * (i / kGJ + 1));
@@ -1268,8 +1269,24 @@ void coarse_E_partials(ofea_ctx *c, Coarse &C, int nchunk) {
 // The geometry of both levels depends on the mesh only: after the pattern it
 // is built on a background host thread while the caller assembles K; every
 // user of it joins the job first (a failure surfaces there).
+// Device buffers the geometry job writes are released here, on the caller's
+// thread, so that the job only allocates: a free waits for the whole device
+// (dev_free), and a device-wide wait on a background thread would invalidate
+// a CUDA graph that the caller's thread may be capturing at that moment (a
+// PCG64 solve does not join the job).
+static void release_geometry(Coarse &C) {
+    for (DevBuf<int> *b : {&C.agg_of, &C.agg_ptr, &C.agg_nodes, &C.agg_cell, &C.cell_agg, &C.nbr, &C.nof}) b->release();
+    C.centroid.release();
+    C.agg_off.release();
+    C.row_off.release();
+    C.row_cell.release();
+    C.geom_ok = C.K_ok = false;
+}
+
 void geometry_start(ofea_ctx *c) {
     geometry_join(c);
+    release_geometry(c->coarse);
+    release_geometry(c->coarse2);
     const int target = c->coarse_nodes;
     c->geom_job = std::async(std::launch::async, [c, target] {
         OFEA_CUDA(cudaSetDevice(c->device));
@@ -1369,7 +1386,9 @@ __global__ void __launch_bounds__(kBlock, 2048 / kBlock) k_vc_resid(int nfree, c
                                                      const int *__restrict__ scols,
                                                      const int *__restrict__ sl_g, const __nv_bfloat16 *__restrict__ svg,
                                                      const float *__restrict__ b,
-                                                     const float *__restrict__ x, float *__restrict__ t) {
+                                                     const float *__restrict__ x, float *__restrict__ t,
+                                                     const int *__restrict__ stop) {
+    if (vc_stopped(stop)) return;
     for_each_sell_row(nfree, sl_ptr, [&](int r, long S, int tt, int W) {
         float y[3];
         sell_row_g4(S, sl_g[r / kSlice], tt, W, scols, svg, [&](int k) { return x[k]; }, y[0], y[1], y[2]);
@@ -1377,16 +1396,16 @@ __global__ void __launch_bounds__(kBlock, 2048 / kBlock) k_vc_resid(int nfree, c
     });
 }
 
-// c_I = Z_I^T t: one CTA per aggregate, fixed-order reduction.
 // cvec_I = Z_I^T t (6 values per aggregate): one CTA of NT threads per
 // aggregate, the rows' offsets and indices read in aggregate order (agg_off),
 // sums in a fixed order (per thread, then warps).
 template <int NT>
 __global__ void __launch_bounds__(NT) k_restrict(int na, const int *__restrict__ agg_ptr,
                                                  const float4 *__restrict__ off, const float *__restrict__ t,
-                                                 float *__restrict__ cvec) {
+                                                 float *__restrict__ cvec, const int *__restrict__ stop) {
     constexpr int NW = NT / 32;
     __shared__ float sh[6][NW];
+    if (vc_stopped(stop)) return;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int I = blockIdx.x; I < na; I += gridDim.x) {
         float a[6] = {0, 0, 0, 0, 0, 0};
@@ -1421,7 +1440,8 @@ __global__ void __launch_bounds__(NT) k_restrict(int na, const int *__restrict__
 // e = Einv32 c: one warp per row.
 __global__ void __launch_bounds__(kBlock) k_coarse_gemv(int m, const float *__restrict__ Ainv,
                                                         const float *__restrict__ cvec,
-                                                        float *__restrict__ evec) {
+                                                        float *__restrict__ evec, const int *__restrict__ stop) {
+    if (vc_stopped(stop)) return;
     const int lane = threadIdx.x & 31;
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) / 32; i < m; i += gridDim.x * blockDim.x / 32) {
         const float *row = Ainv + (long)i * m;
@@ -1435,7 +1455,8 @@ __global__ void __launch_bounds__(kBlock) k_coarse_gemv(int m, const float *__re
 // x_r += Z_r e_I(r), per free row: the row's offset from its aggregate's
 // centroid and the aggregate from row_off (one 16-byte load).
 __global__ void k_prolong(int nfree, const float4 *__restrict__ roff, const float *__restrict__ evec,
-                          float *__restrict__ x) {
+                          float *__restrict__ x, const int *__restrict__ stop) {
+    if (vc_stopped(stop)) return;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nfree; r += gridDim.x * blockDim.x) {
         const float4 o = roff[r];
         const int I = __float_as_int(o.w);
@@ -1452,15 +1473,15 @@ void restrict_level(ofea_ctx *c, const Coarse &C, const float *t, float *cvec) {
     const float4 *off = reinterpret_cast<const float4 *>(C.agg_off.p);
     // 128 threads for aggregates of a few hundred rows (the nested level), 256 beyond
     if (C.max_agg <= 512)
-        k_restrict<128><<<g, 128, 0, c->stream>>>(C.na, C.agg_ptr.p, off, t, cvec);
+        k_restrict<128><<<g, 128, 0, c->stream>>>(C.na, C.agg_ptr.p, off, t, cvec, c->vc_stop);
     else
-        k_restrict<256><<<g, 256, 0, c->stream>>>(C.na, C.agg_ptr.p, off, t, cvec);
+        k_restrict<256><<<g, 256, 0, c->stream>>>(C.na, C.agg_ptr.p, off, t, cvec, c->vc_stop);
     OFEA_CHECK_LAUNCH();
 }
 
 void prolong_level(ofea_ctx *c, const Coarse &C, const float *g, float *x) {
     k_prolong<<<grid_for(c, c->nfree, kBlock), kBlock, 0, c->stream>>>(
-        c->nfree, reinterpret_cast<const float4 *>(C.row_off.p), g, x);
+        c->nfree, reinterpret_cast<const float4 *>(C.row_off.p), g, x, c->vc_stop);
     OFEA_CHECK_LAUNCH();
 }
 
@@ -1468,10 +1489,10 @@ void coarse_gemv(ofea_ctx *c, const float *cvec, float *evec) {
     Coarse &C = c->coarse;
     const int g = grid_for(c, (long)C.m * 32, kBlock);
     if (C.factored) {
-        k_coarse_apply_lower<<<g, kBlock, 0, c->stream>>>(C.m, C.ldf, C.F32.p, cvec, C.zvec.p);
-        k_coarse_apply_upper<<<g, kBlock, 0, c->stream>>>(C.m, C.ldf, C.F32.p, C.zvec.p, evec);
+        k_coarse_apply_lower<<<g, kBlock, 0, c->stream>>>(C.m, C.ldf, C.F32.p, cvec, C.zvec.p, c->vc_stop);
+        k_coarse_apply_upper<<<g, kBlock, 0, c->stream>>>(C.m, C.ldf, C.F32.p, C.zvec.p, evec, c->vc_stop);
     } else {
-        k_coarse_gemv<<<g, kBlock, 0, c->stream>>>(C.m, C.Einv32.p, cvec, evec);
+        k_coarse_gemv<<<g, kBlock, 0, c->stream>>>(C.m, C.Einv32.p, cvec, evec, c->vc_stop);
     }
     OFEA_CHECK_LAUNCH();
 }
@@ -1485,7 +1506,7 @@ void coarse_correct(ofea_ctx *c, const float *t, float *x) {
 
 void vc_resid(ofea_ctx *c, const float *b, const float *x, float *t) {
     k_vc_resid<<<grid_for(c, (c->nfree + 31) / 32, kWarpsPerBlock), kBlock, 0, c->stream>>>(
-        c->nfree, c->sl_ptr.p, c->scols.p, c->sl_g.p, c->sv16g.p, b, x, t);
+        c->nfree, c->sl_ptr.p, c->scols.p, c->sl_g.p, c->sv16g.p, b, x, t, c->vc_stop);
     OFEA_CHECK_LAUNCH();
 }
 

@@ -4,6 +4,18 @@
 
 namespace ofea {
 
+// A V-cycle kernel launched among a solve's iterations returns at once when
+// the solve has stopped (the iterations a chunk runs past convergence cost
+// only their launches).  stop is null outside a solve.  Read once per CTA and
+// broadcast: every thread takes the same path before any barrier.
+__device__ __forceinline__ bool vc_stopped(const int *stop) {
+    if (stop == nullptr) return false;
+    __shared__ int s_stop;
+    if (threadIdx.x == 0) s_stop = *(volatile const int *)stop;
+    __syncthreads();
+    return s_stop != 0;
+}
+
 void build_aggregation(ofea_ctx *c, int target_nodes);
 void build_aggregation_fine(ofea_ctx *c);
 // Aggregation (once per mesh), E = Z^T K Z, its inverse and lambda_max(D^-1 K)

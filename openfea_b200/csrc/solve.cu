@@ -414,7 +414,7 @@ Workspace setup(ofea_ctx *c, int G) {
     ws.fl = reinterpret_cast<Flags *>(w.flags.p);
     OFEA_CUDA(cudaMemsetAsync(w.partials.p, 0, nd * sizeof(double), c->stream));
     OFEA_CUDA(cudaMemsetAsync(w.flags.p, 0, sizeof(Flags), c->stream));
-    w.hflags.ensure(sizeof(Flags) / sizeof(int));
+    w.hflags.ensure(2 * sizeof(Flags) / sizeof(int));  // two slots: drive() reads one chunk's flags while the next runs
     w.hscal.ensure(4);
     return ws;
 }
@@ -425,6 +425,10 @@ double now_s() {
 
 // Replays `chunk(iters)` (as a captured CUDA graph when requested) until the
 // device flags say done, max_iter is reached or the time budget runs out.
+// Without per-chunk host work the next chunk is enqueued before the flags of
+// the one before it are read, so the GPU does not wait for the host's round
+// trip; a chunk that starts after the solve stopped returns at once in every
+// kernel (the stop flag), and the flags are read again after the last one.
 template <class ChunkFn>
 void drive(ofea_ctx *c, const ofea_solve_opts &o, Workspace &ws, int per_chunk, ChunkFn chunk,
            Flags &hf, long long &launches, int kernels_per_iter, bool &timed_out, double t_start,
@@ -444,35 +448,76 @@ void drive(ofea_ctx *c, const ofea_solve_opts &o, Workspace &ws, int per_chunk, 
         }
     }
     int launched = 0;
-    Flags *h = reinterpret_cast<Flags *>(c->w.hflags.p);
+    Flags *h = reinterpret_cast<Flags *>(c->w.hflags.p);  // two slots
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    auto launch_chunk = [&]() {
+        if (exec)
+            OFEA_CUDA(cudaGraphLaunch(exec, s));
+        else
+            chunk(per_chunk);
+        launched += per_chunk;
+        launches += (long long)per_chunk * kernels_per_iter;
+    };
+    auto over_budget = [&]() { return o.time_budget_s > 0 && now_s() - t_start > o.time_budget_s; };
     try {
-        while (true) {
-            if (exec)
-                OFEA_CUDA(cudaGraphLaunch(exec, s));
-            else
-                chunk(per_chunk);
-            launched += per_chunk;
-            launches += (long long)per_chunk * kernels_per_iter;
-            OFEA_CUDA(cudaMemcpyAsync(h, ws.fl, sizeof(Flags), cudaMemcpyDeviceToHost, s));
+        if (!after_chunk) {
+            for (auto &e : ev) OFEA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            int k = 0;
+            launch_chunk();
+            OFEA_CUDA(cudaMemcpyAsync(&h[0], ws.fl, sizeof(Flags), cudaMemcpyDeviceToHost, s));
+            OFEA_CUDA(cudaEventRecord(ev[0], s));
+            while (true) {
+                const bool more = launched < o.max_iter;
+                if (more) {  // slot k ^ 1 was read two chunks ago
+                    launch_chunk();
+                    OFEA_CUDA(cudaMemcpyAsync(&h[k ^ 1], ws.fl, sizeof(Flags), cudaMemcpyDeviceToHost, s));
+                    OFEA_CUDA(cudaEventRecord(ev[k ^ 1], s));
+                }
+                OFEA_CUDA(cudaEventSynchronize(ev[k]));
+                if (h[k].done || !more) break;
+                if (over_budget()) {
+                    timed_out = true;
+                    break;
+                }
+                k ^= 1;
+            }
+            OFEA_CUDA(cudaMemcpyAsync(&h[0], ws.fl, sizeof(Flags), cudaMemcpyDeviceToHost, s));
             OFEA_CUDA(cudaStreamSynchronize(s));
-            if (h->done || launched >= o.max_iter) break;
-            if (after_chunk) after_chunk();
-            if (o.time_budget_s > 0 && now_s() - t_start > o.time_budget_s) {
-                timed_out = true;
-                break;
+        } else {
+            while (true) {
+                launch_chunk();
+                OFEA_CUDA(cudaMemcpyAsync(h, ws.fl, sizeof(Flags), cudaMemcpyDeviceToHost, s));
+                OFEA_CUDA(cudaStreamSynchronize(s));
+                if (h->done || launched >= o.max_iter) break;
+                after_chunk();
+                if (over_budget()) {
+                    timed_out = true;
+                    break;
+                }
             }
         }
     } catch (...) {
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         throw;
     }
+    for (auto &e : ev)
+        if (e) cudaEventDestroy(e);
     hf = *h;
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
 }
 
 int solver_grid(const ofea_ctx *c) { return std::min(kMaxGrid, c->num_sms * (2048 / kBlock)); }
+
+// Clears the context's V-cycle stop flag when the solve's iterations end
+// (normally or by an exception).
+struct StopFlagScope {
+    ofea_ctx *c;
+    ~StopFlagScope() { c->vc_stop = nullptr; }
+};
 
 }  // namespace
 
@@ -580,6 +625,10 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
         ofea_solve_opts oo = o;
         oo.max_iter = o.max_iter - total_iters;
         if (mixed) {
+            // the V-cycle kernels of this attempt return at once once the
+            // solve has stopped (the flag is cleared at every attempt)
+            c->vc_stop = &ws.fl->done;
+            const StopFlagScope stop_scope{c};
             // initial preconditioner application z_0 = M(r_0)
             k_set_itB<<<1, 1, 0, s>>>(ws.fl, -1);
             vc_resid(c, w.b32.p, w.x32.p, w.t32.p);
