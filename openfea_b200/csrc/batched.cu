@@ -1114,7 +1114,7 @@ void build_desc(ofea_batch *b, bool mixed) {
             B.centroid = C.centroid.p;
             B.Einv32 = C.Einv32.p;
             B.inv_scale = C.inv_scale;
-            B.wsm = smoother_weight(c);
+            B.wsm = smoother_weight(c, kBatchSmootherDamping);
             for (int a = 0; a < C.na; ++a) av.push_back(v);
             for (int i = 0; i < C.m; ++i) cv.push_back(v);
             agg0 += C.na;

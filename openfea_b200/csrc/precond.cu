@@ -1,11 +1,11 @@
 // Two-level preconditioner of the mixed-precision solver.
 //
-//   M(r) = V(1,1) cycle in FP32:  x0 = w D^-1 b            (pre-smoothing, Chebyshev degree 1)
+//   M(r) = V(1,1) cycle in FP32:  x0 = w D^-1 b            (pre-smoothing, damped block Jacobi)
 //                                 t  = b - K32 x0
 //                                 x1 = x0 + Z E^-1 Z^T t   (coarse correction)
 //                                 z  = x1 + w D^-1 (b - K32 x1)   (post-smoothing)
-// with b = float(r), D the 3x3 diagonal blocks, w = 1/theta of the Chebyshev
-// interval [lmax/30, 1.1 lmax] of D^-1 K, and Z the rigid-body modes of node
+// with b = float(r), D the 3x3 diagonal blocks, w = 1.5 / lmax (lmax the
+// power iteration's estimate of lambda_max(D^-1 K)), and Z the rigid-body modes of node
 // aggregates: the free nodes are binned into a grid of cells of about
 // `coarse_nodes` nodes; each non-empty cell I is an aggregate with six modes
 // (three translations, three rotations about its centroid, scaled by the

@@ -27,7 +27,14 @@ void setup_coarse_geometry(ofea_ctx *c, int target_nodes);
 double *coarse_begin_E(ofea_ctx *c);
 void coarse_finish(ofea_ctx *c);
 // Damping weight of the block-Jacobi smoother (needs setup_coarse's lmax).
-float smoother_weight(const ofea_ctx *c);
+float smoother_weight(const ofea_ctx *c, double damping);
+// omega lmax of the single-matrix solves and of the batched solver, each the
+// value that took the fewest outer iterations on its workload: the 1.56M-DOF
+// cantilever, LEARNED / MIXED, 1.3: 51 / 69, 1.4: 51 / 67, 1.5: 51 / 65,
+// 1.6: 52 / 64, 1.76: 56 / 71, 1.9: MIXED does not converge; the 64 SIMP
+// variants of the batched reanalysis, 1.4: 86, 1.5: 83, 1.6: 81, 1.76: 78.
+constexpr double kSmootherDamping = 1.5;
+constexpr double kBatchSmootherDamping = 1.76;
 // x += Z E^-1 Z^T t  (FP32 vectors of n entries)
 // evec = E^-1 cvec (FP32 GEMV with the coarse level's inverse)
 void coarse_gemv(ofea_ctx *c, const float *cvec, float *evec);

@@ -521,12 +521,11 @@ struct StopFlagScope {
 
 }  // namespace
 
-// Chebyshev degree-1 damping of the smoother: 1/theta, theta the midpoint of
-// [lmax/30, 1.1 lmax].
-float smoother_weight(const ofea_ctx *c) {
-    const double hi = 1.1 * c->coarse.lmax, lo = hi / 30.0;
-    return (float)(2.0 / (hi + lo));
-}
+// Damping of the block-Jacobi smoother: omega = damping / lmax, lmax the power
+// iteration's estimate of lambda_max(D^-1 K).  The V(1,1) cycle stays
+// positive definite while omega lmax < 2 (with margin for the estimate,
+// which lies below lambda_max).
+float smoother_weight(const ofea_ctx *c, double damping) { return (float)(damping / c->coarse.lmax); }
 
 void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_opts &o,
                   ofea_solve_stats &st, const std::function<void(const double *)> &on_chunk) {
@@ -587,7 +586,7 @@ void solve_device(ofea_ctx *c, const double *d_f, double *d_u, const ofea_solve_
     } else {
         w.z.ensure(n);
     }
-    const float wsm = mixed ? smoother_weight(c) : 0.f;
+    const float wsm = mixed ? smoother_weight(c, kSmootherDamping) : 0.f;
     for (int attempt = 0; attempt < 8; ++attempt) {
         OFEA_CUDA(cudaMemsetAsync(w.p0.p, 0, sizeof(double) * n, s));
         OFEA_CUDA(cudaMemsetAsync(w.p1.p, 0, sizeof(double) * n, s));
@@ -743,7 +742,7 @@ void profile_kernels(ofea_ctx *c, int method, int reps, double *ms, double *byte
         bytes[1] = 72.0 * nf + 8.0 * n * 7;  // Dinv; u r/w, r r/w, p, q, z
     } else {
         if (!w.z32a.p || w.z32a.n < (size_t)n) fail(OFEA_ERR_STATE, "run a GPU_MIXED solve first");
-        const float wsm = smoother_weight(c);
+        const float wsm = smoother_weight(c, kSmootherDamping);
         OFEA_CUDA(cudaEventRecord(e0, s));
         for (int i = 0; i < reps; ++i)
             k_fcg_A<<<G, kBlock, 0, s>>>(nf, c->sl_ptr.p, c->scols.p, c->sv64.p, w.z32a.p, w.z32b.p, w.p0.p,
