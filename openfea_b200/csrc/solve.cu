@@ -429,6 +429,8 @@ double now_s() {
 // the one before it are read, so the GPU does not wait for the host's round
 // trip; a chunk that starts after the solve stopped returns at once in every
 // kernel (the stop flag), and the flags are read again after the last one.
+// There the first chunk is launched directly and the graph is captured and
+// instantiated while the GPU runs it.
 template <class ChunkFn>
 void drive(ofea_ctx *c, const ofea_solve_opts &o, Workspace &ws, int per_chunk, ChunkFn chunk,
            Flags &hf, long long &launches, int kernels_per_iter, bool &timed_out, double t_start,
@@ -436,17 +438,22 @@ void drive(ofea_ctx *c, const ofea_solve_opts &o, Workspace &ws, int per_chunk, 
     cudaStream_t s = c->stream;
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
-    if (o.use_graph) {
+    auto make_graph = [&]() {
+        if (!o.use_graph || exec) return;
         OFEA_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        chunk(per_chunk);
+        try {
+            chunk(per_chunk);
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(s, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
         cudaError_t e = cudaStreamEndCapture(s, &graph);
         if (e != cudaSuccess) fail_cuda(e, "cudaStreamEndCapture", __FILE__, __LINE__);
         e = cudaGraphInstantiate(&exec, graph, 0);
-        if (e != cudaSuccess) {
-            cudaGraphDestroy(graph);
-            fail_cuda(e, "cudaGraphInstantiate", __FILE__, __LINE__);
-        }
-    }
+        if (e != cudaSuccess) fail_cuda(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+    };
     int launched = 0;
     Flags *h = reinterpret_cast<Flags *>(c->w.hflags.p);  // two slots
     cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -466,6 +473,7 @@ void drive(ofea_ctx *c, const ofea_solve_opts &o, Workspace &ws, int per_chunk, 
             launch_chunk();
             OFEA_CUDA(cudaMemcpyAsync(&h[0], ws.fl, sizeof(Flags), cudaMemcpyDeviceToHost, s));
             OFEA_CUDA(cudaEventRecord(ev[0], s));
+            make_graph();
             while (true) {
                 const bool more = launched < o.max_iter;
                 if (more) {  // slot k ^ 1 was read two chunks ago
@@ -484,6 +492,7 @@ void drive(ofea_ctx *c, const ofea_solve_opts &o, Workspace &ws, int per_chunk, 
             OFEA_CUDA(cudaMemcpyAsync(&h[0], ws.fl, sizeof(Flags), cudaMemcpyDeviceToHost, s));
             OFEA_CUDA(cudaStreamSynchronize(s));
         } else {
+            make_graph();
             while (true) {
                 launch_chunk();
                 OFEA_CUDA(cudaMemcpyAsync(h, ws.fl, sizeof(Flags), cudaMemcpyDeviceToHost, s));
